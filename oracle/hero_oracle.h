@@ -1,0 +1,100 @@
+/*
+ * hero_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the HERO read-correction path (guo-xuan/Hero, consensus
+ * mode `-c`).  Only the test suite, the smoke check and the benchmark's CPU
+ * baseline use it, and only as the checker: the product path never links or
+ * calls anything in oracle/.
+ *
+ * Parity pin: the restatement is checked byte-for-byte against the reference
+ * itself (oracle/_ref/hero_ref, built from the reference sources by
+ * oracle/Makefile) on the seeded fixtures under tests/golden/.
+ */
+#ifndef HERO_ORACLE_H_
+#define HERO_ORACLE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int32_t k;              /* Config::iKmer (default 39) */
+    int32_t min_overlap;    /* Config::minimumOverlapLength, flag -l (default 40) */
+    int32_t affine;         /* 1 = `-a a` (bandedAlignAffineGap), 0 = global */
+    int32_t keep_segments;  /* 1 = keep every DP segment with its ops for inspection */
+    double mis_rate;        /* Config::dMaxMismatchRate = atof(-m)/100 (default 1) */
+    double indel_rate;      /* Config::dMaxIndelRate = atof(-i)/100 (default 1) */
+    double consensus_thr;   /* Config::dMinFrequencyCallConsensus (default 0.6) */
+} hero_oracle_params;
+
+typedef struct {
+    uint64_t probes;            /* getListOfReads calls */
+    uint64_t hits;              /* PairKeyPosition entries after self exclusion */
+    uint64_t chains;            /* chains formed */
+    uint64_t chains_kept;       /* chains that survive markTheBestPossibleAlignment */
+    uint64_t records_built;     /* chains that pass the overlap test */
+    uint64_t records_accepted;  /* records passing every isGoodAlignment test */
+    uint64_t records_kept;      /* records left after SubjectRead::addAlignment */
+    uint64_t dp_segments;       /* BandAligner::calculateAlignment calls */
+    uint64_t dp_cells;          /* sum over calls of the band cells of the loop bounds */
+} hero_oracle_stats;
+
+/* Per-step op codes used by every op string of this API (original orientation:
+ * I consumes the query only, D the subject only). */
+enum { HERO_OP_M = 0, HERO_OP_X = 1, HERO_OP_I = 2, HERO_OP_D = 3 };
+
+typedef struct hero_oracle_run_s hero_oracle_run;
+
+/* Runs the whole path.  Reads are uppercase ASCII, concatenated; read i is
+ * seq[off[i]:off[i+1]].  uid = atoi(read name).  Returns NULL on bad input. */
+hero_oracle_run *hero_oracle_correct(const hero_oracle_params *p, int nthreads,
+                                     uint64_t nq, const uint8_t *qseq, const uint64_t *qoff,
+                                     const int64_t *quid,
+                                     uint64_t ns, const uint8_t *sseq, const uint64_t *soff,
+                                     const int64_t *suid);
+void hero_oracle_free(hero_oracle_run *r);
+
+void hero_oracle_stats_get(const hero_oracle_run *r, hero_oracle_stats *out);
+
+/* Corrected reads (same layout as the query input), coverage statistics and
+ * the .info columns.  Reads that are not good are returned unchanged with
+ * zero statistics, as QueryDataset::callConsensus leaves them. */
+void hero_oracle_consensus(const hero_oracle_run *r, uint8_t *seq_out, uint32_t *imin,
+                           uint32_t *imed, uint32_t *imax, double *mismatch_rate,
+                           double *gc, uint8_t *good);
+
+/* Vote matrix after every subject's votes and before the self vote:
+ * uint32 [total query bases][4], column index (c>>1)&3 (A,C,T,G). */
+void hero_oracle_votes(const hero_oracle_run *r, uint32_t *cov);
+
+/* Kept records (one per subject x query), ordered by subject then query. */
+uint64_t hero_oracle_num_records(const hero_oracle_run *r);
+uint64_t hero_oracle_record_ops_total(const hero_oracle_run *r);
+void hero_oracle_records(const hero_oracle_run *r, uint32_t *subject, uint32_t *query,
+                         uint8_t *orient, int64_t *pos, double *rate_sum, double *align_len,
+                         uint64_t *ops_off, uint8_t *ops);
+
+/* Every DP segment (only with keep_segments=1), in call order per subject. */
+uint64_t hero_oracle_num_segments(const hero_oracle_run *r);
+uint64_t hero_oracle_segment_ops_total(const hero_oracle_run *r);
+void hero_oracle_segments(const hero_oracle_run *r, uint32_t *subject, uint8_t *orient,
+                          uint32_t *query, int32_t *s0, int32_t *s1, int32_t *q0, int32_t *q1,
+                          uint8_t *flags, int64_t *band, uint64_t *ops_off, uint8_t *ops);
+
+/* One BandAligner call on explicit segments (setSequences + setBand + flags +
+ * calculateAlignment).  ops: per-step codes in original orientation; returns
+ * the number of steps, or -1 if ops_cap is too small.  *band_used receives the
+ * band after the call (it grows to the length difference). */
+int hero_oracle_align(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query,
+                      int32_t lq, int64_t band, int align_right, int align_left,
+                      uint8_t *ops, int32_t ops_cap, int64_t *band_used);
+
+/* QueryDataset::qualityFilter (QueryDataset.cpp:60-75). */
+int hero_oracle_quality_filter(const uint8_t *seq, uint64_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
