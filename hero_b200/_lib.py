@@ -1,0 +1,233 @@
+"""ctypes binding of libhero_b200.so (the C ABI declared in include/hero_gpu.h).
+
+The library is built in-tree by ``hero_b200.build`` (nvcc, sm_100a).  Loading
+fails loudly when it is missing: there is no CPU path behind this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhero_b200.so")
+
+HERO_OK = 0
+ERRORS = {-1: "HERO_E_INPUT", -2: "HERO_E_OOM", -3: "HERO_E_CUDA", -4: "HERO_E_STATE",
+          -5: "HERO_E_TIMEOUT"}
+ALIGNER_AFFINE = 0
+ALIGNER_GLOBAL = 1
+
+# every entry point include/hero_gpu.h declares
+EXPORTS = [
+    "hero_default_params", "hero_create", "hero_destroy", "hero_last_error",
+    "hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
+    "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments",
+]
+
+
+class HeroParams(C.Structure):
+    _fields_ = [
+        ("k", C.c_int32), ("min_overlap", C.c_int32), ("aligner", C.c_int32),
+        ("device", C.c_int32), ("max_mismatch_rate", C.c_double),
+        ("max_indel_rate", C.c_double), ("consensus_threshold", C.c_double),
+        ("device_memory_budget", C.c_uint64), ("subject_batch", C.c_uint32),
+        ("flags", C.c_uint32), ("stream", C.c_void_p),
+    ]
+
+
+_STAT_FIELDS = [
+    "queries", "good_queries", "index_keys", "index_slots", "subjects", "probes", "hits",
+    "chains", "chains_kept", "records_built", "records_accepted", "records_kept",
+    "dp_segments", "dp_segments_ref", "dp_cells", "vote_anomalies", "device_bytes_peak",
+]
+_STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record", "ms_vote",
+            "ms_consensus", "ms_dp_kernel"]
+
+
+class HeroStats(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS]
+
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"{p} is missing: build it with `python -m hero_b200.build` (nvcc, sm_100a). "
+            "There is no CPU fallback.")
+    lib = C.CDLL(p)
+    vp = C.c_void_p
+    lib.hero_default_params.argtypes = [C.POINTER(HeroParams)]
+    lib.hero_create.argtypes = [C.POINTER(HeroParams), C.POINTER(vp)]
+    lib.hero_create.restype = C.c_int
+    lib.hero_destroy.argtypes = [vp]
+    lib.hero_last_error.argtypes = [vp]
+    lib.hero_last_error.restype = C.c_char_p
+    lib.hero_set_queries.argtypes = [vp, vp, vp, vp, C.c_uint64]
+    lib.hero_build_index.argtypes = [vp]
+    lib.hero_align_subjects.argtypes = [vp, vp, vp, vp, C.c_uint64]
+    lib.hero_align_self.argtypes = [vp]
+    lib.hero_consensus.argtypes = [vp] * 8
+    lib.hero_get_votes.argtypes = [vp, vp]
+    lib.hero_get_stats.argtypes = [vp, C.POINTER(HeroStats)]
+    lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
+                                         C.c_uint64] + [vp] * 12)
+    for f in ("hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
+              "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments"):
+        getattr(lib, f).restype = C.c_int
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+class HeroError(RuntimeError):
+    pass
+
+
+class Hero:
+    """One device context: a query set, its k-mer table and its vote matrix.
+
+    Mirrors the reference's driver sequence (main.cpp:36-104): queries are
+    loaded, the table is built, subject reads are aligned in chunks, then the
+    consensus is called.
+    """
+
+    def __init__(self, k: int = 39, min_overlap: int = 40, aligner: str = "global",
+                 max_mismatch_rate: float = 1.0, max_indel_rate: float = 1.0,
+                 consensus_threshold: float = 0.6, device: int = 0, subject_batch: int = 0,
+                 device_memory_budget: int = 0, stream: int | None = None):
+        self.lib = load_library()
+        p = HeroParams()
+        self.lib.hero_default_params(C.byref(p))
+        p.k = k
+        p.min_overlap = min_overlap
+        p.aligner = ALIGNER_AFFINE if aligner in ("a", "affine") else ALIGNER_GLOBAL
+        p.device = device
+        p.max_mismatch_rate = max_mismatch_rate
+        p.max_indel_rate = max_indel_rate
+        p.consensus_threshold = consensus_threshold
+        p.subject_batch = subject_batch
+        p.device_memory_budget = device_memory_budget
+        p.stream = stream
+        self.params = p
+        h = C.c_void_p()
+        rc = self.lib.hero_create(C.byref(p), C.byref(h))
+        if rc != HERO_OK:
+            raise HeroError(f"hero_create failed: {ERRORS.get(rc, rc)}")
+        self.h = h
+        self.nq = 0
+        self.nqb = 0
+
+    def _check(self, rc: int, what: str):
+        if rc != HERO_OK:
+            msg = self.lib.hero_last_error(self.h)
+            raise HeroError(f"{what}: {ERRORS.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hero_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _arrays(seq, off, uid):
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        uid = np.ascontiguousarray(uid, dtype=np.int64)
+        return seq, off, uid
+
+    def set_queries(self, seq, off, uid):
+        seq, off, uid = self._arrays(seq, off, uid)
+        self._qkeep = (seq, off, uid)
+        self.nq = len(off) - 1
+        self.nqb = int(off[-1]) if self.nq else 0
+        self._check(self.lib.hero_set_queries(self.h, _ptr(seq), _ptr(off), _ptr(uid), self.nq),
+                    "set_queries")
+
+    def build_index(self):
+        self._check(self.lib.hero_build_index(self.h), "build_index")
+
+    def align_self(self):
+        self._check(self.lib.hero_align_self(self.h), "align_self")
+
+    def align_subjects(self, seq, off, uid):
+        seq, off, uid = self._arrays(seq, off, uid)
+        self._check(self.lib.hero_align_subjects(self.h, _ptr(seq), _ptr(off), _ptr(uid),
+                                                 len(off) - 1), "align_subjects")
+
+    def consensus(self, out=None):
+        n, nb = self.nq, self.nqb
+        res = dict(seq=np.empty(nb, np.uint8) if out is None else out,
+                   imin=np.empty(n, np.uint32), imed=np.empty(n, np.uint32),
+                   imax=np.empty(n, np.uint32), mismatch_rate=np.empty(n, np.float64),
+                   gc=np.empty(n, np.float64), good=np.empty(n, np.uint8))
+        self._check(self.lib.hero_consensus(
+            self.h, _ptr(res["seq"]), _ptr(res["imin"]), _ptr(res["imed"]), _ptr(res["imax"]),
+            _ptr(res["mismatch_rate"]), _ptr(res["gc"]), _ptr(res["good"])), "consensus")
+        return res
+
+    def votes(self):
+        cov = np.empty(self.nqb * 4, np.uint32)
+        self._check(self.lib.hero_get_votes(self.h, _ptr(cov)), "votes")
+        return cov
+
+    def stats(self) -> dict:
+        s = HeroStats()
+        self._check(self.lib.hero_get_stats(self.h, C.byref(s)), "stats")
+        return {f: getattr(s, f) for f, _ in s._fields_}
+
+    def align_segments(self, affine, subj_seq, subj_off, query_seq, query_off, seg_subject,
+                       seg_orient, seg_query, s0, s1, q0, q1, flags, band):
+        subj_seq = np.ascontiguousarray(subj_seq, np.uint8)
+        subj_off = np.ascontiguousarray(subj_off, np.uint64)
+        query_seq = np.ascontiguousarray(query_seq, np.uint8)
+        query_off = np.ascontiguousarray(query_off, np.uint64)
+        a = [np.ascontiguousarray(x, t) for x, t in (
+            (seg_subject, np.uint32), (seg_orient, np.uint8), (seg_query, np.uint32),
+            (s0, np.int32), (s1, np.int32), (q0, np.int32), (q1, np.int32), (flags, np.uint8),
+            (band, np.int64))]
+        n = len(a[0])
+        cap = (a[4] - a[3]).astype(np.uint64) + (a[6] - a[5]).astype(np.uint64)
+        ops_off = np.zeros(n + 1, np.uint64)
+        ops_off[1:] = np.cumsum(cap)
+        ops = np.zeros(int(ops_off[-1]), np.uint8)
+        nops = np.zeros(n, np.int32)
+        self._check(self.lib.hero_align_segments(
+            self.h, int(affine), _ptr(subj_seq), _ptr(subj_off), len(subj_off) - 1,
+            _ptr(query_seq), _ptr(query_off), len(query_off) - 1, n, *[_ptr(x) for x in a],
+            _ptr(ops_off), _ptr(ops), _ptr(nops)), "align_segments")
+        return ops, ops_off, nops
+
+
+def correct(reads, **kw):
+    """Corrects a read set against itself (HERO run with -q X -s X); returns consensus arrays."""
+    with Hero(**kw) as h:
+        h.set_queries(reads.seq, reads.off, reads.names)
+        h.build_index()
+        h.align_self()
+        res = h.consensus()
+        res["stats"] = h.stats()
+        return res

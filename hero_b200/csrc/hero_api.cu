@@ -1,0 +1,660 @@
+// hero_api.cu -- host engine behind the C ABI declared in include/hero_gpu.h.
+//
+// One context = one device, one stream, one query set, its k-mer table and
+// its vote matrix.  Subject reads stream through in batches; every stage of a
+// batch runs as its own kernel (the plain one-launch-per-stage form).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hero_gpu.h"
+#include "hero_internal.cuh"
+
+using namespace hero;
+
+namespace {
+
+struct DBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+}  // namespace
+
+struct hero_ctx {
+    hero_params P{};
+    Params p{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::string err;
+    size_t bytes = 0, bytes_peak = 0;
+    std::vector<DBuf *> all;
+
+    // query set
+    uint64_t nq = 0, nqb = 0;
+    DBuf q_raw, q_code, q_off, q_len, q_uid, q_good, q_sgood, q_gc;
+    bool have_queries = false, have_index = false;
+    // k-mer table
+    DBuf t_slots, t_vals;
+    uint64_t t_mask = 0, t_keys = 0;
+    // vote matrix + consensus outputs
+    DBuf cov, out_seq, colsum, o_imin, o_imed, o_imax, o_mis;
+    // subject batch (when not aligning the query set against itself)
+    DBuf s_raw, s_code, s_off, s_len, s_uid, s_good;
+    // batch buffers
+    DBuf seg_hits, hit_off, hits, seg_cstart, seg_ccount;
+    DBuf cs_grp, cs_chain_of, cs_first, cs_last, cs_prev, cs_size, cs_coff, cs_ckeys, cs_kl,
+        cs_gnch, cs_gbest, cs_gkept, cs_gkeys, cs_gdp;
+    DBuf ch_subj, ch_query, ch_key_off, ch_seg_off, ch_nkeys, ch_nseg, ch_orient, ch_status,
+        ch_win, ch_rate, ch_len;
+    DBuf keys, segs, sums, cells, ops, perm, bins, bin_off, tb, bnd;
+    DBuf scan_tmp, counters;
+    uint64_t dp_T = 0;
+
+    hero_stats stats{};
+    unsigned long long ctr[C_COUNT] = {};
+
+    hero_ctx() {
+        DBuf *list[] = {&q_raw, &q_code, &q_off, &q_len, &q_uid, &q_good, &q_sgood, &q_gc,
+                        &t_slots, &t_vals, &cov, &out_seq, &colsum, &o_imin, &o_imed, &o_imax,
+                        &o_mis, &s_raw, &s_code, &s_off, &s_len, &s_uid, &s_good, &seg_hits,
+                        &hit_off, &hits, &seg_cstart, &seg_ccount, &cs_grp, &cs_chain_of,
+                        &cs_first, &cs_last, &cs_prev, &cs_size, &cs_coff, &cs_ckeys, &cs_kl,
+                        &cs_gnch, &cs_gbest, &cs_gkept, &cs_gkeys, &cs_gdp, &ch_subj, &ch_query,
+                        &ch_key_off, &ch_seg_off, &ch_nkeys, &ch_nseg, &ch_orient, &ch_status,
+                        &ch_win, &ch_rate, &ch_len, &keys, &segs, &sums, &cells, &ops, &perm,
+                        &bins, &bin_off, &tb, &bnd, &scan_tmp, &counters};
+        for (DBuf *b : list) all.push_back(b);
+    }
+
+    int fail(int code, const std::string &m) {
+        err = m;
+        return code;
+    }
+    int cuda(cudaError_t e, const char *what) {
+        if (e == cudaSuccess) return HERO_OK;
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return HERO_E_CUDA;
+    }
+    int check_launch(const char *what) {
+        cudaError_t e = cudaGetLastError();
+        return cuda(e, what);
+    }
+    void release(DBuf &b) {
+        if (b.p) {
+            cudaFree(b.p);
+            bytes -= b.cap;
+        }
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    // grows a device buffer to at least `need` bytes (contents are not kept)
+    int ensure(DBuf &b, size_t need, const char *what) {
+        if (need == 0) need = 16;
+        if (b.cap >= need) return HERO_OK;
+        release(b);
+        size_t want = need + need / 4 + 256;
+        if (P.device_memory_budget && bytes + want > P.device_memory_budget) {
+            want = need;
+            if (bytes + want > P.device_memory_budget)
+                return fail(HERO_E_OOM, std::string("device memory budget exceeded at ") + what);
+        }
+        cudaError_t e = cudaMalloc(&b.p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b.p = nullptr;
+            return fail(HERO_E_OOM, std::string("cudaMalloc failed for ") + what + ": " +
+                                        cudaGetErrorString(e));
+        }
+        b.cap = want;
+        bytes += want;
+        bytes_peak = std::max(bytes_peak, bytes);
+        return HERO_OK;
+    }
+    ~hero_ctx() {
+        for (DBuf *b : all) release(*b);
+        if (own_stream && st) cudaStreamDestroy(st);
+    }
+};
+
+template <class T>
+static T *P_(DBuf &b) {
+    return reinterpret_cast<T *>(b.p);
+}
+
+#define HERO_TRY(x)                 \
+    do {                            \
+        int _r = (x);               \
+        if (_r != HERO_OK) return _r; \
+    } while (0)
+
+static ReadsView query_view(hero_ctx *c) {
+    return ReadsView{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
+                     P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_good), c->nq};
+}
+
+static double elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    return double(ms);
+}
+
+extern "C" void hero_default_params(hero_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->k = 39;
+    p->min_overlap = 40;
+    p->aligner = HERO_ALIGNER_GLOBAL;
+    p->device = 0;
+    p->max_mismatch_rate = 1.0;
+    p->max_indel_rate = 1.0;
+    p->consensus_threshold = 0.6;
+}
+
+extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
+    if (!p || !out) return HERO_E_INPUT;
+    *out = nullptr;
+    if (p->k < 1 || p->k > 63) return HERO_E_INPUT;
+    hero_ctx *c = new hero_ctx();
+    c->P = *p;
+    c->p.k = p->k;
+    c->p.l = p->min_overlap;
+    c->p.affine = p->aligner == HERO_ALIGNER_AFFINE ? 1 : 0;
+    c->p.mis_rate = p->max_mismatch_rate;
+    c->p.indel_rate = p->max_indel_rate;
+    c->p.thr = p->consensus_threshold;
+    c->dev = p->device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        delete c;
+        return HERO_E_CUDA;
+    }
+    if (cudaSetDevice(c->dev) != cudaSuccess) {
+        delete c;
+        return HERO_E_CUDA;
+    }
+    if (p->stream) {
+        c->st = reinterpret_cast<cudaStream_t>(p->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return HERO_E_CUDA;
+        }
+        c->own_stream = true;
+    }
+    c->dp_T = dp_threads(c->dev);
+    if (c->ensure(c->counters, sizeof(unsigned long long) * C_COUNT, "counters")) {
+        delete c;
+        return HERO_E_OOM;
+    }
+    *out = c;
+    return HERO_OK;
+}
+
+extern "C" void hero_destroy(hero_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->dev);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    delete ctx;
+}
+
+extern "C" const char *hero_last_error(const hero_ctx *ctx) {
+    return ctx ? ctx->err.c_str() : "no context";
+}
+
+// uploads reads and derives codes, lengths and good flags on the device
+static int upload_reads(hero_ctx *c, const uint8_t *seq, const uint64_t *off, const int64_t *uid,
+                        uint64_t n, DBuf &raw, DBuf &code, DBuf &doff, DBuf &len, DBuf &duid,
+                        DBuf *gq, DBuf *gs, DBuf *gc) {
+    const uint64_t nb = n ? off[n] : 0;
+    HERO_TRY(c->ensure(raw, nb, "reads"));
+    HERO_TRY(c->ensure(code, nb, "codes"));
+    HERO_TRY(c->ensure(doff, (n + 1) * 8, "offsets"));
+    HERO_TRY(c->ensure(len, n * 4, "lengths"));
+    HERO_TRY(c->ensure(duid, n * 8, "ids"));
+    if (gq) HERO_TRY(c->ensure(*gq, n, "good"));
+    if (gs) HERO_TRY(c->ensure(*gs, n, "good"));
+    if (gc) HERO_TRY(c->ensure(*gc, n * 8, "gc"));
+    if (n == 0) {
+        const uint64_t z = 0;
+        return c->cuda(cudaMemcpy(doff.p, &z, 8, cudaMemcpyHostToDevice), "upload");
+    }
+    HERO_TRY(c->cuda(cudaMemcpyAsync(raw.p, seq, nb, cudaMemcpyHostToDevice, c->st), "upload"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(doff.p, off, (n + 1) * 8, cudaMemcpyHostToDevice, c->st), "upload"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(duid.p, uid, n * 8, cudaMemcpyHostToDevice, c->st), "upload"));
+    launch_prep_reads(P_<uint8_t>(raw), nb, P_<uint8_t>(code), P_<uint64_t>(doff), n,
+                      P_<uint32_t>(len), gq ? P_<uint8_t>(*gq) : nullptr,
+                      gs ? P_<uint8_t>(*gs) : nullptr, gc ? P_<double>(*gc) : nullptr, c->p.l, c->st);
+    return c->check_launch("prep reads");
+}
+
+static int validate_reads(hero_ctx *c, const uint8_t *seq, const uint64_t *off, const int64_t *uid,
+                          uint64_t n) {
+    if (n && (!seq || !off || !uid)) return c->fail(HERO_E_INPUT, "null read buffer");
+    if (n >= 0xffffffffull) return c->fail(HERO_E_INPUT, "too many reads");
+    if (!off) return HERO_OK;
+    if (off[0] != 0) return c->fail(HERO_E_INPUT, "offsets must start at 0");
+    for (uint64_t i = 0; i < n; i++) {
+        if (off[i + 1] < off[i]) return c->fail(HERO_E_INPUT, "offsets must not decrease");
+        if (off[i + 1] - off[i] > 32767) return c->fail(HERO_E_INPUT, "reads longer than 32767 bases");
+    }
+    return HERO_OK;
+}
+
+extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t *off,
+                                const int64_t *uid, uint64_t n) {
+    if (!c) return HERO_E_INPUT;
+    cudaSetDevice(c->dev);
+    HERO_TRY(validate_reads(c, seq, off, uid, n));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c->st);
+    c->nq = n;
+    c->nqb = n ? off[n] : 0;
+    c->have_index = false;
+    HERO_TRY(upload_reads(c, seq, n ? off : nullptr, uid, n, c->q_raw, c->q_code, c->q_off,
+                          c->q_len, c->q_uid, &c->q_good, &c->q_sgood, &c->q_gc));
+    HERO_TRY(c->ensure(c->cov, c->nqb * 16, "vote matrix"));
+    HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "memset"));
+    cudaEventRecord(e1, c->st);
+    HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "set queries"));
+    c->stats.ms_upload += elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->stats.queries = n;
+    std::vector<uint8_t> g(n);
+    if (n) HERO_TRY(c->cuda(cudaMemcpy(g.data(), c->q_good.p, n, cudaMemcpyDeviceToHost), "good flags"));
+    uint64_t ng = 0;
+    for (uint8_t x : g) ng += x;
+    c->stats.good_queries = ng;
+    c->have_queries = true;
+    return HERO_OK;
+}
+
+extern "C" int hero_build_index(hero_ctx *c) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    cudaSetDevice(c->dev);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c->st);
+    const uint64_t n = c->nq;
+    ReadsView q = query_view(c);
+    DBuf cnt, koff, klo, khi, kval, owner, count, slot_of, start, fill, tmp;
+    auto cleanup = [&]() {
+        for (DBuf *b : {&cnt, &koff, &klo, &khi, &kval, &owner, &count, &slot_of, &start, &fill, &tmp})
+            c->release(*b);
+    };
+    int r = HERO_OK;
+    do {
+        if ((r = c->ensure(cnt, n * 4 + 4, "key counts"))) break;
+        if ((r = c->ensure(koff, (n + 1) * 8, "key offsets"))) break;
+        if ((r = c->ensure(tmp, scan_tmp_bytes(n + 1), "scan"))) break;
+        launch_key_count(q, c->p.k, P_<uint32_t>(cnt), c->st);
+        launch_scan_u32(P_<uint32_t>(cnt), P_<uint64_t>(koff), n, tmp.p, c->st);
+        uint64_t nkeys = 0;
+        if ((r = c->cuda(cudaMemcpyAsync(&nkeys, P_<uint64_t>(koff) + n, 8, cudaMemcpyDeviceToHost, c->st), "keys"))) break;
+        if ((r = c->cuda(cudaStreamSynchronize(c->st), "keys"))) break;
+        uint64_t slots = 1024;
+        while (slots < 2 * nkeys) slots <<= 1;
+        c->t_keys = nkeys;
+        c->t_mask = slots - 1;
+        if ((r = c->ensure(klo, nkeys * 8, "keys"))) break;
+        if ((r = c->ensure(khi, nkeys * 8, "keys"))) break;
+        if ((r = c->ensure(kval, nkeys * 8, "keys"))) break;
+        if ((r = c->ensure(slot_of, nkeys * 4, "keys"))) break;
+        if ((r = c->ensure(owner, slots * 4, "table"))) break;
+        if ((r = c->ensure(count, slots * 4, "table"))) break;
+        if ((r = c->ensure(fill, slots * 4, "table"))) break;
+        if ((r = c->ensure(start, (slots + 1) * 8, "table"))) break;
+        if ((r = c->ensure(c->t_slots, slots * sizeof(Slot), "table"))) break;
+        if ((r = c->ensure(c->t_vals, nkeys * 8, "table values"))) break;
+        if ((r = c->ensure(tmp, scan_tmp_bytes(slots + 1), "scan"))) break;
+        launch_key_emit(q, c->p.k, P_<uint64_t>(koff), P_<uint64_t>(klo), P_<uint64_t>(khi),
+                        P_<uint64_t>(kval), c->st);
+        cudaMemsetAsync(owner.p, 0xff, slots * 4, c->st);
+        cudaMemsetAsync(count.p, 0, slots * 4, c->st);
+        cudaMemsetAsync(fill.p, 0, slots * 4, c->st);
+        launch_table_insert(P_<uint64_t>(klo), P_<uint64_t>(khi), nkeys, P_<uint32_t>(owner),
+                            P_<uint32_t>(count), P_<uint32_t>(slot_of), c->t_mask, c->st);
+        launch_scan_u32(P_<uint32_t>(count), P_<uint64_t>(start), slots, tmp.p, c->st);
+        launch_table_fill(P_<uint64_t>(kval), nkeys, P_<uint32_t>(slot_of), P_<uint64_t>(start),
+                          P_<uint32_t>(fill), P_<uint64_t>(c->t_vals), c->st);
+        launch_table_finalize(P_<uint64_t>(klo), P_<uint64_t>(khi), P_<uint32_t>(owner),
+                              P_<uint32_t>(count), P_<uint64_t>(start), slots,
+                              P_<Slot>(c->t_slots), c->st);
+        if ((r = c->check_launch("index"))) break;
+        cudaEventRecord(e1, c->st);
+        if ((r = c->cuda(cudaStreamSynchronize(c->st), "index"))) break;
+        c->stats.ms_index += elapsed(e0, e1);
+        c->stats.index_keys = nkeys;
+        c->stats.index_slots = slots;
+        c->have_index = true;
+    } while (0);
+    cleanup();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return r;
+}
+
+// runs every stage for subjects [0, nsub) of the given reads
+static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6]) {
+    const uint64_t nseg = 2 * nsub;
+    ReadsView q = query_view(c);
+    TableView t{P_<Slot>(c->t_slots), P_<uint64_t>(c->t_vals), c->t_mask};
+    unsigned long long *ctr = P_<unsigned long long>(c->counters);
+    cudaEvent_t ev[7];
+    for (auto &e : ev) cudaEventCreate(&e);
+    int r = HERO_OK;
+    do {
+        cudaEventRecord(ev[0], c->st);
+        if ((r = c->ensure(c->seg_hits, nseg * 4 + 4, "segments"))) break;
+        if ((r = c->ensure(c->hit_off, (nseg + 1) * 8, "segments"))) break;
+        if ((r = c->ensure(c->seg_cstart, nseg * 4 + 4, "segments"))) break;
+        if ((r = c->ensure(c->seg_ccount, nseg * 4 + 4, "segments"))) break;
+        if ((r = c->ensure(c->scan_tmp, scan_tmp_bytes(std::max<uint64_t>(nseg + 1, kDpBins + 1)), "scan"))) break;
+        // zero the per-batch counters that size buffers (keep the running totals)
+        cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st);
+        launch_probe(false, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
+        launch_scan_u32(P_<uint32_t>(c->seg_hits), P_<uint64_t>(c->hit_off), nseg, c->scan_tmp.p, c->st);
+        uint64_t H = 0;
+        if ((r = c->cuda(cudaMemcpyAsync(&H, P_<uint64_t>(c->hit_off) + nseg, 8, cudaMemcpyDeviceToHost, c->st), "hits"))) break;
+        if ((r = c->cuda(cudaStreamSynchronize(c->st), "probe count"))) break;
+        const uint64_t Hc = std::max<uint64_t>(H, 1);
+        if ((r = c->ensure(c->hits, Hc * 8, "hits"))) break;
+        launch_probe(true, subj, nsub, q, t, c->p.k, nullptr, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), ctr, c->st);
+        launch_sort_hits(nseg, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), c->st);
+        if ((r = c->check_launch("seed"))) break;
+        cudaEventRecord(ev[1], c->st);
+        // chain scratch and outputs (bounds: chains <= hits, keys <= hits, DP <= 2 hits)
+        struct {
+            DBuf *b;
+            size_t per;
+        } hb[] = {{&c->cs_grp, 4},     {&c->cs_chain_of, 4}, {&c->cs_first, 4}, {&c->cs_last, 4},
+                  {&c->cs_prev, 4},    {&c->cs_size, 4},     {&c->cs_coff, 4},  {&c->cs_ckeys, 4},
+                  {&c->cs_kl, 8},      {&c->cs_gnch, 4},     {&c->cs_gbest, 8}, {&c->cs_gkept, 4},
+                  {&c->cs_gkeys, 4},   {&c->cs_gdp, 4},      {&c->ch_subj, 4},  {&c->ch_query, 4},
+                  {&c->ch_key_off, 4}, {&c->ch_seg_off, 4},  {&c->ch_nkeys, 2}, {&c->ch_nseg, 2},
+                  {&c->ch_orient, 1},  {&c->ch_status, 1},   {&c->ch_win, 1},   {&c->ch_rate, 8},
+                  {&c->ch_len, 8},     {&c->keys, 4}};
+        for (auto &x : hb)
+            if ((r = c->ensure(*x.b, Hc * x.per, "chains"))) break;
+        if (r) break;
+        if ((r = c->ensure(c->segs, 2 * Hc * sizeof(DpSeg), "DP segments"))) break;
+        ChainScratch sc{P_<uint32_t>(c->cs_grp),  P_<uint32_t>(c->cs_chain_of), P_<int32_t>(c->cs_first),
+                        P_<int32_t>(c->cs_last),  P_<int32_t>(c->cs_prev),      P_<int32_t>(c->cs_size),
+                        P_<int32_t>(c->cs_coff),  P_<int32_t>(c->cs_ckeys),     P_<int64_t>(c->cs_kl),
+                        P_<int32_t>(c->cs_gnch),  P_<int64_t>(c->cs_gbest),     P_<uint32_t>(c->cs_gkept),
+                        P_<uint32_t>(c->cs_gkeys), P_<uint32_t>(c->cs_gdp)};
+        ChainArrays ch{P_<uint32_t>(c->ch_subj),   P_<uint32_t>(c->ch_query), P_<uint32_t>(c->ch_key_off),
+                       P_<uint32_t>(c->ch_seg_off), P_<uint16_t>(c->ch_nkeys), P_<uint16_t>(c->ch_nseg),
+                       P_<uint8_t>(c->ch_orient),  P_<uint8_t>(c->ch_status), P_<uint8_t>(c->ch_win),
+                       P_<double>(c->ch_rate),     P_<double>(c->ch_len)};
+        launch_chain(c->p, nseg, subj, q, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), sc,
+                     P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
+                     P_<uint32_t>(c->keys), P_<DpSeg>(c->segs), Hc, Hc, 2 * Hc, ctr, c->st);
+        if ((r = c->check_launch("chain"))) break;
+        unsigned long long h_ctr[C_COUNT];
+        if ((r = c->cuda(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, c->st), "counters"))) break;
+        if ((r = c->cuda(cudaStreamSynchronize(c->st), "chain"))) break;
+        cudaEventRecord(ev[2], c->st);
+        if (h_ctr[C_OVERFLOW]) {
+            r = c->fail(HERO_E_STATE, "chain buffer overflow");
+            break;
+        }
+        const uint64_t NC = h_ctr[C_NC], ND = h_ctr[C_ND];
+        const int32_t rmax = int32_t(std::max<unsigned long long>(h_ctr[C_MAXR], 1));
+        const int32_t cmax = int32_t(std::max<unsigned long long>(h_ctr[C_MAXC], 1));
+        const uint32_t stride = uint32_t((rmax + cmax + 15) / 16);
+        const uint64_t NDc = std::max<uint64_t>(ND, 1);
+        if ((r = c->ensure(c->sums, NDc * sizeof(DpSum), "DP sums"))) break;
+        if ((r = c->ensure(c->cells, NDc * 4, "DP cells"))) break;
+        if ((r = c->ensure(c->perm, NDc * 4, "DP order"))) break;
+        if ((r = c->ensure(c->ops, NDc * stride * 4, "DP ops"))) break;
+        if ((r = c->ensure(c->bins, kDpBins * 4, "DP bins"))) break;
+        if ((r = c->ensure(c->bin_off, (kDpBins + 1) * 8, "DP bins"))) break;
+        const int32_t nst = (cmax + kStripW - 1) / kStripW;
+        if ((r = c->ensure(c->tb, size_t(c->dp_T) * size_t(rmax) * size_t(nst) * 2, "DP traceback scratch"))) break;
+        if ((r = c->ensure(c->bnd, size_t(c->dp_T) * size_t(rmax + 1) * 3 * 4, "DP boundary scratch"))) break;
+        launch_dp_sort(P_<DpSeg>(c->segs), ND, P_<uint32_t>(c->bins), P_<uint32_t>(c->perm),
+                       P_<uint64_t>(c->bin_off), c->scan_tmp.p, c->st);
+        cudaEventRecord(ev[3], c->st);
+        DpLaunch a{P_<DpSeg>(c->segs), P_<uint32_t>(c->perm), ND, subj.code, subj.off, subj.len,
+                   q.code, q.off, P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums),
+                   P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
+                   c->p.affine};
+        launch_dp(a, c->st);
+        if ((r = c->check_launch("dp"))) break;
+        cudaEventRecord(ev[4], c->st);
+        launch_assemble(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSum>(c->sums),
+                        P_<uint32_t>(c->cells), ctr, c->st);
+        launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch, ctr, c->st);
+        cudaEventRecord(ev[5], c->st);
+        launch_vote(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSeg>(c->segs),
+                    P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov), ctr, c->st);
+        if ((r = c->check_launch("record/vote"))) break;
+        cudaEventRecord(ev[6], c->st);
+        if ((r = c->cuda(cudaStreamSynchronize(c->st), "batch"))) break;
+        ms[0] += elapsed(ev[0], ev[1]);
+        ms[1] += elapsed(ev[1], ev[2]);
+        ms[2] += elapsed(ev[2], ev[4]);
+        ms[3] += elapsed(ev[4], ev[5]);
+        ms[4] += elapsed(ev[5], ev[6]);
+        ms[5] += elapsed(ev[3], ev[4]);
+        c->stats.dp_segments += ND;
+        c->stats.chains_kept += NC;
+    } while (0);
+    for (auto &e : ev) cudaEventDestroy(e);
+    return r;
+}
+
+static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
+    uint64_t B = c->P.subject_batch ? c->P.subject_batch : 131072;
+    double ms[6] = {0, 0, 0, 0, 0, 0};
+    for (uint64_t b = 0; b < n; b += B) {
+        const uint64_t nb = std::min(B, n - b);
+        // a batch is a window of the read arrays: shift the per-read pointers
+        ReadsView v{all.code, all.off + b, all.len + b, all.uid + b, all.good + b, nb};
+        HERO_TRY(align_batch(c, v, nb, ms));
+    }
+    c->stats.subjects += n;
+    c->stats.ms_seed += ms[0];
+    c->stats.ms_chain += ms[1];
+    c->stats.ms_dp += ms[2];
+    c->stats.ms_record += ms[3];
+    c->stats.ms_vote += ms[4];
+    c->stats.ms_dp_kernel += ms[5];
+    unsigned long long h[C_COUNT];
+    HERO_TRY(c->cuda(cudaMemcpy(h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost), "counters"));
+    for (int i = 0; i < C_COUNT; i++) c->ctr[i] = h[i];
+    return HERO_OK;
+}
+
+extern "C" int hero_align_self(hero_ctx *c) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_index) return c->fail(HERO_E_STATE, "index not built");
+    cudaSetDevice(c->dev);
+    ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
+                P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq};
+    return align_reads(c, v, c->nq);
+}
+
+extern "C" int hero_align_subjects(hero_ctx *c, const uint8_t *seq, const uint64_t *off,
+                                   const int64_t *uid, uint64_t n) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_index) return c->fail(HERO_E_STATE, "index not built");
+    cudaSetDevice(c->dev);
+    HERO_TRY(validate_reads(c, seq, off, uid, n));
+    if (n == 0) return HERO_OK;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, c->st);
+    HERO_TRY(upload_reads(c, seq, off, uid, n, c->s_raw, c->s_code, c->s_off, c->s_len, c->s_uid,
+                          nullptr, &c->s_good, nullptr));
+    cudaEventRecord(e1, c->st);
+    HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "upload subjects"));
+    c->stats.ms_upload += elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ReadsView v{P_<uint8_t>(c->s_code), P_<uint64_t>(c->s_off), P_<uint32_t>(c->s_len),
+                P_<int64_t>(c->s_uid), P_<uint8_t>(c->s_good), n};
+    return align_reads(c, v, n);
+}
+
+extern "C" int hero_consensus(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uint32_t *imed,
+                              uint32_t *imax, double *mismatch_rate, double *gc_content,
+                              uint8_t *good_out) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    cudaSetDevice(c->dev);
+    const uint64_t n = c->nq, nb = c->nqb;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    HERO_TRY(c->ensure(c->out_seq, nb, "consensus"));
+    HERO_TRY(c->ensure(c->colsum, nb * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imin, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imed, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imax, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_mis, n * 8, "consensus"));
+    cudaEventRecord(e0, c->st);
+    if (nb) cudaMemcpyAsync(c->out_seq.p, c->q_raw.p, nb, cudaMemcpyDeviceToDevice, c->st);
+    launch_consensus(c->p, query_view(c), P_<uint32_t>(c->cov), P_<uint8_t>(c->out_seq),
+                     P_<uint32_t>(c->colsum), P_<uint32_t>(c->o_imin), P_<uint32_t>(c->o_imed),
+                     P_<uint32_t>(c->o_imax), P_<double>(c->o_mis), c->st);
+    HERO_TRY(c->check_launch("consensus"));
+    cudaEventRecord(e1, c->st);
+    if (seq_out && nb) cudaMemcpyAsync(seq_out, c->out_seq.p, nb, cudaMemcpyDeviceToHost, c->st);
+    if (imin && n) cudaMemcpyAsync(imin, c->o_imin.p, n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (imed && n) cudaMemcpyAsync(imed, c->o_imed.p, n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (imax && n) cudaMemcpyAsync(imax, c->o_imax.p, n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (mismatch_rate && n) cudaMemcpyAsync(mismatch_rate, c->o_mis.p, n * 8, cudaMemcpyDeviceToHost, c->st);
+    if (gc_content && n) cudaMemcpyAsync(gc_content, c->q_gc.p, n * 8, cudaMemcpyDeviceToHost, c->st);
+    if (good_out && n) cudaMemcpyAsync(good_out, c->q_good.p, n, cudaMemcpyDeviceToHost, c->st);
+    HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "consensus"));
+    c->stats.ms_consensus += elapsed(e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return HERO_OK;
+}
+
+extern "C" int hero_get_votes(hero_ctx *c, uint32_t *cov) {
+    if (!c || !cov) return HERO_E_INPUT;
+    cudaSetDevice(c->dev);
+    if (c->nqb) HERO_TRY(c->cuda(cudaMemcpy(cov, c->cov.p, c->nqb * 16, cudaMemcpyDeviceToHost), "votes"));
+    return HERO_OK;
+}
+
+extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
+    if (!c || !out) return HERO_E_INPUT;
+    hero_stats s = c->stats;
+    s.probes = c->ctr[C_PROBES];
+    s.hits = c->ctr[C_HITS];
+    s.chains = c->ctr[C_CHAINS];
+    s.records_built = c->ctr[C_BUILT];
+    s.records_accepted = c->ctr[C_ACCEPTED];
+    s.records_kept = c->ctr[C_KEPT];
+    s.dp_segments_ref = c->ctr[C_DP_REF];
+    s.dp_cells = c->ctr[C_CELLS];
+    s.vote_anomalies = c->ctr[C_ANOMALY];
+    s.device_bytes_peak = c->bytes_peak;
+    *out = s;
+    return HERO_OK;
+}
+
+extern "C" int hero_align_segments(hero_ctx *c, int affine, const uint8_t *subj,
+                                   const uint64_t *subj_off, uint64_t n_subj,
+                                   const uint8_t *query, const uint64_t *query_off,
+                                   uint64_t n_query, uint64_t n_seg, const uint32_t *seg_subject,
+                                   const uint8_t *seg_orient, const uint32_t *seg_query,
+                                   const int32_t *s0, const int32_t *s1, const int32_t *q0,
+                                   const int32_t *q1, const uint8_t *seg_flags,
+                                   const int64_t *band, const uint64_t *ops_off, uint8_t *ops,
+                                   int32_t *nops) {
+    if (!c) return HERO_E_INPUT;
+    cudaSetDevice(c->dev);
+    if (n_seg == 0) return HERO_OK;
+    std::vector<int64_t> no_uid(std::max(n_subj, n_query), 0);
+    HERO_TRY(validate_reads(c, subj, subj_off, no_uid.data(), n_subj));
+    HERO_TRY(validate_reads(c, query, query_off, no_uid.data(), n_query));
+    std::vector<DpSeg> h(n_seg);
+    int32_t rmax = 1, cmax = 1;
+    for (uint64_t i = 0; i < n_seg; i++) {
+        if (seg_subject[i] >= n_subj || seg_query[i] >= n_query)
+            return c->fail(HERO_E_INPUT, "segment read index out of range");
+        const int64_t ls_read = int64_t(subj_off[seg_subject[i] + 1] - subj_off[seg_subject[i]]);
+        const int64_t lq_read = int64_t(query_off[seg_query[i] + 1] - query_off[seg_query[i]]);
+        if (s0[i] < 0 || s1[i] <= s0[i] || s1[i] > ls_read || q0[i] < 0 || q1[i] <= q0[i] ||
+            q1[i] > lq_read)
+            return c->fail(HERO_E_INPUT, "segment range out of the read");
+        if (ops_off[i + 1] - ops_off[i] < uint64_t((s1[i] - s0[i]) + (q1[i] - q0[i])))
+            return c->fail(HERO_E_INPUT, "ops capacity too small");
+        DpSeg g;
+        g.subj = seg_subject[i];
+        g.query = seg_query[i];
+        g.s0 = uint16_t(s0[i]);
+        g.s1 = uint16_t(s1[i]);
+        g.q0 = uint16_t(q0[i]);
+        g.q1 = uint16_t(q1[i]);
+        g.band = int32_t(band[i] > 65535 ? 65535 : (band[i] < 0 ? 0 : band[i]));
+        g.flags = (seg_flags[i] & 3u) | (uint32_t(seg_orient[i] & 1u) << kSegOrientShift);
+        g.pad = 0;
+        h[i] = g;
+        const int32_t ls = s1[i] - s0[i], lq = q1[i] - q0[i];
+        rmax = std::max(rmax, std::max(ls, lq));
+        cmax = std::max(cmax, std::min(ls, lq));
+    }
+    const uint32_t stride = uint32_t((rmax + cmax + 15) / 16);
+    DBuf sraw, scode, soff, slen, suid, qraw, qcode, qoff, qlen, quid, dsegs, dsums, dops, dtb, dbnd,
+        doo, dout, dn;
+    auto cleanup = [&]() {
+        for (DBuf *b : {&sraw, &scode, &soff, &slen, &suid, &qraw, &qcode, &qoff, &qlen, &quid,
+                        &dsegs, &dsums, &dops, &dtb, &dbnd, &doo, &dout, &dn})
+            c->release(*b);
+    };
+    int r = HERO_OK;
+    do {
+        if ((r = upload_reads(c, subj, subj_off, no_uid.data(), n_subj, sraw, scode, soff, slen, suid,
+                              nullptr, nullptr, nullptr)))
+            break;
+        if ((r = upload_reads(c, query, query_off, no_uid.data(), n_query, qraw, qcode, qoff, qlen,
+                              quid, nullptr, nullptr, nullptr)))
+            break;
+        const int32_t nst = (cmax + kStripW - 1) / kStripW;
+        if ((r = c->ensure(dsegs, n_seg * sizeof(DpSeg), "segments"))) break;
+        if ((r = c->ensure(dsums, n_seg * sizeof(DpSum), "segments"))) break;
+        if ((r = c->ensure(dops, n_seg * stride * 4, "segments"))) break;
+        if ((r = c->ensure(dtb, size_t(c->dp_T) * rmax * nst * 2, "scratch"))) break;
+        if ((r = c->ensure(dbnd, size_t(c->dp_T) * (rmax + 1) * 3 * 4, "scratch"))) break;
+        if ((r = c->ensure(doo, (n_seg + 1) * 8, "ops"))) break;
+        if ((r = c->ensure(dout, ops_off[n_seg], "ops"))) break;
+        if ((r = c->ensure(dn, n_seg * 4, "ops"))) break;
+        cudaMemcpyAsync(dsegs.p, h.data(), n_seg * sizeof(DpSeg), cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(doo.p, ops_off, (n_seg + 1) * 8, cudaMemcpyHostToDevice, c->st);
+        DpLaunch a{P_<DpSeg>(dsegs), nullptr, n_seg, P_<uint8_t>(scode), P_<uint64_t>(soff),
+                   P_<uint32_t>(slen), P_<uint8_t>(qcode), P_<uint64_t>(qoff), P_<uint32_t>(dops),
+                   stride, P_<DpSum>(dsums), nullptr, P_<uint16_t>(dtb), P_<int32_t>(dbnd),
+                   c->dp_T, rmax, affine ? 1 : 0};
+        launch_dp(a, c->st);
+        launch_unpack_ops(P_<uint32_t>(dops), stride, P_<DpSum>(dsums), n_seg, P_<uint64_t>(doo),
+                          P_<uint8_t>(dout), P_<int32_t>(dn), c->st);
+        if ((r = c->check_launch("align segments"))) break;
+        cudaMemcpyAsync(ops, dout.p, ops_off[n_seg], cudaMemcpyDeviceToHost, c->st);
+        cudaMemcpyAsync(nops, dn.p, n_seg * 4, cudaMemcpyDeviceToHost, c->st);
+        r = c->cuda(cudaStreamSynchronize(c->st), "align segments");
+    } while (0);
+    cleanup();
+    return r;
+}

@@ -1,0 +1,777 @@
+// hero_core.cuh -- per-item logic of the HERO read-correction path.
+//
+// Everything here works on one item (one k-mer, one chain, one DP segment,
+// one record, one read column) and is written once as __host__ __device__
+// code: the CUDA kernels in hero_kernels.cu call it per thread, and the host
+// test harness compiles the same header with g++ to check it item by item.
+//
+// Reference semantics (guo-xuan/Hero, src/) are cited per function.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define HERO_HD __host__ __device__ __forceinline__
+#else
+#define HERO_HD inline
+#endif
+
+#if defined(__CUDA_ARCH__)
+#define HERO_DMUL(a, b) __dmul_rn((a), (b))
+#define HERO_DDIV(a, b) __ddiv_rn((a), (b))
+#define HERO_DADD(a, b) __dadd_rn((a), (b))
+#define HERO_DSUB(a, b) __dsub_rn((a), (b))
+#define HERO_ROUND(a) round(a)
+#define HERO_FABS(a) fabs(a)
+#else
+#include <cmath>
+#define HERO_DMUL(a, b) ((a) * (b))
+#define HERO_DDIV(a, b) ((a) / (b))
+#define HERO_DADD(a, b) ((a) + (b))
+#define HERO_DSUB(a, b) ((a) - (b))
+#define HERO_ROUND(a) std::round(a)
+#define HERO_FABS(a) std::fabs(a)
+#endif
+
+namespace hero {
+
+// ---------------------------------------------------------------------------
+// constants
+// ---------------------------------------------------------------------------
+// BandAligner::setCost (BandAligner.cpp:528-542); sentinel -MAXDUL (BandAligner.h:18)
+constexpr int kDX = -4, kDY = -4, kMISS = -4, kHIT = 1, kSX = 0, kEX = -1;
+constexpr int kNEG = -100000;
+
+// per-step alignment ops in original orientation (I consumes query only, D subject only)
+enum : uint8_t { OP_M = 0, OP_X = 1, OP_I = 2, OP_D = 3 };
+
+// base codes: (c >> 1) & 3 of the ASCII letter, as HERO indexes its coverage
+// matrix (QueryRead.cpp:124-131): A=0 C=1 T=2 G=3; anything else is 4.
+// The complement of an ACGT code is code ^ 2.
+constexpr uint8_t kBad = 4;
+HERO_HD uint8_t base_code(uint8_t c) {
+    return (c == 'A' || c == 'C' || c == 'G' || c == 'T') ? uint8_t((c >> 1) & 3) : kBad;
+}
+HERO_HD char code_base(uint8_t c) {  // aDNA (QueryRead.cpp:11)
+    return c == 0 ? 'A' : c == 1 ? 'C' : c == 2 ? 'T' : 'G';
+}
+
+struct Params {
+    int32_t k;          // Config::iKmer
+    int32_t l;          // Config::minimumOverlapLength
+    int32_t affine;     // Config::iAlignerType == IAFFINE
+    int32_t pad;
+    double mis_rate;    // Config::dMaxMismatchRate
+    double indel_rate;  // Config::dMaxIndelRate
+    double thr;         // Config::dMinFrequencyCallConsensus
+};
+
+// ---------------------------------------------------------------------------
+// k-mer keys: the 2k-bit integer of the k-mer codes, first base most significant
+// (hi holds the bits above 64).  Supports 1 <= k <= 63.
+// ---------------------------------------------------------------------------
+struct Kmer {
+    uint64_t lo, hi;
+};
+
+HERO_HD void kmer_push(Kmer &m, uint32_t code, int k) {
+    m.hi = (m.hi << 2) | (m.lo >> 62);
+    m.lo = (m.lo << 2) | code;
+    if (2 * k < 64) {
+        m.lo &= (1ull << (2 * k)) - 1ull;
+        m.hi = 0;
+    } else if (2 * k == 64) {
+        m.hi = 0;
+    } else {
+        m.hi &= (1ull << (2 * k - 64)) - 1ull;
+    }
+}
+
+HERO_HD uint64_t mix64(uint64_t z) {  // splitmix64 finalizer
+    z ^= z >> 30;
+    z *= 0xbf58476d1ce4e5b9ull;
+    z ^= z >> 27;
+    z *= 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    return z;
+}
+HERO_HD uint64_t kmer_hash(const Kmer &m) { return mix64(m.lo ^ mix64(m.hi + 0x9e3779b97f4a7c15ull)); }
+
+// Keys a good query read contributes (HashTableLongKey::insertQueryDataset,
+// HashTableLongKey.cpp:279-289): positions 0, k, 2k, ... while <= L-k, then
+// a tail key at L-k when the stride did not land on L.
+HERO_HD int32_t query_key_count(int64_t L, int64_t k) {
+    if (L < k) return 0;  // the reference throws on such a read (substr out of range)
+    int64_t n = (L - k) / k + 1;
+    return int32_t(n + (n * k < L ? 1 : 0));
+}
+HERO_HD int64_t query_key_pos(int64_t L, int64_t k, int32_t idx) {
+    int64_t n = (L - k) / k + 1;
+    return idx < n ? int64_t(idx) * k : L - k;
+}
+
+// hit: (query inner id, position on query, position on subject), ordered like
+// comparePairKeyPosition (SubjectRead.cpp:157-173) when compared as u64
+HERO_HD uint64_t hit_pack(uint32_t q, uint32_t posQ, uint32_t posS) {
+    return (uint64_t(q) << 32) | (uint64_t(posQ) << 16) | uint64_t(posS);
+}
+HERO_HD uint32_t hit_q(uint64_t h) { return uint32_t(h >> 32); }
+HERO_HD int32_t hit_posQ(uint64_t h) { return int32_t((h >> 16) & 0xffff); }
+HERO_HD int32_t hit_posS(uint64_t h) { return int32_t(h & 0xffff); }
+
+// ---------------------------------------------------------------------------
+// chaining (SubjectReadAligner.cpp:391-408, 711-751, 805-852)
+// ---------------------------------------------------------------------------
+// isFromTheSameAlignment
+HERO_HD bool same_alignment(const Params &p, int32_t addQ, int32_t addS, int32_t begQ,
+                            int32_t begS, int32_t endQ, int32_t endS) {
+    if (addS <= endS) return false;
+    if (addQ <= endQ) return false;
+    double lq = HERO_FABS(double(addQ - begQ));
+    double ls = HERO_FABS(double(addS - begS));
+    double total = (lq >= ls ? lq : ls);
+    total = HERO_DADD(total, double(p.k));
+    double diff = HERO_FABS(HERO_DSUB(lq, ls));
+    if (HERO_DDIV(diff, total) > p.indel_rate) return false;
+    return true;
+}
+
+// Greedy chain assignment of one query group (hits sorted by posQ, posS).
+// chain_of[h] receives the chain index of each hit; first/last are scratch of
+// the group's size.  Returns the number of chains.
+template <class HitAt>
+HERO_HD int32_t chain_group(const Params &p, const HitAt &hit, int32_t n, uint32_t *chain_of,
+                            int32_t *first, int32_t *last) {
+    int32_t nch = 0;
+    for (int32_t h = 0; h < n; h++) {
+        const uint64_t x = hit(h);
+        const int32_t q = hit_posQ(x), s = hit_posS(x);
+        int32_t c = 0;
+        for (; c < nch; c++) {
+            const uint64_t b = hit(first[c]), e = hit(last[c]);
+            if (same_alignment(p, q, s, hit_posQ(b), hit_posS(b), hit_posQ(e), hit_posS(e))) break;
+        }
+        if (c == nch) {
+            first[nch] = h;
+            nch++;
+        }
+        last[c] = h;
+        chain_of[h] = uint32_t(c);
+    }
+    return nch;
+}
+
+// calKeyLength of every chain of a group; kl must hold nch entries and prev
+// nch scratch slots.  Returns the largest key length.
+template <class HitAt>
+HERO_HD int64_t chain_key_lengths(const Params &p, const HitAt &hit, int32_t n,
+                                  const uint32_t *chain_of, int32_t nch, int64_t *kl,
+                                  int32_t *prev) {
+    for (int32_t c = 0; c < nch; c++) {
+        kl[c] = 0;
+        prev[c] = -1;
+    }
+    for (int32_t h = 0; h < n; h++) {
+        const uint32_t c = chain_of[h];
+        if (prev[c] >= 0) {
+            const int32_t a = hit_posS(hit(prev[c])), b = hit_posS(hit(h));
+            kl[c] += (a + p.k <= b) ? p.k : (b - a);
+        }
+        prev[c] = h;
+    }
+    int64_t best = 0;
+    for (int32_t c = 0; c < nch; c++) {
+        kl[c] += p.k;
+        if (kl[c] > best) best = kl[c];
+    }
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// record pieces: getAlignment2 (SubjectReadAligner.cpp:197-389)
+// ---------------------------------------------------------------------------
+enum : uint32_t { DPF_RIGHT = 1u, DPF_LEFT = 2u };
+
+// Walks one chain the way getAlignment2 builds its record and calls the visitor:
+//   v.begin(extra, maxMis, maxIndel) once the overlap test has passed
+//   v.position(pos)
+//   v.run(op, count)        CIGAR runs added by k-mer arithmetic (addCigar)
+//   v.dp(s0, s1, q0, q1, flags, band)   one BandAligner call; band is the value the
+//                                        aligner holds before the call
+//   v.check(maxMis, maxIndel) -> bool   isGoodAlignment(m, i) early exit point
+//   v.finish()              after the end piece (the rate test is the caller's)
+// keys(i) returns (posQ, posS) of the i-th key of the chain as a hit word.
+// Returns false when the chain yields no record (overlap test or early exit).
+template <class KeyAt, class V>
+HERO_HD bool walk_chain(const Params &p, int64_t Lq, int64_t Ls, const KeyAt &keys, int32_t n,
+                        V &v) {
+    const int64_t k = p.k;
+    int64_t posQ = hit_posQ(keys(0)), posS = hit_posS(keys(0));
+    int64_t ov = (posQ < posS ? posQ : posS);
+    ov += (Lq - posQ < Ls - posS ? Lq - posQ : Ls - posS);
+    if (ov < p.l) return false;
+    const int64_t extra = int64_t(HERO_ROUND(HERO_DMUL(double(ov), p.indel_rate)));
+    const int64_t maxMis = int64_t(HERO_ROUND(HERO_DMUL(double(ov), p.mis_rate)));
+    const int64_t maxIndel = extra;
+    v.begin(extra, maxMis, maxIndel);
+    int64_t band = extra * 2;  // setBand; grows inside the aligner (BandAligner.cpp:59-62)
+    auto dp = [&](int64_t s0, int64_t s1, int64_t q0, int64_t q1, uint32_t flags) {
+        v.dp(s0, s1, q0, q1, flags, band);
+        // setSequences puts the longer segment on the rows; the aligner then
+        // widens its band to the length difference
+        int64_t ls = s1 - s0, lq = q1 - q0;
+        int64_t d = lq <= ls ? ls - lq : lq - ls;
+        if (d > band) band = d;
+    };
+    if (posQ != 0 && posS != 0) {
+        if (posQ < posS) {
+            int64_t s0 = (posS - posQ - extra < 0 ? 0 : posS - posQ - extra);
+            v.position(s0);
+            dp(s0, posS, 0, posQ, DPF_RIGHT);
+        } else if (posQ == posS) {
+            v.position(0);
+            dp(0, posS, 0, posQ, DPF_RIGHT);
+        } else {
+            int64_t q0 = (posQ - posS - extra < 0 ? 0 : posQ - posS - extra);
+            v.position(0);
+            if (posQ - posS - extra > 0) v.run(OP_I, posQ - posS - extra);
+            dp(0, posS, q0, posQ, DPF_RIGHT);
+        }
+        v.run(OP_M, k);
+    } else {
+        if (posS == 0 && posQ == 0) {
+            v.position(0);
+        } else if (posS == 0) {
+            v.position(0);
+            v.run(OP_I, posQ);
+        } else {
+            v.position(posS);
+        }
+        v.run(OP_M, k);
+    }
+    if (!v.check(maxMis, maxIndel)) return false;
+    for (int32_t i = 1; i < n; i++) {
+        const int64_t cQ = hit_posQ(keys(i)), cS = hit_posS(keys(i));
+        if (cQ - posQ == cS - posS && posS + k >= cS) {
+            if (posS + k > cS) {
+                v.run(OP_M, cS - posS);
+            } else {
+                v.run(OP_M, k);
+            }
+        } else {
+            if (posS + k == cS) {
+                if (cQ - posQ - k > 0) {
+                    v.run(OP_I, cQ - posQ - k);
+                    v.run(OP_M, k);
+                } else {
+                    v.run(OP_D, -cQ + posQ + k);
+                    v.run(OP_M, cQ - posQ);
+                }
+            } else if (posS + k > cS) {
+                if (cQ - posQ < cS - posS) {
+                    v.run(OP_D, cS - posS - cQ + posQ);
+                    v.run(OP_M, cQ - posQ);
+                } else {
+                    v.run(OP_I, cQ - posQ + posS - cS);
+                    v.run(OP_M, cS - posS);
+                }
+            } else {
+                if (posQ + k == cQ) {
+                    v.run(OP_D, cS - posS - k);
+                    v.run(OP_M, k);
+                } else if (posQ + k > cQ) {
+                    v.run(OP_D, cS - posS + posQ - cQ);
+                    v.run(OP_M, k + posQ - cQ);
+                } else {
+                    dp(posS + k, cS, posQ + k, cQ, 0);
+                    v.run(OP_M, k);
+                }
+            }
+        }
+        posQ = cQ;
+        posS = cS;
+        if (!v.check(maxMis, maxIndel)) return false;
+    }
+    posQ = hit_posQ(keys(n - 1)) + k;
+    posS = hit_posS(keys(n - 1)) + k;
+    if (posQ < Lq) {
+        if (posS == Ls) {
+            v.run(OP_I, Lq - posQ);
+        } else if (Ls - posS < Lq - posQ) {
+            int64_t qe = (Ls - posS + posQ + extra < Lq ? Ls - posS + posQ + extra : Lq);
+            dp(posS, Ls, posQ, qe, DPF_LEFT);
+            if (Ls - posS + posQ + extra < Lq) v.run(OP_I, Lq - (Ls - posS + posQ + extra));
+        } else if (Ls - posS == Lq - posQ) {
+            dp(posS, Ls, posQ, Lq, DPF_LEFT);
+        } else {
+            int64_t se = (posS + (Lq - posQ) + extra < Ls ? posS + (Lq - posQ) + extra : Ls);
+            dp(posS, se, posQ, Lq, DPF_LEFT);
+        }
+    }
+    v.finish();
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// record score: AlignmentRecord::addCigar + calculateScore (AlignmentRecord.cpp:35-100)
+// Only the first and last runs are treated specially (leading/trailing I or D
+// are not counted), so a record is summarised exactly by its first run, its
+// last run and the totals of the runs strictly between them.  Mismatch runs
+// with different letters are separate CIGAR entries in the reference but are
+// never first-vs-interior ambiguous (they are not I/D), so they merge here.
+// ---------------------------------------------------------------------------
+struct DpSum {  // summary of one DP segment's op path (16 bytes)
+    uint16_t tot[4];  // ops of each kind over the whole path
+    uint16_t fc, lc;  // first / last run lengths
+    uint8_t ft, lt;   // first / last run kinds
+    uint8_t nruns;    // 1, or 2 meaning "two or more"
+    uint8_t pad;
+};
+
+struct RecState {
+    int32_t n = 0;  // runs so far: 0, 1, 2 (= two or more)
+    uint8_t ft = 0, lt = 0;
+    int64_t fc = 0, lc = 0;
+    int64_t im = 0, ix = 0, iid = 0;  // interior totals
+
+    HERO_HD void interior_add(uint8_t t, int64_t c) {
+        if (t == OP_M) {
+            im += c;
+        } else if (t == OP_X) {
+            ix += c;
+        } else {
+            iid += c;
+        }
+    }
+    HERO_HD void add(uint8_t t, int64_t c) {
+        if (n == 0) {
+            ft = t;
+            fc = c;
+            n = 1;
+        } else if (n == 1) {
+            if (ft == t) {
+                fc += c;
+            } else {
+                lt = t;
+                lc = c;
+                n = 2;
+            }
+        } else {
+            if (lt == t) {
+                lc += c;
+            } else {
+                interior_add(lt, lc);
+                lt = t;
+                lc = c;
+            }
+        }
+    }
+    HERO_HD void add_piece(const DpSum &s) {
+        add(s.ft, s.fc);
+        if (s.nruns >= 2) {
+            if (n >= 2) interior_add(lt, lc);
+            // interior runs of the piece: totals minus its first and last runs
+            int64_t t[4] = {s.tot[0], s.tot[1], s.tot[2], s.tot[3]};
+            t[s.ft] -= s.fc;
+            t[s.lt] -= s.lc;
+            im += t[OP_M];
+            ix += t[OP_X];
+            iid += t[OP_I] + t[OP_D];
+            lt = s.lt;
+            lc = s.lc;
+            n = 2;
+        }
+    }
+    // calculateScore: (mismatches, indels, alignment length)
+    HERO_HD void score(int64_t &mis, int64_t &indel, int64_t &len) const {
+        mis = ix;
+        indel = iid;
+        len = im + ix + iid;
+        if (n >= 1 && ft != OP_I && ft != OP_D) {
+            len += fc;
+            if (ft == OP_X) mis += fc;
+        }
+        if (n >= 2 && lt != OP_I && lt != OP_D) {
+            len += lc;
+            if (lt == OP_X) mis += lc;
+        }
+    }
+    // isGoodAlignment(maxMis, maxIndel) (AlignmentRecord.cpp:310-316)
+    HERO_HD bool good_counts(int64_t maxMis, int64_t maxIndel) const {
+        int64_t m, i, l;
+        score(m, i, l);
+        return !(m > maxMis || i > maxIndel);
+    }
+    // isGoodAlignment() rates and the dedupe keys (AlignmentRecord.cpp:92-99, 302-308)
+    HERO_HD bool good_rates(const Params &p, double &rate_sum, double &len_out) const {
+        int64_t m, i, l;
+        score(m, i, l);
+        double indel_rate = 100, mis_rate = 100;
+        if (l != 0) {
+            indel_rate = HERO_DDIV(double(i), double(l));
+            mis_rate = HERO_DDIV(double(m), double(l));
+        }
+        rate_sum = HERO_DADD(indel_rate, mis_rate);
+        len_out = double(l);
+        return mis_rate <= p.mis_rate && indel_rate <= p.indel_rate;
+    }
+};
+
+// SubjectRead::addAlignment (SubjectRead.cpp:25-79): a later record replaces the
+// kept one only if it is strictly better: smaller rate sum, or equal rate sum
+// and longer alignment.  Folding in arrival order keeps the earliest best.
+HERO_HD bool record_better(double rs_new, double len_new, double rs_cur, double len_cur) {
+    if (rs_cur < rs_new) return false;
+    if (rs_cur == rs_new) return !(len_cur >= len_new);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// banded DP: BandAligner::bandedAlign / bandedAlignAffineGap (BandAligner.cpp:56-239)
+//
+// The matrix is computed in vertical strips of W columns held in registers,
+// row by row.  A cell outside the band is forced to the sentinel for every
+// state: the reference guards exactly the neighbours that fall outside the
+// band with -MAXDUL (BandAligner.cpp:72,86,180,189), real scores are always
+// far above any sentinel-derived value, and the direction rules never pick a
+// sentinel option over a real one, so every in-band value and direction
+// matches.  Row 0 and column 0 always trace left / up.
+// ---------------------------------------------------------------------------
+struct SegView {  // a DP segment after setSequences (rows = longer side)
+    const uint8_t *row_base;  // DP "subject" (rows)
+    const uint8_t *col_base;  // DP "query" (columns)
+    int32_t row_dir, col_dir;  // +1 forward, -1 reverse-complement walk
+    uint8_t row_xor, col_xor;  // 2 for reverse complement
+    int32_t R, C;
+    int64_t band;     // after widening to R - C
+    bool right, left, reversed;
+
+    HERO_HD uint8_t row(int32_t i) const { return uint8_t(row_base[int64_t(row_dir) * (i - 1)] ^ row_xor); }
+    HERO_HD uint8_t col(int32_t j) const { return uint8_t(col_base[int64_t(col_dir) * (j - 1)] ^ col_xor); }
+};
+
+// builds the view of segment [s0,s1) of the subject (orientation rc when
+// orient=1) against [q0,q1) of the query, as BandAligner::setSequences does
+HERO_HD SegView make_view(const uint8_t *subj, int32_t Ls, int32_t orient, const uint8_t *qry,
+                          int32_t s0, int32_t s1, int32_t q0, int32_t q1, uint32_t flags,
+                          int64_t band_in) {
+    SegView v;
+    const uint8_t *sb;
+    int32_t sdir;
+    uint8_t sx;
+    if (orient) {  // position p of the reverse complement is comp(fwd[Ls-1-p])
+        sb = subj + (Ls - 1 - s0);
+        sdir = -1;
+        sx = 2;
+    } else {
+        sb = subj + s0;
+        sdir = 1;
+        sx = 0;
+    }
+    const int32_t ls = s1 - s0, lq = q1 - q0;
+    if (lq <= ls) {
+        v.row_base = sb;
+        v.row_dir = sdir;
+        v.row_xor = sx;
+        v.col_base = qry + q0;
+        v.col_dir = 1;
+        v.col_xor = 0;
+        v.R = ls;
+        v.C = lq;
+        v.reversed = false;
+    } else {
+        v.row_base = qry + q0;
+        v.row_dir = 1;
+        v.row_xor = 0;
+        v.col_base = sb;
+        v.col_dir = sdir;
+        v.col_xor = sx;
+        v.R = lq;
+        v.C = ls;
+        v.reversed = true;
+    }
+    int64_t d = int64_t(v.R) - v.C;
+    v.band = band_in > d ? band_in : d;
+    v.right = (flags & DPF_RIGHT) != 0;
+    v.left = (flags & DPF_LEFT) != 0;
+    return v;
+}
+
+// cells of the reference's loop bounds (BandAligner.cpp:63-66)
+HERO_HD uint64_t band_cells(int32_t R, int32_t C, int64_t m) {
+    uint64_t cells = 0;
+    for (int32_t i = 0; i <= R; i++) {
+        int64_t lm = i - m > 0 ? i - m : 0;
+        int64_t rm = C < i + m ? C : i + m;
+        if (rm >= lm) cells += uint64_t(rm - lm + 1);
+    }
+    return cells;
+}
+
+HERO_HD bool in_band(int32_t i, int32_t j, int32_t C, int64_t m) {
+    return j <= C && int64_t(j) >= int64_t(i) - m && int64_t(j) <= int64_t(i) + m;
+}
+
+// Boundary-column storage of one thread: for each row, the state values of the
+// last column of the previous strip.  Scratch provides
+//   int32_t& b(int32_t state, int32_t row)          state 0..2 (FM, IX, IY)
+//   void tb_set(int32_t strip, int32_t row, uint32_t bits)  traceback codes of a
+//   uint32_t tb_get(int32_t strip, int32_t row)             row, 2 bits per cell
+template <int W, class Scratch>
+HERO_HD void dp_fill_global(const SegView &v, Scratch &sc) {
+    const int32_t R = v.R, C = v.C;
+    const int64_t m = v.band;
+    const bool full = m >= R && m >= C;
+    // column 0 (BandAligner.cpp:75-79 with j == 0)
+    sc.b(0, 0) = 0;
+    for (int32_t i = 1; i <= R; i++) sc.b(0, i) = (int64_t(i) <= m) ? i * (v.right ? kSX : kDX) : kNEG;
+    const int32_t nst = (C + W - 1) / W;
+    for (int32_t s = 0; s < nst; s++) {
+        const int32_t j0 = s * W;
+        uint8_t bc[W];
+        int32_t up[W];
+        for (int32_t w = 0; w < W; w++) {
+            const int32_t j = j0 + w + 1;
+            bc[w] = j <= C ? v.col(j) : uint8_t(7);
+            up[w] = (j <= C && int64_t(j) <= m) ? kDY * j : kNEG;  // row 0
+        }
+        int32_t prev_lb = sc.b(0, 0);
+        for (int32_t i = 1; i <= R; i++) {
+            const uint8_t a = v.row(i);
+            const int32_t lb = sc.b(0, i);
+            int32_t left = lb, dg = prev_lb;
+            uint32_t bits = 0;
+#pragma unroll
+            for (int32_t w = 0; w < W; w++) {
+                const int32_t j = j0 + w + 1;
+                int32_t h;
+                uint32_t code;
+                if (full ? (j <= C) : in_band(i, j, C, m)) {
+                    const int32_t vu = up[w] + ((j == C && v.left) ? kSX : kDX);
+                    const int32_t vl = left + kDY;
+                    const int32_t vd = dg + (a == bc[w] ? kHIT : kMISS);
+                    if (vd >= vl && vd >= vu) {
+                        h = vd;
+                        code = 2;
+                    } else if (vl >= vu) {
+                        h = vl;
+                        code = 1;
+                    } else {
+                        h = vu;
+                        code = 0;
+                    }
+                } else {
+                    h = kNEG;
+                    code = 0;
+                }
+                dg = up[w];
+                up[w] = h;
+                left = h;
+                bits |= code << (2 * w);
+            }
+            sc.tb_set(s, i, bits);
+            sc.b(0, i) = left;
+            prev_lb = lb;
+        }
+        // row 0 value of this strip's last column becomes the boundary of row 0
+        const int32_t jl = j0 + W;
+        sc.b(0, 0) = (jl <= C && int64_t(jl) <= m) ? kDY * jl : kNEG;
+    }
+}
+
+template <int W, class Scratch>
+HERO_HD void dp_fill_affine(const SegView &v, Scratch &sc) {
+    const int32_t R = v.R, C = v.C;
+    const int64_t m = v.band;
+    const bool full = m >= R && m >= C;
+    // (0,0) and column 0 (BandAligner.cpp:140-164)
+    sc.b(0, 0) = 0;
+    sc.b(1, 0) = kDX - kEX;
+    sc.b(2, 0) = kDX - kEX;
+    for (int32_t i = 1; i <= R; i++) {
+        if (int64_t(i) <= m) {
+            if (v.right) {
+                sc.b(0, i) = 0;
+                sc.b(1, i) = 0;
+                sc.b(2, i) = kDY;
+            } else {
+                sc.b(0, i) = kDX - kEX + i * kEX;
+                sc.b(1, i) = kDX - kEX + i * kEX;
+                sc.b(2, i) = kDX - kEX + i * kEX;
+            }
+        } else {
+            sc.b(0, i) = kNEG;
+            sc.b(1, i) = kNEG;
+            sc.b(2, i) = kNEG;
+        }
+    }
+    const int32_t nst = (C + W - 1) / W;
+    for (int32_t s = 0; s < nst; s++) {
+        const int32_t j0 = s * W;
+        uint8_t bc[W];
+        int32_t uf[W], ux[W], uy[W];
+        for (int32_t w = 0; w < W; w++) {
+            const int32_t j = j0 + w + 1;
+            bc[w] = j <= C ? v.col(j) : uint8_t(7);
+            // row 0 (BandAligner.cpp:165-171): FM = IX = IY = dx - ex + j*ex
+            const int32_t r0 = (j <= C && int64_t(j) <= m) ? kDX - kEX + j * kEX : kNEG;
+            uf[w] = r0;
+            ux[w] = r0;
+            uy[w] = r0;
+        }
+        int32_t pf = sc.b(0, 0), px = sc.b(1, 0), py = sc.b(2, 0);
+        for (int32_t i = 1; i <= R; i++) {
+            const uint8_t a = v.row(i);
+            const int32_t lf0 = sc.b(0, i), lx0 = sc.b(1, i), ly0 = sc.b(2, i);
+            int32_t lf = lf0, ly = ly0, lx = lx0;
+            int32_t df = pf, dx = px, dy = py;
+            uint32_t bits = 0;
+#pragma unroll
+            for (int32_t w = 0; w < W; w++) {
+                const int32_t j = j0 + w + 1;
+                int32_t F, X, Y;
+                uint32_t code;
+                if (full ? (j <= C) : in_band(i, j, C, m)) {
+                    // IY: gap along the row (BandAligner.cpp:180-188)
+                    const int32_t y0 = lf + kDY, y1 = ly + kEX;
+                    Y = y0 >= y1 ? y0 : y1;
+                    // IX: gap down the column (BandAligner.cpp:189-201)
+                    int32_t x0, x1;
+                    if (v.left && j == C) {
+                        x0 = uf[w] + kSX;
+                        x1 = ux[w] + kSX;
+                    } else {
+                        x0 = uf[w] + kDX;
+                        x1 = ux[w] + kEX;
+                    }
+                    X = x1 > x0 ? x1 : x0;
+                    // FM = max3(FM, IX, IY)(i-1,j-1) + s (BandAligner.cpp:203-207)
+                    const int32_t sub = a == bc[w] ? kHIT : kMISS;
+                    int32_t mm = df >= dx ? df : dx;
+                    mm = mm >= dy ? mm : dy;
+                    F = mm + sub;
+                    // BM1 (BandAligner.cpp:214-222)
+                    code = (F > X && F >= Y) ? 2u : (Y > X ? 1u : 0u);
+                } else {
+                    F = kNEG;
+                    X = kNEG;
+                    Y = kNEG;
+                    code = 0;
+                }
+                df = uf[w];
+                dx = ux[w];
+                dy = uy[w];
+                uf[w] = F;
+                ux[w] = X;
+                uy[w] = Y;
+                lf = F;
+                lx = X;
+                ly = Y;
+                bits |= code << (2 * w);
+            }
+            sc.tb_set(s, i, bits);
+            sc.b(0, i) = lf;
+            sc.b(1, i) = lx;
+            sc.b(2, i) = ly;
+            pf = lf0;
+            px = lx0;
+            py = ly0;
+        }
+        const int32_t jl = j0 + W;
+        const int32_t r0 = (jl <= C && int64_t(jl) <= m) ? kDX - kEX + jl * kEX : kNEG;
+        sc.b(0, 0) = r0;
+        sc.b(1, 0) = r0;
+        sc.b(2, 0) = r0;
+    }
+}
+
+// Traceback (BandAligner.cpp:114-125 / 227-238) from (R, C) to (0, 0).
+// emit(op) receives ops last-to-first.  Fills the path summary.
+template <int W, class Scratch, class Emit>
+HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &sum) {
+    int32_t i = v.R, j = v.C, nops = 0;
+    uint32_t tot[4] = {0, 0, 0, 0};
+    uint8_t cur = 0xff;
+    uint32_t cc = 0;
+    int32_t nr = 0;
+    uint8_t lt = 0;
+    uint32_t lc = 0;
+    const uint8_t op_up = v.reversed ? OP_I : OP_D;
+    const uint8_t op_left = v.reversed ? OP_D : OP_I;
+    while (i > 0 || j > 0) {
+        uint32_t code;
+        if (i == 0) {
+            code = 1;
+        } else if (j == 0) {
+            code = 0;
+        } else {
+            code = (sc.tb_get((j - 1) / W, i) >> (2 * ((j - 1) % W))) & 3u;
+        }
+        uint8_t op;
+        if (code == 2) {
+            op = v.row(i) == v.col(j) ? OP_M : OP_X;
+            i--;
+            j--;
+        } else if (code == 1) {
+            op = op_left;
+            j--;
+        } else {
+            op = op_up;
+            i--;
+        }
+        emit(op);
+        nops++;
+        tot[op]++;
+        if (op == cur) {
+            cc++;
+        } else {
+            if (cc > 0) {
+                if (nr == 0) {
+                    lt = cur;
+                    lc = cc;
+                }
+                nr++;
+            }
+            cur = op;
+            cc = 1;
+        }
+    }
+    // the run open at the end of the walk is the first run of the path
+    sum.ft = cur;
+    sum.fc = uint16_t(cc);
+    if (nr == 0) {
+        sum.lt = cur;
+        sum.lc = uint16_t(cc);
+        sum.nruns = 1;
+    } else {
+        sum.lt = lt;
+        sum.lc = uint16_t(lc);
+        sum.nruns = 2;
+    }
+    for (int t = 0; t < 4; t++) sum.tot[t] = uint16_t(tot[t]);
+    sum.pad = 0;
+    return nops;
+}
+
+// ---------------------------------------------------------------------------
+// consensus of one column: QueryRead::callConsensus (QueryRead.cpp:148-180)
+// c[] already includes the read's own vote.  Returns the new code, or -1 to
+// keep the base.
+// ---------------------------------------------------------------------------
+HERO_HD int32_t column_consensus(const uint32_t c[4], double thr) {
+    double sum = 0;
+    for (int j = 0; j < 4; j++) sum = HERO_DADD(sum, double(c[j]));
+    int32_t id = -1;
+    double fLargest = 0, fLarger = 0;
+    for (int j = 0; j < 4; j++) {
+        const double f = HERO_DDIV(double(c[j]), sum);
+        if (fLargest < f) {
+            fLarger = fLargest;
+            fLargest = f;
+            id = j;
+        }
+    }
+    if (HERO_DSUB(fLargest, fLarger) >= thr) return id;
+    return -1;
+}
+
+}  // namespace hero

@@ -1,0 +1,161 @@
+// hero_internal.cuh -- device data layout and kernel launchers of the B200 path.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hero_core.cuh"
+
+namespace hero {
+
+// open-addressed k-mer slot: one 32-byte sector per probe
+struct __align__(32) Slot {
+    uint64_t lo, hi;      // 2k-bit key
+    uint32_t start;       // first value in the value array
+    uint32_t count;       // number of values; 0 = empty slot
+    uint64_t pad;
+};
+
+// one DP segment: BandAligner::setSequences arguments of one call
+struct __align__(16) DpSeg {
+    uint32_t subj;    // subject index within the batch
+    uint32_t query;   // query inner id
+    uint16_t s0, s1;  // subject range, subject orientation coordinates
+    uint16_t q0, q1;  // query range
+    int32_t band;     // band held by the aligner before the call
+    uint32_t flags;   // DPF_RIGHT | DPF_LEFT | orient << 2
+    uint32_t pad;
+};
+constexpr uint32_t kSegOrientShift = 2;
+
+// reads resident on the device (queries, or one batch of subjects)
+struct ReadsView {
+    const uint8_t *code;  // base codes, A0 C1 T2 G3, other 4
+    const uint64_t *off;  // n+1 offsets
+    const uint32_t *len;
+    const int64_t *uid;
+    const uint8_t *good;
+    uint64_t n;
+};
+
+struct TableView {
+    const Slot *slots;
+    const uint64_t *vals;  // (query << 32) | position
+    uint64_t mask;
+};
+
+// device counters (uint64), indices
+enum Counter : int {
+    C_PROBES = 0,
+    C_HITS,
+    C_CHAINS,
+    C_NC,           // chains kept (allocated)
+    C_NK,           // chain keys
+    C_ND,           // DP segments
+    C_MAXR,
+    C_MAXC,
+    C_BUILT,
+    C_ACCEPTED,
+    C_KEPT,
+    C_DP_REF,
+    C_CELLS,
+    C_ANOMALY,
+    C_OVERFLOW,
+    C_COUNT
+};
+
+// per-batch chain outputs (structure of arrays)
+struct ChainArrays {
+    uint32_t *subj, *query, *key_off, *seg_off;
+    uint16_t *nkeys, *nseg;
+    uint8_t *orient, *status, *win;
+    double *rate, *len;
+};
+enum : uint8_t { CH_NONE = 0, CH_REJECTED = 1, CH_ACCEPTED = 2 };
+
+// scratch parallel to the hit array used by the chaining kernel
+struct ChainScratch {
+    uint32_t *grp;       // group starts
+    uint32_t *chain_of;  // chain of each hit
+    int32_t *first, *last, *prev, *size, *coff, *ckeys;
+    int64_t *kl;
+    int32_t *g_nch;
+    int64_t *g_best;
+    uint32_t *g_kept, *g_keys, *g_dp;
+};
+
+// ---------------------------------------------------------------------------
+// launchers (hero_kernels.cu); all asynchronous on `st`
+// ---------------------------------------------------------------------------
+void launch_prep_reads(const uint8_t *raw, uint64_t nbases, uint8_t *code, const uint64_t *off,
+                       uint64_t n, uint32_t *len, uint8_t *good_query, uint8_t *good_subject,
+                       double *gc, int32_t l, cudaStream_t st);
+// exclusive scan of n uint32 counts into n+1 uint64 offsets; tmp sized by scan_tmp_bytes
+size_t scan_tmp_bytes(uint64_t n);
+void launch_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, void *tmp, cudaStream_t st);
+
+void launch_key_count(ReadsView q, int32_t k, uint32_t *count, cudaStream_t st);
+void launch_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint64_t *klo,
+                     uint64_t *khi, uint64_t *kval, cudaStream_t st);
+void launch_table_insert(const uint64_t *klo, const uint64_t *khi, uint64_t nkeys,
+                         uint32_t *owner, uint32_t *count, uint32_t *slot_of, uint64_t mask,
+                         cudaStream_t st);
+void launch_table_fill(const uint64_t *kval, uint64_t nkeys, const uint32_t *slot_of,
+                       const uint64_t *start, uint32_t *fill, uint64_t *vals, cudaStream_t st);
+void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint32_t *owner,
+                           const uint32_t *count, const uint64_t *start, uint64_t nslots,
+                           Slot *slots, cudaStream_t st);
+
+void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
+                  uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
+                  unsigned long long *counters, cudaStream_t st);
+void launch_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits, cudaStream_t st);
+void launch_chain(const Params &p, uint64_t nseg, ReadsView subj, ReadsView q,
+                  const uint64_t *hit_off, const uint64_t *hits, ChainScratch sc,
+                  uint32_t *seg_chain_start, uint32_t *seg_chain_count, ChainArrays ch,
+                  uint32_t *keys, DpSeg *segs, uint64_t cap_chains, uint64_t cap_keys,
+                  uint64_t cap_segs, unsigned long long *counters, cudaStream_t st);
+
+// DP: shape sort then the strip kernel
+void launch_dp_sort(const DpSeg *segs, uint64_t nd, uint32_t *bins, uint32_t *perm,
+                    uint64_t *bin_off, void *scan_tmp, cudaStream_t st);
+constexpr uint32_t kDpBins = 1u << 16;
+struct DpLaunch {
+    const DpSeg *segs;
+    const uint32_t *perm;   // processing order; NULL = identity
+    uint64_t nd;
+    const uint8_t *scode;   // subject codes + offsets + lengths of the batch
+    const uint64_t *soff;
+    const uint32_t *slen;
+    const uint8_t *qcode;
+    const uint64_t *qoff;
+    uint32_t *ops;          // packed ops, `stride` u32 words per segment
+    uint32_t stride;
+    DpSum *sums;
+    uint32_t *cells;        // reference band cells per segment (may be NULL)
+    uint16_t *tb;           // traceback scratch: threads * rmax * nstrips
+    int32_t *bnd;           // boundary scratch: threads * 3 * (rmax + 1)
+    uint64_t threads;       // resident threads the scratch is laid out for
+    int32_t rmax;
+    int32_t affine;
+};
+constexpr int kStripW = 8;
+void launch_dp(const DpLaunch &a, cudaStream_t st);
+uint64_t dp_threads(int device);
+
+void launch_assemble(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
+                     ReadsView subj, ReadsView q, const DpSum *sums, const uint32_t *cells,
+                     unsigned long long *counters, cudaStream_t st);
+void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
+                   const uint32_t *seg_chain_count, ChainArrays ch, unsigned long long *counters,
+                   cudaStream_t st);
+void launch_vote(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
+                 ReadsView subj, ReadsView q, const DpSeg *segs, const uint32_t *ops,
+                 uint32_t stride, const DpSum *sums, uint32_t *cov, unsigned long long *counters,
+                 cudaStream_t st);
+void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, uint8_t *out,
+                      uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
+                      double *mis, cudaStream_t st);
+void launch_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
+                       const uint64_t *out_off, uint8_t *out, int32_t *nops, cudaStream_t st);
+
+}  // namespace hero

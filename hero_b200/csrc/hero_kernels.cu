@@ -1,0 +1,1155 @@
+// hero_kernels.cu -- sm_100a kernels of the HERO read-correction path.
+//
+// Stage map (reference function -> kernel):
+//   QueryDataset::qualityFilter / setGcContent        k_codes, k_read_flags
+//   HashTableLongKey::insertQueryDataset              k_key_count, k_key_emit,
+//                                                     k_table_insert/fill/finalize
+//   SubjectReadAligner::searchHashTable2 (+ sort)     k_probe, k_sort_hits
+//   processOneSubjectRead2 chaining + getAlignment2
+//   segment layout                                    k_chain
+//   BandAligner::calculateAlignment                   k_dp_hist/scatter, k_dp
+//   AlignmentRecord scoring + early exits             k_assemble
+//   SubjectRead::addAlignment                         k_dedupe
+//   SubjectRead::updateQueryCoverage                  k_vote
+//   QueryRead::callConsensus + coverage statistics    k_consensus
+#include <cuda_runtime.h>
+
+#include "hero_internal.cuh"
+
+namespace hero {
+
+namespace {
+
+constexpr uint32_t kEmptyOwner = 0xffffffffu;
+
+inline unsigned grid_1d(uint64_t n, unsigned block, unsigned cap = 148u * 64u) {
+    uint64_t g = (n + block - 1) / block;
+    if (g == 0) g = 1;
+    if (g > cap) g = cap;
+    return unsigned(g);
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+// exclusive prefix over lanes; *total receives the warp total
+template <class T>
+__device__ __forceinline__ T warp_exclusive(T v, T *total) {
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (int(lane_id()) >= o) x += y;
+    }
+    *total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+// ---------------------------------------------------------------------------
+// reads
+// ---------------------------------------------------------------------------
+__global__ void k_codes(const uint8_t *raw, uint64_t n, uint8_t *code) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += uint64_t(gridDim.x) * blockDim.x)
+        code[i] = base_code(raw[i]);
+}
+
+// QueryDataset::qualityFilter (QueryDataset.cpp:60-75), the good-read tests of
+// QueryDataset.cpp:226 (query) and SubjectDataset.cpp:157-162 (subject), and
+// QueryRead::setGcContent (QueryRead.cpp:73-81)
+__global__ void k_read_flags(const uint8_t *code, const uint64_t *off, uint64_t n, uint32_t *len,
+                             uint8_t *gq, uint8_t *gs, double *gc, int32_t l) {
+    for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n;
+         r += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t b = off[r], L = off[r + 1] - b;
+        uint64_t cnt[4] = {0, 0, 0, 0};
+        bool valid = true;
+        uint64_t ngc = 0;
+        for (uint64_t i = 0; i < L; i++) {
+            const uint8_t c = code[b + i];
+            if (c >= 4) {
+                valid = false;
+            } else {
+                cnt[c]++;
+                ngc += (c & 1u);  // C (1) or G (3)
+            }
+        }
+        bool qf = valid;
+        if (qf) {
+            const uint64_t thr = uint64_t(__dmul_rn(double(L), 0.8));
+            if (cnt[0] >= thr || cnt[1] >= thr || cnt[2] >= thr || cnt[3] >= thr) qf = false;
+        }
+        const uint64_t lu = uint16_t(l);  // the reference compares with a UINT16 copy
+        len[r] = uint32_t(L);
+        if (gq) gq[r] = (L > lu && qf) ? 1 : 0;
+        if (gs) gs[r] = (L < lu || qf) ? 1 : 0;
+        if (gc) gc[r] = __ddiv_rn(double(ngc), double(L));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan (u32 counts -> u64 offsets, n+1 entries)
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
+
+template <class T>
+__global__ void k_scan_tile(const T *in, uint64_t n, uint64_t *out, uint64_t *tile_sums) {
+    __shared__ uint64_t warp_tot[kScanThreads / 32];
+    const uint64_t base = uint64_t(blockIdx.x) * kScanTile + uint64_t(threadIdx.x) * kScanItems;
+    uint64_t loc[kScanItems];
+    uint64_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const uint64_t idx = base + j;
+        const uint64_t v = idx < n ? uint64_t(in[idx]) : 0;
+        loc[j] = s;
+        s += v;
+    }
+    uint64_t tot;
+    uint64_t ex = warp_exclusive<uint64_t>(s, &tot);
+    if (lane_id() == 0) warp_tot[threadIdx.x >> 5] = tot;
+    __syncthreads();
+    uint64_t wpre = 0, btot = 0;
+    for (int w = 0; w < kScanThreads / 32; w++) {
+        if (w < int(threadIdx.x >> 5)) wpre += warp_tot[w];
+        btot += warp_tot[w];
+    }
+    ex += wpre;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        const uint64_t idx = base + j;
+        if (idx < n) out[idx] = ex + loc[j];
+    }
+    if (threadIdx.x == 0) {
+        tile_sums[blockIdx.x] = btot;
+        if (blockIdx.x == gridDim.x - 1) out[n] = btot;
+    }
+}
+
+__global__ void k_scan_add(uint64_t *out, uint64_t n, const uint64_t *tile_prefix) {
+    const uint64_t add = tile_prefix[blockIdx.x];
+    if (add == 0) return;
+    const uint64_t base = uint64_t(blockIdx.x) * kScanTile;
+    for (uint64_t i = threadIdx.x; i < kScanTile; i += blockDim.x) {
+        const uint64_t idx = base + i;
+        if (idx < n) out[idx] += add;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] += add;
+}
+
+size_t scan_levels_bytes(uint64_t n) {
+    size_t b = 0;
+    uint64_t m = n;
+    while (true) {
+        const uint64_t nt = (m + kScanTile - 1) / kScanTile;
+        b += (nt + 1) * 2 * sizeof(uint64_t);
+        if (nt <= 1) break;
+        m = nt;
+    }
+    return b + 256;
+}
+
+template <class T>
+void scan_rec(const T *in, uint64_t *out, uint64_t n, uint64_t *tmp, cudaStream_t st) {
+    if (n == 0) {
+        cudaMemsetAsync(out, 0, sizeof(uint64_t), st);
+        return;
+    }
+    const uint64_t nt = (n + kScanTile - 1) / kScanTile;
+    uint64_t *sums = tmp;
+    uint64_t *pref = tmp + (nt + 1);
+    k_scan_tile<T><<<unsigned(nt), kScanThreads, 0, st>>>(in, n, out, sums);
+    if (nt > 1) {
+        scan_rec<uint64_t>(sums, pref, nt, tmp + 2 * (nt + 1), st);
+        k_scan_add<<<unsigned(nt), kScanThreads, 0, st>>>(out, n, pref);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k-mer table (HashTableLongKey.cpp:41-68, 250-342)
+// ---------------------------------------------------------------------------
+__global__ void k_key_count(ReadsView q, int32_t k, uint32_t *count) {
+    for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < q.n;
+         r += uint64_t(gridDim.x) * blockDim.x)
+        count[r] = q.good[r] ? uint32_t(query_key_count(q.len[r], k)) : 0u;
+}
+
+__global__ void k_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint64_t *klo,
+                           uint64_t *khi, uint64_t *kval) {
+    for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < q.n;
+         r += uint64_t(gridDim.x) * blockDim.x) {
+        if (!q.good[r]) continue;
+        const int64_t L = q.len[r];
+        const int32_t nk = query_key_count(L, k);
+        const uint8_t *c = q.code + q.off[r];
+        uint64_t e = key_off[r];
+        for (int32_t i = 0; i < nk; i++, e++) {
+            const int64_t pos = query_key_pos(L, k, i);
+            Kmer m{0, 0};
+            for (int32_t t = 0; t < k; t++) kmer_push(m, c[pos + t] & 3u, k);
+            klo[e] = m.lo;
+            khi[e] = m.hi;
+            kval[e] = (uint64_t(r) << 32) | uint64_t(pos);
+        }
+    }
+}
+
+__global__ void k_table_insert(const uint64_t *klo, const uint64_t *khi, uint64_t nkeys,
+                               uint32_t *owner, uint32_t *count, uint32_t *slot_of,
+                               uint64_t mask) {
+    for (uint64_t e = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < nkeys;
+         e += uint64_t(gridDim.x) * blockDim.x) {
+        const Kmer m{klo[e], khi[e]};
+        uint64_t h = kmer_hash(m) & mask;
+        for (uint64_t it = 0; it <= mask; it++) {
+            const uint32_t prev = atomicCAS(&owner[h], kEmptyOwner, uint32_t(e));
+            if (prev == kEmptyOwner || (klo[prev] == m.lo && khi[prev] == m.hi)) {
+                slot_of[e] = uint32_t(h);
+                atomicAdd(&count[h], 1u);
+                break;
+            }
+            h = (h + 1) & mask;
+        }
+    }
+}
+
+__global__ void k_table_fill(const uint64_t *kval, uint64_t nkeys, const uint32_t *slot_of,
+                             const uint64_t *start, uint32_t *fill, uint64_t *vals) {
+    for (uint64_t e = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < nkeys;
+         e += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t s = slot_of[e];
+        const uint64_t p = start[s] + atomicAdd(&fill[s], 1u);
+        vals[p] = kval[e];
+    }
+}
+
+__global__ void k_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint32_t *owner,
+                                 const uint32_t *count, const uint64_t *start, uint64_t nslots,
+                                 Slot *slots) {
+    for (uint64_t h = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; h < nslots;
+         h += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t o = owner[h];
+        Slot s;
+        s.pad = 0;
+        if (o != kEmptyOwner) {
+            s.lo = klo[o];
+            s.hi = khi[o];
+            s.start = uint32_t(start[h]);
+            s.count = count[h];
+        } else {
+            s.lo = 0;
+            s.hi = 0;
+            s.start = 0;
+            s.count = 0;
+        }
+        slots[h] = s;
+    }
+}
+
+// exact multimap lookup (HashTableLongKey::getListOfReads, HashTableLongKey.cpp:79-99)
+__device__ __forceinline__ bool table_find(const TableView &t, const Kmer &m, uint32_t &start,
+                                           uint32_t &count) {
+    uint64_t h = kmer_hash(m) & t.mask;
+    for (uint64_t it = 0; it <= t.mask; it++) {
+        const uint4 a = __ldg(reinterpret_cast<const uint4 *>(&t.slots[h]));
+        const uint4 b = __ldg(reinterpret_cast<const uint4 *>(&t.slots[h]) + 1);
+        const uint32_t cnt = b.y;
+        if (cnt == 0) return false;
+        const uint64_t lo = (uint64_t(a.y) << 32) | a.x, hi = (uint64_t(a.w) << 32) | a.z;
+        if (lo == m.lo && hi == m.hi) {
+            start = b.x;
+            count = cnt;
+            return true;
+        }
+        h = (h + 1) & t.mask;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// seeding: SubjectReadAligner::searchHashTable2 (SubjectReadAligner.cpp:444-491)
+// One warp per subject read; lane f takes windows f, f+32, ...  The forward
+// window at f and the reverse-complement window at L-k-f are the same bases.
+// ---------------------------------------------------------------------------
+constexpr int kProbeWarps = 8;
+
+template <bool EMIT>
+__global__ void __launch_bounds__(kProbeWarps * 32)
+    k_probe(ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
+            uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
+            unsigned long long *counters) {
+    __shared__ uint32_t fill[kProbeWarps][2];
+    const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+    const uint64_t warps = uint64_t(gridDim.x) * kProbeWarps;
+    unsigned long long probes = 0, nhits = 0;
+    for (uint64_t s = uint64_t(blockIdx.x) * kProbeWarps + wib; s < nsub; s += warps) {
+        const int32_t L = int32_t(subj.len[s]);
+        const int64_t su = subj.uid[s];
+        const uint8_t *c = subj.code + subj.off[s];
+        uint32_t c0 = 0, c1 = 0;
+        uint64_t o0 = 0, o1 = 0;
+        if (EMIT) {
+            if (lane == 0) {
+                fill[wib][0] = 0;
+                fill[wib][1] = 0;
+            }
+            o0 = hit_off[2 * s];
+            o1 = hit_off[2 * s + 1];
+            __syncwarp();
+        }
+        if (subj.good[s] && L >= k) {
+            const int32_t P = L - k + 1;
+            if (lane == 0) probes += 2ull * uint64_t(P);
+            for (int32_t f = int32_t(lane); f < P; f += 32) {
+                Kmer fm{0, 0}, rm{0, 0};
+                bool bad = false;
+                for (int32_t i = 0; i < k; i++) {
+                    const uint8_t x = c[f + i];
+                    bad |= x >= 4;
+                    kmer_push(fm, x & 3u, k);
+                }
+                if (bad) continue;
+                for (int32_t i = k - 1; i >= 0; i--) kmer_push(rm, (c[f + i] & 3u) ^ 2u, k);
+                for (int o = 0; o < 2; o++) {
+                    uint32_t st = 0, cnt = 0;
+                    if (!table_find(t, o ? rm : fm, st, cnt)) continue;
+                    const uint32_t posS = o ? uint32_t(L - k - f) : uint32_t(f);
+                    for (uint32_t e = 0; e < cnt; e++) {
+                        const uint64_t v = __ldg(&t.vals[st + e]);
+                        const uint32_t qq = uint32_t(v >> 32);
+                        if (__ldg(&q.uid[qq]) == su) continue;  // self hit (SubjectReadAligner.cpp:463-465)
+                        if (EMIT) {
+                            const uint32_t slot = atomicAdd(&fill[wib][o], 1u);
+                            hits[(o ? o1 : o0) + slot] = hit_pack(qq, uint32_t(v & 0xffffffffu), posS);
+                        } else {
+                            if (o) {
+                                c1++;
+                            } else {
+                                c0++;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (!EMIT) {
+            c0 = warp_sum(c0);
+            c1 = warp_sum(c1);
+            if (lane == 0) {
+                seg_hits[2 * s] = c0;
+                seg_hits[2 * s + 1] = c1;
+                nhits += c0 + c1;
+            }
+        } else {
+            __syncwarp();
+        }
+    }
+    if (!EMIT && lane == 0) {
+        atomicAdd(&counters[C_PROBES], probes);
+        atomicAdd(&counters[C_HITS], nhits);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// per-segment sort of hits by (query, posQ, posS) (SubjectRead::sortKeyPosition)
+// Bitonic network in its all-ascending form (mirror step + half cleaners), so
+// positions past n behave as +infinity and need no storage.
+// ---------------------------------------------------------------------------
+constexpr int kSortThreads = 256, kSortSmem = 4096;
+
+__device__ __forceinline__ void cmpx(uint64_t *a, uint64_t lo, uint64_t hi) {
+    const uint64_t x = a[lo], y = a[hi];
+    if (y < x) {
+        a[lo] = y;
+        a[hi] = x;
+    }
+}
+
+__device__ void bitonic(uint64_t *a, uint64_t n, uint64_t N) {
+    for (uint64_t k = 2; k <= N; k <<= 1) {
+        const uint64_t half = k >> 1;
+        for (uint64_t i = threadIdx.x; i < N / 2; i += blockDim.x) {
+            const uint64_t blk = i / half, off = i % half;
+            const uint64_t lo = blk * k + off, hi = blk * k + k - 1 - off;
+            if (hi < n) cmpx(a, lo, hi);
+        }
+        __syncthreads();
+        for (uint64_t j = half >> 1; j >= 1; j >>= 1) {
+            for (uint64_t i = threadIdx.x; i < N / 2; i += blockDim.x) {
+                const uint64_t blk = i / j, off = i % j;
+                const uint64_t lo = blk * 2 * j + off, hi = lo + j;
+                if (hi < n) cmpx(a, lo, hi);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits) {
+    __shared__ uint64_t sm[kSortSmem];
+    for (uint64_t seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+        const uint64_t b = hit_off[seg], n = hit_off[seg + 1] - b;
+        if (n < 2) continue;
+        uint64_t N = 1;
+        while (N < n) N <<= 1;
+        if (n <= uint64_t(kSortSmem)) {
+            for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) sm[i] = hits[b + i];
+            __syncthreads();
+            bitonic(sm, n, N);
+            for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) hits[b + i] = sm[i];
+            __syncthreads();
+        } else {
+            bitonic(hits + b, n, N);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// chaining + record layout: processOneSubjectRead2 (SubjectReadAligner.cpp:805-852)
+// One warp per (subject, orientation); lane g takes query groups g, g+32, ...
+// ---------------------------------------------------------------------------
+struct CountDp {
+    uint32_t n = 0;
+    HERO_HD void begin(int64_t, int64_t, int64_t) {}
+    HERO_HD void position(int64_t) {}
+    HERO_HD void run(uint8_t, int64_t) {}
+    HERO_HD void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) { n++; }
+    HERO_HD bool check(int64_t, int64_t) { return true; }
+    HERO_HD void finish() {}
+};
+
+struct EmitDp {
+    DpSeg *out;
+    uint32_t subj, query, orient;
+    uint32_t n = 0;
+    int32_t maxr = 0, maxc = 0;
+    HERO_HD void begin(int64_t, int64_t, int64_t) {}
+    HERO_HD void position(int64_t) {}
+    HERO_HD void run(uint8_t, int64_t) {}
+    HERO_HD void dp(int64_t s0, int64_t s1, int64_t q0, int64_t q1, uint32_t flags, int64_t band) {
+        DpSeg g;
+        g.subj = subj;
+        g.query = query;
+        g.s0 = uint16_t(s0);
+        g.s1 = uint16_t(s1);
+        g.q0 = uint16_t(q0);
+        g.q1 = uint16_t(q1);
+        // any band >= 65535 covers every cell of a segment of reads below 65536 bases
+        g.band = int32_t(band > 65535 ? 65535 : band);
+        g.flags = flags | (orient << kSegOrientShift);
+        g.pad = 0;
+        out[n++] = g;
+        const int32_t ls = int32_t(s1 - s0), lq = int32_t(q1 - q0);
+        const int32_t r = ls > lq ? ls : lq, c = ls > lq ? lq : ls;
+        if (r > maxr) maxr = r;
+        if (c > maxc) maxc = c;
+    }
+    HERO_HD bool check(int64_t, int64_t) { return true; }
+    HERO_HD void finish() {}
+};
+
+__global__ void __launch_bounds__(256)
+    k_chain(Params p, uint64_t nseg, ReadsView subj, ReadsView q, const uint64_t *hit_off,
+            const uint64_t *hits, ChainScratch sc, uint32_t *seg_chain_start,
+            uint32_t *seg_chain_count, ChainArrays ch, uint32_t *keys, DpSeg *segs,
+            uint64_t cap_chains, uint64_t cap_keys, uint64_t cap_segs,
+            unsigned long long *counters) {
+    const uint32_t lane = lane_id();
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    unsigned long long nchains_all = 0;
+    int32_t maxr = 0, maxc = 0;
+    for (uint64_t seg = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); seg < nseg;
+         seg += warps) {
+        const uint64_t base = hit_off[seg], n = hit_off[seg + 1] - base;
+        const uint32_t s = uint32_t(seg >> 1), orient = uint32_t(seg & 1);
+        if (n == 0) {
+            if (lane == 0) {
+                seg_chain_start[seg] = 0;
+                seg_chain_count[seg] = 0;
+            }
+            continue;
+        }
+        const uint64_t *H = hits + base;
+        // group starts (a group = hits of one query read)
+        uint32_t ng = 0;
+        for (uint64_t c0 = 0; c0 < n; c0 += 32) {
+            const uint64_t i = c0 + lane;
+            const bool flag = i < n && (i == 0 || hit_q(H[i]) != hit_q(H[i - 1]));
+            const uint32_t m = __ballot_sync(0xffffffffu, flag);
+            if (flag) sc.grp[base + ng + __popc(m & ((1u << lane) - 1u))] = uint32_t(i);
+            ng += __popc(m);
+        }
+        __syncwarp();
+        const int32_t Ls = int32_t(subj.len[s]);
+        // pass A: chain every group, keep the results in the scratch
+        uint32_t tk = 0, tkeys = 0, tdp = 0;
+        for (uint32_t g = lane; g < ng; g += 32) {
+            const uint32_t gs = sc.grp[base + g];
+            const uint32_t ge = (g + 1 < ng) ? sc.grp[base + g + 1] : uint32_t(n);
+            const int32_t gn = int32_t(ge - gs);
+            const uint64_t off = base + gs;
+            const uint64_t *G = H + gs;
+            auto hit = [G](int32_t h) { return G[h]; };
+            const int32_t nch = chain_group(p, hit, gn, sc.chain_of + off, sc.first + off, sc.last + off);
+            const int64_t best = chain_key_lengths(p, hit, gn, sc.chain_of + off, nch, sc.kl + off, sc.prev + off);
+            // bucket the keys by chain, in order
+            for (int32_t c = 0; c < nch; c++) sc.size[off + c] = 0;
+            for (int32_t h = 0; h < gn; h++) sc.size[off + sc.chain_of[off + h]]++;
+            int32_t run = 0;
+            for (int32_t c = 0; c < nch; c++) {
+                sc.coff[off + c] = run;
+                sc.prev[off + c] = run;
+                run += sc.size[off + c];
+            }
+            for (int32_t h = 0; h < gn; h++) {
+                const uint32_t c = sc.chain_of[off + h];
+                sc.ckeys[off + sc.prev[off + c]++] = h;
+            }
+            const uint32_t qid = hit_q(G[0]);
+            const int64_t Lq = q.len[qid];
+            uint32_t kept = 0, nkeys = 0, ndp = 0;
+            for (int32_t c = 0; c < nch; c++) {
+                if (sc.kl[off + c] != best) continue;
+                kept++;
+                nkeys += uint32_t(sc.size[off + c]);
+                const int32_t *ck = sc.ckeys + off + sc.coff[off + c];
+                auto key = [G, ck](int32_t i) { return G[ck[i]]; };
+                CountDp cv;
+                walk_chain(p, Lq, Ls, key, sc.size[off + c], cv);
+                ndp += cv.n;
+            }
+            sc.g_nch[off] = nch;
+            sc.g_best[off] = best;
+            sc.g_kept[off] = kept;
+            sc.g_keys[off] = nkeys;
+            sc.g_dp[off] = ndp;
+            tk += kept;
+            tkeys += nkeys;
+            tdp += ndp;
+            nchains_all += uint64_t(nch);
+        }
+        tk = warp_sum(tk);
+        tkeys = warp_sum(tkeys);
+        tdp = warp_sum(tdp);
+        unsigned long long cs = 0, ks = 0, ds = 0;
+        int overflow = 0;
+        if (lane == 0) {
+            cs = atomicAdd(&counters[C_NC], (unsigned long long)tk);
+            ks = atomicAdd(&counters[C_NK], (unsigned long long)tkeys);
+            ds = atomicAdd(&counters[C_ND], (unsigned long long)tdp);
+            if (cs + tk > cap_chains || ks + tkeys > cap_keys || ds + tdp > cap_segs) {
+                overflow = 1;
+                atomicAdd(&counters[C_OVERFLOW], 1ull);
+            }
+            seg_chain_start[seg] = overflow ? 0u : uint32_t(cs);
+            seg_chain_count[seg] = overflow ? 0u : tk;
+        }
+        overflow = __shfl_sync(0xffffffffu, overflow, 0);
+        if (overflow) continue;
+        cs = __shfl_sync(0xffffffffu, cs, 0);
+        ks = __shfl_sync(0xffffffffu, ks, 0);
+        ds = __shfl_sync(0xffffffffu, ds, 0);
+        // pass B: emit chains, keys and DP segments in (query, chain) order
+        for (uint32_t g0 = 0; g0 < ng; g0 += 32) {
+            const uint32_t g = g0 + lane;
+            const bool has = g < ng;
+            uint32_t gs = 0, gk = 0, gkeys = 0, gdp = 0;
+            if (has) {
+                gs = sc.grp[base + g];
+                gk = sc.g_kept[base + gs];
+                gkeys = sc.g_keys[base + gs];
+                gdp = sc.g_dp[base + gs];
+            }
+            uint32_t tot_c, tot_k, tot_d;
+            const uint32_t ec = warp_exclusive<uint32_t>(gk, &tot_c);
+            const uint32_t ek = warp_exclusive<uint32_t>(gkeys, &tot_k);
+            const uint32_t ed = warp_exclusive<uint32_t>(gdp, &tot_d);
+            if (has) {
+                const uint32_t ge = (g + 1 < ng) ? sc.grp[base + g + 1] : uint32_t(n);
+                const uint64_t off = base + gs;
+                const uint64_t *G = H + gs;
+                const uint32_t qid = hit_q(G[0]);
+                const int64_t Lq = q.len[qid];
+                const int32_t nch = sc.g_nch[off];
+                const int64_t best = sc.g_best[off];
+                (void)ge;
+                uint64_t ci = cs + ec, ki = ks + ek, di = ds + ed;
+                for (int32_t c = 0; c < nch; c++) {
+                    if (sc.kl[off + c] != best) continue;
+                    const int32_t sz = sc.size[off + c];
+                    const int32_t *ck = sc.ckeys + off + sc.coff[off + c];
+                    for (int32_t i = 0; i < sz; i++) {
+                        const uint64_t x = G[ck[i]];
+                        keys[ki + i] = (uint32_t(hit_posQ(x)) << 16) | uint32_t(hit_posS(x));
+                    }
+                    auto key = [G, ck](int32_t i) { return G[ck[i]]; };
+                    EmitDp ev;
+                    ev.out = segs + di;
+                    ev.subj = s;
+                    ev.query = qid;
+                    ev.orient = orient;
+                    walk_chain(p, Lq, Ls, key, sz, ev);
+                    if (ev.maxr > maxr) maxr = ev.maxr;
+                    if (ev.maxc > maxc) maxc = ev.maxc;
+                    ch.subj[ci] = s;
+                    ch.query[ci] = qid;
+                    ch.key_off[ci] = uint32_t(ki);
+                    ch.seg_off[ci] = uint32_t(di);
+                    ch.nkeys[ci] = uint16_t(sz);
+                    ch.nseg[ci] = uint16_t(ev.n);
+                    ch.orient[ci] = uint8_t(orient);
+                    ch.status[ci] = CH_NONE;
+                    ch.win[ci] = 0;
+                    ci++;
+                    ki += uint32_t(sz);
+                    di += ev.n;
+                }
+            }
+            cs += tot_c;
+            ks += tot_k;
+            ds += tot_d;
+        }
+    }
+    nchains_all = warp_sum(nchains_all);
+    maxr = warp_max(maxr);
+    maxc = warp_max(maxc);
+    if (lane == 0) {
+        atomicAdd(&counters[C_CHAINS], nchains_all);
+        atomicMax(&counters[C_MAXR], (unsigned long long)maxr);
+        atomicMax(&counters[C_MAXC], (unsigned long long)maxc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// banded DP (BandAligner.cpp:56-419), one thread per segment
+// ---------------------------------------------------------------------------
+struct DevScratch {
+    uint16_t *tb;
+    int32_t *bnd;
+    uint64_t T;
+    int32_t rmax;
+    uint64_t t;
+    __device__ __forceinline__ void tb_set(int32_t s, int32_t i, uint32_t bits) {
+        tb[(uint64_t(s) * uint64_t(rmax) + uint64_t(i - 1)) * T + t] = uint16_t(bits);
+    }
+    __device__ __forceinline__ uint32_t tb_get(int32_t s, int32_t i) const {
+        return tb[(uint64_t(s) * uint64_t(rmax) + uint64_t(i - 1)) * T + t];
+    }
+    __device__ __forceinline__ int32_t &b(int32_t st, int32_t i) {
+        return bnd[(uint64_t(st) * uint64_t(rmax + 1) + uint64_t(i)) * T + t];
+    }
+};
+
+struct OpsWriter {
+    uint32_t *base;
+    int32_t p;
+    uint32_t acc = 0;
+    __device__ __forceinline__ void operator()(uint8_t op) {
+        p--;
+        acc |= uint32_t(op) << (2 * (p & 15));
+        if ((p & 15) == 0) {
+            base[p >> 4] = acc;
+            acc = 0;
+        }
+    }
+    __device__ __forceinline__ void flush() {
+        if (p & 15) base[p >> 4] = acc;
+    }
+};
+
+__device__ __forceinline__ uint32_t shape_key(const DpSeg &g) {
+    const int32_t ls = g.s1 - g.s0, lq = g.q1 - g.q0;
+    const int32_t r = ls > lq ? ls : lq, c = ls > lq ? lq : ls;
+    int32_t nst = (c + kStripW - 1) / kStripW;
+    if (nst > 63) nst = 63;
+    return (uint32_t(nst) << 10) | uint32_t(r > 1023 ? 1023 : r);
+}
+
+__global__ void k_dp_hist(const DpSeg *segs, uint64_t nd, uint32_t *bins) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nd;
+         i += uint64_t(gridDim.x) * blockDim.x)
+        atomicAdd(&bins[shape_key(segs[i])], 1u);
+}
+
+__global__ void k_dp_scatter(const DpSeg *segs, uint64_t nd, uint32_t *cursor,
+                             const uint64_t *bin_off, uint32_t *perm) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nd;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t key = shape_key(segs[i]);
+        perm[bin_off[key] + atomicAdd(&cursor[key], 1u)] = uint32_t(i);
+    }
+}
+
+constexpr int kDpThreads = 128;
+
+template <bool AFFINE>
+__global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
+    const uint64_t T = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    DevScratch sc{a.tb, a.bnd, T, a.rmax, t};
+    for (uint64_t idx = t; idx < a.nd; idx += T) {
+        const uint32_t si = a.perm ? a.perm[idx] : uint32_t(idx);
+        const DpSeg g = a.segs[si];
+        const uint32_t orient = (g.flags >> kSegOrientShift) & 1u;
+        const uint8_t *sb = a.scode + a.soff[g.subj];
+        const int32_t Ls = int32_t(a.slen[g.subj]);
+        const uint8_t *qb = a.qcode + a.qoff[g.query];
+        const SegView v = make_view(sb, Ls, int32_t(orient), qb, g.s0, g.s1, g.q0, g.q1,
+                                    g.flags & 3u, g.band);
+        if (AFFINE) {
+            dp_fill_affine<kStripW>(v, sc);
+        } else {
+            dp_fill_global<kStripW>(v, sc);
+        }
+        OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
+        DpSum sum;
+        dp_traceback<kStripW>(v, sc, w, sum);
+        w.flush();
+        a.sums[si] = sum;
+        if (a.cells) {
+            const uint64_t cl = band_cells(v.R, v.C, v.band);
+            a.cells[si] = uint32_t(cl > 0xffffffffull ? 0xffffffffull : cl);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// records: AlignmentRecord scoring with getAlignment2's early exits
+// ---------------------------------------------------------------------------
+struct AsmVisitor {
+    const DpSum *sums;
+    const uint32_t *cells;
+    RecState st;
+    uint32_t used = 0;
+    unsigned long long cells_used = 0;
+    bool built = false;
+    HERO_HD void begin(int64_t, int64_t, int64_t) { built = true; }
+    HERO_HD void position(int64_t) {}
+    HERO_HD void run(uint8_t t, int64_t c) { st.add(t, c); }
+    HERO_HD void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
+        st.add_piece(sums[used]);
+        if (cells) cells_used += cells[used];
+        used++;
+    }
+    HERO_HD bool check(int64_t m, int64_t i) { return st.good_counts(m, i); }
+    HERO_HD void finish() {}
+};
+
+struct KeyAt {
+    const uint32_t *k;
+    HERO_HD uint64_t operator()(int32_t i) const { return hit_pack(0, k[i] >> 16, k[i] & 0xffffu); }
+};
+
+__global__ void k_assemble(Params p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
+                           ReadsView subj, ReadsView q, const DpSum *sums, const uint32_t *cells,
+                           unsigned long long *counters) {
+    unsigned long long built = 0, acc = 0, used = 0, ncells = 0;
+    for (uint64_t ci = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; ci < nc;
+         ci += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t s = ch.subj[ci], qid = ch.query[ci];
+        AsmVisitor v;
+        v.sums = sums + ch.seg_off[ci];
+        v.cells = cells ? cells + ch.seg_off[ci] : nullptr;
+        KeyAt ka{keys + ch.key_off[ci]};
+        const bool ok = walk_chain(p, int64_t(q.len[qid]), int64_t(subj.len[s]), ka,
+                                   int32_t(ch.nkeys[ci]), v);
+        uint8_t status = CH_NONE;
+        double rate = 0, len = 0;
+        if (v.built) {
+            built++;
+            status = CH_REJECTED;
+            if (ok && v.st.good_rates(p, rate, len)) {
+                status = CH_ACCEPTED;
+                acc++;
+            }
+        }
+        ch.status[ci] = status;
+        ch.rate[ci] = rate;
+        ch.len[ci] = len;
+        used += v.used;
+        ncells += v.cells_used;
+    }
+    built = warp_sum(built);
+    acc = warp_sum(acc);
+    used = warp_sum(used);
+    ncells = warp_sum(ncells);
+    if (lane_id() == 0) {
+        atomicAdd(&counters[C_BUILT], built);
+        atomicAdd(&counters[C_ACCEPTED], acc);
+        atomicAdd(&counters[C_DP_REF], used);
+        atomicAdd(&counters[C_CELLS], ncells);
+    }
+}
+
+// SubjectRead::addAlignment (SubjectRead.cpp:25-79): one record per (subject,
+// query); forward chains arrive before reverse-complement chains.
+__global__ void k_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
+                         const uint32_t *seg_chain_count, ChainArrays ch,
+                         unsigned long long *counters) {
+    unsigned long long kept = 0;
+    for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nsub;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t i = seg_chain_start[2 * s], ie = i + seg_chain_count[2 * s];
+        uint32_t j = seg_chain_start[2 * s + 1], je = j + seg_chain_count[2 * s + 1];
+        while (i < ie || j < je) {
+            const uint32_t qi = i < ie ? ch.query[i] : 0xffffffffu;
+            const uint32_t qj = j < je ? ch.query[j] : 0xffffffffu;
+            const uint32_t qq = qi < qj ? qi : qj;
+            int64_t best = -1;
+            auto consider = [&](uint32_t c) {
+                if (ch.status[c] != CH_ACCEPTED) return;
+                if (best < 0 || record_better(ch.rate[c], ch.len[c], ch.rate[best], ch.len[best]))
+                    best = c;
+            };
+            while (i < ie && ch.query[i] == qq) consider(i++);
+            while (j < je && ch.query[j] == qq) consider(j++);
+            if (best >= 0) {
+                ch.win[best] = 1;
+                kept++;
+            }
+        }
+    }
+    kept = warp_sum(kept);
+    if (lane_id() == 0) atomicAdd(&counters[C_KEPT], kept);
+}
+
+// SubjectRead::updateQueryCoverage (SubjectRead.cpp:208-330): M votes the
+// query's own base, a mismatch votes the subject base, I/D only move.
+struct VoteVisitor {
+    const uint8_t *sc;  // subject codes (forward)
+    int32_t Ls, orient;
+    const uint8_t *qc;  // query codes
+    int32_t Lq;
+    uint32_t *cov;      // query's rows of the vote matrix
+    const uint32_t *ops;
+    uint32_t stride;
+    const DpSum *sums;
+    uint32_t seg;       // segment index of the next DP piece
+    int64_t ps = 0, pq = 0;
+    unsigned long long anomalies = 0;
+
+    __device__ __forceinline__ uint8_t subj_code(int64_t i) const {
+        return orient ? uint8_t(sc[Ls - 1 - i] ^ 2u) : sc[i];
+    }
+    __device__ __forceinline__ void vote(int64_t pos, uint8_t code) {
+        if (pos < 0 || pos >= Lq || code >= 4) {
+            anomalies++;
+            return;
+        }
+        atomicAdd(&cov[pos * 4 + code], 1u);
+    }
+    __device__ __forceinline__ void one(uint8_t t) {
+        if (t == OP_I) {
+            pq++;
+        } else if (t == OP_D) {
+            ps++;
+        } else if (t == OP_M) {
+            vote(pq, pq < Lq ? qc[pq] : uint8_t(kBad));
+            pq++;
+            ps++;
+        } else {
+            vote(pq, (ps >= 0 && ps < Ls) ? subj_code(ps) : uint8_t(kBad));
+            pq++;
+            ps++;
+        }
+    }
+    __device__ void begin(int64_t, int64_t, int64_t) {}
+    __device__ void position(int64_t p) {
+        ps = p;
+        pq = 0;
+    }
+    __device__ void run(uint8_t t, int64_t c) {
+        if (t == OP_I) {
+            pq += c;
+        } else if (t == OP_D) {
+            ps += c;
+        } else {
+            for (int64_t x = 0; x < c; x++) one(t);
+        }
+    }
+    __device__ void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
+        const DpSum s = sums[seg];
+        const uint32_t P = uint32_t(s.tot[0]) + s.tot[1] + s.tot[2] + s.tot[3];
+        const uint32_t *w = ops + uint64_t(seg) * stride;
+        const uint32_t first = stride * 16u - P;
+        for (uint32_t t = 0; t < P; t++) {
+            const uint32_t pos = first + t;
+            one(uint8_t((w[pos >> 4] >> (2 * (pos & 15))) & 3u));
+        }
+        seg++;
+    }
+    __device__ bool check(int64_t, int64_t) { return true; }
+    __device__ void finish() {}
+};
+
+__global__ void k_vote(Params p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
+                       ReadsView subj, ReadsView q, const uint32_t *ops, uint32_t stride,
+                       const DpSum *sums, uint32_t *cov, unsigned long long *counters) {
+    unsigned long long anomalies = 0;
+    for (uint64_t ci = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; ci < nc;
+         ci += uint64_t(gridDim.x) * blockDim.x) {
+        if (!ch.win[ci]) continue;
+        const uint32_t s = ch.subj[ci], qid = ch.query[ci];
+        VoteVisitor v;
+        v.sc = subj.code + subj.off[s];
+        v.Ls = int32_t(subj.len[s]);
+        v.orient = ch.orient[ci];
+        v.qc = q.code + q.off[qid];
+        v.Lq = int32_t(q.len[qid]);
+        v.cov = cov + q.off[qid] * 4;
+        v.ops = ops;
+        v.stride = stride;
+        v.sums = sums;
+        v.seg = ch.seg_off[ci];
+        KeyAt ka{keys + ch.key_off[ci]};
+        walk_chain(p, v.Lq, v.Ls, ka, int32_t(ch.nkeys[ci]), v);
+        anomalies += v.anomalies;
+    }
+    anomalies = warp_sum(anomalies);
+    if (lane_id() == 0 && anomalies) atomicAdd(&counters[C_ANOMALY], anomalies);
+}
+
+// ---------------------------------------------------------------------------
+// consensus: QueryRead::callConsensus + calculateCoverageStatistic
+// (QueryRead.cpp:148-212); one warp per query read
+// ---------------------------------------------------------------------------
+__global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, uint8_t *out,
+                            uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
+                            double *mis) {
+    const uint32_t lane = lane_id();
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t r = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < q.n;
+         r += warps) {
+        if (!q.good[r]) {
+            if (lane == 0) {
+                imin[r] = 0;
+                imed[r] = 0;
+                imax[r] = 0;
+                mis[r] = 0;
+            }
+            continue;
+        }
+        const uint64_t b = q.off[r];
+        const uint32_t L = q.len[r];
+        uint32_t changed = 0, mn = 0xffffffffu, mx = 0;
+        for (uint32_t i = lane; i < L; i += 32) {
+            const uint8_t own = q.code[b + i];
+            uint32_t c[4];
+            for (int j = 0; j < 4; j++) c[j] = cov[(b + i) * 4 + j] + (own == j ? 1u : 0u);
+            const int32_t id = column_consensus(c, p.thr);
+            uint8_t nb = own;
+            if (id >= 0) {
+                if (uint8_t(id) != own) changed++;
+                nb = uint8_t(id);
+            }
+            out[b + i] = uint8_t(code_base(nb));
+            const uint32_t sm = c[0] + c[1] + c[2] + c[3];
+            colsum[b + i] = sm;
+            mn = sm < mn ? sm : mn;
+            mx = sm > mx ? sm : mx;
+        }
+        changed = warp_sum(changed);
+        mn = warp_min(mn);
+        mx = warp_max(mx);
+        __syncwarp();
+        // median of the column sums by rank counting (QueryRead.cpp:204-211)
+        const uint32_t p_hi = L / 2, p_lo = (L % 2 == 0) ? L / 2 - 1 : (L - 1) / 2;
+        uint32_t v_hi = 0, v_lo = 0;
+        bool f_hi = false, f_lo = false;
+        for (uint32_t i = lane; i < L; i += 32) {
+            const uint32_t x = colsum[b + i];
+            uint32_t lt = 0, le = 0;
+            for (uint32_t j = 0; j < L; j++) {
+                const uint32_t y = colsum[b + j];
+                lt += y < x;
+                le += y <= x;
+            }
+            if (lt <= p_hi && p_hi < le) {
+                v_hi = x;
+                f_hi = true;
+            }
+            if (lt <= p_lo && p_lo < le) {
+                v_lo = x;
+                f_lo = true;
+            }
+        }
+        const uint32_t m_hi = __ballot_sync(0xffffffffu, f_hi), m_lo = __ballot_sync(0xffffffffu, f_lo);
+        v_hi = __shfl_sync(0xffffffffu, v_hi, __ffs(m_hi) - 1);
+        v_lo = __shfl_sync(0xffffffffu, v_lo, __ffs(m_lo) - 1);
+        if (lane == 0) {
+            imin[r] = mn;
+            imax[r] = mx;
+            imed[r] = (L % 2 == 0) ? (v_hi + v_lo) / 2u : v_lo;
+            mis[r] = __ddiv_rn(double(changed), double(L));
+        }
+    }
+}
+
+__global__ void k_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
+                             const uint64_t *out_off, uint8_t *out, int32_t *nops) {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nd;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        const DpSum s = sums[i];
+        const uint32_t P = uint32_t(s.tot[0]) + s.tot[1] + s.tot[2] + s.tot[3];
+        const uint32_t *w = ops + i * stride;
+        const uint32_t first = stride * 16u - P;
+        const uint64_t cap = out_off[i + 1] - out_off[i];
+        for (uint32_t t = 0; t < P && t < cap; t++) {
+            const uint32_t pos = first + t;
+            out[out_off[i] + t] = uint8_t((w[pos >> 4] >> (2 * (pos & 15))) & 3u);
+        }
+        nops[i] = int32_t(P);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_prep_reads(const uint8_t *raw, uint64_t nbases, uint8_t *code, const uint64_t *off,
+                       uint64_t n, uint32_t *len, uint8_t *good_query, uint8_t *good_subject,
+                       double *gc, int32_t l, cudaStream_t st) {
+    if (nbases) k_codes<<<grid_1d(nbases, 256), 256, 0, st>>>(raw, nbases, code);
+    if (n) k_read_flags<<<grid_1d(n, 128), 128, 0, st>>>(code, off, n, len, good_query, good_subject, gc, l);
+}
+
+size_t scan_tmp_bytes(uint64_t n) { return scan_levels_bytes(n); }
+
+void launch_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, void *tmp, cudaStream_t st) {
+    scan_rec<uint32_t>(in, out, n, reinterpret_cast<uint64_t *>(tmp), st);
+}
+
+void launch_key_count(ReadsView q, int32_t k, uint32_t *count, cudaStream_t st) {
+    if (q.n) k_key_count<<<grid_1d(q.n, 256), 256, 0, st>>>(q, k, count);
+}
+void launch_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint64_t *klo,
+                     uint64_t *khi, uint64_t *kval, cudaStream_t st) {
+    if (q.n) k_key_emit<<<grid_1d(q.n, 128), 128, 0, st>>>(q, k, key_off, klo, khi, kval);
+}
+void launch_table_insert(const uint64_t *klo, const uint64_t *khi, uint64_t nkeys,
+                         uint32_t *owner, uint32_t *count, uint32_t *slot_of, uint64_t mask,
+                         cudaStream_t st) {
+    if (nkeys) k_table_insert<<<grid_1d(nkeys, 256), 256, 0, st>>>(klo, khi, nkeys, owner, count, slot_of, mask);
+}
+void launch_table_fill(const uint64_t *kval, uint64_t nkeys, const uint32_t *slot_of,
+                       const uint64_t *start, uint32_t *fill, uint64_t *vals, cudaStream_t st) {
+    if (nkeys) k_table_fill<<<grid_1d(nkeys, 256), 256, 0, st>>>(kval, nkeys, slot_of, start, fill, vals);
+}
+void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint32_t *owner,
+                           const uint32_t *count, const uint64_t *start, uint64_t nslots,
+                           Slot *slots, cudaStream_t st) {
+    k_table_finalize<<<grid_1d(nslots, 256), 256, 0, st>>>(klo, khi, owner, count, start, nslots, slots);
+}
+
+void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
+                  uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
+                  unsigned long long *counters, cudaStream_t st) {
+    if (!nsub) return;
+    const unsigned g = grid_1d(nsub, kProbeWarps, 148u * 16u);
+    if (emit) {
+        k_probe<true><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, seg_hits, hit_off, hits, counters);
+    } else {
+        k_probe<false><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, seg_hits, hit_off, hits, counters);
+    }
+}
+
+void launch_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits, cudaStream_t st) {
+    if (!nseg) return;
+    const unsigned g = unsigned(nseg < 148u * 16u ? nseg : 148u * 16u);
+    k_sort_hits<<<g, kSortThreads, 0, st>>>(nseg, hit_off, hits);
+}
+
+void launch_chain(const Params &p, uint64_t nseg, ReadsView subj, ReadsView q,
+                  const uint64_t *hit_off, const uint64_t *hits, ChainScratch sc,
+                  uint32_t *seg_chain_start, uint32_t *seg_chain_count, ChainArrays ch,
+                  uint32_t *keys, DpSeg *segs, uint64_t cap_chains, uint64_t cap_keys,
+                  uint64_t cap_segs, unsigned long long *counters, cudaStream_t st) {
+    if (!nseg) return;
+    k_chain<<<grid_1d(nseg, 8, 148u * 16u), 256, 0, st>>>(p, nseg, subj, q, hit_off, hits, sc,
+                                                        seg_chain_start, seg_chain_count, ch, keys,
+                                                        segs, cap_chains, cap_keys, cap_segs,
+                                                        counters);
+}
+
+void launch_dp_sort(const DpSeg *segs, uint64_t nd, uint32_t *bins, uint32_t *perm,
+                    uint64_t *bin_off, void *scan_tmp, cudaStream_t st) {
+    cudaMemsetAsync(bins, 0, sizeof(uint32_t) * kDpBins, st);
+    if (!nd) return;
+    k_dp_hist<<<grid_1d(nd, 256), 256, 0, st>>>(segs, nd, bins);
+    launch_scan_u32(bins, bin_off, kDpBins, scan_tmp, st);
+    cudaMemsetAsync(bins, 0, sizeof(uint32_t) * kDpBins, st);
+    k_dp_scatter<<<grid_1d(nd, 256), 256, 0, st>>>(segs, nd, bins, bin_off, perm);
+}
+
+uint64_t dp_threads(int device) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return uint64_t(sms) * 8u * kDpThreads;
+}
+
+void launch_dp(const DpLaunch &a, cudaStream_t st) {
+    if (!a.nd) return;
+    const unsigned g = unsigned(a.threads / kDpThreads);
+    if (a.affine) {
+        k_dp<true><<<g, kDpThreads, 0, st>>>(a);
+    } else {
+        k_dp<false><<<g, kDpThreads, 0, st>>>(a);
+    }
+}
+
+void launch_assemble(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
+                     ReadsView subj, ReadsView q, const DpSum *sums, const uint32_t *cells,
+                     unsigned long long *counters, cudaStream_t st) {
+    if (nc) k_assemble<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, sums, cells, counters);
+}
+
+void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
+                   const uint32_t *seg_chain_count, ChainArrays ch, unsigned long long *counters,
+                   cudaStream_t st) {
+    if (nsub) k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch, counters);
+}
+
+void launch_vote(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
+                 ReadsView subj, ReadsView q, const DpSeg *, const uint32_t *ops,
+                 uint32_t stride, const DpSum *sums, uint32_t *cov, unsigned long long *counters,
+                 cudaStream_t st) {
+    if (nc) k_vote<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, ops, stride, sums, cov, counters);
+}
+
+void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, uint8_t *out,
+                      uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
+                      double *mis, cudaStream_t st) {
+    if (q.n) k_consensus<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(p, q, cov, out, colsum, imin, imed, imax, mis);
+}
+
+void launch_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
+                       const uint64_t *out_off, uint8_t *out, int32_t *nops, cudaStream_t st) {
+    if (nd) k_unpack_ops<<<grid_1d(nd, 128), 128, 0, st>>>(ops, stride, sums, nd, out_off, out, nops);
+}
+
+}  // namespace hero

@@ -1,0 +1,133 @@
+/*
+ * hero_gpu.h -- C ABI of the B200 read-correction path (HERO consensus mode).
+ *
+ * The reference (guo-xuan/Hero) has no plugin or FFI layer: its hot path is a
+ * set of C++ classes driven from main.cpp.  These entry points replace the
+ * calls main.cpp makes on those classes, one for one:
+ *
+ *   hero_create           Config statics read by the aligner
+ *                         (Config.h:88-145; SubjectReadAligner.cpp:10-22)
+ *   hero_set_queries      QueryDataset::buildDataset / loadDatasetParallel
+ *                         (QueryDataset.cpp:89-244; main.cpp:36-50) -- reads
+ *                         already parsed on the host, uploaded once
+ *   hero_build_index      HashTableMethod::createHashTables + insertQueryDataset
+ *                         (HashTableLongKey.cpp:41-68, 250-306; main.cpp:60-66)
+ *   hero_align_subjects   SubjectReadAligner::start over one chunk of subject
+ *                         reads (SubjectReadAligner.cpp:493-645); votes accumulate
+ *   hero_align_self       the same with the query set as the subject set (HERO is
+ *                         run with -q X -s X for correction)
+ *   hero_consensus        QueryDataset::callConsensus (QueryDataset.cpp:393-412)
+ *                         plus the fields QueryDataset::writeQueryOut prints
+ *                         (QueryDataset.cpp:414-537)
+ *   hero_get_stats        the per-phase timers the reference prints
+ *                         (SubjectReadAligner.cpp:635-640) and work counters
+ *
+ * Conventions: plain pointers and sizes only; host buffers belong to the
+ * caller and are only read during the call.  Every call returns 0 or a
+ * negative HERO_E_* code; hero_last_error() gives the message.  A context is
+ * bound to one CUDA device and one stream and is not re-entrant.
+ */
+#ifndef HERO_GPU_H_
+#define HERO_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HERO_OK 0
+#define HERO_E_INPUT (-1)   /* bad argument or read set */
+#define HERO_E_OOM (-2)     /* device memory budget exceeded */
+#define HERO_E_CUDA (-3)    /* CUDA runtime error */
+#define HERO_E_STATE (-4)   /* call out of order (e.g. align before index) */
+#define HERO_E_TIMEOUT (-5) /* a bounded device wait gave up */
+
+#define HERO_ALIGNER_AFFINE 0 /* BandAligner::IAFFINE, flag -a a */
+#define HERO_ALIGNER_GLOBAL 1 /* BandAligner::IGLOBAL, default */
+
+typedef struct hero_ctx hero_ctx;
+
+typedef struct {
+    int32_t k;              /* k-mer length, 1..63 (Config::iKmer, -k; default 39) */
+    int32_t min_overlap;    /* Config::minimumOverlapLength, -l (default 40) */
+    int32_t aligner;        /* HERO_ALIGNER_GLOBAL or HERO_ALIGNER_AFFINE (-a) */
+    int32_t device;         /* CUDA device ordinal */
+    double max_mismatch_rate; /* Config::dMaxMismatchRate = atof(-m)/100 (default 1) */
+    double max_indel_rate;    /* Config::dMaxIndelRate = atof(-i)/100 (default 1) */
+    double consensus_threshold; /* Config::dMinFrequencyCallConsensus, -c (default 0.6) */
+    uint64_t device_memory_budget; /* bytes this context may hold; 0 = no limit */
+    uint32_t subject_batch; /* subject reads per device batch; 0 = default */
+    uint32_t flags;         /* reserved, 0 */
+    void *stream;           /* cudaStream_t to run on; NULL = a private stream */
+} hero_params;
+
+typedef struct {
+    uint64_t queries, good_queries, index_keys, index_slots;
+    uint64_t subjects, probes, hits, chains, chains_kept;
+    uint64_t records_built, records_accepted, records_kept;
+    uint64_t dp_segments;      /* DP segments computed on the device */
+    uint64_t dp_segments_ref;  /* of those, the ones the reference would compute */
+    uint64_t dp_cells;         /* band cells of the reference's loop bounds, ref segments */
+    uint64_t vote_anomalies;   /* votes outside a read (reference: undefined behaviour) */
+    uint64_t device_bytes_peak;
+    double ms_upload, ms_index, ms_seed, ms_chain, ms_dp, ms_record, ms_vote, ms_consensus;
+    double ms_dp_kernel;       /* device time of the DP kernels alone */
+} hero_stats;
+
+/* Returns the default parameters of the reference's Config. */
+void hero_default_params(hero_params *p);
+
+int hero_create(const hero_params *p, hero_ctx **out);
+void hero_destroy(hero_ctx *ctx);
+const char *hero_last_error(const hero_ctx *ctx);
+
+/* Query reads: seq holds the concatenated bases (uppercase ASCII, as
+ * QueryDataset stores them after toupper), read i is seq[off[i]..off[i+1]);
+ * uid[i] = atoi(read name).  Replaces any previous query set and resets votes. */
+int hero_set_queries(hero_ctx *ctx, const uint8_t *seq, const uint64_t *off, const int64_t *uid,
+                     uint64_t n);
+
+int hero_build_index(hero_ctx *ctx);
+
+/* One chunk of subject reads (same layout).  May be called repeatedly; the
+ * votes of every chunk accumulate, as SubjectReadAligner::start streams chunks. */
+int hero_align_subjects(hero_ctx *ctx, const uint8_t *seq, const uint64_t *off,
+                        const int64_t *uid, uint64_t n);
+
+/* The query set itself as the subject set, without a second upload. */
+int hero_align_self(hero_ctx *ctx);
+
+/* Consensus over the accumulated votes.  seq_out has the query layout; bases of
+ * reads that are not good are left untouched (the reference leaves them as
+ * read).  Any output pointer may be NULL.  good_out[i] = 1 for a good read. */
+int hero_consensus(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *imed,
+                   uint32_t *imax, double *mismatch_rate, double *gc_content,
+                   uint8_t *good_out);
+
+/* Vote matrix before the self vote: uint32 [total query bases][4] (A,C,T,G). */
+int hero_get_votes(hero_ctx *ctx, uint32_t *cov);
+
+int hero_get_stats(hero_ctx *ctx, hero_stats *out);
+
+/* Aligns an explicit list of DP segments on the device (test and tooling entry
+ * point).  subj/query: concatenated reads (same layout as above); per segment
+ * the subject read index, its orientation (0 forward, 1 reverse complement),
+ * the query read index, half-open ranges [s0,s1) and [q0,q1), flags (1 = align
+ * right, 2 = align left) and the band the aligner holds before the call.
+ * Outputs: ops (per-step codes 0=M 1=X 2=I 3=D, first to last) written at
+ * ops_off[i] (caller sizes ops_off[i+1]-ops_off[i] >= (s1-s0)+(q1-q0)); nops[i]
+ * receives the path length. */
+int hero_align_segments(hero_ctx *ctx, int affine, const uint8_t *subj, const uint64_t *subj_off,
+                        uint64_t n_subj, const uint8_t *query, const uint64_t *query_off,
+                        uint64_t n_query, uint64_t n_seg, const uint32_t *seg_subject,
+                        const uint8_t *seg_orient, const uint32_t *seg_query,
+                        const int32_t *s0, const int32_t *s1, const int32_t *q0,
+                        const int32_t *q1, const uint8_t *seg_flags, const int64_t *band,
+                        const uint64_t *ops_off, uint8_t *ops, int32_t *nops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,404 @@
+// core_emu.cpp -- TEST HARNESS ONLY.
+//
+// Compiles the device-side item logic (hero_b200/csrc/hero_core.cuh) with the
+// host compiler and drives it through a plain sequential loop, so the per-item
+// code (DP strips + traceback, chaining, record scoring, dedupe, votes,
+// consensus) can be checked against the oracle on a machine without a GPU.
+// It is never part of the product: the library has no CPU path.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "../../hero_b200/csrc/hero_core.cuh"
+
+using namespace hero;
+
+namespace {
+
+template <int W>
+struct HostScratch {
+    int32_t R = 0, C = 0;
+    std::vector<uint32_t> tbv;
+    std::vector<int32_t> bv;
+    void reset(int32_t r, int32_t c) {
+        R = r;
+        C = c;
+        const int32_t nst = (c + W - 1) / W;
+        tbv.assign(size_t(nst) * size_t(r + 1), 0xdeadbeefu);
+        bv.assign(size_t(3) * size_t(r + 1), 0x7f7f7f7f);
+    }
+    void tb_set(int32_t s, int32_t i, uint32_t bits) { tbv[size_t(s) * (R + 1) + i] = bits; }
+    uint32_t tb_get(int32_t s, int32_t i) const { return tbv[size_t(s) * (R + 1) + i]; }
+    int32_t &b(int32_t st, int32_t i) { return bv[size_t(st) * (R + 1) + i]; }
+};
+
+template <int W>
+int run_dp(const SegView &v, bool affine, std::vector<uint8_t> &ops, DpSum &sum) {
+    HostScratch<W> sc;
+    sc.reset(v.R, v.C);
+    if (affine) {
+        dp_fill_affine<W>(v, sc);
+    } else {
+        dp_fill_global<W>(v, sc);
+    }
+    std::vector<uint8_t> rev;
+    auto emit = [&](uint8_t op) { rev.push_back(op); };
+    int n = dp_traceback<W>(v, sc, emit, sum);
+    ops.assign(rev.rbegin(), rev.rend());
+    return n;
+}
+
+struct Reads {
+    std::vector<uint8_t> code;
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> len;
+    std::vector<int64_t> uid;
+    std::vector<uint8_t> gq, gs;
+    std::vector<double> gc;
+};
+
+void load(Reads &r, uint64_t n, const uint8_t *seq, const uint64_t *off, const int64_t *uid,
+          int32_t l) {
+    r.off.assign(off, off + n + 1);
+    r.uid.assign(uid, uid + n);
+    r.code.resize(off[n]);
+    for (uint64_t i = 0; i < off[n]; i++) r.code[i] = base_code(seq[i]);
+    r.len.resize(n);
+    r.gq.resize(n);
+    r.gs.resize(n);
+    r.gc.resize(n);
+    for (uint64_t i = 0; i < n; i++) {
+        const uint64_t L = off[i + 1] - off[i];
+        uint64_t cnt[4] = {0, 0, 0, 0}, ngc = 0;
+        bool valid = true;
+        for (uint64_t j = 0; j < L; j++) {
+            uint8_t c = r.code[off[i] + j];
+            if (c >= 4) {
+                valid = false;
+            } else {
+                cnt[c]++;
+                ngc += c & 1;
+            }
+        }
+        bool qf = valid;
+        const uint64_t thr = uint64_t(double(L) * 0.8);
+        if (qf && (cnt[0] >= thr || cnt[1] >= thr || cnt[2] >= thr || cnt[3] >= thr)) qf = false;
+        const uint64_t lu = uint16_t(l);
+        r.len[i] = uint32_t(L);
+        r.gq[i] = (L > lu && qf) ? 1 : 0;
+        r.gs[i] = (L < lu || qf) ? 1 : 0;
+        r.gc[i] = double(ngc) / double(L);
+    }
+}
+
+struct KeyHash {
+    size_t operator()(const std::pair<uint64_t, uint64_t> &k) const {
+        return size_t(kmer_hash(Kmer{k.first, k.second}));
+    }
+};
+
+struct SegRec {
+    int64_t s0, s1, q0, q1, band;
+    uint32_t flags;
+    std::vector<uint8_t> ops;
+    DpSum sum;
+};
+
+struct Collect {
+    std::vector<SegRec> *out;
+    uint32_t n = 0;
+    void begin(int64_t, int64_t, int64_t) {}
+    void position(int64_t) {}
+    void run(uint8_t, int64_t) {}
+    void dp(int64_t s0, int64_t s1, int64_t q0, int64_t q1, uint32_t f, int64_t band) {
+        SegRec r;
+        r.s0 = s0;
+        r.s1 = s1;
+        r.q0 = q0;
+        r.q1 = q1;
+        r.flags = f;
+        r.band = band > 65535 ? 65535 : band;
+        out->push_back(r);
+        n++;
+    }
+    bool check(int64_t, int64_t) { return true; }
+    void finish() {}
+};
+
+struct Asm {
+    const SegRec *segs;
+    RecState st;
+    uint32_t used = 0;
+    bool built = false;
+    void begin(int64_t, int64_t, int64_t) { built = true; }
+    void position(int64_t) {}
+    void run(uint8_t t, int64_t c) { st.add(t, c); }
+    void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) { st.add_piece(segs[used++].sum); }
+    bool check(int64_t m, int64_t i) { return st.good_counts(m, i); }
+    void finish() {}
+};
+
+struct Vote {
+    const uint8_t *sc;
+    int64_t Ls;
+    int orient;
+    const uint8_t *qc;
+    int64_t Lq;
+    uint32_t *cov;
+    const SegRec *segs;
+    uint32_t used = 0;
+    int64_t ps = 0, pq = 0;
+    uint64_t anomalies = 0;
+    uint8_t sub(int64_t i) const { return orient ? uint8_t(sc[Ls - 1 - i] ^ 2) : sc[i]; }
+    void vote(int64_t pos, uint8_t code) {
+        if (pos < 0 || pos >= Lq || code >= 4) {
+            anomalies++;
+            return;
+        }
+        cov[pos * 4 + code]++;
+    }
+    void one(uint8_t t) {
+        if (t == OP_I) {
+            pq++;
+        } else if (t == OP_D) {
+            ps++;
+        } else if (t == OP_M) {
+            vote(pq, pq < Lq ? qc[pq] : kBad);
+            pq++;
+            ps++;
+        } else {
+            vote(pq, (ps >= 0 && ps < Ls) ? sub(ps) : kBad);
+            pq++;
+            ps++;
+        }
+    }
+    void begin(int64_t, int64_t, int64_t) {}
+    void position(int64_t p) {
+        ps = p;
+        pq = 0;
+    }
+    void run(uint8_t t, int64_t c) {
+        if (t == OP_I) {
+            pq += c;
+        } else if (t == OP_D) {
+            ps += c;
+        } else {
+            for (int64_t x = 0; x < c; x++) one(t);
+        }
+    }
+    void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
+        for (uint8_t op : segs[used].ops) one(op);
+        used++;
+    }
+    bool check(int64_t, int64_t) { return true; }
+    void finish() {}
+};
+
+}  // namespace
+
+extern "C" {
+
+// one DP segment through the core strip DP; same argument meaning as
+// hero_oracle_align (segments given directly, orientation forward)
+int emu_align(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query, int32_t lq,
+              int64_t band, int align_right, int align_left, int strip16, uint8_t *ops,
+              int32_t cap) {
+    std::vector<uint8_t> sc(ls), qc(lq);
+    for (int i = 0; i < ls; i++) sc[i] = base_code(subj[i]);
+    for (int i = 0; i < lq; i++) qc[i] = base_code(query[i]);
+    uint32_t flags = (align_right ? DPF_RIGHT : 0) | (align_left ? DPF_LEFT : 0);
+    SegView v = make_view(sc.data(), ls, 0, qc.data(), 0, ls, 0, lq, flags, band);
+    std::vector<uint8_t> out;
+    DpSum sum;
+    int n = strip16 ? run_dp<16>(v, affine != 0, out, sum) : run_dp<8>(v, affine != 0, out, sum);
+    if (n > cap) return -1;
+    std::memcpy(ops, out.data(), out.size());
+    return n;
+}
+
+// whole path, sequentially, through the core item functions
+int emu_correct(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate,
+                double thr, uint64_t nq, const uint8_t *qseq, const uint64_t *qoff,
+                const int64_t *quid, uint8_t *out_seq, uint32_t *imin, uint32_t *imed,
+                uint32_t *imax, double *mis, double *gc, uint32_t *cov_out, uint64_t *counters) {
+    Params p{k, l, affine, 0, mis_rate, indel_rate, thr};
+    Reads Q;
+    load(Q, nq, qseq, qoff, quid, l);
+    // table: exact multimap
+    std::unordered_map<std::pair<uint64_t, uint64_t>, std::vector<uint64_t>, KeyHash> table;
+    for (uint64_t r = 0; r < nq; r++) {
+        if (!Q.gq[r]) continue;
+        const int64_t L = Q.len[r];
+        const int32_t nk = query_key_count(L, k);
+        for (int32_t i = 0; i < nk; i++) {
+            const int64_t pos = query_key_pos(L, k, i);
+            Kmer m{0, 0};
+            for (int32_t t = 0; t < k; t++) kmer_push(m, Q.code[Q.off[r] + pos + t] & 3u, k);
+            table[{m.lo, m.hi}].push_back((uint64_t(r) << 32) | uint64_t(pos));
+        }
+    }
+    std::vector<uint32_t> cov(Q.code.size() * 4, 0);
+    uint64_t nhits = 0, nchains = 0, kept_total = 0, dpseg = 0, anomalies = 0;
+    for (uint64_t s = 0; s < nq; s++) {  // subject set = query set
+        if (!Q.gs[s]) continue;
+        const int32_t L = int32_t(Q.len[s]);
+        const uint8_t *c = Q.code.data() + Q.off[s];
+        std::vector<uint64_t> hits[2];
+        if (L >= k) {
+            for (int32_t f = 0; f + k <= L; f++) {
+                Kmer fm{0, 0}, rm{0, 0};
+                bool bad = false;
+                for (int32_t i = 0; i < k; i++) {
+                    bad |= c[f + i] >= 4;
+                    kmer_push(fm, c[f + i] & 3u, k);
+                }
+                if (bad) continue;
+                for (int32_t i = k - 1; i >= 0; i--) kmer_push(rm, (c[f + i] & 3u) ^ 2u, k);
+                for (int o = 0; o < 2; o++) {
+                    Kmer m = o ? rm : fm;
+                    auto it = table.find({m.lo, m.hi});
+                    if (it == table.end()) continue;
+                    for (uint64_t v : it->second) {
+                        uint32_t qq = uint32_t(v >> 32);
+                        if (Q.uid[qq] == Q.uid[s]) continue;
+                        hits[o].push_back(hit_pack(qq, uint32_t(v), o ? uint32_t(L - k - f) : uint32_t(f)));
+                    }
+                }
+            }
+        }
+        struct Cand {
+            uint32_t q;
+            int orient;
+            std::vector<SegRec> segs;
+            std::vector<uint64_t> keys;
+            int status;
+            double rate, len;
+        };
+        std::vector<Cand> cands;
+        for (int o = 0; o < 2; o++) {
+            auto &H = hits[o];
+            std::sort(H.begin(), H.end());
+            nhits += H.size();
+            size_t g0 = 0;
+            for (size_t i = 0; i < H.size(); i++) {
+                if (i + 1 != H.size() && hit_q(H[i]) == hit_q(H[i + 1])) continue;
+                const int32_t gn = int32_t(i + 1 - g0);
+                const uint64_t *G = H.data() + g0;
+                auto hit = [G](int32_t h) { return G[h]; };
+                std::vector<uint32_t> chain_of(gn);
+                std::vector<int32_t> first(gn), last(gn), prev(gn);
+                std::vector<int64_t> kl(gn);
+                int32_t nch = chain_group(p, hit, gn, chain_of.data(), first.data(), last.data());
+                int64_t best = chain_key_lengths(p, hit, gn, chain_of.data(), nch, kl.data(), prev.data());
+                nchains += nch;
+                const uint32_t qid = hit_q(G[0]);
+                for (int32_t ch = 0; ch < nch; ch++) {
+                    if (kl[ch] != best) continue;
+                    Cand cd;
+                    cd.q = qid;
+                    cd.orient = o;
+                    for (int32_t h = 0; h < gn; h++)
+                        if (chain_of[h] == uint32_t(ch)) cd.keys.push_back(G[h]);
+                    auto key = [&cd](int32_t t) { return cd.keys[t]; };
+                    Collect col{&cd.segs};
+                    walk_chain(p, Q.len[qid], L, key, int32_t(cd.keys.size()), col);
+                    for (SegRec &sr : cd.segs) {
+                        SegView v = make_view(c, L, o, Q.code.data() + Q.off[qid], int32_t(sr.s0),
+                                              int32_t(sr.s1), int32_t(sr.q0), int32_t(sr.q1),
+                                              sr.flags, sr.band);
+                        run_dp<8>(v, affine != 0, sr.ops, sr.sum);
+                        dpseg++;
+                    }
+                    Asm as;
+                    as.segs = cd.segs.data();
+                    bool ok = walk_chain(p, Q.len[qid], L, key, int32_t(cd.keys.size()), as);
+                    cd.status = 0;
+                    cd.rate = 0;
+                    cd.len = 0;
+                    if (as.built) {
+                        cd.status = 1;
+                        if (ok && as.st.good_rates(p, cd.rate, cd.len)) cd.status = 2;
+                    }
+                    cands.push_back(std::move(cd));
+                }
+                g0 = i + 1;
+            }
+        }
+        // dedupe: per query, forward chains then reverse-complement chains
+        std::vector<size_t> order(cands.size());
+        for (size_t i = 0; i < order.size(); i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t b) { return cands[a].q < cands[b].q; });
+        for (size_t a = 0; a < order.size();) {
+            size_t b = a;
+            int64_t best = -1;
+            while (b < order.size() && cands[order[b]].q == cands[order[a]].q) {
+                const Cand &x = cands[order[b]];
+                if (x.status == 2 &&
+                    (best < 0 || record_better(x.rate, x.len, cands[best].rate, cands[best].len)))
+                    best = int64_t(order[b]);
+                b++;
+            }
+            if (best >= 0) {
+                kept_total++;
+                Cand &w = cands[best];
+                Vote vt;
+                vt.sc = c;
+                vt.Ls = L;
+                vt.orient = w.orient;
+                vt.qc = Q.code.data() + Q.off[w.q];
+                vt.Lq = Q.len[w.q];
+                vt.cov = cov.data() + Q.off[w.q] * 4;
+                vt.segs = w.segs.data();
+                auto key = [&w](int32_t t) { return w.keys[t]; };
+                walk_chain(p, vt.Lq, vt.Ls, key, int32_t(w.keys.size()), vt);
+                anomalies += vt.anomalies;
+            }
+            a = b;
+        }
+    }
+    if (cov_out) std::memcpy(cov_out, cov.data(), cov.size() * 4);
+    // consensus
+    for (uint64_t r = 0; r < nq; r++) {
+        const uint64_t b = Q.off[r];
+        const uint32_t L = Q.len[r];
+        gc[r] = Q.gc[r];
+        std::memcpy(out_seq + b, qseq + b, L);
+        if (!Q.gq[r]) {
+            imin[r] = imed[r] = imax[r] = 0;
+            mis[r] = 0;
+            continue;
+        }
+        uint32_t changed = 0;
+        std::vector<uint32_t> sums(L);
+        for (uint32_t i = 0; i < L; i++) {
+            uint32_t cc[4];
+            const uint8_t own = Q.code[b + i];
+            for (int j = 0; j < 4; j++) cc[j] = cov[(b + i) * 4 + j] + (own == j ? 1 : 0);
+            int32_t id = column_consensus(cc, thr);
+            uint8_t nb = own;
+            if (id >= 0) {
+                if (uint8_t(id) != own) changed++;
+                nb = uint8_t(id);
+            }
+            out_seq[b + i] = uint8_t(code_base(nb));
+            sums[i] = cc[0] + cc[1] + cc[2] + cc[3];
+        }
+        std::sort(sums.begin(), sums.end());
+        imin[r] = sums[0];
+        imax[r] = sums.back();
+        imed[r] = (L % 2 == 0) ? (sums[L / 2] + sums[L / 2 - 1]) / 2 : sums[(L - 1) / 2];
+        mis[r] = double(changed) / double(L);
+    }
+    if (counters) {
+        counters[0] = nhits;
+        counters[1] = nchains;
+        counters[2] = kept_total;
+        counters[3] = dpseg;
+        counters[4] = anomalies;
+    }
+    return 0;
+}
+}

@@ -1,0 +1,84 @@
+"""Golden fixtures: seeded inputs and the reference flags they were run with.
+
+Each fixture's input is regenerated from its seed (hero_b200.synth); the
+reference outputs recorded by make_golden.py are stored beside this file
+(manifest.json: md5 of the FASTQ and of the reference .fasta/.info; the
+smallest outputs are also kept gzipped).  Read names are 1..N.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from hero_b200 import synth  # noqa: E402
+
+
+def _mix(seed: int = 11) -> synth.ReadSet:
+    """Mixed lengths 35..160 with N bases and lowercase reads injected (5 % each)."""
+    rs = synth.config3(seed=seed, genome_bp=15000, coverage=25, lmin=35, lmax=160)
+    rng = np.random.default_rng(seed + 1000)
+    seq = rs.seq.copy()
+    for i in range(rs.n):
+        a, b = int(rs.off[i]), int(rs.off[i + 1])
+        if rng.random() < 0.05 and b > a:
+            seq[a + int(rng.integers(b - a))] = ord("N")
+        if rng.random() < 0.05:
+            seq[a:b] = np.frombuffer(bytes(seq[a:b]).lower(), np.uint8)
+    rs.seq = seq
+    return rs
+
+
+# name -> (input generator, reference flags)
+FIXTURES = {
+    "c1_20k": (lambda: synth.config1(genome_bp=20000), []),
+    "c1_20k_affine": (lambda: synth.config1(genome_bp=20000), ["-a", "a"]),
+    "c1_20k_narrow": (lambda: synth.config1(genome_bp=20000), ["-m", "2", "-i", "1"]),
+    "c2_30k": (lambda: synth.config2(genome_bp=30000, n_repeats=4), ["-a", "a"]),
+    "c2_30k_narrow": (lambda: synth.config2(genome_bp=30000, n_repeats=4),
+                      ["-a", "a", "-m", "3", "-i", "2"]),
+    "c2_30k_k31": (lambda: synth.config2(genome_bp=30000, n_repeats=4),
+                   ["-k", "31", "-a", "a", "-c", "0.7"]),
+    "mix": (_mix, []),
+    "mix_affine": (_mix, ["-a", "a"]),
+    "mix_k21_l60": (_mix, ["-k", "21", "-l", "60"]),
+    "mix_i0": (_mix, ["-i", "0", "-m", "4"]),
+}
+
+# fixtures whose reference outputs are stored in full (gzipped)
+STORED = ("c1_20k", "mix_affine")
+
+
+def upper(rs: synth.ReadSet) -> synth.ReadSet:
+    """The reads as HERO holds them after parsing (toupper, QueryDataset.cpp:208-209)."""
+    seq = np.frombuffer(bytes(rs.seq).upper(), np.uint8).copy()
+    return synth.ReadSet(seq, rs.off, rs.names, rs.qual, dict(rs.meta))
+
+
+def params(flags: list[str]) -> dict:
+    """Reference flags -> keyword arguments of hero_b200.Hero (Config::setConfig)."""
+    p = dict(k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
+             max_indel_rate=1.0, consensus_threshold=0.6)
+    i = 0
+    while i < len(flags):
+        f = flags[i]
+        v = flags[i + 1] if i + 1 < len(flags) else None
+        if f == "-k":
+            p["k"] = int(v)
+        elif f == "-l":
+            p["min_overlap"] = int(v)
+        elif f == "-a":
+            p["aligner"] = "affine" if v == "a" else "global"
+        elif f == "-m":
+            p["max_mismatch_rate"] = float(v) / 100.0
+        elif f == "-i":
+            p["max_indel_rate"] = float(v) / 100.0
+        elif f == "-c":
+            p["consensus_threshold"] = float(v)
+        else:
+            raise ValueError(f)
+        i += 2
+    return p

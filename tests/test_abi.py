@@ -1,0 +1,40 @@
+"""The C ABI library builds for sm_100a and exports every declared entry point."""
+import os
+import re
+import subprocess
+
+from hero_b200 import EXPORTS, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    src = open(os.path.join(ROOT, "include", "hero_gpu.h")).read()
+    return sorted(set(re.findall(r"\b(hero_[a-z_]+)\s*\(", src)))
+
+
+def test_header_lists_exports():
+    assert sorted(EXPORTS) == declared()
+
+
+def test_library_exports_every_symbol():
+    lib = build.build_library()
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True,
+                         check=True).stdout
+    syms = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [s for s in declared() if s not in syms]
+    assert not missing, missing
+
+
+def test_library_loads_without_gpu():
+    from hero_b200 import load_library
+    lib = load_library()
+    for s in declared():
+        assert hasattr(lib, s)
+
+
+def test_sass_is_sm100a():
+    lib = build.build_library()
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", lib],
+                         capture_output=True, text=True).stdout
+    assert "sm_100a" in out

@@ -1,0 +1,60 @@
+"""The device item logic (hero_core.cuh), compiled for the host, against the oracle.
+
+These run without a GPU: the same source the kernels execute per thread is
+driven sequentially and must reproduce the oracle exactly."""
+import numpy as np
+import pytest
+from fixtures import FIXTURES, params, upper
+
+from hero_b200 import synth
+
+ACGT = np.frombuffer(b"ACGT", np.uint8)
+
+
+def _pairs(rng, n, lmax=70):
+    for _ in range(n):
+        ls, lq = int(rng.integers(1, lmax)), int(rng.integers(1, lmax))
+        s = ACGT[rng.integers(0, 4, ls)]
+        if rng.random() < 0.5:
+            q = synth.substitute(rng, np.resize(s[rng.integers(0, ls):], lq), 0.1)
+        else:
+            q = ACGT[rng.integers(0, 4, lq)]
+        yield bytes(s), bytes(q.astype(np.uint8))
+
+
+@pytest.mark.parametrize("affine", [0, 1])
+def test_dp_random_segments(oracle, emu, affine):
+    rng = np.random.default_rng(100 + affine)
+    for s, q in _pairs(rng, 3000):
+        band = int(rng.choice([0, 1, 2, 3, 5, 10, 200]))
+        right, left = bool(rng.integers(0, 2)), bool(rng.integers(0, 2))
+        want, _ = oracle.align(affine, s, q, band, right, left)
+        for strip16 in (False, True):
+            got = emu.align(affine, s, q, band, right, left, strip16)
+            assert np.array_equal(want, got), (affine, s, q, band, right, left, strip16)
+
+
+def test_dp_edge_shapes(oracle, emu):
+    cases = [(b"A", b"A"), (b"A", b"C"), (b"ACGT", b"A"), (b"A", b"ACGT"), (b"AAAA", b"TTTT"),
+             (b"ACGTACGTACGTACGTACGT", b"ACG"), (b"ACGTTTTTTTTT", b"ACGTTTTTTTTT")]
+    for affine in (0, 1):
+        for s, q in cases:
+            for band in (0, 1, 2, 50):
+                for right in (False, True):
+                    for left in (False, True):
+                        want, _ = oracle.align(affine, s, q, band, right, left)
+                        got = emu.align(affine, s, q, band, right, left)
+                        assert np.array_equal(want, got), (affine, s, q, band, right, left)
+
+
+@pytest.mark.parametrize("name", ["c1_20k", "c1_20k_narrow", "mix_affine", "mix_k21_l60",
+                                  "mix_i0"])
+def test_pipeline_matches_oracle(oracle, emu, name):
+    gen, flags = FIXTURES[name]
+    rs = upper(gen())
+    kw = params(flags)
+    want = oracle.correct(rs, **kw)
+    got = emu.correct(rs, **kw)
+    from hero_testlib import assert_same_consensus
+    assert_same_consensus(want, got, name)
+    assert np.array_equal(want["votes"], got["votes"])
