@@ -24,6 +24,7 @@ EXPORTS = [
     "hero_default_params", "hero_create", "hero_destroy", "hero_last_error",
     "hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
     "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments",
+    "hero_reset_votes",
 ]
 
 
@@ -41,6 +42,7 @@ _STAT_FIELDS = [
     "queries", "good_queries", "index_keys", "index_slots", "subjects", "probes", "hits",
     "chains", "chains_kept", "records_built", "records_accepted", "records_kept",
     "dp_segments", "dp_segments_ref", "dp_cells", "vote_anomalies", "device_bytes_peak",
+    "kernel_launches",
 ]
 _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record", "ms_vote",
             "ms_consensus", "ms_dp_kernel"]
@@ -75,12 +77,14 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_build_index.argtypes = [vp]
     lib.hero_align_subjects.argtypes = [vp, vp, vp, vp, C.c_uint64]
     lib.hero_align_self.argtypes = [vp]
+    lib.hero_reset_votes.argtypes = [vp]
     lib.hero_consensus.argtypes = [vp] * 8
     lib.hero_get_votes.argtypes = [vp, vp]
     lib.hero_get_stats.argtypes = [vp, C.POINTER(HeroStats)]
     lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          C.c_uint64] + [vp] * 12)
     for f in ("hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
+              "hero_reset_votes",
               "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments"):
         getattr(lib, f).restype = C.c_int
     if path is None:
@@ -166,6 +170,20 @@ class Hero:
         self.nqb = int(off[-1]) if self.nq else 0
         self._check(self.lib.hero_set_queries(self.h, _ptr(seq), _ptr(off), _ptr(uid), self.nq),
                     "set_queries")
+
+    def reset_votes(self):
+        self._check(self.lib.hero_reset_votes(self.h), "reset_votes")
+
+    def set_queries_ptr(self, seq_ptr: int, off_ptr: int, uid_ptr: int, n: int, nbases: int):
+        """Raw host pointers (e.g. pinned buffers); the caller keeps them alive."""
+        self.nq, self.nqb = n, nbases
+        self._check(self.lib.hero_set_queries(self.h, C.c_void_p(seq_ptr), C.c_void_p(off_ptr),
+                                              C.c_void_p(uid_ptr), n), "set_queries")
+
+    def consensus_ptr(self, seq=0, imin=0, imed=0, imax=0, mis=0, gc=0, good=0):
+        """Consensus into raw host pointers; 0 leaves that output on the device."""
+        v = [C.c_void_p(x) if x else None for x in (seq, imin, imed, imax, mis, gc, good)]
+        self._check(self.lib.hero_consensus(self.h, *v), "consensus")
 
     def build_index(self):
         self._check(self.lib.hero_build_index(self.h), "build_index")

@@ -18,6 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 HOST = os.path.join(HERE, "host")
 LIB = os.path.join(HERE, "libhero_b200.so")
+PEAK_LIB = os.path.join(HERE, "libhero_peak.so")
 CLI = os.path.join(HERE, "bin", "hero_b200")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -25,6 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-O3"]
 CU_SOURCES = ["hero_kernels.cu", "hero_api.cu"]
+PEAK_SOURCES = ["int_peak.cu"]
 
 
 def _run(cmd, verbose):
@@ -49,7 +51,8 @@ def _deps(folder, exts):
 
 
 def build_library(verbose: bool = False, force: bool = False) -> str:
-    deps = _deps(CSRC, (".cu", ".cuh", ".h")) + [os.path.join(ROOT, "include", "hero_gpu.h")]
+    deps = ([os.path.join(CSRC, s) for s in CU_SOURCES] + _deps(CSRC, (".cuh", ".h")) +
+            [os.path.join(ROOT, "include", "hero_gpu.h")])
     if not force and not _stale(LIB, deps):
         return LIB
     tmp = LIB + ".tmp"
@@ -57,6 +60,14 @@ def build_library(verbose: bool = False, force: bool = False) -> str:
          [os.path.join(CSRC, s) for s in CU_SOURCES], verbose)
     os.replace(tmp, LIB)
     return LIB
+
+
+def build_peak(verbose: bool = False, force: bool = False) -> str:
+    deps = [os.path.join(CSRC, s) for s in PEAK_SOURCES]
+    if not force and not _stale(PEAK_LIB, deps):
+        return PEAK_LIB
+    _run([NVCC] + ARCH + NVFLAGS + ["-shared", "-o", PEAK_LIB] + deps, verbose)
+    return PEAK_LIB
 
 
 def build_cli(verbose: bool = False, force: bool = False) -> str | None:
@@ -75,6 +86,7 @@ def build_cli(verbose: bool = False, force: bool = False) -> str | None:
 
 def build(verbose: bool = False, force: bool = False):
     build_library(verbose, force)
+    build_peak(verbose, force)
     build_cli(verbose, force)
 
 

@@ -58,6 +58,8 @@ struct hero_ctx {
         ch_win, ch_rate, ch_len;
     DBuf keys, segs, sums, cells, ops, perm, bins, bin_off, tb, bnd;
     DBuf scan_tmp, counters;
+    // index build temporaries (kept between builds)
+    DBuf x_cnt, x_koff, x_klo, x_khi, x_kval, x_owner, x_count, x_slot_of, x_start, x_fill, x_tmp;
     uint64_t dp_T = 0;
 
     hero_stats stats{};
@@ -72,7 +74,9 @@ struct hero_ctx {
                         &cs_gnch, &cs_gbest, &cs_gkept, &cs_gkeys, &cs_gdp, &ch_subj, &ch_query,
                         &ch_key_off, &ch_seg_off, &ch_nkeys, &ch_nseg, &ch_orient, &ch_status,
                         &ch_win, &ch_rate, &ch_len, &keys, &segs, &sums, &cells, &ops, &perm,
-                        &bins, &bin_off, &tb, &bnd, &scan_tmp, &counters};
+                        &bins, &bin_off, &tb, &bnd, &scan_tmp, &counters, &x_cnt, &x_koff,
+                        &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
+                        &x_fill, &x_tmp};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -291,11 +295,9 @@ extern "C" int hero_build_index(hero_ctx *c) {
     cudaEventRecord(e0, c->st);
     const uint64_t n = c->nq;
     ReadsView q = query_view(c);
-    DBuf cnt, koff, klo, khi, kval, owner, count, slot_of, start, fill, tmp;
-    auto cleanup = [&]() {
-        for (DBuf *b : {&cnt, &koff, &klo, &khi, &kval, &owner, &count, &slot_of, &start, &fill, &tmp})
-            c->release(*b);
-    };
+    DBuf &cnt = c->x_cnt, &koff = c->x_koff, &klo = c->x_klo, &khi = c->x_khi, &kval = c->x_kval,
+         &owner = c->x_owner, &count = c->x_count, &slot_of = c->x_slot_of, &start = c->x_start,
+         &fill = c->x_fill, &tmp = c->x_tmp;
     int r = HERO_OK;
     do {
         if ((r = c->ensure(cnt, n * 4 + 4, "key counts"))) break;
@@ -342,7 +344,6 @@ extern "C" int hero_build_index(hero_ctx *c) {
         c->stats.index_slots = slots;
         c->have_index = true;
     } while (0);
-    cleanup();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return r;
@@ -550,6 +551,14 @@ extern "C" int hero_consensus(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uin
     return HERO_OK;
 }
 
+extern "C" int hero_reset_votes(hero_ctx *c) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    cudaSetDevice(c->dev);
+    if (c->nqb) HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "reset votes"));
+    return c->cuda(cudaStreamSynchronize(c->st), "reset votes");
+}
+
 extern "C" int hero_get_votes(hero_ctx *c, uint32_t *cov) {
     if (!c || !cov) return HERO_E_INPUT;
     cudaSetDevice(c->dev);
@@ -570,6 +579,7 @@ extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
     s.dp_cells = c->ctr[C_CELLS];
     s.vote_anomalies = c->ctr[C_ANOMALY];
     s.device_bytes_peak = c->bytes_peak;
+    s.kernel_launches = kernel_launches();
     *out = s;
     return HERO_OK;
 }

@@ -83,6 +83,9 @@ struct ChainScratch {
     uint32_t *g_kept, *g_keys, *g_dp;
 };
 
+// kernels launched through the launchers below since the library was loaded
+uint64_t kernel_launches();
+
 // ---------------------------------------------------------------------------
 // launchers (hero_kernels.cu); all asynchronous on `st`
 // ---------------------------------------------------------------------------

@@ -14,11 +14,16 @@
 //   QueryRead::callConsensus + coverage statistics    k_consensus
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "hero_internal.cuh"
 
 namespace hero {
 
 namespace {
+
+std::atomic<uint64_t> g_launches{0};
+inline void counted() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 constexpr uint32_t kEmptyOwner = 0xffffffffu;
 
@@ -181,9 +186,11 @@ void scan_rec(const T *in, uint64_t *out, uint64_t n, uint64_t *tmp, cudaStream_
     const uint64_t nt = (n + kScanTile - 1) / kScanTile;
     uint64_t *sums = tmp;
     uint64_t *pref = tmp + (nt + 1);
+    counted();
     k_scan_tile<T><<<unsigned(nt), kScanThreads, 0, st>>>(in, n, out, sums);
     if (nt > 1) {
         scan_rec<uint64_t>(sums, pref, nt, tmp + 2 * (nt + 1), st);
+        counted();
         k_scan_add<<<unsigned(nt), kScanThreads, 0, st>>>(out, n, pref);
     }
 }
@@ -1034,35 +1041,56 @@ __global__ void k_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *
 void launch_prep_reads(const uint8_t *raw, uint64_t nbases, uint8_t *code, const uint64_t *off,
                        uint64_t n, uint32_t *len, uint8_t *good_query, uint8_t *good_subject,
                        double *gc, int32_t l, cudaStream_t st) {
-    if (nbases) k_codes<<<grid_1d(nbases, 256), 256, 0, st>>>(raw, nbases, code);
-    if (n) k_read_flags<<<grid_1d(n, 128), 128, 0, st>>>(code, off, n, len, good_query, good_subject, gc, l);
+    if (nbases) {
+        counted();
+        k_codes<<<grid_1d(nbases, 256), 256, 0, st>>>(raw, nbases, code);
+    }
+    if (n) {
+        counted();
+        k_read_flags<<<grid_1d(n, 128), 128, 0, st>>>(code, off, n, len, good_query, good_subject, gc, l);
+    }
 }
 
 size_t scan_tmp_bytes(uint64_t n) { return scan_levels_bytes(n); }
+
+uint64_t kernel_launches() { return g_launches.load(std::memory_order_relaxed); }
 
 void launch_scan_u32(const uint32_t *in, uint64_t *out, uint64_t n, void *tmp, cudaStream_t st) {
     scan_rec<uint32_t>(in, out, n, reinterpret_cast<uint64_t *>(tmp), st);
 }
 
 void launch_key_count(ReadsView q, int32_t k, uint32_t *count, cudaStream_t st) {
-    if (q.n) k_key_count<<<grid_1d(q.n, 256), 256, 0, st>>>(q, k, count);
+    if (q.n) {
+        counted();
+        k_key_count<<<grid_1d(q.n, 256), 256, 0, st>>>(q, k, count);
+    }
 }
 void launch_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint64_t *klo,
                      uint64_t *khi, uint64_t *kval, cudaStream_t st) {
-    if (q.n) k_key_emit<<<grid_1d(q.n, 128), 128, 0, st>>>(q, k, key_off, klo, khi, kval);
+    if (q.n) {
+        counted();
+        k_key_emit<<<grid_1d(q.n, 128), 128, 0, st>>>(q, k, key_off, klo, khi, kval);
+    }
 }
 void launch_table_insert(const uint64_t *klo, const uint64_t *khi, uint64_t nkeys,
                          uint32_t *owner, uint32_t *count, uint32_t *slot_of, uint64_t mask,
                          cudaStream_t st) {
-    if (nkeys) k_table_insert<<<grid_1d(nkeys, 256), 256, 0, st>>>(klo, khi, nkeys, owner, count, slot_of, mask);
+    if (nkeys) {
+        counted();
+        k_table_insert<<<grid_1d(nkeys, 256), 256, 0, st>>>(klo, khi, nkeys, owner, count, slot_of, mask);
+    }
 }
 void launch_table_fill(const uint64_t *kval, uint64_t nkeys, const uint32_t *slot_of,
                        const uint64_t *start, uint32_t *fill, uint64_t *vals, cudaStream_t st) {
-    if (nkeys) k_table_fill<<<grid_1d(nkeys, 256), 256, 0, st>>>(kval, nkeys, slot_of, start, fill, vals);
+    if (nkeys) {
+        counted();
+        k_table_fill<<<grid_1d(nkeys, 256), 256, 0, st>>>(kval, nkeys, slot_of, start, fill, vals);
+    }
 }
 void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint32_t *owner,
                            const uint32_t *count, const uint64_t *start, uint64_t nslots,
                            Slot *slots, cudaStream_t st) {
+    counted();
     k_table_finalize<<<grid_1d(nslots, 256), 256, 0, st>>>(klo, khi, owner, count, start, nslots, slots);
 }
 
@@ -1072,8 +1100,10 @@ void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableVi
     if (!nsub) return;
     const unsigned g = grid_1d(nsub, kProbeWarps, 148u * 16u);
     if (emit) {
+        counted();
         k_probe<true><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, seg_hits, hit_off, hits, counters);
     } else {
+        counted();
         k_probe<false><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, seg_hits, hit_off, hits, counters);
     }
 }
@@ -1081,6 +1111,7 @@ void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableVi
 void launch_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits, cudaStream_t st) {
     if (!nseg) return;
     const unsigned g = unsigned(nseg < 148u * 16u ? nseg : 148u * 16u);
+    counted();
     k_sort_hits<<<g, kSortThreads, 0, st>>>(nseg, hit_off, hits);
 }
 
@@ -1090,6 +1121,7 @@ void launch_chain(const Params &p, uint64_t nseg, ReadsView subj, ReadsView q,
                   uint32_t *keys, DpSeg *segs, uint64_t cap_chains, uint64_t cap_keys,
                   uint64_t cap_segs, unsigned long long *counters, cudaStream_t st) {
     if (!nseg) return;
+    counted();
     k_chain<<<grid_1d(nseg, 8, 148u * 16u), 256, 0, st>>>(p, nseg, subj, q, hit_off, hits, sc,
                                                         seg_chain_start, seg_chain_count, ch, keys,
                                                         segs, cap_chains, cap_keys, cap_segs,
@@ -1100,9 +1132,11 @@ void launch_dp_sort(const DpSeg *segs, uint64_t nd, uint32_t *bins, uint32_t *pe
                     uint64_t *bin_off, void *scan_tmp, cudaStream_t st) {
     cudaMemsetAsync(bins, 0, sizeof(uint32_t) * kDpBins, st);
     if (!nd) return;
+    counted();
     k_dp_hist<<<grid_1d(nd, 256), 256, 0, st>>>(segs, nd, bins);
     launch_scan_u32(bins, bin_off, kDpBins, scan_tmp, st);
     cudaMemsetAsync(bins, 0, sizeof(uint32_t) * kDpBins, st);
+    counted();
     k_dp_scatter<<<grid_1d(nd, 256), 256, 0, st>>>(segs, nd, bins, bin_off, perm);
 }
 
@@ -1116,8 +1150,10 @@ void launch_dp(const DpLaunch &a, cudaStream_t st) {
     if (!a.nd) return;
     const unsigned g = unsigned(a.threads / kDpThreads);
     if (a.affine) {
+        counted();
         k_dp<true><<<g, kDpThreads, 0, st>>>(a);
     } else {
+        counted();
         k_dp<false><<<g, kDpThreads, 0, st>>>(a);
     }
 }
@@ -1125,31 +1161,46 @@ void launch_dp(const DpLaunch &a, cudaStream_t st) {
 void launch_assemble(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
                      ReadsView subj, ReadsView q, const DpSum *sums, const uint32_t *cells,
                      unsigned long long *counters, cudaStream_t st) {
-    if (nc) k_assemble<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, sums, cells, counters);
+    if (nc) {
+        counted();
+        k_assemble<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, sums, cells, counters);
+    }
 }
 
 void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
                    const uint32_t *seg_chain_count, ChainArrays ch, unsigned long long *counters,
                    cudaStream_t st) {
-    if (nsub) k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch, counters);
+    if (nsub) {
+        counted();
+        k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch, counters);
+    }
 }
 
 void launch_vote(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
                  ReadsView subj, ReadsView q, const DpSeg *, const uint32_t *ops,
                  uint32_t stride, const DpSum *sums, uint32_t *cov, unsigned long long *counters,
                  cudaStream_t st) {
-    if (nc) k_vote<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, ops, stride, sums, cov, counters);
+    if (nc) {
+        counted();
+        k_vote<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, ops, stride, sums, cov, counters);
+    }
 }
 
 void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, uint8_t *out,
                       uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
                       double *mis, cudaStream_t st) {
-    if (q.n) k_consensus<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(p, q, cov, out, colsum, imin, imed, imax, mis);
+    if (q.n) {
+        counted();
+        k_consensus<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(p, q, cov, out, colsum, imin, imed, imax, mis);
+    }
 }
 
 void launch_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
                        const uint64_t *out_off, uint8_t *out, int32_t *nops, cudaStream_t st) {
-    if (nd) k_unpack_ops<<<grid_1d(nd, 128), 128, 0, st>>>(ops, stride, sums, nd, out_off, out, nops);
+    if (nd) {
+        counted();
+        k_unpack_ops<<<grid_1d(nd, 128), 128, 0, st>>>(ops, stride, sums, nd, out_off, out, nops);
+    }
 }
 
 }  // namespace hero

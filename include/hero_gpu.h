@@ -16,6 +16,7 @@
  *                         reads (SubjectReadAligner.cpp:493-645); votes accumulate
  *   hero_align_self       the same with the query set as the subject set (HERO is
  *                         run with -q X -s X for correction)
+ *   hero_reset_votes      QueryRead::initilizeCoverageMatrix (QueryRead.cpp:100-115)
  *   hero_consensus        QueryDataset::callConsensus (QueryDataset.cpp:393-412)
  *                         plus the fields QueryDataset::writeQueryOut prints
  *                         (QueryDataset.cpp:414-537)
@@ -72,6 +73,7 @@ typedef struct {
     uint64_t dp_cells;         /* band cells of the reference's loop bounds, ref segments */
     uint64_t vote_anomalies;   /* votes outside a read (reference: undefined behaviour) */
     uint64_t device_bytes_peak;
+    uint64_t kernel_launches;  /* kernels this process launched through the library */
     double ms_upload, ms_index, ms_seed, ms_chain, ms_dp, ms_record, ms_vote, ms_consensus;
     double ms_dp_kernel;       /* device time of the DP kernels alone */
 } hero_stats;
@@ -98,6 +100,10 @@ int hero_align_subjects(hero_ctx *ctx, const uint8_t *seq, const uint64_t *off,
 
 /* The query set itself as the subject set, without a second upload. */
 int hero_align_self(hero_ctx *ctx);
+
+/* Clears the vote matrix for a new correction of the same query set, as
+ * QueryRead::initilizeCoverageMatrix zeroes it at load (QueryRead.cpp:100-115). */
+int hero_reset_votes(hero_ctx *ctx);
 
 /* Consensus over the accumulated votes.  seq_out has the query layout; bases of
  * reads that are not good are left untouched (the reference leaves them as
