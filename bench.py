@@ -220,12 +220,23 @@ def int_peak_tops(device: int) -> float | None:
     return v if v > 0 else None
 
 
+def dpx_peak_tops(device: int) -> float | None:
+    import ctypes as C
+    from hero_b200 import build
+    lib = C.CDLL(build.build_peak())
+    lib.hero_dpx_peak_tops.restype = C.c_double
+    lib.hero_dpx_peak_tops.argtypes = [C.c_int, C.c_int]
+    v = lib.hero_dpx_peak_tops(device, 5)
+    return v if v > 0 else None
+
+
 def bench_hero(args):
     import torch
     import torch.distributed as dist
 
     from hero_b200 import Hero, build
-    build.build_library()
+    if not os.environ.get("HERO_B200_LIB"):
+        build.build_library()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -60,7 +60,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("HERO_B200_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise RuntimeError(
             f"{p} is missing: build it with `python -m hero_b200.build` (nvcc, sm_100a). "

@@ -47,7 +47,7 @@ struct hero_ctx {
     DBuf t_slots, t_vals;
     uint64_t t_mask = 0, t_keys = 0;
     // vote matrix + consensus outputs
-    DBuf cov, out_seq, colsum, o_imin, o_imed, o_imax, o_mis;
+    DBuf cov, mdiff, out_seq, colsum, o_imin, o_imed, o_imax, o_mis;
     // subject batch (when not aligning the query set against itself)
     DBuf s_raw, s_code, s_off, s_len, s_uid, s_good;
     // batch buffers
@@ -56,7 +56,7 @@ struct hero_ctx {
         cs_gnch, cs_gbest, cs_gkept, cs_gkeys, cs_gdp;
     DBuf ch_subj, ch_query, ch_key_off, ch_seg_off, ch_nkeys, ch_nseg, ch_orient, ch_status,
         ch_win, ch_rate, ch_len;
-    DBuf keys, segs, sums, cells, ops, perm, bins, bin_off, tb, bnd;
+    DBuf keys, segs, sums, cells, ops, perm, bins, bin_off, tb, bnd, dp_tasks, winners;
     DBuf scan_tmp, counters;
     // index build temporaries (kept between builds)
     DBuf x_cnt, x_koff, x_klo, x_khi, x_kval, x_owner, x_count, x_slot_of, x_start, x_fill, x_tmp;
@@ -67,14 +67,14 @@ struct hero_ctx {
 
     hero_ctx() {
         DBuf *list[] = {&q_raw, &q_code, &q_off, &q_len, &q_uid, &q_good, &q_sgood, &q_gc,
-                        &t_slots, &t_vals, &cov, &out_seq, &colsum, &o_imin, &o_imed, &o_imax,
+                        &t_slots, &t_vals, &cov, &mdiff, &out_seq, &colsum, &o_imin, &o_imed, &o_imax,
                         &o_mis, &s_raw, &s_code, &s_off, &s_len, &s_uid, &s_good, &seg_hits,
                         &hit_off, &hits, &seg_cstart, &seg_ccount, &cs_grp, &cs_chain_of,
                         &cs_first, &cs_last, &cs_prev, &cs_size, &cs_coff, &cs_ckeys, &cs_kl,
                         &cs_gnch, &cs_gbest, &cs_gkept, &cs_gkeys, &cs_gdp, &ch_subj, &ch_query,
                         &ch_key_off, &ch_seg_off, &ch_nkeys, &ch_nseg, &ch_orient, &ch_status,
                         &ch_win, &ch_rate, &ch_len, &keys, &segs, &sums, &cells, &ops, &perm,
-                        &bins, &bin_off, &tb, &bnd, &scan_tmp, &counters, &x_cnt, &x_koff,
+                        &bins, &bin_off, &tb, &bnd, &dp_tasks, &winners, &scan_tmp, &counters, &x_cnt, &x_koff,
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
                         &x_fill, &x_tmp};
         for (DBuf *b : list) all.push_back(b);
@@ -269,7 +269,9 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     HERO_TRY(upload_reads(c, seq, n ? off : nullptr, uid, n, c->q_raw, c->q_code, c->q_off,
                           c->q_len, c->q_uid, &c->q_good, &c->q_sgood, &c->q_gc));
     HERO_TRY(c->ensure(c->cov, c->nqb * 16, "vote matrix"));
+    HERO_TRY(c->ensure(c->mdiff, c->nqb * 4, "vote matrix"));
     HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "memset"));
+    HERO_TRY(c->cuda(cudaMemsetAsync(c->mdiff.p, 0, c->nqb * 4, c->st), "memset"));
     cudaEventRecord(e1, c->st);
     HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "set queries"));
     c->stats.ms_upload += elapsed(e0, e1);
@@ -367,6 +369,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         if ((r = c->ensure(c->scan_tmp, scan_tmp_bytes(std::max<uint64_t>(nseg + 1, kDpBins + 1)), "scan"))) break;
         // zero the per-batch counters that size buffers (keep the running totals)
         cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st);
+        cudaMemsetAsync(ctr + C_WIN, 0, sizeof(unsigned long long), c->st);
         launch_probe(false, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
         launch_scan_u32(P_<uint32_t>(c->seg_hits), P_<uint64_t>(c->hit_off), nseg, c->scan_tmp.p, c->st);
         uint64_t H = 0;
@@ -426,8 +429,11 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         if ((r = c->ensure(c->bins, kDpBins * 4, "DP bins"))) break;
         if ((r = c->ensure(c->bin_off, (kDpBins + 1) * 8, "DP bins"))) break;
         const int32_t nst = (cmax + kStripW - 1) / kStripW;
-        if ((r = c->ensure(c->tb, size_t(c->dp_T) * size_t(rmax) * size_t(nst) * 2, "DP traceback scratch"))) break;
-        if ((r = c->ensure(c->bnd, size_t(c->dp_T) * size_t(rmax + 1) * 3 * 4, "DP boundary scratch"))) break;
+        if ((r = c->ensure(c->dp_tasks, 128 * 8, "DP tasks"))) break;
+        if (dp_needs_scratch(rmax, cmax)) {
+            if ((r = c->ensure(c->tb, size_t(c->dp_T) * size_t(rmax) * size_t(nst) * 2, "DP traceback scratch"))) break;
+            if ((r = c->ensure(c->bnd, size_t(c->dp_T) * size_t(rmax + 1) * 3 * 4, "DP boundary scratch"))) break;
+        }
         launch_dp_sort(P_<DpSeg>(c->segs), ND, P_<uint32_t>(c->bins), P_<uint32_t>(c->perm),
                        P_<uint64_t>(c->bin_off), c->scan_tmp.p, c->st);
         cudaEventRecord(ev[3], c->st);
@@ -435,15 +441,18 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
                    q.code, q.off, P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums),
                    P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
                    c->p.affine};
-        launch_dp(a, c->st);
+        launch_dp(a, P_<uint64_t>(c->bin_off), P_<uint64_t>(c->dp_tasks), cmax, c->st);
         if ((r = c->check_launch("dp"))) break;
         cudaEventRecord(ev[4], c->st);
         launch_assemble(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSum>(c->sums),
                         P_<uint32_t>(c->cells), ctr, c->st);
-        launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch, ctr, c->st);
+        if ((r = c->ensure(c->winners, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
+        launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
+                      P_<uint32_t>(c->winners), ctr, c->st);
         cudaEventRecord(ev[5], c->st);
-        launch_vote(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSeg>(c->segs),
-                    P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov), ctr, c->st);
+        launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->keys), subj, q,
+                    P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov),
+                    P_<int32_t>(c->mdiff), ctr, c->st);
         if ((r = c->check_launch("record/vote"))) break;
         cudaEventRecord(ev[6], c->st);
         if ((r = c->cuda(cudaStreamSynchronize(c->st), "batch"))) break;
@@ -532,7 +541,8 @@ extern "C" int hero_consensus(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uin
     HERO_TRY(c->ensure(c->o_mis, n * 8, "consensus"));
     cudaEventRecord(e0, c->st);
     if (nb) cudaMemcpyAsync(c->out_seq.p, c->q_raw.p, nb, cudaMemcpyDeviceToDevice, c->st);
-    launch_consensus(c->p, query_view(c), P_<uint32_t>(c->cov), P_<uint8_t>(c->out_seq),
+    launch_consensus(c->p, query_view(c), P_<uint32_t>(c->cov), P_<int32_t>(c->mdiff),
+                     P_<uint8_t>(c->out_seq),
                      P_<uint32_t>(c->colsum), P_<uint32_t>(c->o_imin), P_<uint32_t>(c->o_imed),
                      P_<uint32_t>(c->o_imax), P_<double>(c->o_mis), c->st);
     HERO_TRY(c->check_launch("consensus"));
@@ -556,14 +566,26 @@ extern "C" int hero_reset_votes(hero_ctx *c) {
     if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
     cudaSetDevice(c->dev);
     if (c->nqb) HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "reset votes"));
+    if (c->nqb) HERO_TRY(c->cuda(cudaMemsetAsync(c->mdiff.p, 0, c->nqb * 4, c->st), "reset votes"));
     return c->cuda(cudaStreamSynchronize(c->st), "reset votes");
 }
 
 extern "C" int hero_get_votes(hero_ctx *c, uint32_t *cov) {
     if (!c || !cov) return HERO_E_INPUT;
     cudaSetDevice(c->dev);
-    if (c->nqb) HERO_TRY(c->cuda(cudaMemcpy(cov, c->cov.p, c->nqb * 16, cudaMemcpyDeviceToHost), "votes"));
-    return HERO_OK;
+    if (!c->nqb) return HERO_OK;
+    DBuf tmp;
+    int r = c->ensure(tmp, c->nqb * 16, "votes");
+    if (r == HERO_OK) {
+        launch_expand_votes(query_view(c), P_<uint32_t>(c->cov), P_<int32_t>(c->mdiff),
+                            P_<uint32_t>(tmp), c->st);
+        r = c->check_launch("votes");
+        if (r == HERO_OK)
+            r = c->cuda(cudaMemcpyAsync(cov, tmp.p, c->nqb * 16, cudaMemcpyDeviceToHost, c->st), "votes");
+        if (r == HERO_OK) r = c->cuda(cudaStreamSynchronize(c->st), "votes");
+    }
+    c->release(tmp);
+    return r;
 }
 
 extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
@@ -628,10 +650,11 @@ extern "C" int hero_align_segments(hero_ctx *c, int affine, const uint8_t *subj,
     }
     const uint32_t stride = uint32_t((rmax + cmax + 15) / 16);
     DBuf sraw, scode, soff, slen, suid, qraw, qcode, qoff, qlen, quid, dsegs, dsums, dops, dtb, dbnd,
-        doo, dout, dn;
+        doo, dout, dn, dperm, dbins, dbinoff, dtasks, dtmp;
     auto cleanup = [&]() {
         for (DBuf *b : {&sraw, &scode, &soff, &slen, &suid, &qraw, &qcode, &qoff, &qlen, &quid,
-                        &dsegs, &dsums, &dops, &dtb, &dbnd, &doo, &dout, &dn})
+                        &dsegs, &dsums, &dops, &dtb, &dbnd, &doo, &dout, &dn, &dperm, &dbins,
+                        &dbinoff, &dtasks, &dtmp})
             c->release(*b);
     };
     int r = HERO_OK;
@@ -646,18 +669,27 @@ extern "C" int hero_align_segments(hero_ctx *c, int affine, const uint8_t *subj,
         if ((r = c->ensure(dsegs, n_seg * sizeof(DpSeg), "segments"))) break;
         if ((r = c->ensure(dsums, n_seg * sizeof(DpSum), "segments"))) break;
         if ((r = c->ensure(dops, n_seg * stride * 4, "segments"))) break;
-        if ((r = c->ensure(dtb, size_t(c->dp_T) * rmax * nst * 2, "scratch"))) break;
-        if ((r = c->ensure(dbnd, size_t(c->dp_T) * (rmax + 1) * 3 * 4, "scratch"))) break;
+        if (dp_needs_scratch(rmax, cmax)) {
+            if ((r = c->ensure(dtb, size_t(c->dp_T) * rmax * nst * 2, "scratch"))) break;
+            if ((r = c->ensure(dbnd, size_t(c->dp_T) * (rmax + 1) * 3 * 4, "scratch"))) break;
+        }
+        if ((r = c->ensure(dperm, n_seg * 4, "order"))) break;
+        if ((r = c->ensure(dbins, kDpBins * 4, "bins"))) break;
+        if ((r = c->ensure(dbinoff, (kDpBins + 1) * 8, "bins"))) break;
+        if ((r = c->ensure(dtasks, 128 * 8, "tasks"))) break;
+        if ((r = c->ensure(dtmp, scan_tmp_bytes(kDpBins + 1), "scan"))) break;
         if ((r = c->ensure(doo, (n_seg + 1) * 8, "ops"))) break;
         if ((r = c->ensure(dout, ops_off[n_seg], "ops"))) break;
         if ((r = c->ensure(dn, n_seg * 4, "ops"))) break;
         cudaMemcpyAsync(dsegs.p, h.data(), n_seg * sizeof(DpSeg), cudaMemcpyHostToDevice, c->st);
         cudaMemcpyAsync(doo.p, ops_off, (n_seg + 1) * 8, cudaMemcpyHostToDevice, c->st);
-        DpLaunch a{P_<DpSeg>(dsegs), nullptr, n_seg, P_<uint8_t>(scode), P_<uint64_t>(soff),
+        launch_dp_sort(P_<DpSeg>(dsegs), n_seg, P_<uint32_t>(dbins), P_<uint32_t>(dperm),
+                       P_<uint64_t>(dbinoff), dtmp.p, c->st);
+        DpLaunch a{P_<DpSeg>(dsegs), P_<uint32_t>(dperm), n_seg, P_<uint8_t>(scode), P_<uint64_t>(soff),
                    P_<uint32_t>(slen), P_<uint8_t>(qcode), P_<uint64_t>(qoff), P_<uint32_t>(dops),
                    stride, P_<DpSum>(dsums), nullptr, P_<uint16_t>(dtb), P_<int32_t>(dbnd),
                    c->dp_T, rmax, affine ? 1 : 0};
-        launch_dp(a, c->st);
+        launch_dp(a, P_<uint64_t>(dbinoff), P_<uint64_t>(dtasks), cmax, c->st);
         launch_unpack_ops(P_<uint32_t>(dops), stride, P_<DpSum>(dsums), n_seg, P_<uint64_t>(doo),
                           P_<uint8_t>(dout), P_<int32_t>(dn), c->st);
         if ((r = c->check_launch("align segments"))) break;

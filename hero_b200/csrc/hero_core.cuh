@@ -370,12 +370,12 @@ struct RecState {
         if (s.nruns >= 2) {
             if (n >= 2) interior_add(lt, lc);
             // interior runs of the piece: totals minus its first and last runs
-            int64_t t[4] = {s.tot[0], s.tot[1], s.tot[2], s.tot[3]};
-            t[s.ft] -= s.fc;
-            t[s.lt] -= s.lc;
-            im += t[OP_M];
-            ix += t[OP_X];
-            iid += t[OP_I] + t[OP_D];
+            const int64_t fm = (s.ft == OP_M ? s.fc : 0) + (s.lt == OP_M ? s.lc : 0);
+            const int64_t fx = (s.ft == OP_X ? s.fc : 0) + (s.lt == OP_X ? s.lc : 0);
+            const int64_t fid = (s.ft >= OP_I ? s.fc : 0) + (s.lt >= OP_I ? s.lc : 0);
+            im += int64_t(s.tot[OP_M]) - fm;
+            ix += int64_t(s.tot[OP_X]) - fx;
+            iid += int64_t(s.tot[OP_I]) + int64_t(s.tot[OP_D]) - fid;
             lt = s.lt;
             lc = s.lc;
             n = 2;
@@ -511,176 +511,190 @@ HERO_HD bool in_band(int32_t i, int32_t j, int32_t C, int64_t m) {
     return j <= C && int64_t(j) >= int64_t(i) - m && int64_t(j) <= int64_t(i) + m;
 }
 
-// Boundary-column storage of one thread: for each row, the state values of the
-// last column of the previous strip.  Scratch provides
-//   int32_t& b(int32_t state, int32_t row)          state 0..2 (FM, IX, IY)
-//   void tb_set(int32_t strip, int32_t row, uint32_t bits)  traceback codes of a
-//   uint32_t tb_get(int32_t strip, int32_t row)             row, 2 bits per cell
-template <int W, class Scratch>
-HERO_HD void dp_fill_global(const SegView &v, Scratch &sc) {
-    const int32_t R = v.R, C = v.C;
-    const int64_t m = v.band;
-    const bool full = m >= R && m >= C;
-    // column 0 (BandAligner.cpp:75-79 with j == 0)
-    sc.b(0, 0) = 0;
-    for (int32_t i = 1; i <= R; i++) sc.b(0, i) = (int64_t(i) <= m) ? i * (v.right ? kSX : kDX) : kNEG;
-    const int32_t nst = (C + W - 1) / W;
-    for (int32_t s = 0; s < nst; s++) {
-        const int32_t j0 = s * W;
-        uint8_t bc[W];
-        int32_t up[W];
-        for (int32_t w = 0; w < W; w++) {
-            const int32_t j = j0 + w + 1;
-            bc[w] = j <= C ? v.col(j) : uint8_t(7);
-            up[w] = (j <= C && int64_t(j) <= m) ? kDY * j : kNEG;  // row 0
-        }
-        int32_t prev_lb = sc.b(0, 0);
-        for (int32_t i = 1; i <= R; i++) {
-            const uint8_t a = v.row(i);
-            const int32_t lb = sc.b(0, i);
-            int32_t left = lb, dg = prev_lb;
-            uint32_t bits = 0;
+// State of one DP cell: FM, IX, IY (the global aligner uses f only).
+struct Cell3 {
+    int32_t f, x, y;
+};
+
+// Column 0 (BandAligner.cpp:75-79 with j == 0; affine init BandAligner.cpp:150-164)
+template <bool AFFINE>
+HERO_HD Cell3 dp_col0(const SegView &v, int32_t i) {
+    if (i == 0) return AFFINE ? Cell3{0, kDX - kEX, kDX - kEX} : Cell3{0, 0, 0};
+    if (int64_t(i) > v.band) return Cell3{kNEG, kNEG, kNEG};
+    if (AFFINE) {
+        if (v.right) return Cell3{0, 0, kDY};
+        const int32_t z = kDX - kEX + i * kEX;
+        return Cell3{z, z, z};
+    }
+    const int32_t z = i * (v.right ? kSX : kDX);
+    return Cell3{z, z, z};
+}
+
+// Row 0 (BandAligner.cpp:58-126 with i == 0; affine init BandAligner.cpp:165-171)
+template <bool AFFINE>
+HERO_HD Cell3 dp_row0(const SegView &v, int32_t j) {
+    if (j == 0) return dp_col0<AFFINE>(v, 0);
+    if (j > v.C || int64_t(j) > v.band) return Cell3{kNEG, kNEG, kNEG};
+    const int32_t z = AFFINE ? kDX - kEX + j * kEX : kDY * j;
+    return Cell3{z, z, z};
+}
+
+// One row i of a strip of W columns j0+1 .. j0+W.
+//   u*[w]  : states of row i-1 on entry, of row i on exit
+//   left   : states at (i, j0) on entry, at (i, j0+W) on exit
+//   dg     : states at (i-1, j0)
+// Returns the row's traceback codes, 2 bits per cell (2 diag, 1 left, 0 up).
+// FULL: the band covers every cell of the strip up to column C; cells past C
+//       are then computed as if inside the matrix -- no cell at or left of
+//       column C ever reads them, so they only cost time.
+// LEFT: column wlast (0-based in the strip) is column C of an align-left
+//       segment, whose vertical moves cost sx (BandAligner.cpp:69-82,190-196).
+template <int W, bool AFFINE, bool FULL, bool LEFT>
+HERO_HD uint32_t dp_strip_row(const SegView &v, int32_t i, int32_t j0, uint8_t a,
+                              const uint8_t (&bc)[W], int32_t (&uf)[W], int32_t (&ux)[W],
+                              int32_t (&uy)[W], Cell3 &left, Cell3 dg, int32_t wlast) {
+    uint32_t bits = 0;
 #pragma unroll
-            for (int32_t w = 0; w < W; w++) {
-                const int32_t j = j0 + w + 1;
-                int32_t h;
-                uint32_t code;
-                if (full ? (j <= C) : in_band(i, j, C, m)) {
-                    const int32_t vu = up[w] + ((j == C && v.left) ? kSX : kDX);
-                    const int32_t vl = left + kDY;
-                    const int32_t vd = dg + (a == bc[w] ? kHIT : kMISS);
-                    if (vd >= vl && vd >= vu) {
-                        h = vd;
-                        code = 2;
-                    } else if (vl >= vu) {
-                        h = vl;
-                        code = 1;
-                    } else {
-                        h = vu;
-                        code = 0;
-                    }
+    for (int32_t w = 0; w < W; w++) {
+        const int32_t j = j0 + w + 1;
+        const bool in = FULL || in_band(i, j, v.C, v.band);
+        const bool lastcol = LEFT && (w == wlast);
+        Cell3 c;
+        uint32_t code;
+        if (AFFINE) {
+            if (in) {
+                // IY: gap along the row (BandAligner.cpp:180-188)
+                const int32_t y0 = left.f + kDY, y1 = left.y + kEX;
+                c.y = y0 >= y1 ? y0 : y1;
+                // IX: gap down the column (BandAligner.cpp:189-201)
+                const int32_t x0 = uf[w] + (lastcol ? kSX : kDX);
+                const int32_t x1 = ux[w] + (lastcol ? kSX : kEX);
+                c.x = x1 > x0 ? x1 : x0;
+                // FM = max3(FM, IX, IY)(i-1, j-1) + s (BandAligner.cpp:203-207)
+                int32_t mm = dg.f >= dg.x ? dg.f : dg.x;
+                mm = mm >= dg.y ? mm : dg.y;
+                c.f = mm + (a == bc[w] ? kHIT : kMISS);
+                // BM1 (BandAligner.cpp:214-222)
+                code = (c.f > c.x && c.f >= c.y) ? 2u : (c.y > c.x ? 1u : 0u);
+            } else {
+                c = Cell3{kNEG, kNEG, kNEG};
+                code = 0;
+            }
+            dg = Cell3{uf[w], ux[w], uy[w]};
+            uf[w] = c.f;
+            ux[w] = c.x;
+            uy[w] = c.y;
+        } else {
+            if (in) {
+                // BandAligner.cpp:66-110: up, left, diag; diag wins ties, then left
+                const int32_t vu = uf[w] + (lastcol ? kSX : kDX);
+                const int32_t vl = left.f + kDY;
+                const int32_t vd = dg.f + (a == bc[w] ? kHIT : kMISS);
+                if (vd >= vl && vd >= vu) {
+                    c.f = vd;
+                    code = 2;
+                } else if (vl >= vu) {
+                    c.f = vl;
+                    code = 1;
                 } else {
-                    h = kNEG;
+                    c.f = vu;
                     code = 0;
                 }
-                dg = up[w];
-                up[w] = h;
-                left = h;
-                bits |= code << (2 * w);
+            } else {
+                c.f = kNEG;
+                code = 0;
             }
-            sc.tb_set(s, i, bits);
-            sc.b(0, i) = left;
-            prev_lb = lb;
+            c.x = c.y = c.f;
+            dg.f = uf[w];
+            uf[w] = c.f;
         }
-        // row 0 value of this strip's last column becomes the boundary of row 0
-        const int32_t jl = j0 + W;
-        sc.b(0, 0) = (jl <= C && int64_t(jl) <= m) ? kDY * jl : kNEG;
+        left = c;
+        bits |= code << (2 * w);
+    }
+    return bits;
+}
+
+// 0-based position of column C in the strip starting after j0 when the segment
+// aligns left, else -1
+HERO_HD int32_t dp_strip_wlast(const SegView &v, int32_t j0, int32_t W) {
+    const int32_t w = v.C - j0 - 1;
+    return (v.left && w >= 0 && w < W) ? w : -1;
+}
+
+// dispatch on the strip's band coverage and align-left column
+template <int W, bool AFFINE>
+HERO_HD uint32_t dp_strip_row_any(bool full, int32_t wlast, const SegView &v, int32_t i,
+                                  int32_t j0, uint8_t a, const uint8_t (&bc)[W], int32_t (&uf)[W],
+                                  int32_t (&ux)[W], int32_t (&uy)[W], Cell3 &left, Cell3 dg) {
+    if (full) {
+        if (wlast >= 0) return dp_strip_row<W, AFFINE, true, true>(v, i, j0, a, bc, uf, ux, uy, left, dg, wlast);
+        return dp_strip_row<W, AFFINE, true, false>(v, i, j0, a, bc, uf, ux, uy, left, dg, wlast);
+    }
+    if (wlast >= 0) return dp_strip_row<W, AFFINE, false, true>(v, i, j0, a, bc, uf, ux, uy, left, dg, wlast);
+    return dp_strip_row<W, AFFINE, false, false>(v, i, j0, a, bc, uf, ux, uy, left, dg, wlast);
+}
+
+// strip setup: column codes and row-0 states of columns j0+1 .. j0+W
+template <int W, bool AFFINE>
+HERO_HD void dp_strip_init(const SegView &v, int32_t j0, uint8_t (&bc)[W], int32_t (&uf)[W],
+                           int32_t (&ux)[W], int32_t (&uy)[W]) {
+#pragma unroll
+    for (int32_t w = 0; w < W; w++) {
+        const int32_t j = j0 + w + 1;
+        bc[w] = j <= v.C ? v.col(j) : uint8_t(7);
+        const Cell3 r = dp_row0<AFFINE>(v, j);
+        uf[w] = r.f;
+        ux[w] = r.x;
+        uy[w] = r.y;
     }
 }
 
-template <int W, class Scratch>
-HERO_HD void dp_fill_affine(const SegView &v, Scratch &sc) {
+// a strip is FULL when the band covers every cell of its columns up to C:
+// |i - j| <= m for rows 1..R and columns j0+1 .. min(j0+W, C)
+HERO_HD bool dp_strip_full(const SegView &v, int32_t j0, int32_t W) {
+    const int64_t jl = j0 + W < v.C ? j0 + W : v.C;
+    if (jl < j0 + 1) return true;
+    return v.band >= int64_t(v.R) - (j0 + 1) && v.band >= jl - 1;
+}
+
+// Whole-matrix fill by one thread, strip after strip.  Scratch provides
+//   int32_t& b(int32_t state, int32_t row)          boundary column, state 0..2
+//   void tb_set(int32_t strip, int32_t row, uint32_t bits)  traceback codes of a
+//   uint32_t tb_get(int32_t strip, int32_t row)             row, 2 bits per cell
+template <int W, bool AFFINE, class Scratch>
+HERO_HD void dp_fill(const SegView &v, Scratch &sc) {
     const int32_t R = v.R, C = v.C;
-    const int64_t m = v.band;
-    const bool full = m >= R && m >= C;
-    // (0,0) and column 0 (BandAligner.cpp:140-164)
-    sc.b(0, 0) = 0;
-    sc.b(1, 0) = kDX - kEX;
-    sc.b(2, 0) = kDX - kEX;
-    for (int32_t i = 1; i <= R; i++) {
-        if (int64_t(i) <= m) {
-            if (v.right) {
-                sc.b(0, i) = 0;
-                sc.b(1, i) = 0;
-                sc.b(2, i) = kDY;
-            } else {
-                sc.b(0, i) = kDX - kEX + i * kEX;
-                sc.b(1, i) = kDX - kEX + i * kEX;
-                sc.b(2, i) = kDX - kEX + i * kEX;
-            }
-        } else {
-            sc.b(0, i) = kNEG;
-            sc.b(1, i) = kNEG;
-            sc.b(2, i) = kNEG;
-        }
+    for (int32_t i = 0; i <= R; i++) {
+        const Cell3 c = dp_col0<AFFINE>(v, i);
+        sc.b(0, i) = c.f;
+        sc.b(1, i) = c.x;
+        sc.b(2, i) = c.y;
     }
     const int32_t nst = (C + W - 1) / W;
     for (int32_t s = 0; s < nst; s++) {
         const int32_t j0 = s * W;
         uint8_t bc[W];
         int32_t uf[W], ux[W], uy[W];
-        for (int32_t w = 0; w < W; w++) {
-            const int32_t j = j0 + w + 1;
-            bc[w] = j <= C ? v.col(j) : uint8_t(7);
-            // row 0 (BandAligner.cpp:165-171): FM = IX = IY = dx - ex + j*ex
-            const int32_t r0 = (j <= C && int64_t(j) <= m) ? kDX - kEX + j * kEX : kNEG;
-            uf[w] = r0;
-            ux[w] = r0;
-            uy[w] = r0;
-        }
-        int32_t pf = sc.b(0, 0), px = sc.b(1, 0), py = sc.b(2, 0);
+        dp_strip_init<W, AFFINE>(v, j0, bc, uf, ux, uy);
+        const bool full = dp_strip_full(v, j0, W);
+        const int32_t wlast = dp_strip_wlast(v, j0, W);
+        Cell3 dg{sc.b(0, 0), sc.b(1, 0), sc.b(2, 0)};
         for (int32_t i = 1; i <= R; i++) {
+            Cell3 left{sc.b(0, i), sc.b(1, i), sc.b(2, i)};
+            const Cell3 lb = left;
             const uint8_t a = v.row(i);
-            const int32_t lf0 = sc.b(0, i), lx0 = sc.b(1, i), ly0 = sc.b(2, i);
-            int32_t lf = lf0, ly = ly0, lx = lx0;
-            int32_t df = pf, dx = px, dy = py;
-            uint32_t bits = 0;
-#pragma unroll
-            for (int32_t w = 0; w < W; w++) {
-                const int32_t j = j0 + w + 1;
-                int32_t F, X, Y;
-                uint32_t code;
-                if (full ? (j <= C) : in_band(i, j, C, m)) {
-                    // IY: gap along the row (BandAligner.cpp:180-188)
-                    const int32_t y0 = lf + kDY, y1 = ly + kEX;
-                    Y = y0 >= y1 ? y0 : y1;
-                    // IX: gap down the column (BandAligner.cpp:189-201)
-                    int32_t x0, x1;
-                    if (v.left && j == C) {
-                        x0 = uf[w] + kSX;
-                        x1 = ux[w] + kSX;
-                    } else {
-                        x0 = uf[w] + kDX;
-                        x1 = ux[w] + kEX;
-                    }
-                    X = x1 > x0 ? x1 : x0;
-                    // FM = max3(FM, IX, IY)(i-1,j-1) + s (BandAligner.cpp:203-207)
-                    const int32_t sub = a == bc[w] ? kHIT : kMISS;
-                    int32_t mm = df >= dx ? df : dx;
-                    mm = mm >= dy ? mm : dy;
-                    F = mm + sub;
-                    // BM1 (BandAligner.cpp:214-222)
-                    code = (F > X && F >= Y) ? 2u : (Y > X ? 1u : 0u);
-                } else {
-                    F = kNEG;
-                    X = kNEG;
-                    Y = kNEG;
-                    code = 0;
-                }
-                df = uf[w];
-                dx = ux[w];
-                dy = uy[w];
-                uf[w] = F;
-                ux[w] = X;
-                uy[w] = Y;
-                lf = F;
-                lx = X;
-                ly = Y;
-                bits |= code << (2 * w);
-            }
+            const uint32_t bits =
+                dp_strip_row_any<W, AFFINE>(full, wlast, v, i, j0, a, bc, uf, ux, uy, left, dg);
             sc.tb_set(s, i, bits);
-            sc.b(0, i) = lf;
-            sc.b(1, i) = lx;
-            sc.b(2, i) = ly;
-            pf = lf0;
-            px = lx0;
-            py = ly0;
+            sc.b(0, i) = left.f;
+            sc.b(1, i) = left.x;
+            sc.b(2, i) = left.y;
+            dg = lb;
         }
-        const int32_t jl = j0 + W;
-        const int32_t r0 = (jl <= C && int64_t(jl) <= m) ? kDX - kEX + jl * kEX : kNEG;
-        sc.b(0, 0) = r0;
-        sc.b(1, 0) = r0;
-        sc.b(2, 0) = r0;
+        const Cell3 r0 = dp_row0<AFFINE>(v, j0 + W);
+        sc.b(0, 0) = r0.f;
+        sc.b(1, 0) = r0.x;
+        sc.b(2, 0) = r0.y;
     }
 }
 
@@ -689,14 +703,11 @@ HERO_HD void dp_fill_affine(const SegView &v, Scratch &sc) {
 template <int W, class Scratch, class Emit>
 HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &sum) {
     int32_t i = v.R, j = v.C, nops = 0;
-    uint32_t tot[4] = {0, 0, 0, 0};
-    uint8_t cur = 0xff;
-    uint32_t cc = 0;
+    uint64_t tot = 0;  // four 16-bit op counters (path length < 65536)
+    uint32_t cur = 0xffu, cc = 0, lt = 0, lc = 0;
     int32_t nr = 0;
-    uint8_t lt = 0;
-    uint32_t lc = 0;
-    const uint8_t op_up = v.reversed ? OP_I : OP_D;
-    const uint8_t op_left = v.reversed ? OP_D : OP_I;
+    const uint32_t op_up = v.reversed ? OP_I : OP_D;
+    const uint32_t op_left = v.reversed ? OP_D : OP_I;
     while (i > 0 || j > 0) {
         uint32_t code;
         if (i == 0) {
@@ -706,7 +717,7 @@ HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &s
         } else {
             code = (sc.tb_get((j - 1) / W, i) >> (2 * ((j - 1) % W))) & 3u;
         }
-        uint8_t op;
+        uint32_t op;
         if (code == 2) {
             op = v.row(i) == v.col(j) ? OP_M : OP_X;
             i--;
@@ -718,9 +729,9 @@ HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &s
             op = op_up;
             i--;
         }
-        emit(op);
+        emit(uint8_t(op));
         nops++;
-        tot[op]++;
+        tot += 1ull << (16 * op);
         if (op == cur) {
             cc++;
         } else {
@@ -736,18 +747,21 @@ HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &s
         }
     }
     // the run open at the end of the walk is the first run of the path
-    sum.ft = cur;
+    sum.ft = uint8_t(cur);
     sum.fc = uint16_t(cc);
     if (nr == 0) {
-        sum.lt = cur;
+        sum.lt = uint8_t(cur);
         sum.lc = uint16_t(cc);
         sum.nruns = 1;
     } else {
-        sum.lt = lt;
+        sum.lt = uint8_t(lt);
         sum.lc = uint16_t(lc);
         sum.nruns = 2;
     }
-    for (int t = 0; t < 4; t++) sum.tot[t] = uint16_t(tot[t]);
+    sum.tot[0] = uint16_t(tot);
+    sum.tot[1] = uint16_t(tot >> 16);
+    sum.tot[2] = uint16_t(tot >> 32);
+    sum.tot[3] = uint16_t(tot >> 48);
     sum.pad = 0;
     return nops;
 }

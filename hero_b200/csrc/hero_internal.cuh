@@ -60,6 +60,7 @@ enum Counter : int {
     C_CELLS,
     C_ANOMALY,
     C_OVERFLOW,
+    C_WIN,          // winners of the current batch (compacted list length)
     C_COUNT
 };
 
@@ -121,7 +122,7 @@ void launch_chain(const Params &p, uint64_t nseg, ReadsView subj, ReadsView q,
 // DP: shape sort then the strip kernel
 void launch_dp_sort(const DpSeg *segs, uint64_t nd, uint32_t *bins, uint32_t *perm,
                     uint64_t *bin_off, void *scan_tmp, cudaStream_t st);
-constexpr uint32_t kDpBins = 1u << 16;
+constexpr uint32_t kDpBins = 1u << 17;
 struct DpLaunch {
     const DpSeg *segs;
     const uint32_t *perm;   // processing order; NULL = identity
@@ -142,22 +143,37 @@ struct DpLaunch {
     int32_t affine;
 };
 constexpr int kStripW = 8;
-void launch_dp(const DpLaunch &a, cudaStream_t st);
+// needs the shape sort (perm, bin_off); tasks: 128 uint64 of device scratch.
+// The per-thread scratch (tb, bnd) is only used when dp_needs_scratch().
+void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int32_t cmax,
+               cudaStream_t st);
+bool dp_wave_fits(int32_t rmax);
+inline bool dp_needs_scratch(int32_t rmax, int32_t cmax) {
+    return !dp_wave_fits(rmax) || cmax > 32 * kStripW;
+}
 uint64_t dp_threads(int device);
 
 void launch_assemble(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
                      ReadsView subj, ReadsView q, const DpSum *sums, const uint32_t *cells,
                      unsigned long long *counters, cudaStream_t st);
+// winners (one per subject x query) are appended to `winners`; the count is
+// counters[C_WIN]
 void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
-                   const uint32_t *seg_chain_count, ChainArrays ch, unsigned long long *counters,
-                   cudaStream_t st);
-void launch_vote(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
-                 ReadsView subj, ReadsView q, const DpSeg *segs, const uint32_t *ops,
-                 uint32_t stride, const DpSum *sums, uint32_t *cov, unsigned long long *counters,
-                 cudaStream_t st);
-void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, uint8_t *out,
-                      uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
-                      double *mis, cudaStream_t st);
+                   const uint32_t *seg_chain_count, ChainArrays ch, uint32_t *winners,
+                   unsigned long long *counters, cudaStream_t st);
+// Votes.  A mismatch votes the subject base into cov[pos][4]; a run of matches
+// votes the query's own base, recorded as +1/-1 at the run's ends in mdiff
+// (a per-read difference array, summed by the consensus).
+void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,
+                 const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
+                 uint32_t stride, const DpSum *sums, uint32_t *cov, int32_t *mdiff,
+                 unsigned long long *counters, cudaStream_t st);
+void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, const int32_t *mdiff,
+                      uint8_t *out, uint32_t *colsum, uint32_t *imin, uint32_t *imed,
+                      uint32_t *imax, double *mis, cudaStream_t st);
+// full vote matrix (cov + match runs), as the reference's coverage matrix
+void launch_expand_votes(ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint32_t *out,
+                         cudaStream_t st);
 void launch_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
                        const uint64_t *out_off, uint8_t *out, int32_t *nops, cudaStream_t st);
 

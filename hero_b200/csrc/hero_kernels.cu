@@ -688,12 +688,16 @@ struct OpsWriter {
     }
 };
 
+// (strips, align-left, rows): a warp of the wavefront kernel takes segments
+// with equal strips, so they are grouped first; align-left and row count keep
+// the warps uniform
 __device__ __forceinline__ uint32_t shape_key(const DpSeg &g) {
     const int32_t ls = g.s1 - g.s0, lq = g.q1 - g.q0;
     const int32_t r = ls > lq ? ls : lq, c = ls > lq ? lq : ls;
     int32_t nst = (c + kStripW - 1) / kStripW;
     if (nst > 63) nst = 63;
-    return (uint32_t(nst) << 10) | uint32_t(r > 1023 ? 1023 : r);
+    return (uint32_t(nst) << 11) | ((g.flags & DPF_LEFT) ? 1024u : 0u) |
+           uint32_t(r > 1023 ? 1023 : r);
 }
 
 __global__ void k_dp_hist(const DpSeg *segs, uint64_t nd, uint32_t *bins) {
@@ -727,11 +731,169 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
         const uint8_t *qb = a.qcode + a.qoff[g.query];
         const SegView v = make_view(sb, Ls, int32_t(orient), qb, g.s0, g.s1, g.q0, g.q1,
                                     g.flags & 3u, g.band);
-        if (AFFINE) {
-            dp_fill_affine<kStripW>(v, sc);
-        } else {
-            dp_fill_global<kStripW>(v, sc);
+        dp_fill<kStripW, AFFINE>(v, sc);
+        OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
+        DpSum sum;
+        dp_traceback<kStripW>(v, sc, w, sum);
+        w.flush();
+        a.sums[si] = sum;
+        if (a.cells) {
+            const uint64_t cl = band_cells(v.R, v.C, v.band);
+            a.cells[si] = uint32_t(cl > 0xffffffffull ? 0xffffffffull : cl);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// banded DP as a warp wavefront.  Segments are sorted by (strips, rows); a
+// warp takes S = 32 / G segments that all have G strips of kStripW columns.
+// Lane (g, s) owns strip s of segment g and computes row i = t - s + 1 at step
+// t: the states of its strip's last column go to lane s+1 by __shfl_up_sync,
+// which uses them as its left boundary one step later (and as its diagonal one
+// step after that), so no boundary column is ever stored.  Each lane writes
+// its 2-bit codes of a row to shared memory; lane s = 0 of every group then
+// traces its segment back from there.
+// ---------------------------------------------------------------------------
+constexpr int kWaveWarps = 4;
+constexpr int kWaveMinBlocks = 4;  // caps registers at 128 per thread
+
+__global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks) {
+    // tasks[n] (n = 1..33): first task of segments with n strips; tasks[34+n]:
+    // first sorted segment with n strips; tasks[68+n]: one past the last.
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint64_t t = 0;
+    for (int n = 1; n <= 32; n++) {
+        const uint64_t b = bin_off[uint32_t(n) << 11], e = bin_off[uint32_t(n + 1) << 11];
+        tasks[n] = t;
+        tasks[34 + n] = b;
+        tasks[68 + n] = e;
+        const uint64_t S = uint64_t(32 / n);
+        t += (e - b + S - 1) / S;
+    }
+    tasks[33] = t;
+    tasks[0] = bin_off[uint32_t(33) << 11];  // first segment needing the per-thread kernel
+}
+
+// the wavefront over one warp's segments; FULL / LEFT are warp-uniform
+template <bool AFFINE, bool FULL, bool LEFT>
+__device__ __forceinline__ void wave_fill(const SegView &v, bool active, int32_t R, int32_t Rw,
+                                          int G, int s, int lane, int32_t wlast, uint16_t *tb) {
+    const int32_t j0 = s * kStripW;
+    uint8_t bc[kStripW];
+    int32_t uf[kStripW], ux[kStripW], uy[kStripW];
+    Cell3 prev{0, 0, 0};
+    uint8_t ch = 0;
+    if (active) {
+        dp_strip_init<kStripW, AFFINE>(v, j0, bc, uf, ux, uy);
+        prev = dp_row0<AFFINE>(v, j0);  // diagonal of row 1: (0, j0)
+        if (R >= 1) ch = v.row(1);
+    }
+    Cell3 pub{kNEG, kNEG, kNEG};
+    for (int32_t t = 0; t < Rw + G - 1; t++) {
+        Cell3 in;
+        in.f = __shfl_up_sync(0xffffffffu, pub.f, 1);
+        in.x = __shfl_up_sync(0xffffffffu, pub.x, 1);
+        in.y = __shfl_up_sync(0xffffffffu, pub.y, 1);
+        const int32_t i = t - s + 1;
+        if (active && i >= 1 && i <= R) {
+            const uint8_t a = ch;
+            if (i < R) ch = v.row(i + 1);  // next row's base, loaded a step early
+            Cell3 left = (s == 0) ? dp_col0<AFFINE>(v, i) : in;
+            const Cell3 dg = (s == 0) ? dp_col0<AFFINE>(v, i - 1) : prev;
+            const Cell3 lb = left;
+            const uint32_t bits = dp_strip_row<kStripW, AFFINE, FULL, LEFT>(v, i, j0, a, bc, uf, ux,
+                                                                             uy, left, dg, wlast);
+            tb[size_t(i - 1) * 32u + lane] = uint16_t(bits);
+            pub = left;
+            prev = lb;
+        }
+    }
+}
+
+template <bool AFFINE>
+__global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
+    k_dp_wave(DpLaunch a, const uint64_t *tasks) {
+    extern __shared__ uint16_t tbs[];
+    const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
+    uint16_t *tb = tbs + size_t(wib) * size_t(a.rmax) * 32u;
+    const uint64_t ntask = tasks[33];
+    for (uint64_t task = uint64_t(blockIdx.x) * kWaveWarps + wib; task < ntask;
+         task += uint64_t(gridDim.x) * kWaveWarps) {
+        int G = 1;
+        while (G < 32 && tasks[G + 1] <= task) G++;
+        const int S = 32 / G;
+        const uint64_t first = tasks[34 + G] + (task - tasks[G]) * uint64_t(S);
+        const uint64_t end = tasks[68 + G];
+        const int g = lane / G, s = lane % G;
+        const bool active = g < S && first + uint64_t(g) < end;
+        uint32_t si = 0;
+        SegView v{};
+        int32_t R = 0;
+        if (active) {
+            si = a.perm[first + g];
+            const DpSeg sg = a.segs[si];
+            const uint32_t orient = (sg.flags >> kSegOrientShift) & 1u;
+            v = make_view(a.scode + a.soff[sg.subj], int32_t(a.slen[sg.subj]), int32_t(orient),
+                          a.qcode + a.qoff[sg.query], sg.s0, sg.s1, sg.q0, sg.q1, sg.flags & 3u,
+                          sg.band);
+            R = v.R;
+        }
+        const int32_t Rw = warp_max(R);
+        const int32_t j0 = s * kStripW;
+        const bool full = !active || dp_strip_full(v, j0, kStripW);
+        const int32_t wlast = active ? dp_strip_wlast(v, j0, kStripW) : -1;
+        const bool wfull = __all_sync(0xffffffffu, full);
+        const bool wleft = __any_sync(0xffffffffu, wlast >= 0);
+        if (wfull) {
+            if (wleft) {
+                wave_fill<AFFINE, true, true>(v, active, R, Rw, G, s, lane, wlast, tb);
+            } else {
+                wave_fill<AFFINE, true, false>(v, active, R, Rw, G, s, lane, wlast, tb);
+            }
+        } else {
+            if (wleft) {
+                wave_fill<AFFINE, false, true>(v, active, R, Rw, G, s, lane, wlast, tb);
+            } else {
+                wave_fill<AFFINE, false, false>(v, active, R, Rw, G, s, lane, wlast, tb);
+            }
+        }
+        __syncwarp();
+        if (active && s == 0) {
+            struct SmemCodes {
+                const uint16_t *tb;
+                int base;
+                __device__ __forceinline__ uint32_t tb_get(int32_t st, int32_t i) const {
+                    return tb[size_t(i - 1) * 32u + base + st];
+                }
+            } sc{tb, g * G};
+            OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
+            DpSum sum;
+            dp_traceback<kStripW>(v, sc, w, sum);
+            w.flush();
+            a.sums[si] = sum;
+            if (a.cells) {
+                const uint64_t cl = band_cells(v.R, v.C, v.band);
+                a.cells[si] = uint32_t(cl > 0xffffffffull ? 0xffffffffull : cl);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// per-thread kernel for the segments wider than 32 strips (after the wavefront ranges)
+template <bool AFFINE>
+__global__ void __launch_bounds__(kDpThreads) k_dp_wide(DpLaunch a, const uint64_t *tasks) {
+    const uint64_t T = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    DevScratch sc{a.tb, a.bnd, T, a.rmax, t};
+    for (uint64_t idx = tasks[0] + t; idx < a.nd; idx += T) {
+        const uint32_t si = a.perm[idx];
+        const DpSeg g = a.segs[si];
+        const uint32_t orient = (g.flags >> kSegOrientShift) & 1u;
+        const SegView v = make_view(a.scode + a.soff[g.subj], int32_t(a.slen[g.subj]),
+                                    int32_t(orient), a.qcode + a.qoff[g.query], g.s0, g.s1, g.q0,
+                                    g.q1, g.flags & 3u, g.band);
+        dp_fill<kStripW, AFFINE>(v, sc);
         OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
         DpSum sum;
         dp_traceback<kStripW>(v, sc, w, sum);
@@ -815,7 +977,7 @@ __global__ void k_assemble(Params p, uint64_t nc, ChainArrays ch, const uint32_t
 // SubjectRead::addAlignment (SubjectRead.cpp:25-79): one record per (subject,
 // query); forward chains arrive before reverse-complement chains.
 __global__ void k_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
-                         const uint32_t *seg_chain_count, ChainArrays ch,
+                         const uint32_t *seg_chain_count, ChainArrays ch, uint32_t *winners,
                          unsigned long long *counters) {
     unsigned long long kept = 0;
     for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nsub;
@@ -836,6 +998,7 @@ __global__ void k_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
             while (j < je && ch.query[j] == qq) consider(j++);
             if (best >= 0) {
                 ch.win[best] = 1;
+                winners[atomicAdd(&counters[C_WIN], 1ull)] = uint32_t(best);
                 kept++;
             }
         }
@@ -845,44 +1008,53 @@ __global__ void k_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
 }
 
 // SubjectRead::updateQueryCoverage (SubjectRead.cpp:208-330): M votes the
-// query's own base, a mismatch votes the subject base, I/D only move.
+// query's own base, a mismatch votes the subject base, I/D only move.  Runs of
+// M are kept open across pieces and land as two difference-array updates.
 struct VoteVisitor {
     const uint8_t *sc;  // subject codes (forward)
     int32_t Ls, orient;
-    const uint8_t *qc;  // query codes
     int32_t Lq;
-    uint32_t *cov;      // query's rows of the vote matrix
+    uint32_t *cov;      // query's rows of the mismatch-vote matrix
+    int32_t *md;        // query's match-run difference array
     const uint32_t *ops;
     uint32_t stride;
     const DpSum *sums;
     uint32_t seg;       // segment index of the next DP piece
     int64_t ps = 0, pq = 0;
+    int64_t open = -1;  // start of the open match run
     unsigned long long anomalies = 0;
 
     __device__ __forceinline__ uint8_t subj_code(int64_t i) const {
         return orient ? uint8_t(sc[Ls - 1 - i] ^ 2u) : sc[i];
     }
-    __device__ __forceinline__ void vote(int64_t pos, uint8_t code) {
-        if (pos < 0 || pos >= Lq || code >= 4) {
-            anomalies++;
-            return;
+    __device__ __forceinline__ void close() {
+        if (open < 0) return;
+        int64_t e = pq;
+        if (e > Lq) {  // match votes past the read (the reference reads out of range)
+            anomalies += uint64_t(e - (open > Lq ? open : Lq));
+            e = Lq;
         }
-        atomicAdd(&cov[pos * 4 + code], 1u);
+        if (open < e) {
+            atomicAdd(&md[open], 1);
+            if (e < Lq) atomicAdd(&md[e], -1);
+        }
+        open = -1;
     }
-    __device__ __forceinline__ void one(uint8_t t) {
-        if (t == OP_I) {
-            pq++;
-        } else if (t == OP_D) {
-            ps++;
-        } else if (t == OP_M) {
-            vote(pq, pq < Lq ? qc[pq] : uint8_t(kBad));
-            pq++;
-            ps++;
+    __device__ __forceinline__ void match(int64_t c) {
+        if (open < 0) open = pq;
+        pq += c;
+        ps += c;
+    }
+    __device__ __forceinline__ void mismatch() {
+        close();
+        const uint8_t code = (ps >= 0 && ps < Ls) ? subj_code(ps) : uint8_t(kBad);
+        if (pq < 0 || pq >= Lq || code >= 4) {
+            anomalies++;
         } else {
-            vote(pq, (ps >= 0 && ps < Ls) ? subj_code(ps) : uint8_t(kBad));
-            pq++;
-            ps++;
+            atomicAdd(&cov[pq * 4 + code], 1u);
         }
+        pq++;
+        ps++;
     }
     __device__ void begin(int64_t, int64_t, int64_t) {}
     __device__ void position(int64_t p) {
@@ -890,44 +1062,65 @@ struct VoteVisitor {
         pq = 0;
     }
     __device__ void run(uint8_t t, int64_t c) {
-        if (t == OP_I) {
-            pq += c;
-        } else if (t == OP_D) {
-            ps += c;
+        if (t == OP_M) {
+            match(c);
         } else {
-            for (int64_t x = 0; x < c; x++) one(t);
+            close();
+            if (t == OP_I) {
+                pq += c;
+            } else {
+                ps += c;
+            }
         }
     }
     __device__ void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
         const DpSum s = sums[seg];
         const uint32_t P = uint32_t(s.tot[0]) + s.tot[1] + s.tot[2] + s.tot[3];
-        const uint32_t *w = ops + uint64_t(seg) * stride;
-        const uint32_t first = stride * 16u - P;
-        for (uint32_t t = 0; t < P; t++) {
-            const uint32_t pos = first + t;
-            one(uint8_t((w[pos >> 4] >> (2 * (pos & 15))) & 3u));
+        if (s.tot[OP_M] == P) {  // one match run
+            match(P);
+        } else {
+            const uint32_t *w = ops + uint64_t(seg) * stride;
+            const uint32_t first = stride * 16u - P;
+            for (uint32_t t = 0; t < P; t++) {
+                const uint32_t pos = first + t;
+                const uint8_t op = uint8_t((w[pos >> 4] >> (2 * (pos & 15))) & 3u);
+                if (op == OP_M) {
+                    match(1);
+                } else if (op == OP_X) {
+                    mismatch();
+                } else {
+                    close();
+                    if (op == OP_I) {
+                        pq++;
+                    } else {
+                        ps++;
+                    }
+                }
+            }
         }
         seg++;
     }
     __device__ bool check(int64_t, int64_t) { return true; }
-    __device__ void finish() {}
+    __device__ void finish() { close(); }
 };
 
-__global__ void k_vote(Params p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
-                       ReadsView subj, ReadsView q, const uint32_t *ops, uint32_t stride,
-                       const DpSum *sums, uint32_t *cov, unsigned long long *counters) {
+__global__ void k_vote(Params p, const unsigned long long *counters_in, ChainArrays ch,
+                       const uint32_t *winners, const uint32_t *keys, ReadsView subj, ReadsView q,
+                       const uint32_t *ops, uint32_t stride, const DpSum *sums, uint32_t *cov,
+                       int32_t *mdiff, unsigned long long *counters) {
     unsigned long long anomalies = 0;
-    for (uint64_t ci = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; ci < nc;
-         ci += uint64_t(gridDim.x) * blockDim.x) {
-        if (!ch.win[ci]) continue;
+    const uint64_t nw = counters_in[C_WIN];
+    for (uint64_t wi = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; wi < nw;
+         wi += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t ci = winners[wi];
         const uint32_t s = ch.subj[ci], qid = ch.query[ci];
         VoteVisitor v;
         v.sc = subj.code + subj.off[s];
         v.Ls = int32_t(subj.len[s]);
         v.orient = ch.orient[ci];
-        v.qc = q.code + q.off[qid];
         v.Lq = int32_t(q.len[qid]);
         v.cov = cov + q.off[qid] * 4;
+        v.md = mdiff + q.off[qid];
         v.ops = ops;
         v.stride = stride;
         v.sums = sums;
@@ -944,9 +1137,9 @@ __global__ void k_vote(Params p, uint64_t nc, ChainArrays ch, const uint32_t *ke
 // consensus: QueryRead::callConsensus + calculateCoverageStatistic
 // (QueryRead.cpp:148-212); one warp per query read
 // ---------------------------------------------------------------------------
-__global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, uint8_t *out,
-                            uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
-                            double *mis) {
+__global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, const int32_t *mdiff,
+                            uint8_t *out, uint32_t *colsum, uint32_t *imin, uint32_t *imed,
+                            uint32_t *imax, double *mis) {
     const uint32_t lane = lane_id();
     const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
     for (uint64_t r = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < q.n;
@@ -963,21 +1156,30 @@ __global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, uint8_t 
         const uint64_t b = q.off[r];
         const uint32_t L = q.len[r];
         uint32_t changed = 0, mn = 0xffffffffu, mx = 0;
-        for (uint32_t i = lane; i < L; i += 32) {
-            const uint8_t own = q.code[b + i];
-            uint32_t c[4];
-            for (int j = 0; j < 4; j++) c[j] = cov[(b + i) * 4 + j] + (own == j ? 1u : 0u);
-            const int32_t id = column_consensus(c, p.thr);
-            uint8_t nb = own;
-            if (id >= 0) {
-                if (uint8_t(id) != own) changed++;
-                nb = uint8_t(id);
+        int32_t carry = 0;  // match-run coverage entering the current chunk
+        for (uint32_t c0 = 0; c0 < L; c0 += 32) {
+            const uint32_t i = c0 + lane;
+            const int32_t d = i < L ? mdiff[b + i] : 0;
+            int32_t tot;
+            const int32_t run = carry + warp_exclusive<int32_t>(d, &tot) + d;
+            carry += tot;
+            if (i < L) {
+                const uint8_t own = q.code[b + i];
+                uint32_t c[4];
+                for (int j = 0; j < 4; j++) c[j] = cov[(b + i) * 4 + j];
+                c[own] += uint32_t(run) + 1u;  // match votes + the read's own vote
+                const int32_t id = column_consensus(c, p.thr);
+                uint8_t nb = own;
+                if (id >= 0) {
+                    if (uint8_t(id) != own) changed++;
+                    nb = uint8_t(id);
+                }
+                out[b + i] = uint8_t(code_base(nb));
+                const uint32_t sm = c[0] + c[1] + c[2] + c[3];
+                colsum[b + i] = sm;
+                mn = sm < mn ? sm : mn;
+                mx = sm > mx ? sm : mx;
             }
-            out[b + i] = uint8_t(code_base(nb));
-            const uint32_t sm = c[0] + c[1] + c[2] + c[3];
-            colsum[b + i] = sm;
-            mn = sm < mn ? sm : mn;
-            mx = sm > mx ? sm : mx;
         }
         changed = warp_sum(changed);
         mn = warp_min(mn);
@@ -1012,6 +1214,33 @@ __global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, uint8_t 
             imax[r] = mx;
             imed[r] = (L % 2 == 0) ? (v_hi + v_lo) / 2u : v_lo;
             mis[r] = __ddiv_rn(double(changed), double(L));
+        }
+    }
+}
+
+__global__ void k_expand_votes(ReadsView q, const uint32_t *cov, const int32_t *mdiff,
+                               uint32_t *out) {
+    const uint32_t lane = lane_id();
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t r = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < q.n;
+         r += warps) {
+        const uint64_t b = q.off[r];
+        const uint32_t L = q.len[r];
+        int32_t carry = 0;
+        for (uint32_t c0 = 0; c0 < L; c0 += 32) {
+            const uint32_t i = c0 + lane;
+            const int32_t d = i < L ? mdiff[b + i] : 0;
+            int32_t tot;
+            const int32_t run = carry + warp_exclusive<int32_t>(d, &tot) + d;
+            carry += tot;
+            if (i < L) {
+                const uint8_t own = q.code[b + i];
+                for (int j = 0; j < 4; j++) {
+                    uint32_t v = cov[(b + i) * 4 + j];
+                    if (j == own) v += uint32_t(run);
+                    out[(b + i) * 4 + j] = v;
+                }
+            }
         }
     }
 }
@@ -1146,15 +1375,44 @@ uint64_t dp_threads(int device) {
     return uint64_t(sms) * 8u * kDpThreads;
 }
 
-void launch_dp(const DpLaunch &a, cudaStream_t st) {
+bool dp_wave_fits(int32_t rmax) { return size_t(kWaveWarps) * size_t(rmax) * 64u <= 200u * 1024u; }
+
+void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int32_t cmax,
+               cudaStream_t st) {
     if (!a.nd) return;
-    const unsigned g = unsigned(a.threads / kDpThreads);
+    if (!dp_wave_fits(a.rmax)) {  // rows too long for the shared-memory codes
+        const unsigned g = unsigned(a.threads / kDpThreads);
+        counted();
+        if (a.affine) {
+            k_dp<true><<<g, kDpThreads, 0, st>>>(a);
+        } else {
+            k_dp<false><<<g, kDpThreads, 0, st>>>(a);
+        }
+        return;
+    }
+    counted();
+    k_dp_tasks<<<1, 32, 0, st>>>(bin_off, tasks);
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = size_t(kWaveWarps) * size_t(a.rmax) * 64u;
+    const unsigned g = unsigned(sms) * 8u;
+    counted();
     if (a.affine) {
-        counted();
-        k_dp<true><<<g, kDpThreads, 0, st>>>(a);
+        cudaFuncSetAttribute(k_dp_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_dp_wave<true><<<g, kWaveWarps * 32, smem, st>>>(a, tasks);
     } else {
+        cudaFuncSetAttribute(k_dp_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        k_dp_wave<false><<<g, kWaveWarps * 32, smem, st>>>(a, tasks);
+    }
+    if (cmax > 32 * kStripW) {
+        const unsigned gw = unsigned(a.threads / kDpThreads);
         counted();
-        k_dp<false><<<g, kDpThreads, 0, st>>>(a);
+        if (a.affine) {
+            k_dp_wide<true><<<gw, kDpThreads, 0, st>>>(a, tasks);
+        } else {
+            k_dp_wide<false><<<gw, kDpThreads, 0, st>>>(a, tasks);
+        }
     }
 }
 
@@ -1168,30 +1426,40 @@ void launch_assemble(const Params &p, uint64_t nc, ChainArrays ch, const uint32_
 }
 
 void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
-                   const uint32_t *seg_chain_count, ChainArrays ch, unsigned long long *counters,
-                   cudaStream_t st) {
+                   const uint32_t *seg_chain_count, ChainArrays ch, uint32_t *winners,
+                   unsigned long long *counters, cudaStream_t st) {
     if (nsub) {
         counted();
-        k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch, counters);
+        k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch,
+                                                     winners, counters);
     }
 }
 
-void launch_vote(const Params &p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
-                 ReadsView subj, ReadsView q, const DpSeg *, const uint32_t *ops,
-                 uint32_t stride, const DpSum *sums, uint32_t *cov, unsigned long long *counters,
-                 cudaStream_t st) {
-    if (nc) {
-        counted();
-        k_vote<<<grid_1d(nc, 128), 128, 0, st>>>(p, nc, ch, keys, subj, q, ops, stride, sums, cov, counters);
-    }
+void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,
+                 const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
+                 uint32_t stride, const DpSum *sums, uint32_t *cov, int32_t *mdiff,
+                 unsigned long long *counters, cudaStream_t st) {
+    if (!max_winners) return;
+    counted();
+    k_vote<<<grid_1d(max_winners, 128), 128, 0, st>>>(p, counters, ch, winners, keys, subj, q, ops,
+                                                      stride, sums, cov, mdiff, counters);
 }
 
-void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, uint8_t *out,
-                      uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax,
-                      double *mis, cudaStream_t st) {
+void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, const int32_t *mdiff,
+                      uint8_t *out, uint32_t *colsum, uint32_t *imin, uint32_t *imed,
+                      uint32_t *imax, double *mis, cudaStream_t st) {
     if (q.n) {
         counted();
-        k_consensus<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(p, q, cov, out, colsum, imin, imed, imax, mis);
+        k_consensus<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(p, q, cov, mdiff, out, colsum,
+                                                                 imin, imed, imax, mis);
+    }
+}
+
+void launch_expand_votes(ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint32_t *out,
+                         cudaStream_t st) {
+    if (q.n) {
+        counted();
+        k_expand_votes<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(q, cov, mdiff, out);
     }
 }
 

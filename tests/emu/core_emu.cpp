@@ -39,9 +39,9 @@ int run_dp(const SegView &v, bool affine, std::vector<uint8_t> &ops, DpSum &sum)
     HostScratch<W> sc;
     sc.reset(v.R, v.C);
     if (affine) {
-        dp_fill_affine<W>(v, sc);
+        dp_fill<W, true>(v, sc);
     } else {
-        dp_fill_global<W>(v, sc);
+        dp_fill<W, false>(v, sc);
     }
     std::vector<uint8_t> rev;
     auto emit = [&](uint8_t op) { rev.push_back(op); };
@@ -215,6 +215,80 @@ int emu_align(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query,
     int n = strip16 ? run_dp<16>(v, affine != 0, out, sum) : run_dp<8>(v, affine != 0, out, sum);
     if (n > cap) return -1;
     std::memcpy(ops, out.data(), out.size());
+    return n;
+}
+
+// one DP segment through the warp-wavefront schedule of k_dp_wave: lane s owns
+// strip s and computes row t - s + 1 at step t; the left boundary of a row is
+// what lane s-1 published one step earlier.  Lanes are simulated in order.
+int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query, int32_t lq,
+                   int64_t band, int align_right, int align_left, uint8_t *ops, int32_t cap) {
+    constexpr int W = 8;
+    std::vector<uint8_t> scd(ls), qcd(lq);
+    for (int i = 0; i < ls; i++) scd[i] = base_code(subj[i]);
+    for (int i = 0; i < lq; i++) qcd[i] = base_code(query[i]);
+    uint32_t flags = (align_right ? DPF_RIGHT : 0) | (align_left ? DPF_LEFT : 0);
+    SegView v = make_view(scd.data(), ls, 0, qcd.data(), 0, ls, 0, lq, flags, band);
+    const int G = (v.C + W - 1) / W;
+    struct Lane {
+        uint8_t bc[W];
+        int32_t uf[W], ux[W], uy[W];
+        bool full;
+        int32_t wlast;
+        Cell3 prev, pub;
+    };
+    std::vector<Lane> L(G);
+    std::vector<uint16_t> tb(size_t(v.R) * 32, 0);
+    for (int s = 0; s < G; s++) {
+        if (affine) {
+            dp_strip_init<W, true>(v, s * W, L[s].bc, L[s].uf, L[s].ux, L[s].uy);
+            L[s].prev = dp_row0<true>(v, s * W);
+        } else {
+            dp_strip_init<W, false>(v, s * W, L[s].bc, L[s].uf, L[s].ux, L[s].uy);
+            L[s].prev = dp_row0<false>(v, s * W);
+        }
+        L[s].full = dp_strip_full(v, s * W, W);
+        L[s].wlast = dp_strip_wlast(v, s * W, W);
+        L[s].pub = Cell3{kNEG, kNEG, kNEG};
+    }
+    for (int t = 0; t < v.R + G - 1; t++) {
+        std::vector<Cell3> in(G);
+        for (int s = 0; s < G; s++) in[s] = s > 0 ? L[s - 1].pub : Cell3{0, 0, 0};  // shfl_up
+        for (int s = 0; s < G; s++) {
+            const int i = t - s + 1;
+            if (i < 1 || i > v.R) continue;
+            Lane &x = L[s];
+            Cell3 left, dg;
+            if (affine) {
+                left = s == 0 ? dp_col0<true>(v, i) : in[s];
+                dg = s == 0 ? dp_col0<true>(v, i - 1) : x.prev;
+            } else {
+                left = s == 0 ? dp_col0<false>(v, i) : in[s];
+                dg = s == 0 ? dp_col0<false>(v, i - 1) : x.prev;
+            }
+            const Cell3 lb = left;
+            const uint8_t ch = v.row(i);
+            uint32_t bits;
+            if (affine) {
+                bits = dp_strip_row_any<W, true>(x.full, x.wlast, v, i, s * W, ch, x.bc, x.uf, x.ux, x.uy, left, dg);
+            } else {
+                bits = dp_strip_row_any<W, false>(x.full, x.wlast, v, i, s * W, ch, x.bc, x.uf, x.ux, x.uy, left, dg);
+            }
+            tb[size_t(i - 1) * 32 + s] = uint16_t(bits);
+            x.pub = left;
+            x.prev = lb;
+        }
+    }
+    struct Codes {
+        const uint16_t *tb;
+        uint32_t tb_get(int32_t st, int32_t i) const { return tb[size_t(i - 1) * 32 + st]; }
+    } sc{tb.data()};
+    std::vector<uint8_t> rev;
+    auto emit = [&](uint8_t op) { rev.push_back(op); };
+    DpSum sum;
+    const int n = dp_traceback<W>(v, sc, emit, sum);
+    if (n > cap) return -1;
+    for (int i = 0; i < n; i++) ops[i] = rev[n - 1 - i];
     return n;
 }
 

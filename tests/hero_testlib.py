@@ -139,6 +139,8 @@ class Emu:
         vp = C.c_void_p
         lib.emu_align.argtypes = [C.c_int, vp, C.c_int32, vp, C.c_int32, C.c_int64, C.c_int,
                                   C.c_int, C.c_int, vp, C.c_int32]
+        lib.emu_align_wave.argtypes = [C.c_int, vp, C.c_int32, vp, C.c_int32, C.c_int64, C.c_int,
+                                       C.c_int, vp, C.c_int32]
         lib.emu_correct.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                      C.c_double, C.c_uint64] + [vp] * 11)
         self.lib = lib
@@ -149,6 +151,14 @@ class Emu:
         ops = np.zeros(len(s) + len(q) + 1, np.uint8)
         n = self.lib.emu_align(int(affine), _vp(s), len(s), _vp(q), len(q), int(band), int(right),
                                int(left), int(strip16), _vp(ops), len(ops))
+        return ops[:n].copy()
+
+    def align_wave(self, affine, subj: bytes, query: bytes, band, right=False, left=False):
+        s = np.frombuffer(subj, np.uint8).copy()
+        q = np.frombuffer(query, np.uint8).copy()
+        ops = np.zeros(len(s) + len(q) + 1, np.uint8)
+        n = self.lib.emu_align_wave(int(affine), _vp(s), len(s), _vp(q), len(q), int(band),
+                                    int(right), int(left), _vp(ops), len(ops))
         return ops[:n].copy()
 
     def correct(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,

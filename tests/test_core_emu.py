@@ -32,6 +32,8 @@ def test_dp_random_segments(oracle, emu, affine):
         for strip16 in (False, True):
             got = emu.align(affine, s, q, band, right, left, strip16)
             assert np.array_equal(want, got), (affine, s, q, band, right, left, strip16)
+        got = emu.align_wave(affine, s, q, band, right, left)
+        assert np.array_equal(want, got), (affine, s, q, band, right, left, "wave")
 
 
 def test_dp_edge_shapes(oracle, emu):
@@ -45,6 +47,8 @@ def test_dp_edge_shapes(oracle, emu):
                         want, _ = oracle.align(affine, s, q, band, right, left)
                         got = emu.align(affine, s, q, band, right, left)
                         assert np.array_equal(want, got), (affine, s, q, band, right, left)
+                        got = emu.align_wave(affine, s, q, band, right, left)
+                        assert np.array_equal(want, got), (affine, s, q, band, right, left, "wave")
 
 
 @pytest.mark.parametrize("name", ["c1_20k", "c1_20k_narrow", "mix_affine", "mix_k21_l60",
