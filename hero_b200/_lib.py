@@ -24,7 +24,7 @@ EXPORTS = [
     "hero_default_params", "hero_create", "hero_destroy", "hero_last_error",
     "hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
     "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments",
-    "hero_reset_votes",
+    "hero_reset_votes", "hero_align_segments_noalloc",
 ]
 
 

@@ -133,6 +133,31 @@ int hero_align_segments(hero_ctx *ctx, int affine, const uint8_t *subj, const ui
                         const int32_t *q1, const uint8_t *seg_flags, const int64_t *band,
                         const uint64_t *ops_off, uint8_t *ops, int32_t *nops);
 
+/* Allocation-free form of hero_align_segments, for callers that cannot
+ * allocate device memory (code inside a host framework that owns the GPU's
+ * allocator, or a fixed memory plan that forbids new allocations).  It has no
+ * counterpart in the reference.  Every pointer is caller-owned DEVICE memory:
+ * the reads as uppercase ASCII with their offsets, the per-segment arrays of
+ * hero_align_segments, ops_off/ops/nops for the results (ops per step, 0=M
+ * 1=X 2=I 3=D, first to last, at ops_off[i]).  It needs no context, calls no
+ * cudaMalloc/cudaFree and uses one fixed working array of about 48 MB that the
+ * library keeps on every device where it has run, until the process exits.
+ * Limits: max_side (the caller's bound on either side of any segment) must be
+ * 1..128, else HERO_E_INPUT before any launch; a segment beyond 128 on a side,
+ * outside its read or with too little ops room gets nops[i] = -1 and the call
+ * returns HERO_E_INPUT.  The first call on a device looks up the working
+ * array's address: make it before any stream capture.  Calls share the array,
+ * so calls that overlap on the GPU (other streams, other host threads) race;
+ * the call runs on `stream` and returns after it has completed. */
+int hero_align_segments_noalloc(int affine, const uint8_t *subj, const uint64_t *subj_off,
+                                uint64_t n_subj, const uint8_t *query, const uint64_t *query_off,
+                                uint64_t n_query, uint64_t n_seg, const uint32_t *seg_subject,
+                                const uint8_t *seg_orient, const uint32_t *seg_query,
+                                const int32_t *s0, const int32_t *s1, const int32_t *q0,
+                                const int32_t *q1, const uint8_t *seg_flags, const int64_t *band,
+                                int32_t max_side, const uint64_t *ops_off, uint8_t *ops,
+                                int32_t *nops, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
