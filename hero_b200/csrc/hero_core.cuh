@@ -699,15 +699,13 @@ HERO_HD void dp_fill(const SegView &v, Scratch &sc) {
 }
 
 // Traceback (BandAligner.cpp:114-125 / 227-238) from (R, C) to (0, 0).
-// emit(op) receives ops last-to-first.  Fills the path summary.
+// emit(op) receives ops last-to-first; returns the path length.
 template <int W, class Scratch, class Emit>
-HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &sum) {
-    int32_t i = v.R, j = v.C, nops = 0;
-    uint64_t tot = 0;  // four 16-bit op counters (path length < 65536)
-    uint32_t cur = 0xffu, cc = 0, lt = 0, lc = 0;
-    int32_t nr = 0;
-    const uint32_t op_up = v.reversed ? OP_I : OP_D;
-    const uint32_t op_left = v.reversed ? OP_D : OP_I;
+HERO_HD int32_t dp_walk(const SegView &v, const Scratch &sc, Emit &emit) {
+    int32_t i = v.R, j = v.C, n = 0;
+    // op of each move: up, left, diagonal mismatch, diagonal match
+    const uint32_t lut = uint32_t(v.reversed ? OP_I : OP_D) | (uint32_t(v.reversed ? OP_D : OP_I) << 2) |
+                         (uint32_t(OP_X) << 4) | (uint32_t(OP_M) << 6);
     while (i > 0 || j > 0) {
         uint32_t code;
         if (i == 0) {
@@ -717,20 +715,99 @@ HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &s
         } else {
             code = (sc.tb_get((j - 1) / W, i) >> (2 * ((j - 1) % W))) & 3u;
         }
-        uint32_t op;
+        uint32_t sel;
         if (code == 2) {
-            op = v.row(i) == v.col(j) ? OP_M : OP_X;
+            sel = v.row(i) == v.col(j) ? 3u : 2u;
             i--;
             j--;
         } else if (code == 1) {
-            op = op_left;
+            sel = 1;
             j--;
         } else {
-            op = op_up;
+            sel = 0;
             i--;
         }
-        emit(uint8_t(op));
-        nops++;
+        emit(uint8_t((lut >> (2 * sel)) & 3u));
+        n++;
+    }
+    return n;
+}
+
+// DpSum of the ops at positions [first, first + P) of a packed op array (16
+// ops per word, op at position p in word p / 16, bits 2 (p % 16)), by counting
+// 2-bit fields a word at a time.
+HERO_HD uint32_t ops_field(const uint32_t *w, uint32_t p) { return (w[p >> 4] >> (2 * (p & 15))) & 3u; }
+
+HERO_HD uint32_t ops_mask(uint32_t lo, uint32_t hi) {  // 0x55.. pattern over fields lo..hi
+    return 0x55555555u & (0xffffffffu << (2 * lo)) & (0xffffffffu >> (30 - 2 * hi));
+}
+
+HERO_HD int32_t popc32(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __popc(x);
+#else
+    return __builtin_popcount(x);
+#endif
+}
+
+HERO_HD void ops_summary(const uint32_t *w, uint32_t first, uint32_t P, DpSum &sum) {
+    const uint32_t end = first + P, k0 = first >> 4, k1 = (end - 1) >> 4;
+    int32_t c1 = 0, c2 = 0, c3 = 0;
+    for (uint32_t k = k0; k <= k1; k++) {
+        const uint32_t m = ops_mask(k == k0 ? (first & 15) : 0, k == k1 ? ((end - 1) & 15) : 15);
+        const uint32_t x = w[k], xl = x & 0x55555555u, xh = (x >> 1) & 0x55555555u;
+        c1 += popc32(xl & ~xh & m);
+        c2 += popc32(xh & ~xl & m);
+        c3 += popc32(xl & xh & m);
+    }
+    sum.tot[0] = uint16_t(int32_t(P) - c1 - c2 - c3);
+    sum.tot[1] = uint16_t(c1);
+    sum.tot[2] = uint16_t(c2);
+    sum.tot[3] = uint16_t(c3);
+    // first run: fields equal to the first op, from `first` on
+    const uint32_t f = ops_field(w, first);
+    uint32_t fc = P;
+    for (uint32_t k = k0; k <= k1; k++) {
+        const uint32_t m = ops_mask(k == k0 ? (first & 15) : 0, k == k1 ? ((end - 1) & 15) : 15);
+        const uint32_t y = w[k] ^ (f * 0x55555555u);
+        const uint32_t z = (y | (y >> 1)) & m;
+        if (z) {
+            int32_t bit = 0;
+            while (!((z >> bit) & 1u)) bit++;
+            fc = (k << 4) + uint32_t(bit >> 1) - first;
+            break;
+        }
+    }
+    // last run: fields equal to the last op, backwards from end - 1
+    const uint32_t l = ops_field(w, end - 1);
+    uint32_t lc = P;
+    for (uint32_t k = k1 + 1; k-- > k0;) {
+        const uint32_t m = ops_mask(k == k0 ? (first & 15) : 0, k == k1 ? ((end - 1) & 15) : 15);
+        const uint32_t y = w[k] ^ (l * 0x55555555u);
+        const uint32_t z = (y | (y >> 1)) & m;
+        if (z) {
+            int32_t bit = 31;
+            while (!((z >> bit) & 1u)) bit--;
+            lc = end - 1 - ((k << 4) + uint32_t(bit >> 1));
+            break;
+        }
+    }
+    sum.ft = uint8_t(f);
+    sum.fc = uint16_t(fc);
+    sum.lt = uint8_t(l);
+    sum.lc = uint16_t(lc);
+    sum.nruns = fc == P ? 1 : 2;
+    sum.pad = 0;
+}
+
+// walk + per-op run tracking, for callers that emit ops one by one
+template <int W, class Scratch, class Emit>
+HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &sum) {
+    uint64_t tot = 0;  // four 16-bit op counters (path length < 65536)
+    uint32_t cur = 0xffu, cc = 0, lt = 0, lc = 0;
+    int32_t nr = 0;
+    auto track = [&](uint8_t op) {
+        emit(op);
         tot += 1ull << (16 * op);
         if (op == cur) {
             cc++;
@@ -745,7 +822,8 @@ HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &s
             cur = op;
             cc = 1;
         }
-    }
+    };
+    const int32_t nops = dp_walk<W>(v, sc, track);
     // the run open at the end of the walk is the first run of the path
     sum.ft = uint8_t(cur);
     sum.fc = uint16_t(cc);

@@ -866,10 +866,12 @@ __global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
                     return tb[size_t(i - 1) * 32u + base + st];
                 }
             } sc{tb, g * G};
-            OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
-            DpSum sum;
-            dp_traceback<kStripW>(v, sc, w, sum);
+            uint32_t *words = a.ops + uint64_t(si) * a.stride;
+            OpsWriter w{words, int32_t(a.stride * 16u)};
+            const int32_t n = dp_walk<kStripW>(v, sc, w);
             w.flush();
+            DpSum sum;
+            ops_summary(words, a.stride * 16u - uint32_t(n), uint32_t(n), sum);
             a.sums[si] = sum;
             if (a.cells) {
                 const uint64_t cl = band_cells(v.R, v.C, v.band);

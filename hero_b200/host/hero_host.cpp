@@ -1,0 +1,343 @@
+// hero_host.cpp -- host side of the drop-in (see hero_host.h).
+#include "hero_host.h"
+
+#include <cctype>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+
+namespace herohost {
+
+// ---------------------------------------------------------------------------
+// Config::setConfig (Config.cpp:118-243); flags outside the consensus path are
+// refused with a message instead of being silently ignored.
+// ---------------------------------------------------------------------------
+void Config::help() {
+    std::cout << "Usage: hero_b200 -q <query[,query...]> -s <subject[,subject...]> -c [thr]\n"
+                 "  -o/--out      output prefix (default: query) -> <out>.fasta, <out>.info\n"
+                 "  -c [thr]      call the consensus (default threshold 0.6)\n"
+                 "  --covinfo     write <out>.info (coverage min/median/max, rates)\n"
+                 "  --singleReads inputs are unpaired reads\n"
+                 "  -k            k-mer length (default 39, at most 63)\n"
+                 "  -m / -i       maximum mismatch / indel rate in percent (default 100)\n"
+                 "  -l            minimum overlap length (default 40)\n"
+                 "  -a a|g        affine or global aligner (default g)\n"
+                 "  -t -y -z -f   accepted for compatibility (host threads, chunk sizes, table factor)\n"
+                 "  --device N    CUDA device; --batch N subject reads per device batch\n";
+}
+
+bool Config::parse(int argc, char **argv) {
+    auto split = [](const std::string &s, std::vector<std::string> &out) {
+        std::stringstream ss(s);
+        std::string item;
+        while (std::getline(ss, item, ',')) out.push_back(item);
+    };
+    if (argc <= 1) {
+        help();
+        return false;
+    }
+    for (int i = 1; i < argc; i++) {
+        const std::string a = argv[i];
+        auto next = [&](std::string &v) -> bool {
+            if (i + 1 >= argc) {
+                std::cerr << "missing value after " << a << "\n";
+                return false;
+            }
+            v = argv[++i];
+            return true;
+        };
+        std::string v;
+        if (a == "-h" || a == "--help") {
+            help();
+            return false;
+        } else if (a == "-s" || a == "--subject") {
+            if (!next(v)) return false;
+            split(v, subject_files);
+        } else if (a == "-q" || a == "--query") {
+            if (!next(v)) return false;
+            split(v, query_files);
+        } else if (a == "-o" || a == "--out") {
+            if (!next(v)) return false;
+            out = v;
+            // a trailing ".aln" is dropped (Config.cpp:213-221 intends this)
+            if (out.size() >= 4 && out.compare(out.size() - 4, 4, ".aln") == 0)
+                out = out.substr(0, out.size() - 4);
+        } else if (a == "-k") {
+            if (!next(v)) return false;
+            k = std::atoi(v.c_str());
+        } else if (a == "-m") {
+            if (!next(v)) return false;
+            mis_rate = std::atof(v.c_str()) / 100.0;
+        } else if (a == "-i") {
+            if (!next(v)) return false;
+            indel_rate = std::atof(v.c_str()) / 100.0;
+        } else if (a == "-l") {
+            if (!next(v)) return false;
+            min_overlap = std::atoi(v.c_str());
+        } else if (a == "-t") {
+            if (!next(v)) return false;
+            threads = std::atoi(v.c_str());
+        } else if (a == "-z") {
+            if (!next(v)) return false;
+            stream_chunk = std::strtoull(v.c_str(), nullptr, 10);
+        } else if (a == "-y") {
+            if (!next(v)) return false;
+            query_chunk = std::strtoull(v.c_str(), nullptr, 10);
+        } else if (a == "-f") {
+            if (!next(v)) return false;  // table size factor: the device table sizes itself
+        } else if (a == "-a") {
+            if (!next(v)) return false;
+            if (v == "a") affine = true;
+            if (v == "g") affine = false;
+        } else if (a == "-c") {
+            consensus = true;
+            if (i + 1 < argc && argv[i + 1][0] >= '0' && argv[i + 1][0] <= '9')
+                consensus_thr = std::atof(argv[++i]);
+        } else if (a == "--covinfo") {
+            covinfo = true;
+        } else if (a == "--singleReads") {
+            single_reads = true;
+        } else if (a == "--device") {
+            if (!next(v)) return false;
+            device = std::atoi(v.c_str());
+        } else if (a == "--batch") {
+            if (!next(v)) return false;
+            subject_batch = uint32_t(std::strtoul(v.c_str(), nullptr, 10));
+        } else if (a == "-v" || a == "--mapping" || a == "--merge" || a == "--covfilter" ||
+                   a == "--suffix" || a == "--size" || a == "--notification") {
+            std::cerr << a << ": not part of the consensus path this build replaces\n";
+            return false;
+        } else {
+            std::cerr << "unknown flag " << a << "\n";
+            help();
+            return false;
+        }
+    }
+    if (subject_files.empty() || query_files.empty()) {
+        std::cerr << "missed -subject or -query input files!\n";
+        return false;
+    }
+    if (!consensus) {
+        std::cerr << "only the consensus mode (-c) is provided; the .aln alignment output is not\n";
+        return false;
+    }
+    if (k < 1 || k > 63) {
+        std::cerr << "-k must be in 1..63\n";
+        return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// read loading (QueryDataset.cpp:103-244): FASTQ = four lines per read, FASTA =
+// header line then everything up to the next '>' with newlines removed; names
+// lose a leading '>' or '@'; bases are upper-cased; id = atoi(name).
+// ---------------------------------------------------------------------------
+bool load_reads(const std::string &path, ReadSet &out, std::string *err) {
+    std::ifstream f(path.c_str(), std::ios::binary);
+    if (!f.is_open()) {
+        if (err) *err = "Unable to open file: " + path;
+        return false;
+    }
+    std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    if (data.empty()) return true;
+    const bool fasta = data[0] == '>';
+    if (!fasta && data[0] != '@') {
+        if (err) *err = "Unknown input file format: " + path;
+        return false;
+    }
+    size_t p = 0;
+    const size_t n = data.size();
+    auto line = [&](std::string_view &v) -> bool {
+        if (p >= n) return false;
+        size_t e = data.find('\n', p);
+        if (e == std::string::npos) e = n;
+        v = std::string_view(data.data() + p, e - p);
+        p = e < n ? e + 1 : n;
+        return true;
+    };
+    auto add = [&](std::string_view name, const char *s, size_t len, bool skip_newlines) {
+        if (!name.empty() && (name[0] == '>' || name[0] == '@')) name.remove_prefix(1);
+        std::string nm(name);
+        out.uid.push_back(int64_t(std::atoi(nm.c_str())));
+        for (size_t i = 0; i < len; i++) {
+            const char c = s[i];
+            if (skip_newlines && c == '\n') continue;
+            out.seq.push_back(char(std::toupper(static_cast<unsigned char>(c))));
+        }
+        out.off.push_back(out.seq.size());
+    };
+    if (!fasta) {
+        std::string_view l0, l1, l2, l3;
+        while (line(l0)) {
+            if (!line(l1)) {
+                if (!l0.empty()) {  // a lone header line at the end
+                    if (err) *err = "truncated FASTQ record in " + path;
+                    return false;
+                }
+                break;
+            }
+            line(l2);
+            line(l3);
+            if (l0.empty() && l1.empty()) continue;  // trailing blank lines
+            add(l0, l1.data(), l1.size(), false);
+        }
+    } else {
+        while (p < n) {
+            std::string_view l0;
+            line(l0);
+            size_t e = data.find('>', p);
+            if (e == std::string::npos) e = n;
+            const size_t b = p;
+            p = e < n ? e + 1 : n;
+            if (l0.empty() && e == b) continue;  // blank trailing record
+            add(l0, data.data() + b, e - b, true);
+        }
+    }
+    return true;
+}
+
+bool QueryDataset::build(const Config &c, std::string *err) {
+    for (const std::string &path : c.query_files)
+        if (!load_reads(path, reads, err)) return false;
+    return true;
+}
+
+bool QueryDataset::write(const Config &c, std::string *err) const {
+    const uint64_t n = reads.n();
+    if (!c.single_reads && (n % 2)) {
+        if (err) *err = "an odd number of reads needs --singleReads (the paired writer reads past the end)";
+        return false;
+    }
+    // both files are opened in append mode, as the reference does
+    std::ofstream fa((c.out + ".fasta").c_str(), std::ios_base::app);
+    if (!fa.is_open()) {
+        if (err) *err = "cannot write " + c.out + ".fasta";
+        return false;
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        fa << ">" << reads.uid[i] << std::endl;
+        fa.write(corrected.data() + reads.off[i], std::streamsize(reads.off[i + 1] - reads.off[i]));
+        fa << std::endl;
+    }
+    fa.close();
+    if (c.covinfo) {
+        std::ofstream fi((c.out + ".info").c_str(), std::ios_base::app);
+        if (!fi.is_open()) {
+            if (err) *err = "cannot write " + c.out + ".info";
+            return false;
+        }
+        for (uint64_t i = 0; i < n; i++) {
+            fi << reads.uid[i] << "\t" << imin[i] << "\t" << imed[i] << "\t" << imax[i] << "\t"
+               << (reads.off[i + 1] - reads.off[i]) << "\t" << mismatch_rate[i] << "\t" << gc[i]
+               << std::endl;
+        }
+    }
+    return true;
+}
+
+bool SubjectDataset::next(ReadSet &chunk, std::string *err) {
+    chunk = ReadSet();
+    // large chunks: the device batches internally; the result does not depend
+    // on the chunking (votes commute)
+    const uint64_t want = 4u << 20;
+    while (chunk.n() < want) {
+        if (!loaded || pos >= cur.n()) {
+            if (file >= cfg.subject_files.size()) break;
+            cur = ReadSet();
+            if (!load_reads(cfg.subject_files[file++], cur, err)) return false;
+            pos = 0;
+            loaded = true;
+            continue;
+        }
+        const uint64_t take = std::min<uint64_t>(want - chunk.n(), cur.n() - pos);
+        const uint64_t b = cur.off[pos], e = cur.off[pos + take];
+        chunk.seq.append(cur.seq, b, e - b);
+        for (uint64_t i = 0; i < take; i++) {
+            chunk.uid.push_back(cur.uid[pos + i]);
+            chunk.off.push_back(chunk.off.back() + (cur.off[pos + i + 1] - cur.off[pos + i]));
+        }
+        pos += take;
+    }
+    return true;
+}
+
+static bool ok(hero_ctx *ctx, int rc, const char *what, std::string *err) {
+    if (rc == HERO_OK) return true;
+    if (err) *err = std::string(what) + ": " + (ctx ? hero_last_error(ctx) : "") +
+                    " (status " + std::to_string(rc) + ")";
+    return false;
+}
+
+bool HashTableGpu::createHashTables(const Config &c, QueryDataset *q, std::string *err) {
+    dataSet = q;
+    hero_params p;
+    hero_default_params(&p);
+    p.k = c.k;
+    p.min_overlap = c.min_overlap;
+    p.aligner = c.affine ? HERO_ALIGNER_AFFINE : HERO_ALIGNER_GLOBAL;
+    p.max_mismatch_rate = c.mis_rate;
+    p.max_indel_rate = c.indel_rate;
+    p.consensus_threshold = c.consensus_thr;
+    p.device = c.device;
+    p.subject_batch = c.subject_batch;
+    if (!ok(nullptr, hero_create(&p, &ctx), "hero_create", err)) return false;
+    const ReadSet &r = q->reads;
+    return ok(ctx, hero_set_queries(ctx, reinterpret_cast<const uint8_t *>(r.seq.data()),
+                                    r.off.data(), r.uid.data(), r.n()),
+              "hero_set_queries", err);
+}
+
+bool HashTableGpu::insertQueryDataset(std::string *err) {
+    return ok(ctx, hero_build_index(ctx), "hero_build_index", err);
+}
+
+HashTableGpu::~HashTableGpu() {
+    if (ctx) hero_destroy(ctx);
+}
+
+bool SubjectReadAligner::start(const Config &c, std::string *err) {
+    using clk = std::chrono::steady_clock;
+    if (c.subject_files == c.query_files) {  // -q X -s X: the resident query set
+        const auto t0 = clk::now();
+        const bool r = ok(table->ctx, hero_align_self(table->ctx), "hero_align_self", err);
+        seconds_aligning += std::chrono::duration<double>(clk::now() - t0).count();
+        return r;
+    }
+    SubjectDataset sd(c);
+    ReadSet chunk;
+    while (true) {
+        const auto t0 = clk::now();
+        if (!sd.next(chunk, err)) return false;
+        seconds_loading += std::chrono::duration<double>(clk::now() - t0).count();
+        if (chunk.n() == 0) break;
+        const auto t1 = clk::now();
+        if (!ok(table->ctx, hero_align_subjects(table->ctx,
+                                                reinterpret_cast<const uint8_t *>(chunk.seq.data()),
+                                                chunk.off.data(), chunk.uid.data(), chunk.n()),
+                "hero_align_subjects", err))
+            return false;
+        seconds_aligning += std::chrono::duration<double>(clk::now() - t1).count();
+    }
+    return true;
+}
+
+bool call_consensus(HashTableGpu &t, QueryDataset &q, std::string *err) {
+    const uint64_t n = q.reads.n();
+    q.corrected.assign(q.reads.seq.size(), 0);
+    q.imin.assign(n, 0);
+    q.imed.assign(n, 0);
+    q.imax.assign(n, 0);
+    q.mismatch_rate.assign(n, 0);
+    q.gc.assign(n, 0);
+    return ok(t.ctx, hero_consensus(t.ctx, reinterpret_cast<uint8_t *>(&q.corrected[0]),
+                                    q.imin.data(), q.imed.data(), q.imax.data(),
+                                    q.mismatch_rate.data(), q.gc.data(), nullptr),
+              "hero_consensus", err);
+}
+
+}  // namespace herohost

@@ -283,12 +283,33 @@ int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *q
         const uint16_t *tb;
         uint32_t tb_get(int32_t st, int32_t i) const { return tb[size_t(i - 1) * 32 + st]; }
     } sc{tb.data()};
-    std::vector<uint8_t> rev;
-    auto emit = [&](uint8_t op) { rev.push_back(op); };
+    // packed words written back to front, as the kernel's OpsWriter does
+    const uint32_t words = uint32_t((v.R + v.C + 15) / 16);
+    std::vector<uint32_t> wv(words + 1, 0);
+    int32_t p = int32_t(words * 16);
+    auto emit = [&](uint8_t op) {
+        p--;
+        wv[p >> 4] |= uint32_t(op) << (2 * (p & 15));
+    };
+    const int n = dp_walk<W>(v, sc, emit);
     DpSum sum;
-    const int n = dp_traceback<W>(v, sc, emit, sum);
+    ops_summary(wv.data(), words * 16 - uint32_t(n), uint32_t(n), sum);
+    // cross-check the word-level summary against per-op counting
+    uint32_t tot[4] = {0, 0, 0, 0};
+    for (int i = 0; i < n; i++) tot[ops_field(wv.data(), words * 16 - n + i)]++;
+    for (int t = 0; t < 4; t++)
+        if (tot[t] != sum.tot[t]) return -2;
+    const uint32_t f0 = ops_field(wv.data(), words * 16 - n);
+    uint32_t fc = 0;
+    while (int(fc) < n && ops_field(wv.data(), words * 16 - n + fc) == f0) fc++;
+    const uint32_t l0 = ops_field(wv.data(), words * 16 - 1);
+    uint32_t lc = 0;
+    while (int(lc) < n && ops_field(wv.data(), words * 16 - 1 - lc) == l0) lc++;
+    if (sum.ft != f0 || sum.fc != fc || sum.lt != l0 || sum.lc != lc ||
+        sum.nruns != (int(fc) == n ? 1 : 2))
+        return -3;
     if (n > cap) return -1;
-    for (int i = 0; i < n; i++) ops[i] = rev[n - 1 - i];
+    for (int i = 0; i < n; i++) ops[i] = uint8_t(ops_field(wv.data(), words * 16 - n + i));
     return n;
 }
 
