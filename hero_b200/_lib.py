@@ -24,7 +24,7 @@ EXPORTS = [
     "hero_default_params", "hero_create", "hero_destroy", "hero_last_error",
     "hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
     "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments",
-    "hero_reset_votes", "hero_align_segments_noalloc",
+    "hero_reset_votes", "hero_align_segments_noalloc", "hero_round", "hero_fetch",
 ]
 
 
@@ -45,11 +45,12 @@ _STAT_FIELDS = [
     "kernel_launches",
 ]
 _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record", "ms_vote",
-            "ms_consensus", "ms_dp_kernel"]
+            "ms_consensus", "ms_dp_kernel", "ms_align_wall"]
 
 
 class HeroStats(C.Structure):
-    _fields_ = [(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS]
+    _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
+                [("graph_rounds", C.c_uint64)])
 
 
 _lib = None
@@ -78,13 +79,15 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_align_subjects.argtypes = [vp, vp, vp, vp, C.c_uint64]
     lib.hero_align_self.argtypes = [vp]
     lib.hero_reset_votes.argtypes = [vp]
+    lib.hero_round.argtypes = [vp, C.c_uint32]
+    lib.hero_fetch.argtypes = [vp] * 8
     lib.hero_consensus.argtypes = [vp] * 8
     lib.hero_get_votes.argtypes = [vp, vp]
     lib.hero_get_stats.argtypes = [vp, C.POINTER(HeroStats)]
     lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          C.c_uint64] + [vp] * 12)
     for f in ("hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
-              "hero_reset_votes",
+              "hero_reset_votes", "hero_round", "hero_fetch",
               "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments"):
         getattr(lib, f).restype = C.c_int
     if path is None:
@@ -184,6 +187,25 @@ class Hero:
         """Consensus into raw host pointers; 0 leaves that output on the device."""
         v = [C.c_void_p(x) if x else None for x in (seq, imin, imed, imax, mis, gc, good)]
         self._check(self.lib.hero_consensus(self.h, *v), "consensus")
+
+    def round(self, graph: bool = True):
+        """One correction round over the resident reads (batched form: CUDA graph)."""
+        self._check(self.lib.hero_round(self.h, 1 if graph else 0), "round")
+
+    def fetch(self):
+        n, nb = self.nq, self.nqb
+        res = dict(seq=np.empty(nb, np.uint8), imin=np.empty(n, np.uint32),
+                   imed=np.empty(n, np.uint32), imax=np.empty(n, np.uint32),
+                   mismatch_rate=np.empty(n, np.float64), gc=np.empty(n, np.float64),
+                   good=np.empty(n, np.uint8))
+        self._check(self.lib.hero_fetch(
+            self.h, _ptr(res["seq"]), _ptr(res["imin"]), _ptr(res["imed"]), _ptr(res["imax"]),
+            _ptr(res["mismatch_rate"]), _ptr(res["gc"]), _ptr(res["good"])), "fetch")
+        return res
+
+    def fetch_ptr(self, seq=0, imin=0, imed=0, imax=0, mis=0, gc=0, good=0):
+        v = [C.c_void_p(x) if x else None for x in (seq, imin, imed, imax, mis, gc, good)]
+        self._check(self.lib.hero_fetch(self.h, *v), "fetch")
 
     def build_index(self):
         self._check(self.lib.hero_build_index(self.h), "build_index")

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -64,6 +65,20 @@ struct hero_ctx {
 
     hero_stats stats{};
     unsigned long long ctr[C_COUNT] = {};
+
+    // batched form: per-batch sizes of the last eager round, and its graph
+    struct BatchPlan {
+        uint64_t H, NC, ND;
+        int32_t rmax, cmax;
+    };
+    std::vector<BatchPlan> plan;
+    uint64_t plan_nkeys = 0, plan_fp = 0, qfp = 0;
+    bool plan_ok = false, capturing = false;
+    size_t batch_idx = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    DBuf stamps;  // DP kernel start/stop times per batch (ns), written inside the graph
+    DBuf fp;
 
     hero_ctx() {
         DBuf *list[] = {&q_raw, &q_code, &q_off, &q_len, &q_uid, &q_good, &q_sgood, &q_gc,
@@ -124,7 +139,16 @@ struct hero_ctx {
         bytes_peak = std::max(bytes_peak, bytes);
         return HERO_OK;
     }
+    void drop_graph() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        gexec = nullptr;
+        graph = nullptr;
+    }
     ~hero_ctx() {
+        drop_graph();
+        release(fp);
+        release(stamps);
         for (DBuf *b : all) release(*b);
         if (own_stream && st) cudaStreamDestroy(st);
     }
@@ -268,6 +292,9 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     c->have_index = false;
     HERO_TRY(upload_reads(c, seq, n ? off : nullptr, uid, n, c->q_raw, c->q_code, c->q_off,
                           c->q_len, c->q_uid, &c->q_good, &c->q_sgood, &c->q_gc));
+    HERO_TRY(c->ensure(c->fp, 8, "fingerprint"));
+    launch_fingerprint(P_<uint8_t>(c->q_raw), c->nqb, P_<uint64_t>(c->q_off), P_<int64_t>(c->q_uid), n,
+                       P_<unsigned long long>(c->fp), c->st);
     HERO_TRY(c->ensure(c->cov, c->nqb * 16, "vote matrix"));
     HERO_TRY(c->ensure(c->mdiff, c->nqb * 4, "vote matrix"));
     HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "memset"));
@@ -278,6 +305,10 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->stats.queries = n;
+    unsigned long long fpv = 0;
+    HERO_TRY(c->cuda(cudaMemcpy(&fpv, c->fp.p, 8, cudaMemcpyDeviceToHost), "fingerprint"));
+    c->qfp = fpv ^ (uint64_t(n) * 0x9e3779b97f4a7c15ull) ^ c->nqb;
+    if (c->qfp != c->plan_fp) c->plan_ok = false;
     std::vector<uint8_t> g(n);
     if (n) HERO_TRY(c->cuda(cudaMemcpy(g.data(), c->q_good.p, n, cudaMemcpyDeviceToHost), "good flags"));
     uint64_t ng = 0;
@@ -294,7 +325,7 @@ extern "C" int hero_build_index(hero_ctx *c) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    cudaEventRecord(e0, c->st);
+    if (!c->capturing) cudaEventRecord(e0, c->st);
     const uint64_t n = c->nq;
     ReadsView q = query_view(c);
     DBuf &cnt = c->x_cnt, &koff = c->x_koff, &klo = c->x_klo, &khi = c->x_khi, &kval = c->x_kval,
@@ -305,11 +336,19 @@ extern "C" int hero_build_index(hero_ctx *c) {
         if ((r = c->ensure(cnt, n * 4 + 4, "key counts"))) break;
         if ((r = c->ensure(koff, (n + 1) * 8, "key offsets"))) break;
         if ((r = c->ensure(tmp, scan_tmp_bytes(n + 1), "scan"))) break;
+        if ((r = c->check_launch("index: before"))) break;
         launch_key_count(q, c->p.k, P_<uint32_t>(cnt), c->st);
+        if ((r = c->check_launch("index: key count"))) break;
         launch_scan_u32(P_<uint32_t>(cnt), P_<uint64_t>(koff), n, tmp.p, c->st);
+        if ((r = c->check_launch("index: key scan"))) break;
         uint64_t nkeys = 0;
-        if ((r = c->cuda(cudaMemcpyAsync(&nkeys, P_<uint64_t>(koff) + n, 8, cudaMemcpyDeviceToHost, c->st), "keys"))) break;
-        if ((r = c->cuda(cudaStreamSynchronize(c->st), "keys"))) break;
+        if (c->capturing) {
+            nkeys = c->plan_nkeys;
+        } else {
+            if ((r = c->cuda(cudaMemcpyAsync(&nkeys, P_<uint64_t>(koff) + n, 8, cudaMemcpyDeviceToHost, c->st), "keys"))) break;
+            if ((r = c->cuda(cudaStreamSynchronize(c->st), "keys"))) break;
+            c->plan_nkeys = nkeys;
+        }
         uint64_t slots = 1024;
         while (slots < 2 * nkeys) slots <<= 1;
         c->t_keys = nkeys;
@@ -327,9 +366,10 @@ extern "C" int hero_build_index(hero_ctx *c) {
         if ((r = c->ensure(tmp, scan_tmp_bytes(slots + 1), "scan"))) break;
         launch_key_emit(q, c->p.k, P_<uint64_t>(koff), P_<uint64_t>(klo), P_<uint64_t>(khi),
                         P_<uint64_t>(kval), c->st);
-        cudaMemsetAsync(owner.p, 0xff, slots * 4, c->st);
-        cudaMemsetAsync(count.p, 0, slots * 4, c->st);
-        cudaMemsetAsync(fill.p, 0, slots * 4, c->st);
+        if ((r = c->check_launch("index: key emit"))) break;
+        if ((r = c->cuda(cudaMemsetAsync(owner.p, 0xff, slots * 4, c->st), "index: memset"))) break;
+        if ((r = c->cuda(cudaMemsetAsync(count.p, 0, slots * 4, c->st), "index: memset"))) break;
+        if ((r = c->cuda(cudaMemsetAsync(fill.p, 0, slots * 4, c->st), "index: memset"))) break;
         launch_table_insert(P_<uint64_t>(klo), P_<uint64_t>(khi), nkeys, P_<uint32_t>(owner),
                             P_<uint32_t>(count), P_<uint32_t>(slot_of), c->t_mask, c->st);
         launch_scan_u32(P_<uint32_t>(count), P_<uint64_t>(start), slots, tmp.p, c->st);
@@ -339,9 +379,11 @@ extern "C" int hero_build_index(hero_ctx *c) {
                               P_<uint32_t>(count), P_<uint64_t>(start), slots,
                               P_<Slot>(c->t_slots), c->st);
         if ((r = c->check_launch("index"))) break;
-        cudaEventRecord(e1, c->st);
-        if ((r = c->cuda(cudaStreamSynchronize(c->st), "index"))) break;
-        c->stats.ms_index += elapsed(e0, e1);
+        if (!c->capturing) {
+            cudaEventRecord(e1, c->st);
+            if ((r = c->cuda(cudaStreamSynchronize(c->st), "index"))) break;
+            c->stats.ms_index += elapsed(e0, e1);
+        }
         c->stats.index_keys = nkeys;
         c->stats.index_slots = slots;
         c->have_index = true;
@@ -357,30 +399,40 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
     ReadsView q = query_view(c);
     TableView t{P_<Slot>(c->t_slots), P_<uint64_t>(c->t_vals), c->t_mask};
     unsigned long long *ctr = P_<unsigned long long>(c->counters);
+    const bool cap = c->capturing;
+    hero_ctx::BatchPlan &bp = c->plan[c->batch_idx];
     cudaEvent_t ev[7];
     for (auto &e : ev) cudaEventCreate(&e);
+    auto rec = [&](int k) {
+        if (!cap) cudaEventRecord(ev[k], c->st);
+    };
     int r = HERO_OK;
     do {
-        cudaEventRecord(ev[0], c->st);
+        rec(0);
         if ((r = c->ensure(c->seg_hits, nseg * 4 + 4, "segments"))) break;
         if ((r = c->ensure(c->hit_off, (nseg + 1) * 8, "segments"))) break;
         if ((r = c->ensure(c->seg_cstart, nseg * 4 + 4, "segments"))) break;
         if ((r = c->ensure(c->seg_ccount, nseg * 4 + 4, "segments"))) break;
         if ((r = c->ensure(c->scan_tmp, scan_tmp_bytes(std::max<uint64_t>(nseg + 1, kDpBins + 1)), "scan"))) break;
         // zero the per-batch counters that size buffers (keep the running totals)
-        cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st);
-        cudaMemsetAsync(ctr + C_WIN, 0, sizeof(unsigned long long), c->st);
+        if ((r = c->cuda(cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st), "batch: counters"))) break;
+        if ((r = c->cuda(cudaMemsetAsync(ctr + C_WIN, 0, sizeof(unsigned long long), c->st), "batch: counters"))) break;
         launch_probe(false, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
         launch_scan_u32(P_<uint32_t>(c->seg_hits), P_<uint64_t>(c->hit_off), nseg, c->scan_tmp.p, c->st);
         uint64_t H = 0;
-        if ((r = c->cuda(cudaMemcpyAsync(&H, P_<uint64_t>(c->hit_off) + nseg, 8, cudaMemcpyDeviceToHost, c->st), "hits"))) break;
-        if ((r = c->cuda(cudaStreamSynchronize(c->st), "probe count"))) break;
+        if (cap) {
+            H = bp.H;
+        } else {
+            if ((r = c->cuda(cudaMemcpyAsync(&H, P_<uint64_t>(c->hit_off) + nseg, 8, cudaMemcpyDeviceToHost, c->st), "hits"))) break;
+            if ((r = c->cuda(cudaStreamSynchronize(c->st), "probe count"))) break;
+            bp.H = H;
+        }
         const uint64_t Hc = std::max<uint64_t>(H, 1);
         if ((r = c->ensure(c->hits, Hc * 8, "hits"))) break;
         launch_probe(true, subj, nsub, q, t, c->p.k, nullptr, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), ctr, c->st);
         launch_sort_hits(nseg, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), c->st);
         if ((r = c->check_launch("seed"))) break;
-        cudaEventRecord(ev[1], c->st);
+        rec(1);
         // chain scratch and outputs (bounds: chains <= hits, keys <= hits, DP <= 2 hits)
         struct {
             DBuf *b;
@@ -409,17 +461,22 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
                      P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
                      P_<uint32_t>(c->keys), P_<DpSeg>(c->segs), Hc, Hc, 2 * Hc, ctr, c->st);
         if ((r = c->check_launch("chain"))) break;
-        unsigned long long h_ctr[C_COUNT];
-        if ((r = c->cuda(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, c->st), "counters"))) break;
-        if ((r = c->cuda(cudaStreamSynchronize(c->st), "chain"))) break;
-        cudaEventRecord(ev[2], c->st);
-        if (h_ctr[C_OVERFLOW]) {
-            r = c->fail(HERO_E_STATE, "chain buffer overflow");
-            break;
+        if (!cap) {
+            unsigned long long h_ctr[C_COUNT];
+            if ((r = c->cuda(cudaMemcpyAsync(h_ctr, ctr, sizeof(h_ctr), cudaMemcpyDeviceToHost, c->st), "counters"))) break;
+            if ((r = c->cuda(cudaStreamSynchronize(c->st), "chain"))) break;
+            if (h_ctr[C_OVERFLOW]) {
+                r = c->fail(HERO_E_STATE, "chain buffer overflow");
+                break;
+            }
+            bp.NC = h_ctr[C_NC];
+            bp.ND = h_ctr[C_ND];
+            bp.rmax = int32_t(std::max<unsigned long long>(h_ctr[C_MAXR], 1));
+            bp.cmax = int32_t(std::max<unsigned long long>(h_ctr[C_MAXC], 1));
         }
-        const uint64_t NC = h_ctr[C_NC], ND = h_ctr[C_ND];
-        const int32_t rmax = int32_t(std::max<unsigned long long>(h_ctr[C_MAXR], 1));
-        const int32_t cmax = int32_t(std::max<unsigned long long>(h_ctr[C_MAXC], 1));
+        rec(2);
+        const uint64_t NC = bp.NC, ND = bp.ND;
+        const int32_t rmax = bp.rmax, cmax = bp.cmax;
         const uint32_t stride = uint32_t((rmax + cmax + 15) / 16);
         const uint64_t NDc = std::max<uint64_t>(ND, 1);
         if ((r = c->ensure(c->sums, NDc * sizeof(DpSum), "DP sums"))) break;
@@ -436,25 +493,28 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         }
         launch_dp_sort(P_<DpSeg>(c->segs), ND, P_<uint32_t>(c->bins), P_<uint32_t>(c->perm),
                        P_<uint64_t>(c->bin_off), c->scan_tmp.p, c->st);
-        cudaEventRecord(ev[3], c->st);
+        rec(3);
+        if (cap) launch_stamp(P_<unsigned long long>(c->stamps) + 2 * c->batch_idx, c->st);
         DpLaunch a{P_<DpSeg>(c->segs), P_<uint32_t>(c->perm), ND, subj.code, subj.off, subj.len,
                    q.code, q.off, P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums),
                    P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
                    c->p.affine};
         launch_dp(a, P_<uint64_t>(c->bin_off), P_<uint64_t>(c->dp_tasks), cmax, c->st);
         if ((r = c->check_launch("dp"))) break;
-        cudaEventRecord(ev[4], c->st);
+        rec(4);
+        if (cap) launch_stamp(P_<unsigned long long>(c->stamps) + 2 * c->batch_idx + 1, c->st);
         launch_assemble(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSum>(c->sums),
                         P_<uint32_t>(c->cells), ctr, c->st);
         if ((r = c->ensure(c->winners, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
         launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
                       P_<uint32_t>(c->winners), ctr, c->st);
-        cudaEventRecord(ev[5], c->st);
+        rec(5);
         launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->keys), subj, q,
                     P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov),
                     P_<int32_t>(c->mdiff), ctr, c->st);
         if ((r = c->check_launch("record/vote"))) break;
-        cudaEventRecord(ev[6], c->st);
+        if (cap) break;
+        rec(6);
         if ((r = c->cuda(cudaStreamSynchronize(c->st), "batch"))) break;
         ms[0] += elapsed(ev[0], ev[1]);
         ms[1] += elapsed(ev[1], ev[2]);
@@ -470,14 +530,20 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
 }
 
 static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
+    const auto wall0 = std::chrono::steady_clock::now();
     uint64_t B = c->P.subject_batch ? c->P.subject_batch : 131072;
     double ms[6] = {0, 0, 0, 0, 0, 0};
+    const size_t nbatch = size_t((n + B - 1) / B);
+    if (!c->capturing) c->plan.assign(nbatch, hero_ctx::BatchPlan{0, 0, 0, 1, 1});
+    if (c->plan.size() != nbatch) return c->fail(HERO_E_STATE, "plan does not match the reads");
     for (uint64_t b = 0; b < n; b += B) {
         const uint64_t nb = std::min(B, n - b);
+        c->batch_idx = size_t(b / B);
         // a batch is a window of the read arrays: shift the per-read pointers
         ReadsView v{all.code, all.off + b, all.len + b, all.uid + b, all.good + b, nb};
         HERO_TRY(align_batch(c, v, nb, ms));
     }
+    if (c->capturing) return HERO_OK;
     c->stats.subjects += n;
     c->stats.ms_seed += ms[0];
     c->stats.ms_chain += ms[1];
@@ -488,6 +554,8 @@ static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
     unsigned long long h[C_COUNT];
     HERO_TRY(c->cuda(cudaMemcpy(h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost), "counters"));
     for (int i = 0; i < C_COUNT; i++) c->ctr[i] = h[i];
+    c->stats.ms_align_wall +=
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
     return HERO_OK;
 }
 
@@ -570,6 +638,97 @@ extern "C" int hero_reset_votes(hero_ctx *c) {
     return c->cuda(cudaStreamSynchronize(c->st), "reset votes");
 }
 
+// consensus kernel of a round; results stay on the device until hero_fetch
+static int consensus_device(hero_ctx *c) {
+    const uint64_t n = c->nq, nb = c->nqb;
+    HERO_TRY(c->ensure(c->out_seq, nb, "consensus"));
+    HERO_TRY(c->ensure(c->colsum, nb * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imin, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imed, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imax, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_mis, n * 8, "consensus"));
+    if (nb) cudaMemcpyAsync(c->out_seq.p, c->q_raw.p, nb, cudaMemcpyDeviceToDevice, c->st);
+    launch_consensus(c->p, query_view(c), P_<uint32_t>(c->cov), P_<int32_t>(c->mdiff),
+                     P_<uint8_t>(c->out_seq), P_<uint32_t>(c->colsum), P_<uint32_t>(c->o_imin),
+                     P_<uint32_t>(c->o_imed), P_<uint32_t>(c->o_imax), P_<double>(c->o_mis), c->st);
+    return c->check_launch("consensus");
+}
+
+// reset + index + align (queries as subjects) + consensus, enqueued on the stream
+static int round_body(hero_ctx *c) {
+    if (c->nqb) {
+        HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "round: clear votes"));
+        HERO_TRY(c->cuda(cudaMemsetAsync(c->mdiff.p, 0, c->nqb * 4, c->st), "round: clear votes"));
+    }
+    HERO_TRY(hero_build_index(c));
+    ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
+                P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq};
+    HERO_TRY(align_reads(c, v, c->nq));
+    return consensus_device(c);
+}
+
+extern "C" int hero_round(hero_ctx *c, uint32_t flags) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    cudaSetDevice(c->dev);
+    const bool graph = (flags & HERO_ROUND_GRAPH) != 0;
+    if (graph && c->gexec && c->plan_ok && c->plan_fp == c->qfp) {
+        HERO_TRY(c->cuda(cudaGraphLaunch(c->gexec, c->st), "graph launch"));
+        HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "graph round"));
+        std::vector<unsigned long long> t(2 * c->plan.size());
+        HERO_TRY(c->cuda(cudaMemcpy(t.data(), c->stamps.p, t.size() * 8, cudaMemcpyDeviceToHost),
+                         "graph stamps"));
+        for (size_t b = 0; b < c->plan.size(); b++) {
+            c->stats.ms_dp_kernel += double(t[2 * b + 1] - t[2 * b]) * 1e-6;
+            c->stats.dp_segments += c->plan[b].ND;
+            c->stats.chains_kept += c->plan[b].NC;
+        }
+        c->stats.subjects += c->nq;
+        c->stats.graph_rounds++;
+        return HERO_OK;
+    }
+    // eager round: runs the work and records the per-batch plan
+    HERO_TRY(round_body(c));
+    HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "round"));
+    c->plan_fp = c->qfp;
+    c->plan_ok = true;
+    if (!graph) return HERO_OK;
+    // capture the same round (every size from the plan, no host syncs)
+    c->drop_graph();
+    HERO_TRY(c->ensure(c->stamps, 16 * c->plan.size(), "stamps"));
+    c->capturing = true;
+    cudaError_t e = cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal);
+    int r = e == cudaSuccess ? round_body(c) : c->cuda(e, "begin capture");
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(c->st, &g) : cudaSuccess;
+    c->capturing = false;
+    if (r != HERO_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e2 != cudaSuccess) return c->cuda(e2, "end capture");
+    c->graph = g;
+    HERO_TRY(c->cuda(cudaGraphInstantiate(&c->gexec, c->graph, 0), "graph instantiate"));
+    return HERO_OK;
+}
+
+extern "C" int hero_fetch(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uint32_t *imed,
+                          uint32_t *imax, double *mismatch_rate, double *gc_content,
+                          uint8_t *good_out) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->plan_ok) return c->fail(HERO_E_STATE, "no round to fetch");
+    cudaSetDevice(c->dev);
+    const uint64_t n = c->nq, nb = c->nqb;
+    if (seq_out && nb) cudaMemcpyAsync(seq_out, c->out_seq.p, nb, cudaMemcpyDeviceToHost, c->st);
+    if (imin && n) cudaMemcpyAsync(imin, c->o_imin.p, n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (imed && n) cudaMemcpyAsync(imed, c->o_imed.p, n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (imax && n) cudaMemcpyAsync(imax, c->o_imax.p, n * 4, cudaMemcpyDeviceToHost, c->st);
+    if (mismatch_rate && n) cudaMemcpyAsync(mismatch_rate, c->o_mis.p, n * 8, cudaMemcpyDeviceToHost, c->st);
+    if (gc_content && n) cudaMemcpyAsync(gc_content, c->q_gc.p, n * 8, cudaMemcpyDeviceToHost, c->st);
+    if (good_out && n) cudaMemcpyAsync(good_out, c->q_good.p, n, cudaMemcpyDeviceToHost, c->st);
+    return c->cuda(cudaStreamSynchronize(c->st), "fetch");
+}
+
 extern "C" int hero_get_votes(hero_ctx *c, uint32_t *cov) {
     if (!c || !cov) return HERO_E_INPUT;
     cudaSetDevice(c->dev);
@@ -590,6 +749,13 @@ extern "C" int hero_get_votes(hero_ctx *c, uint32_t *cov) {
 
 extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
     if (!c || !out) return HERO_E_INPUT;
+    cudaSetDevice(c->dev);
+    if (c->counters.p) {  // device counters also advance inside graph rounds
+        unsigned long long h[C_COUNT];
+        HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "stats"));
+        HERO_TRY(c->cuda(cudaMemcpy(h, c->counters.p, sizeof(h), cudaMemcpyDeviceToHost), "stats"));
+        for (int i = 0; i < C_COUNT; i++) c->ctr[i] = h[i];
+    }
     hero_stats s = c->stats;
     s.probes = c->ctr[C_PROBES];
     s.hits = c->ctr[C_HITS];

@@ -174,6 +174,9 @@ void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, const i
 // full vote matrix (cov + match runs), as the reference's coverage matrix
 void launch_expand_votes(ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint32_t *out,
                          cudaStream_t st);
+void launch_stamp(unsigned long long *out, cudaStream_t st);
+void launch_fingerprint(const uint8_t *raw, uint64_t nb, const uint64_t *off, const int64_t *uid,
+                        uint64_t n, unsigned long long *out, cudaStream_t st);
 void launch_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
                        const uint64_t *out_off, uint8_t *out, int32_t *nops, cudaStream_t st);
 

@@ -14,6 +14,7 @@
 //   QueryRead::callConsensus + coverage statistics    k_consensus
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 
 #include "hero_internal.cuh"
@@ -1247,6 +1248,32 @@ __global__ void k_expand_votes(ReadsView q, const uint32_t *cov, const int32_t *
     }
 }
 
+// device timestamp (ns) for timing kernels inside a replayed graph
+__global__ void k_stamp(unsigned long long *out) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    *out = t;
+}
+
+// order-independent 64-bit fingerprint of a read set (bytes, offsets, ids)
+__global__ void k_fingerprint(const uint8_t *raw, uint64_t nb, const uint64_t *off,
+                              const int64_t *uid, uint64_t n, unsigned long long *out) {
+    unsigned long long h = 0;
+    const uint64_t T = uint64_t(gridDim.x) * blockDim.x;
+    const uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    for (uint64_t w = t0; w * 8 < nb; w += T) {
+        uint64_t x = 0;
+        for (int b = 0; b < 8 && w * 8 + b < nb; b++) x |= uint64_t(raw[w * 8 + b]) << (8 * b);
+        h += mix64(x ^ (w * 0x9e3779b97f4a7c15ull));
+    }
+    for (uint64_t i = t0; i < n; i += T) {
+        h += mix64(off[i + 1] ^ 0x5bd1e995ull ^ (i << 20));
+        h += mix64(uint64_t(uid[i]) ^ 0xc2b2ae3d27d4eb4full ^ (i << 1));
+    }
+    h = warp_sum(h);
+    if (lane_id() == 0) atomicAdd(out, h);
+}
+
 __global__ void k_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,
                              const uint64_t *out_off, uint8_t *out, int32_t *nops) {
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nd;
@@ -1399,12 +1426,21 @@ void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int3
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const size_t smem = size_t(kWaveWarps) * size_t(a.rmax) * 64u;
     const unsigned g = unsigned(sms) * 8u;
+    // the opt-in is set once per size increase (never while a graph is being captured
+    // for a size not seen before: the eager round that precedes a capture sets it)
+    static size_t opted[2] = {0, 0};
+    if (smem > 48u * 1024u && smem > opted[a.affine ? 1 : 0]) {
+        if (a.affine) {
+            cudaFuncSetAttribute(k_dp_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        } else {
+            cudaFuncSetAttribute(k_dp_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        }
+        opted[a.affine ? 1 : 0] = smem;
+    }
     counted();
     if (a.affine) {
-        cudaFuncSetAttribute(k_dp_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         k_dp_wave<true><<<g, kWaveWarps * 32, smem, st>>>(a, tasks);
     } else {
-        cudaFuncSetAttribute(k_dp_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         k_dp_wave<false><<<g, kWaveWarps * 32, smem, st>>>(a, tasks);
     }
     if (cmax > 32 * kStripW) {
@@ -1463,6 +1499,19 @@ void launch_expand_votes(ReadsView q, const uint32_t *cov, const int32_t *mdiff,
         counted();
         k_expand_votes<<<grid_1d(q.n, 8, 148u * 32u), 256, 0, st>>>(q, cov, mdiff, out);
     }
+}
+
+void launch_fingerprint(const uint8_t *raw, uint64_t nb, const uint64_t *off, const int64_t *uid,
+                        uint64_t n, unsigned long long *out, cudaStream_t st) {
+    cudaMemsetAsync(out, 0, 8, st);
+    counted();
+    k_fingerprint<<<grid_1d(std::max<uint64_t>(nb / 8, n), 256, 148u * 8u), 256, 0, st>>>(
+        raw, nb, off, uid, n, out);
+}
+
+void launch_stamp(unsigned long long *out, cudaStream_t st) {
+    counted();
+    k_stamp<<<1, 1, 0, st>>>(out);
 }
 
 void launch_unpack_ops(const uint32_t *ops, uint32_t stride, const DpSum *sums, uint64_t nd,

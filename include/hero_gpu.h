@@ -20,6 +20,8 @@
  *   hero_consensus        QueryDataset::callConsensus (QueryDataset.cpp:393-412)
  *                         plus the fields QueryDataset::writeQueryOut prints
  *                         (QueryDataset.cpp:414-537)
+ *   hero_round            one whole correction round (plain, or the batched
+ *                         form replayed as a CUDA graph); hero_fetch its results
  *   hero_get_stats        the per-phase timers the reference prints
  *                         (SubjectReadAligner.cpp:635-640) and work counters
  *
@@ -76,6 +78,8 @@ typedef struct {
     uint64_t kernel_launches;  /* kernels this process launched through the library */
     double ms_upload, ms_index, ms_seed, ms_chain, ms_dp, ms_record, ms_vote, ms_consensus;
     double ms_dp_kernel;       /* device time of the DP kernels alone */
+    double ms_align_wall;      /* host wall time inside the align calls */
+    uint64_t graph_rounds;     /* rounds replayed from a CUDA graph */
 } hero_stats;
 
 /* Returns the default parameters of the reference's Config. */
@@ -111,6 +115,21 @@ int hero_reset_votes(hero_ctx *ctx);
 int hero_consensus(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *imed,
                    uint32_t *imax, double *mismatch_rate, double *gc_content,
                    uint8_t *good_out);
+
+/* One correction round over the resident query set (main.cpp:60-104: table,
+ * aligner with the query set as subjects, consensus); results stay on the
+ * device until hero_fetch.  flags: HERO_ROUND_GRAPH = the batched form -- the
+ * first round runs eagerly and records every batch's sizes, then the whole
+ * round is captured as one CUDA graph; later rounds over the same reads (checked
+ * by a device fingerprint taken in hero_set_queries) replay the graph, with no
+ * host synchronisation inside the round.  0 = the plain form, one launch per
+ * stage with host-sized buffers. */
+#define HERO_ROUND_GRAPH 1u
+int hero_round(hero_ctx *ctx, uint32_t flags);
+
+/* Results of the last round (same outputs as hero_consensus). */
+int hero_fetch(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *imed, uint32_t *imax,
+               double *mismatch_rate, double *gc_content, uint8_t *good_out);
 
 /* Vote matrix before the self vote: uint32 [total query bases][4] (A,C,T,G). */
 int hero_get_votes(hero_ctx *ctx, uint32_t *cov);
