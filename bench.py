@@ -290,6 +290,7 @@ def bench_hero(args):
         for _ in range(args.warmup + args.steps):
             device_step(graph=False)
         torch.cuda.synchronize()
+        log(json.dumps({"rounds": args.warmup + args.steps, "stats": h.stats()}))
         h.close()
         return
 

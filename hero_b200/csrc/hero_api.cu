@@ -498,7 +498,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         DpLaunch a{P_<DpSeg>(c->segs), P_<uint32_t>(c->perm), ND, subj.code, subj.off, subj.len,
                    q.code, q.off, P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums),
                    P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
-                   c->p.affine};
+                   c->p.affine, 1};  // reads with a non-ACGT base never reach the DP
         launch_dp(a, P_<uint64_t>(c->bin_off), P_<uint64_t>(c->dp_tasks), cmax, c->st);
         if ((r = c->check_launch("dp"))) break;
         rec(4);
@@ -765,6 +765,7 @@ extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
     s.records_kept = c->ctr[C_KEPT];
     s.dp_segments_ref = c->ctr[C_DP_REF];
     s.dp_cells = c->ctr[C_CELLS];
+    s.dp_cells_computed = c->ctr[C_CELLS_ALL];
     s.vote_anomalies = c->ctr[C_ANOMALY];
     s.device_bytes_peak = c->bytes_peak;
     s.kernel_launches = kernel_launches();
@@ -815,6 +816,10 @@ extern "C" int hero_align_segments(hero_ctx *c, int affine, const uint8_t *subj,
         cmax = std::max(cmax, std::min(ls, lq));
     }
     const uint32_t stride = uint32_t((rmax + cmax + 15) / 16);
+    // the whole-band rows score only A/C/G/T; other bases take the general rows
+    bool acgt = true;
+    for (const auto &rd : {std::make_pair(subj, subj_off[n_subj]), std::make_pair(query, query_off[n_query])})
+        for (uint64_t k = 0; k < rd.second && acgt; k++) acgt = base_code(rd.first[k]) < 4;
     DBuf sraw, scode, soff, slen, suid, qraw, qcode, qoff, qlen, quid, dsegs, dsums, dops, dtb, dbnd,
         doo, dout, dn, dperm, dbins, dbinoff, dtasks, dtmp;
     auto cleanup = [&]() {
@@ -854,7 +859,7 @@ extern "C" int hero_align_segments(hero_ctx *c, int affine, const uint8_t *subj,
         DpLaunch a{P_<DpSeg>(dsegs), P_<uint32_t>(dperm), n_seg, P_<uint8_t>(scode), P_<uint64_t>(soff),
                    P_<uint32_t>(slen), P_<uint8_t>(qcode), P_<uint64_t>(qoff), P_<uint32_t>(dops),
                    stride, P_<DpSum>(dsums), nullptr, P_<uint16_t>(dtb), P_<int32_t>(dbnd),
-                   c->dp_T, rmax, affine ? 1 : 0};
+                   c->dp_T, rmax, affine ? 1 : 0, acgt ? 1 : 0};
         launch_dp(a, P_<uint64_t>(dbinoff), P_<uint64_t>(dtasks), cmax, c->st);
         launch_unpack_ops(P_<uint32_t>(dops), stride, P_<DpSum>(dsums), n_seg, P_<uint64_t>(doo),
                           P_<uint8_t>(dout), P_<int32_t>(dn), c->st);

@@ -543,7 +543,8 @@ HERO_HD Cell3 dp_row0(const SegView &v, int32_t j) {
 //   u*[w]  : states of row i-1 on entry, of row i on exit
 //   left   : states at (i, j0) on entry, at (i, j0+W) on exit
 //   dg     : states at (i-1, j0)
-// Returns the row's traceback codes, 2 bits per cell (2 diag, 1 left, 0 up).
+// Returns the row's traceback codes, 2 bits per cell: 0 up, 1 left, 2 diagonal
+// mismatch, 3 diagonal match (the match bit spares the traceback the bases).
 // FULL: the band covers every cell of the strip up to column C; cells past C
 //       are then computed as if inside the matrix -- no cell at or left of
 //       column C ever reads them, so they only cost time.
@@ -573,9 +574,10 @@ HERO_HD uint32_t dp_strip_row(const SegView &v, int32_t i, int32_t j0, uint8_t a
                 // FM = max3(FM, IX, IY)(i-1, j-1) + s (BandAligner.cpp:203-207)
                 int32_t mm = dg.f >= dg.x ? dg.f : dg.x;
                 mm = mm >= dg.y ? mm : dg.y;
-                c.f = mm + (a == bc[w] ? kHIT : kMISS);
+                const bool eq = a == bc[w];
+                c.f = mm + (eq ? kHIT : kMISS);
                 // BM1 (BandAligner.cpp:214-222)
-                code = (c.f > c.x && c.f >= c.y) ? 2u : (c.y > c.x ? 1u : 0u);
+                code = (c.f > c.x && c.f >= c.y) ? (2u | uint32_t(eq)) : (c.y > c.x ? 1u : 0u);
             } else {
                 c = Cell3{kNEG, kNEG, kNEG};
                 code = 0;
@@ -589,10 +591,11 @@ HERO_HD uint32_t dp_strip_row(const SegView &v, int32_t i, int32_t j0, uint8_t a
                 // BandAligner.cpp:66-110: up, left, diag; diag wins ties, then left
                 const int32_t vu = uf[w] + (lastcol ? kSX : kDX);
                 const int32_t vl = left.f + kDY;
-                const int32_t vd = dg.f + (a == bc[w] ? kHIT : kMISS);
+                const bool eq = a == bc[w];
+                const int32_t vd = dg.f + (eq ? kHIT : kMISS);
                 if (vd >= vl && vd >= vu) {
                     c.f = vd;
-                    code = 2;
+                    code = 2u | uint32_t(eq);
                 } else if (vl >= vu) {
                     c.f = vl;
                     code = 1;
@@ -657,6 +660,126 @@ HERO_HD bool dp_strip_full(const SegView &v, int32_t j0, int32_t W) {
     return v.band >= int64_t(v.R) - (j0 + 1) && v.band >= jl - 1;
 }
 
+// ---------------------------------------------------------------------------
+// Whole-band rows.  When the band covers the whole matrix (m >= R >= C; every
+// segment of a typical correction) no cell is outside the band and column 0
+// never holds the sentinel, so a row of a strip is the bare recurrence.  The
+// stored state per column is (FM, IX, M) with M = max3(FM, IX, IY): IY is only
+// ever read through that maximum (as the next row's diagonal input) and by the
+// cell to its right.  The score of each column against each row base and the
+// diagonal codes (2 | match) come from a per-strip table built once per
+// segment: kTabWords 32-bit words, score[base][w] then diag[base].
+// The global aligner keeps FM alone (M = FM).
+// ---------------------------------------------------------------------------
+constexpr int kTabWords = 36;
+
+HERO_HD int32_t add_max(int32_t a, int32_t b, int32_t c) {  // max(a + b, c)
+#if defined(__CUDA_ARCH__)
+    return __viaddmax_s32(a, b, c);
+#else
+    return a + b > c ? a + b : c;
+#endif
+}
+
+HERO_HD int32_t max3(int32_t a, int32_t b, int32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __vimax3_s32(a, b, c);
+#else
+    const int32_t m = a > b ? a : b;
+    return m > c ? m : c;
+#endif
+}
+
+HERO_HD bool dp_whole_band(const SegView &v) { return v.band >= int64_t(v.R); }
+
+// 0-based column of C in the last strip of an align-left segment, else -1
+template <int W>
+HERO_HD int32_t dp_left_col(const SegView &v) { return v.left ? (v.C - 1) % W : -1; }
+
+// table of the strip j0+1 .. j0+W (columns past C never match)
+template <int W>
+HERO_HD void dp_whole_table(const SegView &v, int32_t j0, int32_t *tab) {
+    uint32_t dg[4] = {0, 0, 0, 0};
+    for (int32_t w = 0; w < W; w++) {
+        const int32_t j = j0 + w + 1;
+        const uint32_t b = j <= v.C ? v.col(j) : 7u;
+        for (uint32_t c = 0; c < 4; c++) {
+            const bool eq = b == c;
+            tab[c * W + w] = eq ? kHIT : kMISS;
+            dg[c] |= (2u | uint32_t(eq)) << (2 * w);
+        }
+    }
+    for (int c = 0; c < 4; c++) tab[4 * W + c] = int32_t(dg[c]);
+}
+
+// row-0 states of the strip and the M state at (0, j0)
+template <bool AFFINE, int W>
+HERO_HD void dp_whole_init(const SegView &v, int32_t j0, int32_t (&f)[W], int32_t (&x)[W],
+                           int32_t (&m)[W], int32_t &pm) {
+#pragma unroll
+    for (int32_t w = 0; w < W; w++) {
+        const Cell3 r = dp_row0<AFFINE>(v, j0 + w + 1);
+        f[w] = r.f;
+        x[w] = r.x;
+        m[w] = AFFINE ? max3(r.f, r.x, r.y) : r.f;
+    }
+    const Cell3 r = dp_row0<AFFINE>(v, j0);
+    pm = AFFINE ? max3(r.f, r.x, r.y) : r.f;
+}
+
+// column-0 states of row i >= 1 (dp_col0 inside the band) as i * mul + add:
+// FM (and M) = i * c0[0] + c0[1], IY = i * c0[0] + c0[2]
+template <bool AFFINE>
+HERO_HD void dp_whole_col0(const SegView &v, int32_t (&c0)[3]) {
+    if (AFFINE) {
+        c0[0] = v.right ? 0 : kEX;
+        c0[1] = v.right ? 0 : kDX - kEX;
+        c0[2] = v.right ? kDY : kDX - kEX;
+    } else {
+        c0[0] = v.right ? kSX : kDX;
+        c0[1] = 0;
+        c0[2] = 0;
+    }
+}
+
+// One row of a whole-band strip.  lf, ly: FM, IY at (i, j0) on entry, at
+// (i, j0 + W) on exit; dm: M at (i-1, j0); m: M of row i-1 on entry, row i on
+// exit.  WL is the align-left column C inside this strip (-1: none); its
+// vertical costs are dxl / exl (sx for the lane holding column C).
+template <bool AFFINE, int W, int WL>
+HERO_HD uint32_t dp_whole_row(const int32_t (&sc)[W], uint32_t diag, int32_t dxl, int32_t exl,
+                              int32_t (&f)[W], int32_t (&x)[W], int32_t (&m)[W], int32_t &lf,
+                              int32_t &ly, int32_t dm) {
+    uint32_t dmask = 0, lbits = 0;
+#pragma unroll
+    for (int32_t w = 0; w < W; w++) {
+        const int32_t dx = w == WL ? dxl : kDX;
+        if (AFFINE) {
+            const int32_t ex = w == WL ? exl : kEX;
+            const int32_t yv = add_max(lf, kDY, ly + kEX);    // BandAligner.cpp:180-188
+            const int32_t xv = add_max(f[w], dx, x[w] + ex);  // BandAligner.cpp:189-201
+            const int32_t fv = dm + sc[w];                    // BandAligner.cpp:203-207
+            dm = m[w];
+            m[w] = max3(fv, xv, yv);
+            if (fv > xv && fv >= yv) dmask |= 3u << (2 * w);  // BM1, BandAligner.cpp:214-222
+            if (yv > xv) lbits |= 1u << (2 * w);
+            f[w] = fv;
+            x[w] = xv;
+            lf = fv;
+            ly = yv;
+        } else {
+            const int32_t vu = f[w] + dx, vl = lf + kDY, vd = dm + sc[w];  // BandAligner.cpp:66-110
+            dm = f[w];
+            const int32_t fv = max3(vd, vl, vu);
+            if (vd >= vl && vd >= vu) dmask |= 3u << (2 * w);
+            if (vl >= vu) lbits |= 1u << (2 * w);
+            f[w] = fv;
+            lf = fv;
+        }
+    }
+    return (dmask & diag) | (~dmask & lbits);
+}
+
 // Whole-matrix fill by one thread, strip after strip.  Scratch provides
 //   int32_t& b(int32_t state, int32_t row)          boundary column, state 0..2
 //   void tb_set(int32_t strip, int32_t row, uint32_t bits)  traceback codes of a
@@ -707,27 +830,15 @@ HERO_HD int32_t dp_walk(const SegView &v, const Scratch &sc, Emit &emit) {
     const uint32_t lut = uint32_t(v.reversed ? OP_I : OP_D) | (uint32_t(v.reversed ? OP_D : OP_I) << 2) |
                          (uint32_t(OP_X) << 4) | (uint32_t(OP_M) << 6);
     while (i > 0 || j > 0) {
-        uint32_t code;
-        if (i == 0) {
-            code = 1;
-        } else if (j == 0) {
-            code = 0;
-        } else {
-            code = (sc.tb_get((j - 1) / W, i) >> (2 * ((j - 1) % W))) & 3u;
+        // row 0 traces left, column 0 up; inside, the code names the move
+        uint32_t code = i == 0 ? 1u : 0u;
+        if (i > 0 && j > 0) {
+            const uint32_t jj = uint32_t(j - 1);
+            code = (sc.tb_get(int32_t(jj / W), i) >> (2 * (jj % W))) & 3u;
         }
-        uint32_t sel;
-        if (code == 2) {
-            sel = v.row(i) == v.col(j) ? 3u : 2u;
-            i--;
-            j--;
-        } else if (code == 1) {
-            sel = 1;
-            j--;
-        } else {
-            sel = 0;
-            i--;
-        }
-        emit(uint8_t((lut >> (2 * sel)) & 3u));
+        i -= code != 1u;
+        j -= code != 0u;
+        emit(uint8_t((lut >> (2 * code)) & 3u));
         n++;
     }
     return n;

@@ -58,6 +58,7 @@ enum Counter : int {
     C_KEPT,
     C_DP_REF,
     C_CELLS,
+    C_CELLS_ALL,    // band cells of every segment computed
     C_ANOMALY,
     C_OVERFLOW,
     C_WIN,          // winners of the current batch (compacted list length)
@@ -122,7 +123,8 @@ void launch_chain(const Params &p, uint64_t nseg, ReadsView subj, ReadsView q,
 // DP: shape sort then the strip kernel
 void launch_dp_sort(const DpSeg *segs, uint64_t nd, uint32_t *bins, uint32_t *perm,
                     uint64_t *bin_off, void *scan_tmp, cudaStream_t st);
-constexpr uint32_t kDpBins = 1u << 17;
+constexpr uint32_t kShapeStripShift = 14;  // shape key: strips << 14 | align-left column << 10 | rows
+constexpr uint32_t kDpBins = 1u << 20;
 struct DpLaunch {
     const DpSeg *segs;
     const uint32_t *perm;   // processing order; NULL = identity
@@ -141,6 +143,7 @@ struct DpLaunch {
     uint64_t threads;       // resident threads the scratch is laid out for
     int32_t rmax;
     int32_t affine;
+    int32_t whole;          // 1: every base is A/C/G/T, the whole-band rows may run
 };
 constexpr int kStripW = 8;
 // needs the shape sort (perm, bin_off); tasks: 128 uint64 of device scratch.

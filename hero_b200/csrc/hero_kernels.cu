@@ -689,16 +689,17 @@ struct OpsWriter {
     }
 };
 
-// (strips, align-left, rows): a warp of the wavefront kernel takes segments
-// with equal strips, so they are grouped first; align-left and row count keep
-// the warps uniform
+// (strips, align-left column, rows): a warp of the wavefront kernel takes
+// segments with equal strips, so they are grouped first; the align-left column
+// (1 + position of column C in the last strip, 0 when not aligned left) and the
+// row count keep the warps uniform
 __device__ __forceinline__ uint32_t shape_key(const DpSeg &g) {
     const int32_t ls = g.s1 - g.s0, lq = g.q1 - g.q0;
     const int32_t r = ls > lq ? ls : lq, c = ls > lq ? lq : ls;
     int32_t nst = (c + kStripW - 1) / kStripW;
     if (nst > 63) nst = 63;
-    return (uint32_t(nst) << 11) | ((g.flags & DPF_LEFT) ? 1024u : 0u) |
-           uint32_t(r > 1023 ? 1023 : r);
+    const uint32_t wl = (g.flags & DPF_LEFT) ? 1u + uint32_t((c - 1) % kStripW) : 0u;
+    return (uint32_t(nst) << kShapeStripShift) | (wl << 10) | uint32_t(r > 1023 ? 1023 : r);
 }
 
 __global__ void k_dp_hist(const DpSeg *segs, uint64_t nd, uint32_t *bins) {
@@ -764,7 +765,8 @@ __global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     uint64_t t = 0;
     for (int n = 1; n <= 32; n++) {
-        const uint64_t b = bin_off[uint32_t(n) << 11], e = bin_off[uint32_t(n + 1) << 11];
+        const uint64_t b = bin_off[uint32_t(n) << kShapeStripShift];
+        const uint64_t e = bin_off[uint32_t(n + 1) << kShapeStripShift];
         tasks[n] = t;
         tasks[34 + n] = b;
         tasks[68 + n] = e;
@@ -772,12 +774,14 @@ __global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks) {
         t += (e - b + S - 1) / S;
     }
     tasks[33] = t;
-    tasks[0] = bin_off[uint32_t(33) << 11];  // first segment needing the per-thread kernel
+    tasks[0] = bin_off[uint32_t(33) << kShapeStripShift];  // first segment for the per-thread kernel
 }
 
-// the wavefront over one warp's segments; FULL / LEFT are warp-uniform
+// the wavefront over one warp's segments; FULL / LEFT are warp-uniform.  The
+// wavefront paths are separate functions so that each gets its own register
+// allocation (inlined into one kernel body they spill)
 template <bool AFFINE, bool FULL, bool LEFT>
-__device__ __forceinline__ void wave_fill(const SegView &v, bool active, int32_t R, int32_t Rw,
+__device__ __noinline__ void wave_fill(const SegView v, bool active, int32_t R, int32_t Rw,
                                           int G, int s, int lane, int32_t wlast, uint16_t *tb) {
     const int32_t j0 = s * kStripW;
     uint8_t bc[kStripW];
@@ -811,12 +815,83 @@ __device__ __forceinline__ void wave_fill(const SegView &v, bool active, int32_t
     }
 }
 
+// the wavefront over one warp's whole-band segments (dp_whole_row); WL is the
+// warp's align-left column, tab the lane's strip table in shared memory
+template <bool AFFINE, int WL>
+__device__ __noinline__ void wave_whole(const SegView v, bool active, int32_t R, int32_t Rw,
+                                           int G, int s, int lane, uint16_t *tb, int32_t *tab) {
+    const int32_t j0 = s * kStripW;
+    int32_t f[kStripW], x[kStripW], m[kStripW], c0[3];
+    int32_t pm = 0;
+    const uint8_t *rp = v.row_base;
+    uint32_t ch = 0;
+    if (active) {
+        dp_whole_table<kStripW>(v, j0, tab);
+        dp_whole_init<AFFINE, kStripW>(v, j0, f, x, m, pm);
+        dp_whole_col0<AFFINE>(v, c0);
+        ch = (rp[0] ^ v.row_xor) & 3u;
+    }
+    const bool last = s == G - 1;
+    const int32_t dxl = last ? kSX : kDX, exl = last ? kSX : kEX;
+    int32_t pf = kNEG, py = kNEG, pmv = kNEG;  // FM, IY, M published to lane s+1
+    uint16_t *tp = tb + lane;
+#pragma unroll 1
+    for (int32_t t = 0; t < Rw + G - 1; t++) {
+        const int32_t inf = __shfl_up_sync(0xffffffffu, pf, 1);
+        const int32_t iny = AFFINE ? __shfl_up_sync(0xffffffffu, py, 1) : 0;
+        const int32_t inm = __shfl_up_sync(0xffffffffu, pmv, 1);
+        const int32_t i = t - s + 1;
+        if (active && uint32_t(i - 1) < uint32_t(R)) {
+            const uint32_t a = ch;
+            if (i < R) {
+                rp += v.row_dir;
+                ch = (rp[0] ^ v.row_xor) & 3u;  // next row's base, loaded a step early
+            }
+            const int32_t c0f = i * c0[0] + c0[1];
+            int32_t lf = s == 0 ? c0f : inf;
+            int32_t ly = s == 0 ? i * c0[0] + c0[2] : iny;
+            const int4 s0 = reinterpret_cast<const int4 *>(tab + a * kStripW)[0];
+            const int4 s1 = reinterpret_cast<const int4 *>(tab + a * kStripW)[1];
+            const int32_t sc[kStripW] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+            const uint32_t diag = uint32_t(tab[4 * kStripW + a]);
+            const uint32_t bits = dp_whole_row<AFFINE, kStripW, WL>(sc, diag, dxl, exl, f, x, m, lf,
+                                                                     ly, pm);
+            *tp = uint16_t(bits);
+            tp += 32;
+            pf = lf;
+            py = ly;
+            pmv = AFFINE ? m[kStripW - 1] : f[kStripW - 1];
+            pm = s == 0 ? c0f : inm;
+        }
+    }
+}
+
+template <bool AFFINE>
+__device__ __forceinline__ void wave_whole_any(int wl, const SegView &v, bool active, int32_t R,
+                                               int32_t Rw, int G, int s, int lane, uint16_t *tb,
+                                               int32_t *tab) {
+    switch (wl) {
+        case 0: wave_whole<AFFINE, 0>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 1: wave_whole<AFFINE, 1>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 2: wave_whole<AFFINE, 2>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 3: wave_whole<AFFINE, 3>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 4: wave_whole<AFFINE, 4>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 5: wave_whole<AFFINE, 5>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 6: wave_whole<AFFINE, 6>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        case 7: wave_whole<AFFINE, 7>(v, active, R, Rw, G, s, lane, tb, tab); break;
+        default: wave_whole<AFFINE, -1>(v, active, R, Rw, G, s, lane, tb, tab); break;
+    }
+}
+
 template <bool AFFINE>
 __global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
     k_dp_wave(DpLaunch a, const uint64_t *tasks) {
-    extern __shared__ uint16_t tbs[];
+    extern __shared__ int4 wave_smem[];
     const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
-    uint16_t *tb = tbs + size_t(wib) * size_t(a.rmax) * 32u;
+    int32_t *tab = reinterpret_cast<int32_t *>(wave_smem) + (size_t(wib) * 32u + lane) * kTabWords;
+    uint16_t *tb = reinterpret_cast<uint16_t *>(reinterpret_cast<int32_t *>(wave_smem) +
+                                                size_t(kWaveWarps) * 32u * kTabWords) +
+                   size_t(wib) * size_t(a.rmax) * 32u;
     const uint64_t ntask = tasks[33];
     for (uint64_t task = uint64_t(blockIdx.x) * kWaveWarps + wib; task < ntask;
          task += uint64_t(gridDim.x) * kWaveWarps) {
@@ -845,7 +920,15 @@ __global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
         const int32_t wlast = active ? dp_strip_wlast(v, j0, kStripW) : -1;
         const bool wfull = __all_sync(0xffffffffu, full);
         const bool wleft = __any_sync(0xffffffffu, wlast >= 0);
-        if (wfull) {
+        // whole-band fast path: every segment of the warp inside its band and all
+        // with the same align-left column (the shape key makes it so)
+        const int32_t wl = active ? dp_left_col<kStripW>(v) : -2;
+        const int32_t wl0 = warp_max(wl);
+        const bool whole = a.whole &&
+                           __all_sync(0xffffffffu, !active || (dp_whole_band(v) && wl == wl0));
+        if (whole) {
+            wave_whole_any<AFFINE>(wl0, v, active, R, Rw, G, s, lane, tb, tab);
+        } else if (wfull) {
             if (wleft) {
                 wave_fill<AFFINE, true, true>(v, active, R, Rw, G, s, lane, wlast, tb);
             } else {
@@ -939,7 +1022,7 @@ struct KeyAt {
 __global__ void k_assemble(Params p, uint64_t nc, ChainArrays ch, const uint32_t *keys,
                            ReadsView subj, ReadsView q, const DpSum *sums, const uint32_t *cells,
                            unsigned long long *counters) {
-    unsigned long long built = 0, acc = 0, used = 0, ncells = 0;
+    unsigned long long built = 0, acc = 0, used = 0, ncells = 0, nall = 0;
     for (uint64_t ci = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; ci < nc;
          ci += uint64_t(gridDim.x) * blockDim.x) {
         const uint32_t s = ch.subj[ci], qid = ch.query[ci];
@@ -964,16 +1047,20 @@ __global__ void k_assemble(Params p, uint64_t nc, ChainArrays ch, const uint32_t
         ch.len[ci] = len;
         used += v.used;
         ncells += v.cells_used;
+        if (cells)
+            for (uint32_t k = 0; k < ch.nseg[ci]; k++) nall += cells[ch.seg_off[ci] + k];
     }
     built = warp_sum(built);
     acc = warp_sum(acc);
     used = warp_sum(used);
     ncells = warp_sum(ncells);
+    nall = warp_sum(nall);
     if (lane_id() == 0) {
         atomicAdd(&counters[C_BUILT], built);
         atomicAdd(&counters[C_ACCEPTED], acc);
         atomicAdd(&counters[C_DP_REF], used);
         atomicAdd(&counters[C_CELLS], ncells);
+        atomicAdd(&counters[C_CELLS_ALL], nall);
     }
 }
 
@@ -1404,7 +1491,13 @@ uint64_t dp_threads(int device) {
     return uint64_t(sms) * 8u * kDpThreads;
 }
 
-bool dp_wave_fits(int32_t rmax) { return size_t(kWaveWarps) * size_t(rmax) * 64u <= 200u * 1024u; }
+// shared memory of a wavefront block: per warp, the lanes' strip tables and
+// rmax rows of 2-bit codes (32 lanes x 16 bits)
+static size_t wave_smem(int32_t rmax) {
+    return size_t(kWaveWarps) * (32u * kTabWords * 4u + size_t(rmax) * 64u);
+}
+
+bool dp_wave_fits(int32_t rmax) { return wave_smem(rmax) <= 200u * 1024u; }
 
 void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int32_t cmax,
                cudaStream_t st) {
@@ -1424,7 +1517,7 @@ void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int3
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = size_t(kWaveWarps) * size_t(a.rmax) * 64u;
+    const size_t smem = wave_smem(a.rmax);
     const unsigned g = unsigned(sms) * 8u;
     // the opt-in is set once per size increase (never while a graph is being captured
     // for a size not seen before: the eager round that precedes a capture sets it)

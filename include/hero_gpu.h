@@ -80,6 +80,7 @@ typedef struct {
     double ms_dp_kernel;       /* device time of the DP kernels alone */
     double ms_align_wall;      /* host wall time inside the align calls */
     uint64_t graph_rounds;     /* rounds replayed from a CUDA graph */
+    uint64_t dp_cells_computed; /* band cells of every DP segment computed on the device */
 } hero_stats;
 
 /* Returns the default parameters of the reference's Config. */

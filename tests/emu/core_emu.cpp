@@ -221,6 +221,79 @@ int emu_align(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query,
 // one DP segment through the warp-wavefront schedule of k_dp_wave: lane s owns
 // strip s and computes row t - s + 1 at step t; the left boundary of a row is
 // what lane s-1 published one step earlier.  Lanes are simulated in order.
+extern "C++" {
+// whole-band wavefront lanes (the kernel's wave_whole), stepped sequentially:
+// at step t every lane reads what its left neighbour published at step t-1
+template <bool AFFINE, int WL>
+void emu_whole(const SegView &v, int G, std::vector<uint16_t> &tb) {
+    constexpr int W = 8;
+    struct Lane {
+        int32_t f[W], x[W], m[W], c0[3], tab[kTabWords];
+        int32_t pm, pf, py, pmv;
+        const uint8_t *rp;
+        uint32_t ch;
+    };
+    std::vector<Lane> L(G);
+    for (int s = 0; s < G; s++) {
+        Lane &x = L[s];
+        dp_whole_table<W>(v, s * W, x.tab);
+        dp_whole_init<AFFINE, W>(v, s * W, x.f, x.x, x.m, x.pm);
+        dp_whole_col0<AFFINE>(v, x.c0);
+        x.rp = v.row_base;
+        x.ch = (x.rp[0] ^ v.row_xor) & 3u;
+        x.pf = x.py = x.pmv = kNEG;
+    }
+    std::vector<int32_t> inf(G), iny(G), inm(G);
+    for (int t = 0; t < v.R + G - 1; t++) {
+        for (int s = 0; s < G; s++) {  // __shfl_up_sync
+            inf[s] = s > 0 ? L[s - 1].pf : 0;
+            iny[s] = s > 0 ? L[s - 1].py : 0;
+            inm[s] = s > 0 ? L[s - 1].pmv : 0;
+        }
+        for (int s = 0; s < G; s++) {
+            const int32_t i = t - s + 1;
+            if (i < 1 || i > v.R) continue;
+            Lane &x = L[s];
+            const uint32_t a = x.ch;
+            if (i < v.R) {
+                x.rp += v.row_dir;
+                x.ch = (x.rp[0] ^ v.row_xor) & 3u;
+            }
+            const int32_t c0f = i * x.c0[0] + x.c0[1];
+            int32_t lf = s == 0 ? c0f : inf[s];
+            int32_t ly = s == 0 ? i * x.c0[0] + x.c0[2] : iny[s];
+            int32_t sc[W];
+            for (int w = 0; w < W; w++) sc[w] = x.tab[a * W + w];
+            const uint32_t diag = uint32_t(x.tab[4 * W + a]);
+            const bool last = s == G - 1;
+            const uint32_t bits = dp_whole_row<AFFINE, W, WL>(sc, diag, last ? kSX : kDX,
+                                                              last ? kSX : kEX, x.f, x.x, x.m, lf,
+                                                              ly, x.pm);
+            tb[size_t(i - 1) * 32 + s] = uint16_t(bits);
+            x.pf = lf;
+            x.py = ly;
+            x.pmv = AFFINE ? x.m[W - 1] : x.f[W - 1];
+            x.pm = s == 0 ? c0f : inm[s];
+        }
+    }
+}
+
+template <bool AFFINE>
+void emu_whole_any(int wl, const SegView &v, int G, std::vector<uint16_t> &tb) {
+    switch (wl) {
+        case 0: emu_whole<AFFINE, 0>(v, G, tb); break;
+        case 1: emu_whole<AFFINE, 1>(v, G, tb); break;
+        case 2: emu_whole<AFFINE, 2>(v, G, tb); break;
+        case 3: emu_whole<AFFINE, 3>(v, G, tb); break;
+        case 4: emu_whole<AFFINE, 4>(v, G, tb); break;
+        case 5: emu_whole<AFFINE, 5>(v, G, tb); break;
+        case 6: emu_whole<AFFINE, 6>(v, G, tb); break;
+        case 7: emu_whole<AFFINE, 7>(v, G, tb); break;
+        default: emu_whole<AFFINE, -1>(v, G, tb); break;
+    }
+}
+}  // extern "C++"
+
 int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query, int32_t lq,
                    int64_t band, int align_right, int align_left, uint8_t *ops, int32_t cap) {
     constexpr int W = 8;
@@ -251,7 +324,14 @@ int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *q
         L[s].wlast = dp_strip_wlast(v, s * W, W);
         L[s].pub = Cell3{kNEG, kNEG, kNEG};
     }
-    for (int t = 0; t < v.R + G - 1; t++) {
+    if (dp_whole_band(v)) {  // the kernel's whole-band path
+        if (affine) {
+            emu_whole_any<true>(dp_left_col<W>(v), v, G, tb);
+        } else {
+            emu_whole_any<false>(dp_left_col<W>(v), v, G, tb);
+        }
+    }
+    for (int t = 0; t < (dp_whole_band(v) ? 0 : v.R + G - 1); t++) {
         std::vector<Cell3> in(G);
         for (int s = 0; s < G; s++) in[s] = s > 0 ? L[s - 1].pub : Cell3{0, 0, 0};  // shfl_up
         for (int s = 0; s < G; s++) {
