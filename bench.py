@@ -55,7 +55,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hero", choices=["hero", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config1", "config2"])
+    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config4"])
+    ap.add_argument("--served-jobs", type=int, default=60,
+                    help="jobs of the served block added to the default line (0: none)")
+    ap.add_argument("--jobs-scale", type=float, default=0.0,
+                    help="genome-size scale of the served jobs (default 0.02, config4 0.05)")
     ap.add_argument("--genome-bp", type=int, default=0, help="override the genome size")
     ap.add_argument("--cpu-sample-bp", type=int, default=60000,
                     help="genome size of the bounded sample the CPU reference runs on")
@@ -230,6 +234,120 @@ def dpx_peak_tops(device: int) -> float | None:
     return v if v > 0 else None
 
 
+def _job_reads(job):
+    rs = job.reads()
+    return job.job_id, rs.seq, rs.off, rs.names
+
+
+def served_jobs(n_jobs: int, scale: float):
+    """The serving stream (Poisson arrivals, genome log-uniform 0.5-20 Mbp times
+    `scale`, L in {100,150,250}, coverage U(20,80), affine errors), generated in a
+    spawn pool so no process is forked after CUDA starts."""
+    import multiprocessing as mp
+
+    from hero_b200 import synth
+    jobs = synth.config4_jobs(n_jobs=n_jobs, scale=scale)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        out = pool.map(_job_reads, jobs, chunksize=1)
+    reads = {j: (seq, off, names) for j, seq, off, names in out}
+    return jobs, [reads[j.job_id] for j in jobs]
+
+
+def run_served(jobs, reads, dev: int, busy_target: float = 0.85, check: int = 3) -> dict:
+    """Submits the jobs at their (rescaled) Poisson arrival times to one server and
+    reports job latency (submit -> results ready) and aggregate throughput."""
+    import threading
+
+    from hero_b200 import HeroServer, correct
+    srv = HeroServer(aligner="affine", device=dev)
+    try:
+        # warm-up and calibration: the first jobs submitted at once, back to back
+        cal = list(range(min(8, len(jobs))))
+        t0 = time.perf_counter()
+        ids = [srv.submit(*reads[i]) for i in cal]
+        for j in ids:
+            srv.wait(j)
+            srv.release(j)
+        cal_s = time.perf_counter() - t0
+        cal_bases = sum(int(reads[i][1][-1]) for i in cal)
+        thr = cal_bases / cal_s
+        mean_bases = float(np.mean([int(r[1][-1]) for r in reads]))
+        lam = busy_target * thr / mean_bases  # jobs/s that keep the GPU ~busy_target busy
+        base_rate = 1.0  # config4_jobs draws arrivals at 1 job/s
+        arrivals = [j.arrival_s * base_rate / lam for j in jobs]
+        s0 = srv.stats()
+        ids = [None] * len(jobs)
+
+        def submitter():
+            start = time.perf_counter()
+            for k in range(len(jobs)):
+                dt = arrivals[k] - (time.perf_counter() - start)
+                if dt > 0:
+                    time.sleep(dt)
+                ids[k] = srv.submit(*reads[k])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        infos = [srv.wait(j) for j in ids]
+        s1 = srv.stats()
+        lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
+        first = min(i["submit_ms"] for i in infos)
+        last = max(i["done_ms"] for i in infos)
+        bases = sum(i["bases"] for i in infos)
+        # served == alone on a few jobs (byte-identical corrected reads and statistics)
+        rng = np.random.default_rng(7)
+        picks = rng.choice(len(jobs), size=min(check, len(jobs)), replace=False)
+        ok = 0
+        for k in picks:
+            got = srv.result(ids[k])
+            seq, off, names = reads[k]
+            from hero_b200.synth import ReadSet
+            want = correct(ReadSet(seq, off, names), aligner="affine", device=dev)
+            same = all(np.array_equal(want[f], got[f]) for f in ("seq", "imin", "imed", "imax"))
+            ok += int(same)
+        for j in ids:
+            srv.release(j)
+        rounds = s1["rounds"] - s0["rounds"]
+        return {
+            "jobs": len(jobs), "bases": bases,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "bases_per_s": bases / ((last - first) / 1e3),
+            "arrival_rate_per_s": lam, "calibrated_bases_per_s": thr,
+            "busy_frac": (s1["busy_ms"] - s0["busy_ms"]) / (last - first),
+            "rounds": rounds, "mean_jobs_per_round": len(jobs) / max(rounds, 1),
+            "served_equals_alone": f"{ok}/{len(picks)}",
+        }
+    finally:
+        srv.close()
+
+
+def bench_served(args):
+    """The serving workload alone: one JSON line with p50/p99 job latency."""
+    import torch
+
+    from hero_b200 import build
+    if not os.environ.get("HERO_B200_LIB"):
+        build.build_library()
+    scale = args.jobs_scale or 0.05
+    jobs, reads = served_jobs(200, scale)
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    with ClockSampler(dev) as clk:
+        r = run_served(jobs, reads, dev)
+    line = {"metric": "p50/p99 job latency", "value": r["p50_ms"], "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "p99_ms": r["p99_ms"],
+            "served_bases_per_s": r["bases_per_s"], "dtype": "int32",
+            "data": "synthetic (seeded generator, no public dataset)",
+            "config": {"workload": f"serving stream: 200 jobs, Poisson arrivals, genome "
+                                   f"log-uniform 0.5-20 Mbp x {scale}, L in {{100,150,250}}, "
+                                   f"coverage U(20,80), affine/indel errors",
+                       "flags": "-c --covinfo --singleReads -a a"},
+            "served": r, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def bench_hero(args):
     import torch
     import torch.distributed as dist
@@ -258,6 +376,9 @@ def bench_hero(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    served_in = None
+    if args.served_jobs and world == 1 and not args.profile:
+        served_in = served_jobs(args.served_jobs, args.jobs_scale or 0.02)
     rs, kw, flags, desc = make_workload(args.workload, args.genome_bp)
     n, nb = rs.n, rs.total_bases
     log(f"[rank {rank}] workload: {desc}")
@@ -347,6 +468,16 @@ def bench_hero(args):
                if DP_DRAM_BYTES_PER_CELL is not None else None)
     clocks = clk.summary()
 
+    h.close()
+    served = None
+    if served_in is not None:
+        with ClockSampler(dev) as sclk:
+            served = run_served(*served_in, dev)
+        served["clocks"] = sclk.summary()
+        served["workload"] = (f"{args.served_jobs} jobs, Poisson arrivals, genome log-uniform "
+                              f"0.5-20 Mbp x {args.jobs_scale or 0.02}, L in {{100,150,250}}, "
+                              "coverage U(20,80), affine/indel errors")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = measure_cpu_baseline(args)
@@ -379,9 +510,9 @@ def bench_hero(args):
             "gpu_launches": launches,
             "work_per_step": {"dp_cells": cells // steps,
                               "dp_segments": (s1["dp_segments"] - s0["dp_segments"]) // steps},
+            "served": served,
         }
         print(json.dumps(line), flush=True)
-    h.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -390,6 +521,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         bench_reference(args)
+    elif args.workload == "config4":
+        bench_served(args)
     else:
         bench_hero(args)
 

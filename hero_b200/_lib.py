@@ -25,7 +25,12 @@ EXPORTS = [
     "hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
     "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments",
     "hero_reset_votes", "hero_align_segments_noalloc", "hero_round", "hero_fetch",
+    "hero_set_query_jobs", "hero_server_create", "hero_server_destroy", "hero_job_submit",
+    "hero_job_poll", "hero_job_wait", "hero_job_result", "hero_job_error", "hero_job_release",
+    "hero_server_get_stats", "hero_job_bytes", "hero_round_admit",
 ]
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 
 
 class HeroParams(C.Structure):
@@ -51,6 +56,19 @@ _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record"
 class HeroStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
                 [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64)])
+
+
+class JobInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("round", C.c_uint64),
+                ("round_jobs", C.c_uint32), ("reserved", C.c_uint32), ("bases", C.c_uint64),
+                ("reads", C.c_uint64), ("submit_ms", C.c_double), ("start_ms", C.c_double),
+                ("done_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = ([(f, C.c_uint64) for f in ("jobs_submitted", "jobs_done", "jobs_failed", "rounds",
+                                            "bases_done", "round_bytes_budget")] +
+                [("busy_ms", C.c_double), ("uptime_ms", C.c_double)])
 
 
 _lib = None
@@ -86,9 +104,26 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_get_stats.argtypes = [vp, C.POINTER(HeroStats)]
     lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          C.c_uint64] + [vp] * 12)
+    lib.hero_set_query_jobs.argtypes = [vp, vp, C.c_uint64]
+    lib.hero_server_create.argtypes = [C.POINTER(HeroParams), C.c_uint64, C.POINTER(vp)]
+    lib.hero_server_destroy.argtypes = [vp]
+    lib.hero_job_submit.argtypes = [vp, vp, vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+    lib.hero_job_poll.argtypes = [vp, C.c_uint64, C.POINTER(JobInfo)]
+    lib.hero_job_wait.argtypes = [vp, C.c_uint64, C.c_int64, C.POINTER(JobInfo)]
+    lib.hero_job_result.argtypes = [vp, C.c_uint64] + [vp] * 7
+    lib.hero_job_error.argtypes = [vp, C.c_uint64]
+    lib.hero_job_error.restype = C.c_char_p
+    lib.hero_job_release.argtypes = [vp, C.c_uint64]
+    lib.hero_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    lib.hero_job_bytes.argtypes = [C.c_uint64, C.c_uint64, C.c_int32]
+    lib.hero_job_bytes.restype = C.c_uint64
+    lib.hero_round_admit.argtypes = [vp, C.c_uint64, C.c_uint64]
+    lib.hero_round_admit.restype = C.c_uint64
     for f in ("hero_set_queries", "hero_build_index", "hero_align_subjects", "hero_align_self",
               "hero_reset_votes", "hero_round", "hero_fetch",
-              "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments"):
+              "hero_consensus", "hero_get_votes", "hero_get_stats", "hero_align_segments",
+              "hero_set_query_jobs", "hero_server_create", "hero_job_submit", "hero_job_poll",
+              "hero_job_wait", "hero_job_result", "hero_job_release", "hero_server_get_stats"):
         getattr(lib, f).restype = C.c_int
     if path is None:
         _lib = lib
@@ -173,6 +208,12 @@ class Hero:
         self.nqb = int(off[-1]) if self.nq else 0
         self._check(self.lib.hero_set_queries(self.h, _ptr(seq), _ptr(off), _ptr(uid), self.nq),
                     "set_queries")
+
+    def set_query_jobs(self, job):
+        """Tags each query read with its job so one round corrects several jobs."""
+        job = np.ascontiguousarray(job, dtype=np.uint32)
+        self._jobkeep = job
+        self._check(self.lib.hero_set_query_jobs(self.h, _ptr(job), len(job)), "set_query_jobs")
 
     def reset_votes(self):
         self._check(self.lib.hero_reset_votes(self.h), "reset_votes")
@@ -260,6 +301,94 @@ class Hero:
             _ptr(query_seq), _ptr(query_off), len(query_off) - 1, n, *[_ptr(x) for x in a],
             _ptr(ops_off), _ptr(ops), _ptr(nops)), "align_segments")
         return ops, ops_off, nops
+
+
+def _params(k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0, max_indel_rate=1.0,
+            consensus_threshold=0.6, device=0, subject_batch=0, device_memory_budget=0):
+    lib = load_library()
+    p = HeroParams()
+    lib.hero_default_params(C.byref(p))
+    p.k, p.min_overlap, p.device = k, min_overlap, device
+    p.aligner = ALIGNER_AFFINE if aligner in ("a", "affine") else ALIGNER_GLOBAL
+    p.max_mismatch_rate, p.max_indel_rate = max_mismatch_rate, max_indel_rate
+    p.consensus_threshold = consensus_threshold
+    p.subject_batch, p.device_memory_budget = subject_batch, device_memory_budget
+    return p
+
+
+class HeroServer:
+    """Serving form: independent correction jobs, continuous batching (hero_server_*)."""
+
+    def __init__(self, round_bytes: int = 0, **kw):
+        self.lib = load_library()
+        self.params = _params(**kw)
+        h = C.c_void_p()
+        rc = self.lib.hero_server_create(C.byref(self.params), int(round_bytes), C.byref(h))
+        if rc != HERO_OK:
+            raise HeroError(f"hero_server_create failed: {ERRORS.get(rc, rc)}")
+        self.h = h
+        self._sizes: dict[int, tuple[int, int]] = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hero_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, seq, off, uid) -> int:
+        seq, off, uid = Hero._arrays(seq, off, uid)
+        jid = C.c_uint64()
+        rc = self.lib.hero_job_submit(self.h, _ptr(seq), _ptr(off), _ptr(uid), len(off) - 1,
+                                      C.byref(jid))
+        if rc != HERO_OK:
+            raise HeroError(f"hero_job_submit: {ERRORS.get(rc, rc)}")
+        self._sizes[jid.value] = (len(off) - 1, int(off[-1]) if len(off) > 1 else 0)
+        return jid.value
+
+    @staticmethod
+    def _info(i: JobInfo) -> dict:
+        return {f: getattr(i, f) for f, _ in i._fields_ if f != "reserved"}
+
+    def poll(self, jid: int) -> dict:
+        i = JobInfo()
+        rc = self.lib.hero_job_poll(self.h, jid, C.byref(i))
+        if rc != HERO_OK:
+            raise HeroError(f"hero_job_poll: {ERRORS.get(rc, rc)}")
+        return self._info(i)
+
+    def wait(self, jid: int, timeout_ms: int = -1) -> dict:
+        i = JobInfo()
+        rc = self.lib.hero_job_wait(self.h, jid, int(timeout_ms), C.byref(i))
+        if rc != HERO_OK:
+            raise HeroError(f"hero_job_wait: {ERRORS.get(rc, rc)}")
+        return self._info(i)
+
+    def result(self, jid: int) -> dict:
+        n, nb = self._sizes[jid]
+        res = dict(seq=np.empty(nb, np.uint8), imin=np.empty(n, np.uint32),
+                   imed=np.empty(n, np.uint32), imax=np.empty(n, np.uint32),
+                   mismatch_rate=np.empty(n, np.float64), gc=np.empty(n, np.float64),
+                   good=np.empty(n, np.uint8))
+        rc = self.lib.hero_job_result(self.h, jid, *[_ptr(res[k]) for k in (
+            "seq", "imin", "imed", "imax", "mismatch_rate", "gc", "good")])
+        if rc != HERO_OK:
+            err = self.lib.hero_job_error(self.h, jid)
+            raise HeroError(f"hero_job_result: {ERRORS.get(rc, rc)}: {err.decode() if err else ''}")
+        return res
+
+    def release(self, jid: int):
+        self.lib.hero_job_release(self.h, jid)
+        self._sizes.pop(jid, None)
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        self.lib.hero_server_get_stats(self.h, C.byref(s))
+        return {f: getattr(s, f) for f, _ in s._fields_}
 
 
 def correct(reads, **kw):

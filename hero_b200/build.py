@@ -25,7 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-O3"]
-CU_SOURCES = ["hero_kernels.cu", "hero_api.cu", "hero_noalloc.cu"]
+CU_SOURCES = ["hero_kernels.cu", "hero_api.cu", "hero_noalloc.cu", "hero_server.cu"]
 PEAK_SOURCES = ["int_peak.cu"]
 
 

@@ -43,6 +43,8 @@ struct hero_ctx {
     // query set
     uint64_t nq = 0, nqb = 0;
     DBuf q_raw, q_code, q_off, q_len, q_uid, q_good, q_sgood, q_gc;
+    DBuf q_job;            // job of each query read (jobs served together)
+    bool tagged = false;   // q_job holds the reads' jobs
     bool have_queries = false, have_index = false;
     // k-mer table
     DBuf t_slots, t_vals;
@@ -91,7 +93,7 @@ struct hero_ctx {
                         &ch_win, &ch_rate, &ch_len, &keys, &segs, &sums, &cells, &ops, &perm,
                         &bins, &bin_off, &tb, &bnd, &dp_tasks, &winners, &scan_tmp, &counters, &x_cnt, &x_koff,
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
-                        &x_fill, &x_tmp};
+                        &x_fill, &x_tmp, &q_job};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -165,9 +167,11 @@ static T *P_(DBuf &b) {
         if (_r != HERO_OK) return _r; \
     } while (0)
 
+static const uint32_t *job_tags(hero_ctx *c) { return c->tagged ? P_<uint32_t>(c->q_job) : nullptr; }
+
 static ReadsView query_view(hero_ctx *c) {
     return ReadsView{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
-                     P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_good), c->nq};
+                     P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_good), c->nq, job_tags(c)};
 }
 
 static double elapsed(cudaEvent_t a, cudaEvent_t b) {
@@ -290,6 +294,7 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     c->nq = n;
     c->nqb = n ? off[n] : 0;
     c->have_index = false;
+    c->tagged = false;
     HERO_TRY(upload_reads(c, seq, n ? off : nullptr, uid, n, c->q_raw, c->q_code, c->q_off,
                           c->q_len, c->q_uid, &c->q_good, &c->q_sgood, &c->q_gc));
     HERO_TRY(c->ensure(c->fp, 8, "fingerprint"));
@@ -315,6 +320,29 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     for (uint8_t x : g) ng += x;
     c->stats.good_queries = ng;
     c->have_queries = true;
+    return HERO_OK;
+}
+
+extern "C" int hero_set_query_jobs(hero_ctx *c, const uint32_t *job, uint64_t n) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (n != c->nq) return c->fail(HERO_E_INPUT, "one job per query read");
+    if (n && !job) return c->fail(HERO_E_INPUT, "null job buffer");
+    cudaSetDevice(c->dev);
+    const int bits = kmer_job_bits(c->p.k);
+    uint64_t h = 0x51ed270b27a4f3b1ull;
+    for (uint64_t i = 0; i < n; i++) {
+        if (bits < 32 && (job[i] >> bits) != 0)
+            return c->fail(HERO_E_INPUT, "job index does not fit beside the k-mer in a key");
+        h = mix64(h ^ (uint64_t(job[i]) + i));
+    }
+    HERO_TRY(c->ensure(c->q_job, n * 4, "jobs"));
+    if (n)
+        HERO_TRY(c->cuda(cudaMemcpy(c->q_job.p, job, n * 4, cudaMemcpyHostToDevice), "upload jobs"));
+    c->tagged = true;
+    c->have_index = false;
+    c->qfp ^= h;  // the graph of a round is keyed on the tagged read set
+    if (c->qfp != c->plan_fp) c->plan_ok = false;
     return HERO_OK;
 }
 
@@ -540,7 +568,8 @@ static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
         const uint64_t nb = std::min(B, n - b);
         c->batch_idx = size_t(b / B);
         // a batch is a window of the read arrays: shift the per-read pointers
-        ReadsView v{all.code, all.off + b, all.len + b, all.uid + b, all.good + b, nb};
+        ReadsView v{all.code, all.off + b,  all.len + b, all.uid + b, all.good + b,
+                    nb,       all.job ? all.job + b : nullptr};
         HERO_TRY(align_batch(c, v, nb, ms));
     }
     if (c->capturing) return HERO_OK;
@@ -564,7 +593,7 @@ extern "C" int hero_align_self(hero_ctx *c) {
     if (!c->have_index) return c->fail(HERO_E_STATE, "index not built");
     cudaSetDevice(c->dev);
     ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
-                P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq};
+                P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq, job_tags(c)};
     return align_reads(c, v, c->nq);
 }
 
@@ -662,7 +691,7 @@ static int round_body(hero_ctx *c) {
     }
     HERO_TRY(hero_build_index(c));
     ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
-                P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq};
+                P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq, job_tags(c)};
     HERO_TRY(align_reads(c, v, c->nq));
     return consensus_device(c);
 }

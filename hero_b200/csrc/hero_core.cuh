@@ -86,6 +86,18 @@ HERO_HD void kmer_push(Kmer &m, uint32_t code, int k) {
     }
 }
 
+// Jobs served together share one k-mer table: a key carries its job above the
+// 2k k-mer bits, so keys of different jobs never compare equal (job must fit
+// in the 128 - 2k bits left: kmer_job_bits).
+HERO_HD void kmer_tag(Kmer &m, uint32_t job, int k) {
+    if (2 * k <= 64) {
+        m.hi = job;
+    } else if (job) {
+        m.hi |= uint64_t(job) << (2 * k - 64);
+    }
+}
+HERO_HD int kmer_job_bits(int k) { return 2 * k <= 64 ? 32 : (128 - 2 * k < 32 ? 128 - 2 * k : 32); }
+
 HERO_HD uint64_t mix64(uint64_t z) {  // splitmix64 finalizer
     z ^= z >> 30;
     z *= 0xbf58476d1ce4e5b9ull;

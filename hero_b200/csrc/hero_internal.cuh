@@ -35,6 +35,7 @@ struct ReadsView {
     const int64_t *uid;
     const uint8_t *good;
     uint64_t n;
+    const uint32_t *job;  // job of each read when jobs share a table; NULL: one job
 };
 
 struct TableView {

@@ -218,6 +218,7 @@ __global__ void k_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint
             const int64_t pos = query_key_pos(L, k, i);
             Kmer m{0, 0};
             for (int32_t t = 0; t < k; t++) kmer_push(m, c[pos + t] & 3u, k);
+            if (q.job) kmer_tag(m, q.job[r], k);
             klo[e] = m.lo;
             khi[e] = m.hi;
             kval[e] = (uint64_t(r) << 32) | uint64_t(pos);
@@ -341,6 +342,10 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
                 }
                 if (bad) continue;
                 for (int32_t i = k - 1; i >= 0; i--) kmer_push(rm, (c[f + i] & 3u) ^ 2u, k);
+                if (subj.job) {
+                    kmer_tag(fm, subj.job[s], k);
+                    kmer_tag(rm, subj.job[s], k);
+                }
                 for (int o = 0; o < 2; o++) {
                     uint32_t st = 0, cnt = 0;
                     if (!table_find(t, o ? rm : fm, st, cnt)) continue;

@@ -1,0 +1,395 @@
+// hero_server.cu -- serving form: many independent correction jobs on one GPU.
+//
+// The reference corrects one read set per process (main.cpp:36-104).  A server
+// runs a stream of such jobs with continuous batching: a worker thread runs
+// correction rounds back to back, and each round admits the oldest queued jobs
+// that fit in a device-memory budget.  The admitted jobs' reads are
+// concatenated into one query set whose reads carry their job
+// (hero_set_query_jobs), so one set of launches -- index build, seeding,
+// chaining, DP, votes, consensus -- serves every job of the round, and a job's
+// k-mers only ever meet its own reads: each job's output is the output it gets
+// alone.  Results are split back per job and kept until released.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/hero_gpu.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+    uint64_t id = 0;
+    int32_t state = HERO_JOB_QUEUED, status = HERO_OK;
+    std::string err;
+    std::vector<uint8_t> seq;
+    std::vector<uint64_t> off;
+    std::vector<int64_t> uid;
+    uint64_t bytes = 0;  // admission estimate
+    // results
+    std::vector<uint8_t> out_seq, good;
+    std::vector<uint32_t> imin, imed, imax;
+    std::vector<double> mis, gc;
+    uint64_t round = 0;
+    uint32_t round_jobs = 0;
+    double submit_ms = 0, start_ms = 0, done_ms = 0;
+    uint64_t n() const { return uid.size(); }
+};
+
+}  // namespace
+
+struct hero_server {
+    hero_params p{};
+    hero_ctx *ctx = nullptr;
+    uint64_t round_bytes = 0;
+    Clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<uint64_t> queue;
+    std::unordered_map<uint64_t, Job> jobs;
+    std::thread worker;
+    bool stop = false;
+    uint64_t next_id = 1, rounds = 0, submitted = 0, done = 0, failed = 0, bases_done = 0;
+    uint64_t max_jobs = 0;   // jobs a key can tell apart (k-mer bits leave room for the job)
+    uint64_t cap_jobs = 0;   // jobs per round after a round ran out of memory (0: no cap)
+    double busy_ms = 0;
+
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    }
+    void run();
+    void run_round(std::vector<uint64_t> ids);
+};
+
+extern "C" uint64_t hero_job_bytes(uint64_t bases, uint64_t reads, int32_t k) {
+    // per base: read copies and codes (2), vote matrix (16 + 4), corrected bases (1);
+    // per read: offsets, lengths, ids, flags, GC, job, statistics and index
+    // temporaries (~70); per k-mer key (one every k bases, plus a tail key per
+    // read): table slots at <= 4 per key plus build temporaries (~260).  Device
+    // buffers grow with 25 % slack.
+    const uint64_t kk = k > 0 ? uint64_t(k) : 39u;
+    const uint64_t keys = bases / kk + reads;
+    const uint64_t raw = 24u * bases + 70u * reads + 260u * keys;
+    return raw + raw / 4 + 4096u;
+}
+
+extern "C" uint64_t hero_round_admit(const uint64_t *bytes, uint64_t n_queued, uint64_t round_bytes) {
+    if (n_queued == 0) return 0;
+    uint64_t sum = 0, n = 0;
+    while (n < n_queued && (n == 0 || sum + bytes[n] <= round_bytes)) sum += bytes[n++];
+    return n;
+}
+
+void hero_server::run() {
+    std::unique_lock<std::mutex> lk(mu);
+    while (true) {
+        cv_work.wait(lk, [&] { return stop || !queue.empty(); });
+        if (stop) break;
+        std::vector<uint64_t> sizes;
+        for (uint64_t id : queue) sizes.push_back(jobs[id].bytes);
+        uint64_t take = hero_round_admit(sizes.data(), sizes.size(), round_bytes);
+        take = std::min(take, max_jobs);
+        if (cap_jobs) take = std::min(take, cap_jobs);
+        std::vector<uint64_t> ids(queue.begin(), queue.begin() + long(take));
+        queue.erase(queue.begin(), queue.begin() + long(take));
+        const double t = now_ms();
+        for (uint64_t id : ids) {
+            jobs[id].state = HERO_JOB_RUNNING;
+            jobs[id].start_ms = t;
+        }
+        lk.unlock();
+        run_round(ids);
+        lk.lock();
+        cv_done.notify_all();
+    }
+    // jobs still queued at shutdown fail
+    for (uint64_t id : queue) {
+        Job &j = jobs[id];
+        j.state = HERO_JOB_FAILED;
+        j.status = HERO_E_STATE;
+        j.err = "server stopped";
+        failed++;
+    }
+    queue.clear();
+    cv_done.notify_all();
+}
+
+// One round over the given jobs (the worker owns the context; job inputs are
+// not touched by other threads while the job is running).
+void hero_server::run_round(std::vector<uint64_t> ids) {
+    const double t_begin = now_ms();
+    std::vector<Job *> js;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        for (uint64_t id : ids) js.push_back(&jobs[id]);
+    }
+    uint64_t n = 0, nb = 0;
+    for (Job *j : js) {
+        n += j->n();
+        nb += j->seq.size();
+    }
+    std::vector<uint8_t> seq(nb);
+    std::vector<uint64_t> off(n + 1, 0);
+    std::vector<int64_t> uid(n);
+    std::vector<uint32_t> tag(n);
+    uint64_t r = 0, b = 0;
+    for (size_t t = 0; t < js.size(); t++) {
+        const Job &j = *js[t];
+        if (!j.seq.empty()) std::memcpy(seq.data() + b, j.seq.data(), j.seq.size());
+        for (uint64_t i = 0; i < j.n(); i++) {
+            off[r + i + 1] = b + j.off[i + 1];
+            uid[r + i] = j.uid[i];
+            tag[r + i] = uint32_t(t);
+        }
+        r += j.n();
+        b += j.seq.size();
+    }
+    std::vector<uint8_t> out_seq(seq), good(n);  // reads that are not good stay as read
+    std::vector<uint32_t> imin(n), imed(n), imax(n);
+    std::vector<double> mis(n), gc(n);
+    int st = hero_set_queries(ctx, seq.data(), off.data(), uid.data(), n);
+    if (st == HERO_OK && js.size() > 1) st = hero_set_query_jobs(ctx, tag.data(), n);
+    if (st == HERO_OK) st = hero_build_index(ctx);
+    if (st == HERO_OK) st = hero_align_self(ctx);
+    if (st == HERO_OK)
+        st = hero_consensus(ctx, out_seq.data(), imin.data(), imed.data(), imax.data(), mis.data(),
+                            gc.data(), good.data());
+    const std::string err = st == HERO_OK ? std::string() : std::string(hero_last_error(ctx));
+    if (st == HERO_E_OOM && js.size() > 1) {
+        // the estimate was short: requeue the jobs in order and admit half as many
+        std::lock_guard<std::mutex> g(mu);
+        for (size_t t = js.size(); t-- > 0;) {
+            js[t]->state = HERO_JOB_QUEUED;
+            queue.push_front(ids[t]);
+        }
+        cap_jobs = js.size() / 2;
+        busy_ms += now_ms() - t_begin;
+        return;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    if (st == HERO_OK && cap_jobs) cap_jobs *= 2;
+    rounds++;
+    const double t_end = now_ms();
+    busy_ms += t_end - t_begin;
+    r = 0;
+    b = 0;
+    for (Job *j : js) {
+        const uint64_t jn = j->n(), jb = j->seq.size();
+        j->round = rounds;
+        j->round_jobs = uint32_t(js.size());
+        j->done_ms = t_end;
+        if (st == HERO_OK) {
+            j->out_seq.assign(out_seq.begin() + long(b), out_seq.begin() + long(b + jb));
+            j->good.assign(good.begin() + long(r), good.begin() + long(r + jn));
+            j->imin.assign(imin.begin() + long(r), imin.begin() + long(r + jn));
+            j->imed.assign(imed.begin() + long(r), imed.begin() + long(r + jn));
+            j->imax.assign(imax.begin() + long(r), imax.begin() + long(r + jn));
+            j->mis.assign(mis.begin() + long(r), mis.begin() + long(r + jn));
+            j->gc.assign(gc.begin() + long(r), gc.begin() + long(r + jn));
+            j->state = HERO_JOB_DONE;
+            done++;
+            bases_done += jb;
+        } else {
+            j->state = HERO_JOB_FAILED;
+            j->status = st;
+            j->err = err;
+            failed++;
+        }
+        // inputs are no longer needed
+        std::vector<uint8_t>().swap(j->seq);
+        r += jn;
+        b += jb;
+    }
+}
+
+extern "C" int hero_server_create(const hero_params *p, uint64_t round_bytes, hero_server **out) {
+    if (!p || !out) return HERO_E_INPUT;
+    *out = nullptr;
+    hero_server *s = new hero_server();
+    s->p = *p;
+    s->t0 = Clock::now();
+    int st = hero_create(p, &s->ctx);
+    if (st != HERO_OK) {
+        delete s;
+        return st;
+    }
+    if (round_bytes == 0) {
+        // per-batch working set (hits, chains, DP segments of one subject batch)
+        const uint64_t reserve = 12ull << 30;
+        uint64_t budget = p->device_memory_budget;
+        if (!budget) {
+            size_t fr = 0, tot = 0;
+            cudaSetDevice(p->device);
+            if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+                hero_destroy(s->ctx);
+                delete s;
+                return HERO_E_CUDA;
+            }
+            budget = uint64_t(double(fr) * 0.8);
+        }
+        round_bytes = budget > 2 * reserve ? budget - reserve : budget / 2;
+    }
+    s->round_bytes = round_bytes;
+    // job tags share a 128-bit key with the 2k k-mer bits (hero_set_query_jobs)
+    const int free_bits = 2 * p->k <= 64 ? 32 : std::min(32, 128 - 2 * p->k);
+    s->max_jobs = free_bits >= 32 ? 0xffffffffull : (1ull << free_bits);
+    s->worker = std::thread([s] { s->run(); });
+    *out = s;
+    return HERO_OK;
+}
+
+extern "C" void hero_server_destroy(hero_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    hero_destroy(s->ctx);
+    delete s;
+}
+
+extern "C" int hero_job_submit(hero_server *s, const uint8_t *seq, const uint64_t *off,
+                               const int64_t *uid, uint64_t n, uint64_t *job_id) {
+    if (!s || !job_id || (n && (!seq || !off || !uid))) return HERO_E_INPUT;
+    if (n && off[0] != 0) return HERO_E_INPUT;
+    for (uint64_t i = 0; i < n; i++)
+        if (off[i + 1] < off[i] || off[i + 1] - off[i] > 32767) return HERO_E_INPUT;
+    Job j;
+    const uint64_t nb = n ? off[n] : 0;
+    j.seq.assign(seq, seq + nb);
+    j.off.assign(off, off + n + 1);
+    if (!n) j.off.assign(1, 0);
+    j.uid.assign(uid, uid + n);
+    j.bytes = hero_job_bytes(nb, n, s->p.k);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->stop) return HERO_E_STATE;
+    j.id = s->next_id++;
+    j.submit_ms = s->now_ms();
+    *job_id = j.id;
+    s->submitted++;
+    if (n == 0) {  // nothing to correct
+        j.state = HERO_JOB_DONE;
+        j.start_ms = j.done_ms = j.submit_ms;
+        s->done++;
+        s->jobs.emplace(j.id, std::move(j));
+        s->cv_done.notify_all();
+        return HERO_OK;
+    }
+    const uint64_t id = j.id;
+    s->jobs.emplace(id, std::move(j));
+    s->queue.push_back(id);
+    s->cv_work.notify_one();
+    return HERO_OK;
+}
+
+static void fill_info(const Job &j, hero_job_info *info) {
+    if (!info) return;
+    std::memset(info, 0, sizeof(*info));
+    info->state = j.state;
+    info->status = j.status;
+    info->round = j.round;
+    info->round_jobs = j.round_jobs;
+    info->bases = j.off.empty() ? 0 : j.off.back();
+    info->reads = j.n();
+    info->submit_ms = j.submit_ms;
+    info->start_ms = j.start_ms;
+    info->done_ms = j.done_ms;
+}
+
+extern "C" int hero_job_poll(hero_server *s, uint64_t job_id, hero_job_info *info) {
+    if (!s) return HERO_E_INPUT;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return HERO_E_INPUT;
+    fill_info(it->second, info);
+    return HERO_OK;
+}
+
+extern "C" int hero_job_wait(hero_server *s, uint64_t job_id, int64_t timeout_ms,
+                             hero_job_info *info) {
+    if (!s) return HERO_E_INPUT;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto finished = [&] {
+        auto it = s->jobs.find(job_id);
+        return it == s->jobs.end() || it->second.state == HERO_JOB_DONE ||
+               it->second.state == HERO_JOB_FAILED;
+    };
+    if (timeout_ms < 0) {
+        s->cv_done.wait(lk, finished);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), finished)) {
+        auto it = s->jobs.find(job_id);
+        if (it != s->jobs.end()) fill_info(it->second, info);
+        return HERO_E_TIMEOUT;
+    }
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return HERO_E_INPUT;
+    fill_info(it->second, info);
+    return HERO_OK;
+}
+
+extern "C" int hero_job_result(hero_server *s, uint64_t job_id, uint8_t *seq_out, uint32_t *imin,
+                               uint32_t *imed, uint32_t *imax, double *mismatch_rate,
+                               double *gc_content, uint8_t *good_out) {
+    if (!s) return HERO_E_INPUT;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return HERO_E_INPUT;
+    const Job &j = it->second;
+    if (j.state == HERO_JOB_FAILED) return j.status;
+    if (j.state != HERO_JOB_DONE) return HERO_E_STATE;
+    auto put = [](auto *dst, const auto &v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    put(seq_out, j.out_seq);
+    put(imin, j.imin);
+    put(imed, j.imed);
+    put(imax, j.imax);
+    put(mismatch_rate, j.mis);
+    put(gc_content, j.gc);
+    put(good_out, j.good);
+    return HERO_OK;
+}
+
+extern "C" const char *hero_job_error(hero_server *s, uint64_t job_id) {
+    if (!s) return "";
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->jobs.find(job_id);
+    return it == s->jobs.end() ? "" : it->second.err.c_str();
+}
+
+extern "C" int hero_job_release(hero_server *s, uint64_t job_id) {
+    if (!s) return HERO_E_INPUT;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return HERO_E_INPUT;
+    if (it->second.state != HERO_JOB_DONE && it->second.state != HERO_JOB_FAILED)
+        return HERO_E_STATE;
+    s->jobs.erase(it);
+    return HERO_OK;
+}
+
+extern "C" int hero_server_get_stats(hero_server *s, hero_server_stats *out) {
+    if (!s || !out) return HERO_E_INPUT;
+    std::lock_guard<std::mutex> g(s->mu);
+    out->jobs_submitted = s->submitted;
+    out->jobs_done = s->done;
+    out->jobs_failed = s->failed;
+    out->rounds = s->rounds;
+    out->bases_done = s->bases_done;
+    out->round_bytes_budget = s->round_bytes;
+    out->busy_ms = s->busy_ms;
+    out->uptime_ms = s->now_ms();
+    return HERO_OK;
+}

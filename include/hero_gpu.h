@@ -178,6 +178,79 @@ int hero_align_segments_noalloc(int affine, const uint8_t *subj, const uint64_t 
                                 int32_t max_side, const uint64_t *ops_off, uint8_t *ops,
                                 int32_t *nops, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Serving: many independent correction jobs (each its own -q X -s X run)
+ * corrected together.  No reference counterpart: HERO runs one job per
+ * process.  These build on the single-job calls above.
+ * ------------------------------------------------------------------------ */
+
+/* Tags each read of the current query set with its job (job[i] for read i) so
+ * that one round corrects several independent jobs: a read's k-mers only meet
+ * reads of its own job, so every job's output equals its output alone.  The
+ * job index must fit beside the k-mer in a 128-bit key (below 2^(128-2k), and
+ * below 2^32).  Cleared by hero_set_queries; only the self alignment
+ * (hero_align_self, hero_round) honours the tags. */
+int hero_set_query_jobs(hero_ctx *ctx, const uint32_t *job, uint64_t n);
+
+typedef struct hero_server hero_server;
+
+#define HERO_JOB_QUEUED 0
+#define HERO_JOB_RUNNING 1
+#define HERO_JOB_DONE 2
+#define HERO_JOB_FAILED 3
+
+typedef struct {
+    int32_t state;        /* HERO_JOB_* */
+    int32_t status;       /* HERO_OK, or the error that failed the job */
+    uint64_t round;       /* round that corrected the job (1-based; 0 = not yet) */
+    uint32_t round_jobs;  /* jobs corrected in that round */
+    uint32_t reserved;
+    uint64_t bases, reads;
+    double submit_ms, start_ms, done_ms; /* server clock (ms since creation) */
+} hero_job_info;
+
+typedef struct {
+    uint64_t jobs_submitted, jobs_done, jobs_failed, rounds, bases_done;
+    uint64_t round_bytes_budget; /* admission limit of one round (estimated device bytes) */
+    double busy_ms;              /* wall time spent inside rounds */
+    double uptime_ms;
+} hero_server_stats;
+
+/* A server owns one context on p->device and a worker thread that runs
+ * correction rounds back to back (continuous batching).  Each round admits the
+ * oldest queued jobs whose estimated device memory (hero_job_bytes) fits in
+ * round_bytes (0 = p->device_memory_budget, or 80 % of the device's free memory
+ * at creation, minus the per-batch working set); a job larger than that runs
+ * in a round of its own.  All jobs of a server share p's parameters. */
+int hero_server_create(const hero_params *p, uint64_t round_bytes, hero_server **out);
+/* Stops the worker after the round in flight; jobs still queued fail. */
+void hero_server_destroy(hero_server *s);
+
+/* Copies a job's reads (layout of hero_set_queries) into the server and queues
+ * it; thread-safe.  *job_id identifies it in the calls below. */
+int hero_job_submit(hero_server *s, const uint8_t *seq, const uint64_t *off, const int64_t *uid,
+                    uint64_t n, uint64_t *job_id);
+int hero_job_poll(hero_server *s, uint64_t job_id, hero_job_info *info);
+/* Waits until the job is done or failed, at most timeout_ms (< 0: no limit);
+ * HERO_E_TIMEOUT when the limit passes first. */
+int hero_job_wait(hero_server *s, uint64_t job_id, int64_t timeout_ms, hero_job_info *info);
+/* Results of a done job (hero_consensus outputs, the job's own layout). */
+int hero_job_result(hero_server *s, uint64_t job_id, uint8_t *seq_out, uint32_t *imin,
+                    uint32_t *imed, uint32_t *imax, double *mismatch_rate, double *gc_content,
+                    uint8_t *good_out);
+/* Error message of a failed job ("" otherwise); valid until the job is released. */
+const char *hero_job_error(hero_server *s, uint64_t job_id);
+/* Frees a finished job's results. */
+int hero_job_release(hero_server *s, uint64_t job_id);
+int hero_server_get_stats(hero_server *s, hero_server_stats *out);
+
+/* Admission estimate: device bytes a job of `bases` bases in `reads` reads adds
+ * to a round (read copies, vote matrix, k-mer table, consensus outputs). */
+uint64_t hero_job_bytes(uint64_t bases, uint64_t reads, int32_t k);
+/* How many of the queued jobs (in order, sizes bytes[i]) the next round
+ * admits under round_bytes: the longest prefix that fits, at least 1. */
+uint64_t hero_round_admit(const uint64_t *bytes, uint64_t n_queued, uint64_t round_bytes);
+
 #ifdef __cplusplus
 }
 #endif
