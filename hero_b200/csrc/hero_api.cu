@@ -228,6 +228,12 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
         delete c;
         return HERO_E_OOM;
     }
+    // running totals and the overflow flag start at zero (recycled device memory
+    // holds whatever its last owner left there)
+    if (cudaMemset(c->counters.p, 0, sizeof(unsigned long long) * C_COUNT) != cudaSuccess) {
+        hero_destroy(c);
+        return HERO_E_CUDA;
+    }
     *out = c;
     return HERO_OK;
 }
@@ -444,7 +450,8 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         if ((r = c->ensure(c->scan_tmp, scan_tmp_bytes(std::max<uint64_t>(nseg + 1, kDpBins + 1)), "scan"))) break;
         // zero the per-batch counters that size buffers (keep the running totals)
         if ((r = c->cuda(cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st), "batch: counters"))) break;
-        if ((r = c->cuda(cudaMemsetAsync(ctr + C_WIN, 0, sizeof(unsigned long long), c->st), "batch: counters"))) break;
+        static_assert(C_WIN == C_OVERFLOW + 1, "overflow flag and winner count are cleared together");
+        if ((r = c->cuda(cudaMemsetAsync(ctr + C_OVERFLOW, 0, 2 * sizeof(unsigned long long), c->st), "batch: counters"))) break;
         launch_probe(false, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
         launch_scan_u32(P_<uint32_t>(c->seg_hits), P_<uint64_t>(c->hit_off), nseg, c->scan_tmp.p, c->st);
         uint64_t H = 0;

@@ -101,3 +101,23 @@ def test_wait_with_a_limit_times_out_and_later_completes():
         info = srv.wait(j, 120_000)
         assert info["state"] == 2 and info["done_ms"] >= info["submit_ms"]
         assert info["bases"] == int(rs.off[-1]) and info["reads"] == rs.n
+
+
+@pytest.mark.gpu
+def test_new_contexts_start_from_zeroed_counters():
+    """Device memory freed by an earlier owner is not zero: a new context's work
+    counters (and its buffer-overflow flag) must not inherit what was there."""
+    import torch
+
+    from hero_b200 import Hero, correct
+    x = torch.full((1 << 30,), 0xFF, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    del x
+    torch.cuda.empty_cache()
+    for _ in range(4):
+        with Hero(aligner="affine") as h:
+            s = h.stats()
+        assert s["hits"] == 0 and s["dp_segments_ref"] == 0 and s["dp_cells"] == 0, s
+    rs = synth.config2(seed=11, genome_bp=30_000)
+    res = correct(rs, aligner="affine")
+    assert res["stats"]["dp_cells"] > 0
