@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hero", choices=["hero", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config1", "config2", "config4"])
+    ap.add_argument("--workload", default="config2",
+                    choices=["config1", "config2", "config3", "config4", "config5"])
     ap.add_argument("--served-jobs", type=int, default=60,
                     help="jobs of the served block added to the default line (0: none)")
     ap.add_argument("--jobs-scale", type=float, default=0.0,
@@ -76,6 +77,17 @@ def make_workload(name: str, genome_bp: int = 0, seed: int | None = None):
         desc = (f"plain/global: {rs.meta['genome_bp']} bp iid genome, 100 bp reads at 30x "
                 f"({rs.n} reads), 1% substitutions")
         return rs, dict(aligner="global"), ["-c", "--covinfo", "--singleReads"], desc
+    aff = ["-c", "--covinfo", "--singleReads", "-a", "a"]
+    if name == "config3":
+        rs = synth.config3(seed=seed or 3, genome_bp=genome_bp or 20_000_000)
+        desc = (f"mixed lengths: {rs.meta['genome_bp']} bp genome (GC 42 %), reads U{{75..250}} bp "
+                f"at 100x ({rs.n} reads), subs 0.1->2%, indels 0.05%/base")
+        return rs, dict(aligner="affine"), aff, desc
+    if name == "config5":
+        rs = synth.config5(seed=seed or 5, genome_bp=genome_bp or 100_000_000)
+        desc = (f"diploid: two {rs.meta['genome_bp']} bp haplotypes (0.1 % SNPs, 0.01 % indels), "
+                f"150 bp reads at 30x ({rs.n} reads), subs 0.1->2%, indels 0.05%/base")
+        return rs, dict(aligner="affine"), aff, desc
     rs = synth.config2(seed=seed or 2, genome_bp=genome_bp or 5_000_000)
     desc = (f"affine/indel: {rs.meta['genome_bp']} bp genome + 40 repeat copies, 150 bp reads "
             f"at 50x ({rs.n} reads), subs 0.1->2%, indels 0.05%/base")
@@ -377,7 +389,7 @@ def bench_hero(args):
         return float(t.item())
 
     served_in = None
-    if args.served_jobs and world == 1 and not args.profile:
+    if args.served_jobs and world == 1 and not args.profile and args.workload == "config2":
         served_in = served_jobs(args.served_jobs, args.jobs_scale or 0.02)
     rs, kw, flags, desc = make_workload(args.workload, args.genome_bp)
     n, nb = rs.n, rs.total_bases
@@ -464,7 +476,9 @@ def bench_hero(args):
     per = {k: round((p1[k] - p0[k]) / plain_steps, 3)
            for k in ("ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_dp_kernel", "ms_record",
                      "ms_vote", "ms_consensus", "ms_align_wall")}
-    traffic = (DP_DRAM_BYTES_PER_CELL * cells / steps
+    # one DP launch per subject batch of 131072 reads
+    dp_launches = steps * ((n + 131071) // 131072)
+    traffic = (DP_DRAM_BYTES_PER_CELL * cells / dp_launches
                if DP_DRAM_BYTES_PER_CELL is not None else None)
     clocks = clk.summary()
 
@@ -491,7 +505,8 @@ def bench_hero(args):
             "data": "synthetic (seeded generator, no public dataset)",
             "config": {"workload": desc, "reads": n, "bases": nb, "flags": " ".join(flags),
                        "parallelism": f"independent jobs x{world}",
-                       "l2": "inputs larger than L2 (250 Mbp reads, 4 GB vote matrix)"},
+                       "l2": f"inputs larger than L2 ({nb / 1e6:.0f} Mbp reads, "
+                             f"{20 * nb / 1e9:.1f} GB vote matrix)"},
             "e2e": {"value": e2e_value, "unit": "bases/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "alu", "kernel": "k_dp (banded affine DP + traceback)",

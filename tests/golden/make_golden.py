@@ -4,6 +4,11 @@ Runs the unmodified reference (oracle/_ref/hero_ref, built from the reference
 sources by oracle/Makefile) on every fixture input and records md5 sums of the
 input FASTQ and of the reference .fasta/.info; the outputs of the fixtures in
 STORED are kept gzipped.  Usage:  python tests/golden/make_golden.py
+
+    python tests/golden/make_golden.py --full NAME...
+
+regenerates the named entries of manifest_full.json (whole-size workloads and
+reduced-genome instances of the larger ones; minutes each) and keeps the rest.
 """
 from __future__ import annotations
 
@@ -19,6 +24,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
 from fixtures import FIXTURES, STORED  # noqa: E402
+
+from hero_b200 import synth  # noqa: E402
+
+# name -> (generator call as recorded, generator, reference flags)
+FULL = {
+    "config1_full": ("synth.config1()", lambda: synth.config1(), []),
+    "config2_full": ("synth.config2()", lambda: synth.config2(), ["-a", "a"]),
+    "config3_reduced": ("synth.config3(genome_bp=200000)",
+                        lambda: synth.config3(genome_bp=200_000), ["-a", "a"]),
+    "config5_reduced": ("synth.config5(genome_bp=1000000)",
+                        lambda: synth.config5(genome_bp=1_000_000), ["-a", "a"]),
+}
 
 REF = os.path.join(ROOT, "oracle", "_ref", "hero_ref")
 
@@ -42,7 +59,33 @@ def run_reference(fq: str, flags: list[str], workdir: str) -> tuple[bytes, bytes
     return fa, info
 
 
+def main_full(names: list[str]):
+    import time
+    path = os.path.join(HERE, "manifest_full.json")
+    manifest = json.load(open(path)) if os.path.exists(path) else {}
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        for name in names:
+            call, gen, flags = FULL[name]
+            rs = gen()
+            fqb = rs.to_fastq()
+            fq = os.path.join(d, "in.fq")
+            with open(fq, "wb") as f:
+                f.write(fqb)
+            t0 = time.perf_counter()
+            fa, info = run_reference(fq, flags, d)
+            secs = time.perf_counter() - t0
+            manifest[name] = {"generator": call, "flags": flags, "reads": rs.n,
+                              "fastq_md5": md5(fqb), "fasta_md5": md5(fa), "info_md5": md5(info),
+                              f"reference_seconds_{threads}_threads": round(secs, 2)}
+            print(name, manifest[name], flush=True)
+    with open(path, "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "--full":
+        return main_full(sys.argv[2:] or list(FULL))
     manifest = {}
     with tempfile.TemporaryDirectory() as d:
         for name, (gen, flags) in FIXTURES.items():

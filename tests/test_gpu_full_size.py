@@ -1,6 +1,8 @@
 """Full-size parity: the GPU path reproduces the reference's .fasta/.info byte
 for byte on the whole plain workload (1 Mbp, 300k x 100 bp, global aligner) and
-the whole affine/indel workload (5 Mbp + repeats, 1.67 M x 150 bp, affine).
+the whole affine/indel workload (5 Mbp + repeats, 1.67 M x 150 bp, affine),
+and on reduced-genome instances of the mixed-length workload (200 kbp, 75-250
+bp reads at 100x) and the diploid workload (1 Mbp haplotype pair, 30x).
 The md5 sums in golden/manifest_full.json come from the reference itself run
 on the same seeded inputs (15 s and 666 s on 8 host threads)."""
 import hashlib
@@ -21,8 +23,13 @@ def md5(b):
     return hashlib.md5(b).hexdigest()
 
 
-@pytest.mark.parametrize("name,gen,aligner", [("config1_full", synth.config1, "global"),
-                                              ("config2_full", synth.config2, "affine")])
+@pytest.mark.parametrize("name,gen,aligner", [
+    ("config1_full", synth.config1, "global"),
+    ("config2_full", synth.config2, "affine"),
+    # reduced-genome instances of the mixed-length (75-250 bp) and diploid workloads
+    ("config3_reduced", lambda: synth.config3(genome_bp=200_000), "affine"),
+    ("config5_reduced", lambda: synth.config5(genome_bp=1_000_000), "affine"),
+])
 def test_full_size_matches_reference(gpu_lib, name, gen, aligner):
     from hero_b200 import Hero
     m = MANIFEST[name]
