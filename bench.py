@@ -40,9 +40,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM traffic of the affine DP kernel per reference band cell, from the ncu
-# capture summarised in profiles/ (None until profiled)
-DP_DRAM_BYTES_PER_CELL = None
+# DRAM traffic (read + write) of the affine DP kernel per band cell, from one ncu
+# capture of a whole launch (profiles/k_dp_wave_affine_100kbp.md: 2.913 GB for
+# 23.19 G cells); the traffic is per segment (codes in, ops and summaries out),
+# so it scales with the cells of a launch
+DP_DRAM_BYTES_PER_CELL = 2.913069e9 / 23_186_600_877
 
 
 def log(*a):
