@@ -508,15 +508,22 @@ HERO_HD SegView make_view(const uint8_t *subj, int32_t Ls, int32_t orient, const
     return v;
 }
 
-// cells of the reference's loop bounds (BandAligner.cpp:63-66)
+// Cells of the reference's loop bounds (BandAligner.cpp:63-66): the sum over
+// rows i = 0..R of min(C, i + m) - max(0, i - m) + 1.  With m >= R - C (the
+// aligner widens its band to the length difference) every row is non-empty,
+// so the sum splits into two arithmetic series.
 HERO_HD uint64_t band_cells(int32_t R, int32_t C, int64_t m) {
-    uint64_t cells = 0;
-    for (int32_t i = 0; i <= R; i++) {
-        int64_t lm = i - m > 0 ? i - m : 0;
-        int64_t rm = C < i + m ? C : i + m;
-        if (rm >= lm) cells += uint64_t(rm - lm + 1);
+    const int64_t r = R, c = C;
+    int64_t hi;  // sum of min(C, i + m)
+    const int64_t t = (c - m < r) ? c - m : r;  // last row with i + m <= C
+    if (t >= 0) {
+        hi = (t + 1) * m + t * (t + 1) / 2 + (r - t) * c;
+    } else {
+        hi = (r + 1) * c;
     }
-    return cells;
+    const int64_t k = r - m;  // rows with i > m contribute i - m to the sum of max(0, i - m)
+    const int64_t lo = k > 0 ? k * (k + 1) / 2 : 0;
+    return uint64_t(hi - lo + r + 1);
 }
 
 HERO_HD bool in_band(int32_t i, int32_t j, int32_t C, int64_t m) {
@@ -756,18 +763,20 @@ HERO_HD void dp_whole_col0(const SegView &v, int32_t (&c0)[3]) {
 
 // One row of a whole-band strip.  lf, ly: FM, IY at (i, j0) on entry, at
 // (i, j0 + W) on exit; dm: M at (i-1, j0); m: M of row i-1 on entry, row i on
-// exit.  WL is the align-left column C inside this strip (-1: none); its
-// vertical costs are dxl / exl (sx for the lane holding column C).
-template <bool AFFINE, int W, int WL>
-HERO_HD uint32_t dp_whole_row(const int32_t (&sc)[W], uint32_t diag, int32_t dxl, int32_t exl,
-                              int32_t (&f)[W], int32_t (&x)[W], int32_t (&m)[W], int32_t &lf,
-                              int32_t &ly, int32_t dm) {
+// exit.  The align-left column C (vertical moves cost sx there,
+// BandAligner.cpp:189-201) is handled by the caller: FM and IX of the row above
+// at that column feed only its IX, so raising them by sx - dx and sx - ex before
+// the row (dp_whole_left) makes the same recurrence give its value and code.
+template <bool AFFINE, int W>
+HERO_HD uint32_t dp_whole_row(const int32_t (&sc)[W], uint32_t diag, int32_t (&f)[W],
+                              int32_t (&x)[W], int32_t (&m)[W], int32_t &lf, int32_t &ly,
+                              int32_t dm) {
     uint32_t dmask = 0, lbits = 0;
 #pragma unroll
     for (int32_t w = 0; w < W; w++) {
-        const int32_t dx = w == WL ? dxl : kDX;
+        const int32_t dx = kDX;
         if (AFFINE) {
-            const int32_t ex = w == WL ? exl : kEX;
+            const int32_t ex = kEX;
             const int32_t yv = add_max(lf, kDY, ly + kEX);    // BandAligner.cpp:180-188
             const int32_t xv = add_max(f[w], dx, x[w] + ex);  // BandAligner.cpp:189-201
             const int32_t fv = dm + sc[w];                    // BandAligner.cpp:203-207
@@ -790,6 +799,35 @@ HERO_HD uint32_t dp_whole_row(const int32_t (&sc)[W], uint32_t diag, int32_t dxl
         }
     }
     return (dmask & diag) | (~dmask & lbits);
+}
+
+// Before a row: the lane holding column C of an align-left segment raises the
+// row-above FM and IX of that column (wl, 0-based in the strip) so that the
+// plain recurrence charges sx for the vertical moves there.  wl is the same for
+// the whole warp; the switch costs a uniform branch per row.
+template <bool AFFINE, int W>
+HERO_HD void dp_whole_left(int32_t wl, bool holds_c, int32_t (&f)[W], int32_t (&x)[W]) {
+    if (!holds_c) return;
+    switch (wl) {
+#define HERO_LEFT_CASE(w)                        \
+    case w:                                      \
+        if (w < W) {                             \
+            f[w < W ? w : 0] += kSX - kDX;       \
+            if (AFFINE) x[w < W ? w : 0] += kSX - kEX; \
+        }                                        \
+        break;
+        HERO_LEFT_CASE(0)
+        HERO_LEFT_CASE(1)
+        HERO_LEFT_CASE(2)
+        HERO_LEFT_CASE(3)
+        HERO_LEFT_CASE(4)
+        HERO_LEFT_CASE(5)
+        HERO_LEFT_CASE(6)
+        HERO_LEFT_CASE(7)
+#undef HERO_LEFT_CASE
+        default:
+            break;
+    }
 }
 
 // Whole-matrix fill by one thread, strip after strip.  Scratch provides
@@ -833,14 +871,19 @@ HERO_HD void dp_fill(const SegView &v, Scratch &sc) {
     }
 }
 
+// Op of each move code: up, left, diagonal mismatch, diagonal match (the
+// rows hold the longer segment; reversed = the query is on the rows).
+HERO_HD uint32_t dp_op_lut(const SegView &v) {
+    return uint32_t(v.reversed ? OP_I : OP_D) | (uint32_t(v.reversed ? OP_D : OP_I) << 2) |
+           (uint32_t(OP_X) << 4) | (uint32_t(OP_M) << 6);
+}
+
 // Traceback (BandAligner.cpp:114-125 / 227-238) from (R, C) to (0, 0).
 // emit(op) receives ops last-to-first; returns the path length.
 template <int W, class Scratch, class Emit>
 HERO_HD int32_t dp_walk(const SegView &v, const Scratch &sc, Emit &emit) {
     int32_t i = v.R, j = v.C, n = 0;
-    // op of each move: up, left, diagonal mismatch, diagonal match
-    const uint32_t lut = uint32_t(v.reversed ? OP_I : OP_D) | (uint32_t(v.reversed ? OP_D : OP_I) << 2) |
-                         (uint32_t(OP_X) << 4) | (uint32_t(OP_M) << 6);
+    const uint32_t lut = dp_op_lut(v);
     while (i > 0 || j > 0) {
         // row 0 traces left, column 0 up; inside, the code names the move
         uint32_t code = i == 0 ? 1u : 0u;
@@ -854,6 +897,72 @@ HERO_HD int32_t dp_walk(const SegView &v, const Scratch &sc, Emit &emit) {
         n++;
     }
     return n;
+}
+
+// ---------------------------------------------------------------------------
+// Traceback in row chunks, for the lanes of a wavefront group.  The path from
+// (R, C) to (0, 0) visits every row; lane s of G takes the moves that start in
+// rows (rbot, rtop] (the last chunk also takes the left moves along row 0).
+// A lane starts from a guessed column, walks its chunk, and is right once its
+// start equals the end of the lane before it (the true path enters row rtop
+// there); lanes that are not get new guesses and walk again.  Moves are the
+// ones dp_walk makes, so the concatenated chunks are its path exactly.
+// ---------------------------------------------------------------------------
+HERO_HD void dp_chunk_rows(int32_t R, int32_t G, int32_t s, int32_t &rtop, int32_t &rbot) {
+    const int32_t h = (R + G - 1) / G;
+    rtop = R - s * h > 0 ? R - s * h : 0;
+    rbot = R - (s + 1) * h > 0 ? R - (s + 1) * h : 0;
+}
+
+// First guess of the column where the path meets row rtop.  An align-left
+// segment climbs column C for free (vertical moves there cost sx), then runs
+// diagonally to (0, 0): column min(rtop, C).  Otherwise the path runs
+// diagonally from (R, C) (an align-right segment then climbs column 0).
+HERO_HD int32_t dp_chunk_guess(const SegView &v, int32_t rtop) {
+    if (v.left) return rtop < v.C ? rtop : v.C;
+    const int32_t c = v.C - (v.R - rtop);
+    return c > 0 ? c : 0;
+}
+
+// Walks from (i, j) while i > stop (column 0 moves up); with stop == 0 it also
+// makes the left moves along row 0.  Returns the number of moves; j is left at
+// the end column.
+template <int W, class Scratch>
+HERO_HD int32_t dp_walk_span(const Scratch &sc, int32_t i, int32_t &j, int32_t stop) {
+    int32_t n = 0;
+    while (i > stop) {
+        uint32_t code = 0u;
+        if (j > 0) {
+            const uint32_t jj = uint32_t(j - 1);
+            code = (sc.tb_get(int32_t(jj / W), i) >> (2 * (jj % W))) & 3u;
+        }
+        i -= code != 1u;
+        j -= code != 0u;
+        n++;
+    }
+    if (stop == 0) {
+        n += j;
+        j = 0;
+    }
+    return n;
+}
+
+// the same moves, handing each op to put() in walk order
+template <int W, class Scratch, class Put>
+HERO_HD void dp_walk_span_ops(const Scratch &sc, uint32_t lut, int32_t i, int32_t j, int32_t stop,
+                              Put &put) {
+    while (i > stop) {
+        uint32_t code = 0u;
+        if (j > 0) {
+            const uint32_t jj = uint32_t(j - 1);
+            code = (sc.tb_get(int32_t(jj / W), i) >> (2 * (jj % W))) & 3u;
+        }
+        i -= code != 1u;
+        j -= code != 0u;
+        put((lut >> (2 * code)) & 3u);
+    }
+    if (stop == 0)
+        for (; j > 0; j--) put((lut >> 2) & 3u);
 }
 
 // DpSum of the ops at positions [first, first + P) of a packed op array (16

@@ -762,6 +762,8 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
 // traces its segment back from there.
 // ---------------------------------------------------------------------------
 constexpr int kWaveWarps = 4;
+// traceback of a group: every lane a chunk of rows (true) or lane 0 alone (false)
+constexpr bool kChunkWalk = true;
 constexpr int kWaveMinBlocks = 4;  // caps registers at 128 per thread
 
 __global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks) {
@@ -820,11 +822,13 @@ __device__ __noinline__ void wave_fill(const SegView v, bool active, int32_t R, 
     }
 }
 
-// the wavefront over one warp's whole-band segments (dp_whole_row); WL is the
-// warp's align-left column, tab the lane's strip table in shared memory
-template <bool AFFINE, int WL>
+// the wavefront over one warp's whole-band segments (dp_whole_row); LEFT: the
+// warp's segments align left with column C at position wl of their last strip;
+// tab is the lane's strip table in shared memory
+template <bool AFFINE, bool LEFT>
 __device__ __noinline__ void wave_whole(const SegView v, bool active, int32_t R, int32_t Rw,
-                                           int G, int s, int lane, uint16_t *tb, int32_t *tab) {
+                                        int G, int s, int lane, int32_t wl, uint16_t *tb,
+                                        int32_t *tab) {
     const int32_t j0 = s * kStripW;
     int32_t f[kStripW], x[kStripW], m[kStripW], c0[3];
     int32_t pm = 0;
@@ -836,8 +840,7 @@ __device__ __noinline__ void wave_whole(const SegView v, bool active, int32_t R,
         dp_whole_col0<AFFINE>(v, c0);
         ch = (rp[0] ^ v.row_xor) & 3u;
     }
-    const bool last = s == G - 1;
-    const int32_t dxl = last ? kSX : kDX, exl = last ? kSX : kEX;
+    const bool holds_c = LEFT && s == G - 1;
     int32_t pf = kNEG, py = kNEG, pmv = kNEG;  // FM, IY, M published to lane s+1
     uint16_t *tp = tb + lane;
 #pragma unroll 1
@@ -859,8 +862,8 @@ __device__ __noinline__ void wave_whole(const SegView v, bool active, int32_t R,
             const int4 s1 = reinterpret_cast<const int4 *>(tab + a * kStripW)[1];
             const int32_t sc[kStripW] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
             const uint32_t diag = uint32_t(tab[4 * kStripW + a]);
-            const uint32_t bits = dp_whole_row<AFFINE, kStripW, WL>(sc, diag, dxl, exl, f, x, m, lf,
-                                                                     ly, pm);
+            if (LEFT) dp_whole_left<AFFINE, kStripW>(wl, holds_c, f, x);
+            const uint32_t bits = dp_whole_row<AFFINE, kStripW>(sc, diag, f, x, m, lf, ly, pm);
             *tp = uint16_t(bits);
             tp += 32;
             pf = lf;
@@ -871,22 +874,6 @@ __device__ __noinline__ void wave_whole(const SegView v, bool active, int32_t R,
     }
 }
 
-template <bool AFFINE>
-__device__ __forceinline__ void wave_whole_any(int wl, const SegView &v, bool active, int32_t R,
-                                               int32_t Rw, int G, int s, int lane, uint16_t *tb,
-                                               int32_t *tab) {
-    switch (wl) {
-        case 0: wave_whole<AFFINE, 0>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 1: wave_whole<AFFINE, 1>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 2: wave_whole<AFFINE, 2>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 3: wave_whole<AFFINE, 3>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 4: wave_whole<AFFINE, 4>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 5: wave_whole<AFFINE, 5>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 6: wave_whole<AFFINE, 6>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        case 7: wave_whole<AFFINE, 7>(v, active, R, Rw, G, s, lane, tb, tab); break;
-        default: wave_whole<AFFINE, -1>(v, active, R, Rw, G, s, lane, tb, tab); break;
-    }
-}
 
 template <bool AFFINE>
 __global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
@@ -932,7 +919,11 @@ __global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
         const bool whole = a.whole &&
                            __all_sync(0xffffffffu, !active || (dp_whole_band(v) && wl == wl0));
         if (whole) {
-            wave_whole_any<AFFINE>(wl0, v, active, R, Rw, G, s, lane, tb, tab);
+            if (wl0 >= 0) {
+                wave_whole<AFFINE, true>(v, active, R, Rw, G, s, lane, wl0, tb, tab);
+            } else {
+                wave_whole<AFFINE, false>(v, active, R, Rw, G, s, lane, -1, tb, tab);
+            }
         } else if (wfull) {
             if (wleft) {
                 wave_fill<AFFINE, true, true>(v, active, R, Rw, G, s, lane, wlast, tb);
@@ -947,25 +938,110 @@ __global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
             }
         }
         __syncwarp();
-        if (active && s == 0) {
-            struct SmemCodes {
-                const uint16_t *tb;
-                int base;
-                __device__ __forceinline__ uint32_t tb_get(int32_t st, int32_t i) const {
-                    return tb[size_t(i - 1) * 32u + base + st];
+        // Traceback.  When the ops fit in the group's strip tables in shared
+        // memory (free once the fill is done), every lane of the group walks a
+        // chunk of rows (dp_walk_span) from a guessed start; a start is right
+        // once it equals the end of the lane before, and each round makes at
+        // least one more lane right (mostly one round in all).  The verified
+        // chunks then write their ops at their offsets.  Otherwise lane s = 0
+        // walks the whole path.
+        uint32_t *const stage =
+            reinterpret_cast<uint32_t *>(wave_smem) + (size_t(wib) * 32u + size_t(g) * G) * kTabWords;
+        const bool staged = a.stride <= uint32_t(G) * kTabWords;
+        struct SmemCodes {
+            const uint16_t *tb;
+            int base;
+            __device__ __forceinline__ uint32_t tb_get(int32_t st, int32_t i) const {
+                return tb[size_t(i - 1) * 32u + base + st];
+            }
+        } sc{tb, g * G};
+        int32_t n = 0;
+        if (staged && !kChunkWalk) {
+            if (active && s == 0) {
+                OpsWriter w{stage, int32_t(a.stride * 16u)};
+                n = dp_walk<kStripW>(v, sc, w);
+                w.flush();
+            }
+            n = __shfl_sync(0xffffffffu, n, (g * G) & 31);
+        } else if (staged) {
+            if (active)
+                for (uint32_t k = uint32_t(s); k < a.stride; k += uint32_t(G)) stage[k] = 0u;
+            int32_t rtop = 0, rbot = 0, c = 0, e = 0, cnt = 0;
+            if (active) {
+                dp_chunk_rows(v.R, G, s, rtop, rbot);
+                c = s == 0 ? v.C : dp_chunk_guess(v, rtop);
+            }
+            const uint32_t gbits = G >= 32 ? 0xffffffffu : (1u << G) - 1u;
+            bool todo = active;
+            for (int round = 0; round <= 32; round++) {  // at most G rounds
+                if (todo) {
+                    int32_t jj = c;
+                    cnt = dp_walk_span<kStripW>(sc, rtop, jj, rbot);
+                    e = jj;
                 }
-            } sc{tb, g * G};
+                const int32_t pe = __shfl_up_sync(0xffffffffu, e, 1);
+                const bool wrong = active && s > 0 && c != pe;
+                const uint32_t gm = (__ballot_sync(0xffffffffu, wrong) >> (g * G)) & gbits;
+                if (!__any_sync(0xffffffffu, gm != 0u)) break;
+                // lanes from the first wrong one on start again where the lane
+                // before them ended (right for the first wrong lane, whose
+                // predecessor is right; a good guess for the rest)
+                const int32_t f = gm ? __ffs(int(gm)) - 1 : G;
+                todo = active && s >= f;
+                if (todo) c = pe;
+            }
+            int32_t before = cnt;  // ops of the lanes before this one (exclusive scan)
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int32_t y = __shfl_up_sync(0xffffffffu, before, d);
+                if (s >= d) before += y;
+            }
+            n = __shfl_sync(0xffffffffu, before, (g * G + G - 1) & 31);  // the group's total
+            before -= cnt;
+            __syncwarp();  // stage zeroed
+            if (active && cnt > 0) {
+                struct Put {
+                    uint32_t *stage;
+                    int32_t p;
+                    int32_t q;
+                    uint32_t acc;
+                    __device__ __forceinline__ void operator()(uint32_t op) {
+                        p--;
+                        if ((p >> 4) != q) {
+                            atomicOr(stage + q, acc);
+                            acc = 0u;
+                            q = p >> 4;
+                        }
+                        acc |= op << (2 * (p & 15));
+                    }
+                };
+                const int32_t p0 = int32_t(a.stride * 16u) - before;
+                Put put{stage, p0, (p0 - 1) >> 4, 0u};
+                dp_walk_span_ops<kStripW>(sc, dp_op_lut(v), rtop, c, rbot, put);
+                atomicOr(stage + put.q, put.acc);
+            }
+        } else if (active && s == 0) {
             uint32_t *words = a.ops + uint64_t(si) * a.stride;
             OpsWriter w{words, int32_t(a.stride * 16u)};
-            const int32_t n = dp_walk<kStripW>(v, sc, w);
+            n = dp_walk<kStripW>(v, sc, w);
             w.flush();
+        }
+        __syncwarp();
+        if (active && s == 0) {
             DpSum sum;
-            ops_summary(words, a.stride * 16u - uint32_t(n), uint32_t(n), sum);
+            ops_summary(staged ? stage : a.ops + uint64_t(si) * a.stride,
+                        a.stride * 16u - uint32_t(n), uint32_t(n), sum);
             a.sums[si] = sum;
             if (a.cells) {
                 const uint64_t cl = band_cells(v.R, v.C, v.band);
                 a.cells[si] = uint32_t(cl > 0xffffffffull ? 0xffffffffull : cl);
             }
+        }
+        if (staged && active) {  // the group's lanes copy the ops out together
+            uint32_t *out = a.ops + uint64_t(si) * a.stride;
+            for (uint32_t k = ((a.stride * 16u - uint32_t(n)) >> 4) + uint32_t(s); k < a.stride;
+                 k += uint32_t(G))
+                out[k] = stage[k];
         }
         __syncwarp();
     }

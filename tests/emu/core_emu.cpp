@@ -198,7 +198,14 @@ struct Vote {
 
 }  // namespace
 
+// test-harness instrumentation: rounds the chunked traceback of the last segment took
+int g_chunk_rounds = 0;
+
 extern "C" {
+int emu_chunk_rounds() { return g_chunk_rounds; }
+
+uint64_t emu_band_cells(int32_t R, int32_t C, int64_t m) { return band_cells(R, C, m); }
+
 
 // one DP segment through the core strip DP; same argument meaning as
 // hero_oracle_align (segments given directly, orientation forward)
@@ -224,8 +231,8 @@ int emu_align(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query,
 extern "C++" {
 // whole-band wavefront lanes (the kernel's wave_whole), stepped sequentially:
 // at step t every lane reads what its left neighbour published at step t-1
-template <bool AFFINE, int WL>
-void emu_whole(const SegView &v, int G, std::vector<uint16_t> &tb) {
+template <bool AFFINE, bool LEFT>
+void emu_whole(const SegView &v, int G, int32_t wl, std::vector<uint16_t> &tb) {
     constexpr int W = 8;
     struct Lane {
         int32_t f[W], x[W], m[W], c0[3], tab[kTabWords];
@@ -265,10 +272,8 @@ void emu_whole(const SegView &v, int G, std::vector<uint16_t> &tb) {
             int32_t sc[W];
             for (int w = 0; w < W; w++) sc[w] = x.tab[a * W + w];
             const uint32_t diag = uint32_t(x.tab[4 * W + a]);
-            const bool last = s == G - 1;
-            const uint32_t bits = dp_whole_row<AFFINE, W, WL>(sc, diag, last ? kSX : kDX,
-                                                              last ? kSX : kEX, x.f, x.x, x.m, lf,
-                                                              ly, x.pm);
+            if (LEFT) dp_whole_left<AFFINE, W>(wl, s == G - 1, x.f, x.x);
+            const uint32_t bits = dp_whole_row<AFFINE, W>(sc, diag, x.f, x.x, x.m, lf, ly, x.pm);
             tb[size_t(i - 1) * 32 + s] = uint16_t(bits);
             x.pf = lf;
             x.py = ly;
@@ -280,16 +285,10 @@ void emu_whole(const SegView &v, int G, std::vector<uint16_t> &tb) {
 
 template <bool AFFINE>
 void emu_whole_any(int wl, const SegView &v, int G, std::vector<uint16_t> &tb) {
-    switch (wl) {
-        case 0: emu_whole<AFFINE, 0>(v, G, tb); break;
-        case 1: emu_whole<AFFINE, 1>(v, G, tb); break;
-        case 2: emu_whole<AFFINE, 2>(v, G, tb); break;
-        case 3: emu_whole<AFFINE, 3>(v, G, tb); break;
-        case 4: emu_whole<AFFINE, 4>(v, G, tb); break;
-        case 5: emu_whole<AFFINE, 5>(v, G, tb); break;
-        case 6: emu_whole<AFFINE, 6>(v, G, tb); break;
-        case 7: emu_whole<AFFINE, 7>(v, G, tb); break;
-        default: emu_whole<AFFINE, -1>(v, G, tb); break;
+    if (wl >= 0) {
+        emu_whole<AFFINE, true>(v, G, wl, tb);
+    } else {
+        emu_whole<AFFINE, false>(v, G, -1, tb);
     }
 }
 }  // extern "C++"
@@ -372,6 +371,55 @@ int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *q
         wv[p >> 4] |= uint32_t(op) << (2 * (p & 15));
     };
     const int n = dp_walk<W>(v, sc, emit);
+    {  // the kernel's chunked traceback (one chunk of rows per lane), lanes in turn
+        const int32_t P = int32_t(words * 16);
+        std::vector<int32_t> rtop(G), rbot(G), c(G), e(G), cnt(G);
+        std::vector<char> todo(G, 1);
+        for (int s = 0; s < G; s++) {
+            dp_chunk_rows(v.R, G, s, rtop[s], rbot[s]);
+            c[s] = s == 0 ? v.C : dp_chunk_guess(v, rtop[s]);
+        }
+        int f = 0;
+        g_chunk_rounds = 0;
+        for (int round = 0; round <= 32; round++) {
+            g_chunk_rounds++;
+            for (int s = 0; s < G; s++)
+                if (todo[s]) {
+                    int32_t jj = c[s];
+                    cnt[s] = dp_walk_span<W>(sc, rtop[s], jj, rbot[s]);
+                    e[s] = jj;
+                }
+            f = G;
+            for (int s = 1; s < G; s++)
+                if (c[s] != e[s - 1]) {
+                    f = s;
+                    break;
+                }
+            if (f == G) break;
+            for (int s = 0; s < G; s++) {  // from the first wrong lane on: the previous end
+                todo[s] = s >= f;
+                if (todo[s]) c[s] = e[s - 1];
+            }
+        }
+        if (f != G) return -6;
+        std::vector<uint32_t> cw(words + 1, 0);
+        int32_t Ps = P;
+        const uint32_t lut = dp_op_lut(v);
+        for (int s = 0; s < G; s++) {
+            int32_t pp = Ps;
+            auto put = [&](uint32_t op) {
+                pp--;
+                cw[pp >> 4] |= op << (2 * (pp & 15));
+            };
+            dp_walk_span_ops<W>(sc, lut, rtop[s], c[s], rbot[s], put);
+            if (Ps - pp != cnt[s]) return -7;
+            Ps -= cnt[s];
+        }
+        if (P - Ps != n) return -5;
+        for (int32_t q = 0; q < n; q++)
+            if (ops_field(cw.data(), uint32_t(P - n + q)) != ops_field(wv.data(), uint32_t(P - n + q)))
+                return -5;
+    }
     DpSum sum;
     ops_summary(wv.data(), words * 16 - uint32_t(n), uint32_t(n), sum);
     // cross-check the word-level summary against per-op counting

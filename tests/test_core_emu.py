@@ -62,3 +62,49 @@ def test_pipeline_matches_oracle(oracle, emu, name):
     from hero_testlib import assert_same_consensus
     assert_same_consensus(want, got, name)
     assert np.array_equal(want["votes"], got["votes"])
+
+
+def _indels(rng, x, rate):
+    out = []
+    for b in x:
+        r = rng.random()
+        if r < rate:             # deletion
+            continue
+        out.append(b)
+        if r > 1 - rate:         # insertion
+            out.append(ACGT[rng.integers(0, 4)])
+    return np.array(out, np.uint8)
+
+
+@pytest.mark.parametrize("affine", [0, 1])
+def test_wave_long_segments_with_indels(oracle, emu, affine):
+    """Segments of 150-260 bases with substitutions and indels: many strips per
+    segment, so the traceback runs in row chunks over many lanes, and paths
+    that leave the diagonal make the first guesses wrong."""
+    rng = np.random.default_rng(300 + affine)
+    for _ in range(150):
+        ls = int(rng.integers(150, 261))
+        s = ACGT[rng.integers(0, 4, ls)]
+        q = _indels(rng, synth.substitute(rng, s.copy(), 0.03), float(rng.choice([0.002, 0.01, 0.05])))
+        q = q[:int(rng.integers(max(1, len(q) - 40), len(q) + 1))]
+        band = int(rng.choice([300, 1000]))
+        right, left = bool(rng.integers(0, 2)), bool(rng.integers(0, 2))
+        want, _ = oracle.align(affine, bytes(s), bytes(q), band, right, left)
+        got = emu.align_wave(affine, bytes(s), bytes(q), band, right, left)
+        assert np.array_equal(want, got), (affine, len(s), len(q), band, right, left)
+
+
+def test_band_cells_closed_form(emu):
+    """band_cells (the reference's loop bounds, BandAligner.cpp:63-66) against the loop."""
+    import ctypes as C
+    f = emu.lib.emu_band_cells
+    f.restype = C.c_uint64
+    f.argtypes = [C.c_int32, C.c_int32, C.c_int64]
+    rng = np.random.default_rng(5)
+    for _ in range(3000):
+        c = int(rng.integers(0, 300))
+        r = c + int(rng.integers(0, 300))
+        m = max(int(rng.choice([0, 1, 3, 10, 80, 300, 70000])), r - c)  # band >= R - C
+        want = sum(min(c, i + m) - max(0, i - m) + 1 for i in range(r + 1)
+                   if min(c, i + m) >= max(0, i - m))
+        assert f(r, c, m) == want, (r, c, m)
