@@ -1250,23 +1250,34 @@ struct VoteVisitor {
         if (s.tot[OP_M] == P) {  // one match run
             match(P);
         } else {
+            // ops a word (16) at a time: match stretches advance at once, the
+            // other ops are found by their non-zero 2-bit fields (OP_M is 0)
             const uint32_t *w = ops + uint64_t(seg) * stride;
-            const uint32_t first = stride * 16u - P;
-            for (uint32_t t = 0; t < P; t++) {
-                const uint32_t pos = first + t;
-                const uint8_t op = uint8_t((w[pos >> 4] >> (2 * (pos & 15))) & 3u);
-                if (op == OP_M) {
-                    match(1);
-                } else if (op == OP_X) {
-                    mismatch();
-                } else {
-                    close();
-                    if (op == OP_I) {
-                        pq++;
+            const uint32_t end = stride * 16u;
+            for (uint32_t pos = end - P; pos < end;) {
+                const uint32_t f0 = pos & 15u, nf = 16u - f0;  // fields left in this word
+                const uint32_t word = w[pos >> 4] >> (2 * f0);
+                uint32_t nm = (word | (word >> 1)) & 0x55555555u;
+                uint32_t done = 0;
+                while (nm) {
+                    const uint32_t b = uint32_t(__ffs(int(nm))) - 1u, fi = b >> 1;
+                    if (fi > done) match(int64_t(fi - done));
+                    const uint32_t op = (word >> b) & 3u;
+                    if (op == OP_X) {
+                        mismatch();
                     } else {
-                        ps++;
+                        close();
+                        if (op == OP_I) {
+                            pq++;
+                        } else {
+                            ps++;
+                        }
                     }
+                    done = fi + 1u;
+                    nm &= nm - 1u;
                 }
+                if (nf > done) match(int64_t(nf - done));
+                pos += nf;
             }
         }
         seg++;
