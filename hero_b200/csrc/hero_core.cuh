@@ -86,6 +86,20 @@ HERO_HD void kmer_push(Kmer &m, uint32_t code, int k) {
     }
 }
 
+// Adds a base as the most significant of k digits (the reverse complement of a
+// window rolls this way: the base entering the window goes on top, the base
+// leaving it drops off the bottom).
+HERO_HD void kmer_push_front(Kmer &m, uint32_t code, int k) {
+    m.lo = (m.lo >> 2) | (m.hi << 62);
+    m.hi >>= 2;
+    const int b = 2 * (k - 1);
+    if (b < 64) {
+        m.lo |= uint64_t(code) << b;
+    } else {
+        m.hi |= uint64_t(code) << (b - 64);
+    }
+}
+
 // Jobs served together share one k-mer table: a key carries its job above the
 // 2k k-mer bits, so keys of different jobs never compare equal (job must fit
 // in the 128 - 2k bits left: kmer_job_bits).

@@ -332,16 +332,26 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
         if (subj.good[s] && L >= k) {
             const int32_t P = L - k + 1;
             if (lane == 0) probes += 2ull * uint64_t(P);
-            for (int32_t f = int32_t(lane); f < P; f += 32) {
-                Kmer fm{0, 0}, rm{0, 0};
-                bool bad = false;
-                for (int32_t i = 0; i < k; i++) {
-                    const uint8_t x = c[f + i];
-                    bad |= x >= 4;
-                    kmer_push(fm, x & 3u, k);
+            // lane takes the windows [fa, fb): contiguous, so both k-mers roll one
+            // base per window; nbad counts the non-ACGT bases in the window
+            const int32_t fa = int32_t(int64_t(P) * lane / 32), fb = int32_t(int64_t(P) * (lane + 1) / 32);
+            Kmer fr{0, 0}, rr{0, 0};
+            int32_t nbad = 0;
+            if (fa < fb)
+                for (int32_t i = 0; i < k - 1; i++) {
+                    const uint8_t x = c[fa + i];
+                    nbad += x >= 4;
+                    kmer_push(fr, x & 3u, k);
+                    kmer_push_front(rr, (x & 3u) ^ 2u, k);
                 }
-                if (bad) continue;
-                for (int32_t i = k - 1; i >= 0; i--) kmer_push(rm, (c[f + i] & 3u) ^ 2u, k);
+            for (int32_t f = fa; f < fb; f++) {
+                const uint8_t x = c[f + k - 1];
+                nbad += x >= 4;
+                if (f > fa) nbad -= c[f - 1] >= 4;
+                kmer_push(fr, x & 3u, k);
+                kmer_push_front(rr, (x & 3u) ^ 2u, k);
+                if (nbad) continue;
+                Kmer fm = fr, rm = rr;
                 if (subj.job) {
                     kmer_tag(fm, subj.job[s], k);
                     kmer_tag(rm, subj.job[s], k);
@@ -421,12 +431,57 @@ __device__ void bitonic(uint64_t *a, uint64_t n, uint64_t N) {
     }
 }
 
+// The same network run by one warp on up to kWarpSort hits in shared memory,
+// with power-of-two index arithmetic (segments hold ~100 hits).
+constexpr int kWarpSort = 512;
+
+__device__ __forceinline__ void bitonic_warp(uint64_t *a, uint32_t n, uint32_t lgN) {
+    const uint32_t lane = threadIdx.x & 31u, N = 1u << lgN;
+    for (uint32_t lk = 1; lk <= lgN; lk++) {
+        const uint32_t k = 1u << lk, hm = (k >> 1) - 1u;
+        for (uint32_t i = lane; i < N / 2; i += 32u) {  // mirror step of stage k
+            const uint32_t base = (i >> (lk - 1)) << lk, off = i & hm;
+            const uint32_t lo = base + off, hi = base + k - 1u - off;
+            if (hi < n) cmpx(a, lo, hi);
+        }
+        __syncwarp();
+        for (uint32_t lj = lk - 1; lj-- > 0;) {  // half cleaners, j = 2^lj
+            const uint32_t jm = (1u << lj) - 1u;
+            for (uint32_t i = lane; i < N / 2; i += 32u) {
+                const uint32_t lo = ((i >> lj) << (lj + 1)) + (i & jm), hi = lo + (1u << lj);
+                if (hi < n) cmpx(a, lo, hi);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// small segments: one warp each, in shared memory
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_hits_warp(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits) {
+    __shared__ uint64_t sm[kSortThreads / 32][kWarpSort];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    for (uint64_t seg = uint64_t(blockIdx.x) * (kSortThreads / 32) + wib; seg < nseg;
+         seg += uint64_t(gridDim.x) * (kSortThreads / 32)) {
+        const uint64_t b = hit_off[seg], n = hit_off[seg + 1] - b;
+        if (n < 2 || n > uint64_t(kWarpSort)) continue;
+        uint32_t lgN = 0;
+        while ((1u << lgN) < uint32_t(n)) lgN++;
+        uint64_t *a = sm[wib];
+        for (uint32_t i = lane; i < uint32_t(n); i += 32u) a[i] = hits[b + i];
+        __syncwarp();
+        bitonic_warp(a, uint32_t(n), lgN);
+        for (uint32_t i = lane; i < uint32_t(n); i += 32u) hits[b + i] = a[i];
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(kSortThreads)
     k_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits) {
     __shared__ uint64_t sm[kSortSmem];
     for (uint64_t seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
         const uint64_t b = hit_off[seg], n = hit_off[seg + 1] - b;
-        if (n < 2) continue;
+        if (n <= uint64_t(kWarpSort)) continue;  // sorted by k_sort_hits_warp
         uint64_t N = 1;
         while (N < n) N <<= 1;
         if (n <= uint64_t(kSortSmem)) {
@@ -1548,6 +1603,9 @@ void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableVi
 void launch_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits, cudaStream_t st) {
     if (!nseg) return;
     const unsigned g = unsigned(nseg < 148u * 16u ? nseg : 148u * 16u);
+    counted();
+    k_sort_hits_warp<<<grid_1d(nseg, kSortThreads / 32, 148u * 8u), kSortThreads, 0, st>>>(
+        nseg, hit_off, hits);
     counted();
     k_sort_hits<<<g, kSortThreads, 0, st>>>(nseg, hit_off, hits);
 }

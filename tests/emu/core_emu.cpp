@@ -206,6 +206,25 @@ int emu_chunk_rounds() { return g_chunk_rounds; }
 
 uint64_t emu_band_cells(int32_t R, int32_t C, int64_t m) { return band_cells(R, C, m); }
 
+// rolling forward / reverse-complement k-mers (the probe kernel) against
+// building each window from scratch; returns the first bad window or -1
+int64_t emu_kmer_roll_check(const uint8_t *codes, int64_t n, int32_t k) {
+    Kmer fr{0, 0}, rr{0, 0};
+    for (int64_t i = 0; i + 1 < k && i < n; i++) {
+        kmer_push(fr, codes[i] & 3u, k);
+        kmer_push_front(rr, (codes[i] & 3u) ^ 2u, k);
+    }
+    for (int64_t f = 0; f + k <= n; f++) {
+        kmer_push(fr, codes[f + k - 1] & 3u, k);
+        kmer_push_front(rr, (codes[f + k - 1] & 3u) ^ 2u, k);
+        Kmer fm{0, 0}, rm{0, 0};
+        for (int32_t i = 0; i < k; i++) kmer_push(fm, codes[f + i] & 3u, k);
+        for (int32_t i = k - 1; i >= 0; i--) kmer_push(rm, (codes[f + i] & 3u) ^ 2u, k);
+        if (fm.lo != fr.lo || fm.hi != fr.hi || rm.lo != rr.lo || rm.hi != rr.hi) return f;
+    }
+    return -1;
+}
+
 
 // one DP segment through the core strip DP; same argument meaning as
 // hero_oracle_align (segments given directly, orientation forward)

@@ -108,3 +108,16 @@ def test_band_cells_closed_form(emu):
         want = sum(min(c, i + m) - max(0, i - m) + 1 for i in range(r + 1)
                    if min(c, i + m) >= max(0, i - m))
         assert f(r, c, m) == want, (r, c, m)
+
+
+def test_rolling_kmers_match_direct(emu):
+    """The probe kernel rolls forward and reverse-complement k-mers one base per
+    window; every window equals the k-mer built from scratch, for all k."""
+    import ctypes as C
+    f = emu.lib.emu_kmer_roll_check
+    f.restype = C.c_int64
+    f.argtypes = [C.c_void_p, C.c_int64, C.c_int32]
+    rng = np.random.default_rng(9)
+    codes = rng.integers(0, 4, 400).astype(np.uint8)
+    for k in (1, 2, 15, 21, 31, 32, 33, 39, 47, 63):
+        assert f(codes.ctypes.data, len(codes), k) == -1, k
