@@ -41,10 +41,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM traffic (read + write) of the affine DP kernel per band cell, from one ncu
-# capture of a whole launch (profiles/k_dp_wave_affine_100kbp.md: 2.913 GB for
+# capture of a whole launch (profiles/k_dp_wave_affine_100kbp.md: 2.200 GB for
 # 23.19 G cells); the traffic is per segment (codes in, ops and summaries out),
 # so it scales with the cells of a launch
-DP_DRAM_BYTES_PER_CELL = 2.913069e9 / 23_186_600_877
+DP_DRAM_BYTES_PER_CELL = 2.199761e9 / 23_186_600_877
 
 
 def log(*a):
@@ -275,8 +275,13 @@ def run_served(jobs, reads, dev: int, busy_target: float = 0.85, check: int = 3)
     from hero_b200 import HeroServer, correct
     srv = HeroServer(aligner="affine", device=dev)
     try:
-        # warm-up and calibration: the first jobs submitted at once, back to back
-        cal = list(range(min(8, len(jobs))))
+        # warm-up (the server's context sizes its device buffers), then capacity:
+        # jobs submitted all at once, back to back (closed loop)
+        for i in range(min(2, len(jobs))):
+            j = srv.submit(*reads[i])
+            srv.wait(j)
+            srv.release(j)
+        cal = list(range(min(16, len(jobs))))
         t0 = time.perf_counter()
         ids = [srv.submit(*reads[i]) for i in cal]
         for j in ids:
@@ -328,7 +333,7 @@ def run_served(jobs, reads, dev: int, busy_target: float = 0.85, check: int = 3)
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
             "bases_per_s": bases / ((last - first) / 1e3),
-            "arrival_rate_per_s": lam, "calibrated_bases_per_s": thr,
+            "arrival_rate_per_s": lam, "capacity_bases_per_s": thr,
             "busy_frac": (s1["busy_ms"] - s0["busy_ms"]) / (last - first),
             "rounds": rounds, "mean_jobs_per_round": len(jobs) / max(rounds, 1),
             "served_equals_alone": f"{ok}/{len(picks)}",
