@@ -228,6 +228,16 @@ def bench_reference(args):
 # ---------------------------------------------------------------------------
 # GPU path
 # ---------------------------------------------------------------------------
+def hbm_peak_gbs() -> tuple[float, str]:
+    """Measured HBM copy bandwidth of this pool's B200s (MEASURED_PEAKS.json), else
+    the recorded fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
 def int_peak_tops(device: int) -> float | None:
     import ctypes as C
     from hero_b200 import build
@@ -488,6 +498,15 @@ def bench_hero(args):
     traffic = (DP_DRAM_BYTES_PER_CELL * cells / dp_launches
                if DP_DRAM_BYTES_PER_CELL is not None else None)
     clocks = clk.summary()
+    # seeding against HBM: per probe one 24-byte key+value slot read, per hit the
+    # hit value (8 B) read and the hit tuple (16 B) written, the subject reads at
+    # 2 bits a base (algorithmic bytes of the probe phase)
+    probes = (p1["probes"] - p0["probes"]) / plain_steps
+    hits = (p1["hits"] - p0["hits"]) / plain_steps
+    seed_bytes = 24 * probes + 24 * hits + nb / 4
+    seed_ms = per["ms_seed"]
+    hbm_peak, hbm_src = hbm_peak_gbs()
+    seed_gbs = seed_bytes / (seed_ms / 1e3) / 1e9 if seed_ms > 0 else None
 
     h.close()
     served = None
@@ -523,6 +542,11 @@ def bench_hero(args):
                          "ops_per_cell": ops_per_cell,
                          "peak_source": "int add+max microbenchmark in this run "
                                         "(MEASURED_PEAKS.json has no integer peak)"},
+            "seeding_roofline": {"bound": "hbm", "kernels": "k_probe (count, emit) + k_sort_hits",
+                                 "achieved": seed_gbs, "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": (seed_gbs / hbm_peak) if seed_gbs else None,
+                                 "algorithmic_bytes_per_step": seed_bytes,
+                                 "peak_source": hbm_src},
             "gcups": cells / (dp_ms / 1e3) / 1e9 if dp_ms > 0 else None,
             "form": "batched (whole round replayed as one CUDA graph)",
             "plain_form": {"value": plain_value, "ms_per_step": 1e3 * t_plain / plain_steps,

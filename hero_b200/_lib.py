@@ -27,8 +27,12 @@ EXPORTS = [
     "hero_reset_votes", "hero_align_segments_noalloc", "hero_round", "hero_fetch",
     "hero_set_query_jobs", "hero_server_create", "hero_server_destroy", "hero_job_submit",
     "hero_job_poll", "hero_job_wait", "hero_job_result", "hero_job_error", "hero_job_release",
-    "hero_server_get_stats", "hero_job_bytes", "hero_round_admit",
+    "hero_server_get_stats", "hero_job_bytes", "hero_round_admit", "hero_set_dp_tuning",
+    "hero_server_set_dp_tuning",
 ]
+
+# the autotuner's record (hero_b200.autotune); loaded by every Hero unless told otherwise
+TUNING_PATH = os.path.join(HERE, "tuning.json")
 
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 
@@ -56,6 +60,21 @@ _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record"
 class HeroStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
                 [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64)])
+
+
+class DpTuning(C.Structure):
+    _fields_ = [("rows_max", C.c_int32), ("warps_per_block", C.c_int32),
+                ("pair_strips", C.c_uint32), ("chunk_strips", C.c_uint32)]
+
+
+def load_tuning(path: str | None = None) -> list[dict]:
+    """Classes recorded by the autotuner (empty when there is no record)."""
+    import json
+    p = path or os.environ.get("HERO_B200_TUNING") or TUNING_PATH
+    if not p or not os.path.exists(p):
+        return []
+    with open(p) as f:
+        return json.load(f).get("classes", [])
 
 
 class JobInfo(C.Structure):
@@ -105,6 +124,10 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          C.c_uint64] + [vp] * 12)
     lib.hero_set_query_jobs.argtypes = [vp, vp, C.c_uint64]
+    lib.hero_set_dp_tuning.argtypes = [vp, C.POINTER(DpTuning), C.c_uint32]
+    lib.hero_set_dp_tuning.restype = C.c_int
+    lib.hero_server_set_dp_tuning.argtypes = [vp, C.POINTER(DpTuning), C.c_uint32]
+    lib.hero_server_set_dp_tuning.restype = C.c_int
     lib.hero_server_create.argtypes = [C.POINTER(HeroParams), C.c_uint64, C.POINTER(vp)]
     lib.hero_server_destroy.argtypes = [vp]
     lib.hero_job_submit.argtypes = [vp, vp, vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
@@ -149,7 +172,8 @@ class Hero:
     def __init__(self, k: int = 39, min_overlap: int = 40, aligner: str = "global",
                  max_mismatch_rate: float = 1.0, max_indel_rate: float = 1.0,
                  consensus_threshold: float = 0.6, device: int = 0, subject_batch: int = 0,
-                 device_memory_budget: int = 0, stream: int | None = None):
+                 device_memory_budget: int = 0, stream: int | None = None,
+                 tuning: list[dict] | str | None = None):
         self.lib = load_library()
         p = HeroParams()
         self.lib.hero_default_params(C.byref(p))
@@ -171,6 +195,16 @@ class Hero:
         self.h = h
         self.nq = 0
         self.nqb = 0
+        # DP kernel shapes: the given classes, a record file, or the default record
+        self.set_tuning(load_tuning(tuning) if not isinstance(tuning, list) else tuning)
+
+    def set_tuning(self, classes: list[dict]):
+        """DP kernel shapes per class of batch ([] = the library's defaults)."""
+        arr = (DpTuning * max(1, len(classes)))()
+        for i, t in enumerate(classes):
+            arr[i] = DpTuning(int(t["rows_max"]), int(t["warps_per_block"]),
+                              int(t["pair_strips"]), int(t["chunk_strips"]))
+        self._check(self.lib.hero_set_dp_tuning(self.h, arr, len(classes)), "set_tuning")
 
     def _check(self, rc: int, what: str):
         if rc != HERO_OK:
@@ -319,7 +353,7 @@ def _params(k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0, max_i
 class HeroServer:
     """Serving form: independent correction jobs, continuous batching (hero_server_*)."""
 
-    def __init__(self, round_bytes: int = 0, **kw):
+    def __init__(self, round_bytes: int = 0, tuning: list[dict] | str | None = None, **kw):
         self.lib = load_library()
         self.params = _params(**kw)
         h = C.c_void_p()
@@ -328,6 +362,12 @@ class HeroServer:
             raise HeroError(f"hero_server_create failed: {ERRORS.get(rc, rc)}")
         self.h = h
         self._sizes: dict[int, tuple[int, int]] = {}
+        classes = load_tuning(tuning) if not isinstance(tuning, list) else tuning
+        arr = (DpTuning * max(1, len(classes)))()
+        for i, t in enumerate(classes):
+            arr[i] = DpTuning(int(t["rows_max"]), int(t["warps_per_block"]),
+                              int(t["pair_strips"]), int(t["chunk_strips"]))
+        self.lib.hero_server_set_dp_tuning(self.h, arr, len(classes))
 
     def close(self):
         if getattr(self, "h", None):

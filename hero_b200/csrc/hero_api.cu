@@ -81,6 +81,7 @@ struct hero_ctx {
     cudaGraphExec_t gexec = nullptr;
     DBuf stamps;  // DP kernel start/stop times per batch (ns), written inside the graph
     DBuf fp;
+    std::vector<hero_dp_tuning> tuning;  // DP kernel shapes per class of batch
 
     hero_ctx() {
         DBuf *list[] = {&q_raw, &q_code, &q_off, &q_len, &q_uid, &q_good, &q_sgood, &q_gc,
@@ -172,6 +173,17 @@ static const uint32_t *job_tags(hero_ctx *c) { return c->tagged ? P_<uint32_t>(c
 static ReadsView query_view(hero_ctx *c) {
     return ReadsView{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
                      P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_good), c->nq, job_tags(c)};
+}
+
+// kernel shape of a DP launch from the tuning table (first class covering rmax)
+static void apply_tuning(const hero_ctx *c, DpLaunch &a) {
+    for (const hero_dp_tuning &t : c->tuning)
+        if (a.rmax <= t.rows_max) {
+            a.warps = t.warps_per_block == 2 ? 2 : 4;
+            a.pair_mask = t.pair_strips;
+            a.chunk_mask = t.chunk_strips;
+            return;
+        }
 }
 
 static double elapsed(cudaEvent_t a, cudaEvent_t b) {
@@ -326,6 +338,17 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     for (uint8_t x : g) ng += x;
     c->stats.good_queries = ng;
     c->have_queries = true;
+    return HERO_OK;
+}
+
+extern "C" int hero_set_dp_tuning(hero_ctx *c, const hero_dp_tuning *t, uint32_t n) {
+    if (!c) return HERO_E_INPUT;
+    if (n && !t) return c->fail(HERO_E_INPUT, "null tuning table");
+    for (uint32_t i = 0; i < n; i++)
+        if (t[i].warps_per_block != 2 && t[i].warps_per_block != 4)
+            return c->fail(HERO_E_INPUT, "warps_per_block must be 2 or 4");
+    c->tuning.assign(t, t + n);
+    c->plan_ok = false;  // a captured round keeps the shapes it was captured with
     return HERO_OK;
 }
 
@@ -533,7 +556,9 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         DpLaunch a{P_<DpSeg>(c->segs), P_<uint32_t>(c->perm), ND, subj.code, subj.off, subj.len,
                    q.code, q.off, P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums),
                    P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
-                   c->p.affine, 1};  // reads with a non-ACGT base never reach the DP
+                   c->p.affine, 1,  // reads with a non-ACGT base never reach the DP
+                   0u, 0u, kStripsAll, 4};
+        apply_tuning(c, a);
         launch_dp(a, P_<uint64_t>(c->bin_off), P_<uint64_t>(c->dp_tasks), cmax, c->st);
         if ((r = c->check_launch("dp"))) break;
         rec(4);
@@ -895,7 +920,8 @@ extern "C" int hero_align_segments(hero_ctx *c, int affine, const uint8_t *subj,
         DpLaunch a{P_<DpSeg>(dsegs), P_<uint32_t>(dperm), n_seg, P_<uint8_t>(scode), P_<uint64_t>(soff),
                    P_<uint32_t>(slen), P_<uint8_t>(qcode), P_<uint64_t>(qoff), P_<uint32_t>(dops),
                    stride, P_<DpSum>(dsums), nullptr, P_<uint16_t>(dtb), P_<int32_t>(dbnd),
-                   c->dp_T, rmax, affine ? 1 : 0, acgt ? 1 : 0};
+                   c->dp_T, rmax, affine ? 1 : 0, acgt ? 1 : 0, 0u, 0u, kStripsAll, 4};
+        apply_tuning(c, a);
         launch_dp(a, P_<uint64_t>(dbinoff), P_<uint64_t>(dtasks), cmax, c->st);
         launch_unpack_ops(P_<uint32_t>(dops), stride, P_<DpSum>(dsums), n_seg, P_<uint64_t>(doo),
                           P_<uint8_t>(dout), P_<int32_t>(dn), c->st);

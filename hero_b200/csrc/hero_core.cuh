@@ -844,6 +844,157 @@ HERO_HD void dp_whole_left(int32_t wl, bool holds_c, int32_t (&f)[W], int32_t (&
     }
 }
 
+// ---------------------------------------------------------------------------
+// Whole-band rows of two segments at once, as signed 16-bit halves of each
+// 32-bit register (segment A low, B high): one DPX instruction advances a cell
+// of each.  Two segments share a lane when they have the same rows, strips and
+// align-left column (the shape key), so their wavefronts run in lockstep.
+// Every value of a whole-band matrix is a real score, -4(R+C) <= v <= R, and
+// the columns past C start at kNEG16 and lose at most 5 per row, so with
+// R + C <= kPairMaxSide no half ever wraps.
+// ---------------------------------------------------------------------------
+constexpr int32_t kNEG16 = -16384;
+constexpr int32_t kPairMaxSide = 2000;  // R + C of a segment in a packed pair
+constexpr int kTabWords2 = 40;          // per lane: int16 scores [2][4][8], diag words [2][4]
+
+HERO_HD uint32_t pack2(int32_t lo, int32_t hi) { return (uint32_t(lo) & 0xffffu) | (uint32_t(hi) << 16); }
+HERO_HD int32_t half_lo(uint32_t v) { return int32_t(int16_t(uint16_t(v & 0xffffu))); }
+HERO_HD int32_t half_hi(uint32_t v) { return int32_t(int16_t(uint16_t(v >> 16))); }
+
+// per half: max(a + b, c)
+HERO_HD uint32_t add_max2(uint32_t a, uint32_t b, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __viaddmax_s16x2(a, b, c);
+#else
+    const int32_t l = half_lo(a) + half_lo(b), h = half_hi(a) + half_hi(b);
+    return pack2(l > half_lo(c) ? l : half_lo(c), h > half_hi(c) ? h : half_hi(c));
+#endif
+}
+
+// per half: a + b (the floor of the add-max is never reached)
+HERO_HD uint32_t add2(uint32_t a, uint32_t b) { return add_max2(a, b, 0x80008000u); }
+
+// per half: max(a, b, c)
+HERO_HD uint32_t max3_2(uint32_t a, uint32_t b, uint32_t c) {
+#if defined(__CUDA_ARCH__)
+    return __vimax3_s16x2(a, b, c);
+#else
+    const int32_t l = max3(half_lo(a), half_lo(b), half_lo(c));
+    const int32_t h = max3(half_hi(a), half_hi(b), half_hi(c));
+    return pack2(l, h);
+#endif
+}
+
+// per half: a >= b (lo, hi)
+HERO_HD void ge2(uint32_t a, uint32_t b, bool &lo, bool &hi) {
+#if defined(__CUDA_ARCH__)
+    (void)__vibmax_s16x2(a, b, &hi, &lo);
+#else
+    lo = half_lo(a) >= half_lo(b);
+    hi = half_hi(a) >= half_hi(b);
+#endif
+}
+
+// Tables of strip j0+1 .. j0+W for segments A and B: int16 scores per base
+// (tab16[seg][base][w]) and the diagonal codes (words 32.. : [seg][base]).
+template <int W>
+HERO_HD void dp_pair_table(const SegView &va, const SegView &vb, int32_t j0, uint32_t *tab) {
+    uint16_t *sc = reinterpret_cast<uint16_t *>(tab);
+    for (int h = 0; h < 2; h++) {
+        const SegView &v = h ? vb : va;
+        uint32_t dg[4] = {0, 0, 0, 0};
+        for (int32_t w = 0; w < W; w++) {
+            const int32_t j = j0 + w + 1;
+            const uint32_t b = j <= v.C ? v.col(j) : 7u;
+            for (uint32_t c = 0; c < 4; c++) {
+                const bool eq = b == c;
+                sc[(h * 4 + c) * W + w] = uint16_t(int16_t(eq ? kHIT : kMISS));
+                dg[c] |= (2u | uint32_t(eq)) << (2 * w);
+            }
+        }
+        for (int c = 0; c < 4; c++) tab[32 + h * 4 + c] = dg[c];
+    }
+}
+
+// row-0 states of the strip (packed) and M at (0, j0)
+template <int W>
+HERO_HD void dp_pair_init(const SegView &va, const SegView &vb, int32_t j0, uint32_t (&f)[W],
+                          uint32_t (&x)[W], uint32_t (&m)[W], uint32_t &pm) {
+#pragma unroll
+    for (int32_t w = 0; w < W; w++) {
+        const int32_t j = j0 + w + 1;
+        const Cell3 a = j <= va.C ? dp_row0<true>(va, j) : Cell3{kNEG16, kNEG16, kNEG16};
+        const Cell3 b = j <= vb.C ? dp_row0<true>(vb, j) : Cell3{kNEG16, kNEG16, kNEG16};
+        f[w] = pack2(a.f, b.f);
+        x[w] = pack2(a.x, b.x);
+        m[w] = pack2(max3(a.f, a.x, a.y), max3(b.f, b.x, b.y));
+    }
+    const Cell3 a = dp_row0<true>(va, j0), b = dp_row0<true>(vb, j0);
+    pm = pack2(max3(a.f, a.x, a.y), max3(b.f, b.x, b.y));
+}
+
+// One affine row of a pair (dp_whole_row on both halves).  Returns the codes
+// of A in the low 16 bits and of B in the high 16 bits.
+template <int W>
+HERO_HD uint32_t dp_pair_row(const uint32_t (&sc)[W], uint32_t diag_a, uint32_t diag_b,
+                             uint32_t (&f)[W], uint32_t (&x)[W], uint32_t (&m)[W], uint32_t &lf,
+                             uint32_t &ly, uint32_t dm) {
+    constexpr uint32_t DY2 = (uint32_t(kDY) & 0xffffu) * 0x10001u;
+    constexpr uint32_t DX2 = (uint32_t(kDX) & 0xffffu) * 0x10001u;
+    constexpr uint32_t EX2 = (uint32_t(kEX) & 0xffffu) * 0x10001u;
+    uint32_t da = 0, db = 0, la = 0, lb = 0;
+#pragma unroll
+    for (int32_t w = 0; w < W; w++) {
+        const uint32_t yv = add_max2(lf, DY2, add2(ly, EX2));      // BandAligner.cpp:180-188
+        const uint32_t xv = add_max2(f[w], DX2, add2(x[w], EX2));  // BandAligner.cpp:189-201
+        const uint32_t fv = add2(dm, sc[w]);                       // BandAligner.cpp:203-207
+        dm = m[w];
+        m[w] = max3_2(fv, xv, yv);
+        // BM1 (BandAligner.cpp:214-222): diagonal iff FM > max(IX, IY - 1); left iff IY > IX
+        bool dlo, dhi, llo, lhi;
+        ge2(add_max2(yv, EX2, xv), fv, dlo, dhi);  // max(IY - 1, IX) >= FM: not diagonal
+        ge2(xv, yv, llo, lhi);                     // IX >= IY: not left
+        if (!dlo) da |= 3u << (2 * w);
+        if (!dhi) db |= 3u << (2 * w);
+        if (!llo) la |= 1u << (2 * w);
+        if (!lhi) lb |= 1u << (2 * w);
+        f[w] = fv;
+        x[w] = xv;
+        lf = fv;
+        ly = yv;
+    }
+    const uint32_t ca = (da & diag_a) | (~da & la), cb = (db & diag_b) | (~db & lb);
+    return (ca & 0xffffu) | (cb << 16);
+}
+
+// the align-left column of a pair (both segments share it): dp_whole_left on both halves
+template <int W>
+HERO_HD void dp_pair_left(int32_t wl, bool holds_c, uint32_t (&f)[W], uint32_t (&x)[W]) {
+    if (!holds_c) return;
+    constexpr uint32_t SD2 = (uint32_t(kSX - kDX) & 0xffffu) * 0x10001u;
+    constexpr uint32_t SE2 = (uint32_t(kSX - kEX) & 0xffffu) * 0x10001u;
+    switch (wl) {
+#define HERO_PAIR_CASE(w)                                 \
+    case w:                                               \
+        if (w < W) {                                      \
+            f[w < W ? w : 0] = add2(f[w < W ? w : 0], SD2); \
+            x[w < W ? w : 0] = add2(x[w < W ? w : 0], SE2); \
+        }                                                 \
+        break;
+        HERO_PAIR_CASE(0)
+        HERO_PAIR_CASE(1)
+        HERO_PAIR_CASE(2)
+        HERO_PAIR_CASE(3)
+        HERO_PAIR_CASE(4)
+        HERO_PAIR_CASE(5)
+        HERO_PAIR_CASE(6)
+        HERO_PAIR_CASE(7)
+#undef HERO_PAIR_CASE
+        default:
+            break;
+    }
+}
+
 // Whole-matrix fill by one thread, strip after strip.  Scratch provides
 //   int32_t& b(int32_t state, int32_t row)          boundary column, state 0..2
 //   void tb_set(int32_t strip, int32_t row, uint32_t bits)  traceback codes of a

@@ -145,8 +145,13 @@ struct DpLaunch {
     int32_t rmax;
     int32_t affine;
     int32_t whole;          // 1: every base is A/C/G/T, the whole-band rows may run
+    uint32_t pair_mask;     // bit n: segments of n strips run as 16-bit pairs (affine)
+    uint32_t tb_bytes;      // bytes of traceback codes per lane and row (set by launch_dp)
+    uint32_t chunk_mask;    // bit n: tracebacks of n-strip segments walk in row chunks
+    int32_t warps;          // warps per block of the wavefront kernel (2 or 4)
 };
 constexpr int kStripW = 8;
+constexpr uint32_t kStripsAll = 0xfffffffeu;  // every strip count 1..31 (bit n: n strips)
 // needs the shape sort (perm, bin_off); tasks: 128 uint64 of device scratch.
 // The per-thread scratch (tb, bnd) is only used when dp_needs_scratch().
 void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int32_t cmax,

@@ -816,12 +816,19 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
 // its 2-bit codes of a row to shared memory; lane s = 0 of every group then
 // traces its segment back from there.
 // ---------------------------------------------------------------------------
+// warps per block of k_dp_wave: 4 (default) or 2; blocks per SM are set so that
+// every thread keeps 128 registers
 constexpr int kWaveWarps = 4;
-// traceback of a group: every lane a chunk of rows (true) or lane 0 alone (false)
-constexpr bool kChunkWalk = true;
-constexpr int kWaveMinBlocks = 4;  // caps registers at 128 per thread
+constexpr int kWaveRegBlocks(int warps) { return 16 / warps; }
 
-__global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks) {
+constexpr int kTaskQueue = 127;  // tasks[127]: next task to hand out
+
+// segments of n strips run as 16-bit pairs (n <= 32; bit 32 does not exist)
+__device__ __forceinline__ bool pair_strips(uint32_t mask, int n) {
+    return n < 32 && ((mask >> n) & 1u) != 0u;
+}
+
+__global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks, uint32_t pair_mask) {
     // tasks[n] (n = 1..33): first task of segments with n strips; tasks[34+n]:
     // first sorted segment with n strips; tasks[68+n]: one past the last.
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -832,11 +839,12 @@ __global__ void k_dp_tasks(const uint64_t *bin_off, uint64_t *tasks) {
         tasks[n] = t;
         tasks[34 + n] = b;
         tasks[68 + n] = e;
-        const uint64_t S = uint64_t(32 / n);
+        const uint64_t S = uint64_t(32 / n) * (pair_strips(pair_mask, n) ? 2u : 1u);  // segments a task
         t += (e - b + S - 1) / S;
     }
     tasks[33] = t;
     tasks[0] = bin_off[uint32_t(33) << kShapeStripShift];  // first segment for the per-thread kernel
+    tasks[kTaskQueue] = 0;  // work queue head of k_dp_wave
 }
 
 // the wavefront over one warp's segments; FULL / LEFT are warp-uniform.  The
@@ -930,175 +938,341 @@ __device__ __noinline__ void wave_whole(const SegView v, bool active, int32_t R,
 }
 
 
-template <bool AFFINE>
-__global__ void __launch_bounds__(kWaveWarps * 32, kWaveMinBlocks)
-    k_dp_wave(DpLaunch a, const uint64_t *tasks) {
-    extern __shared__ int4 wave_smem[];
-    const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
-    int32_t *tab = reinterpret_cast<int32_t *>(wave_smem) + (size_t(wib) * 32u + lane) * kTabWords;
-    uint16_t *tb = reinterpret_cast<uint16_t *>(reinterpret_cast<int32_t *>(wave_smem) +
-                                                size_t(kWaveWarps) * 32u * kTabWords) +
-                   size_t(wib) * size_t(a.rmax) * 32u;
-    const uint64_t ntask = tasks[33];
-    for (uint64_t task = uint64_t(blockIdx.x) * kWaveWarps + wib; task < ntask;
-         task += uint64_t(gridDim.x) * kWaveWarps) {
-        int G = 1;
-        while (G < 32 && tasks[G + 1] <= task) G++;
-        const int S = 32 / G;
-        const uint64_t first = tasks[34 + G] + (task - tasks[G]) * uint64_t(S);
-        const uint64_t end = tasks[68 + G];
-        const int g = lane / G, s = lane % G;
-        const bool active = g < S && first + uint64_t(g) < end;
-        uint32_t si = 0;
-        SegView v{};
-        int32_t R = 0;
-        if (active) {
-            si = a.perm[first + g];
-            const DpSeg sg = a.segs[si];
-            const uint32_t orient = (sg.flags >> kSegOrientShift) & 1u;
-            v = make_view(a.scode + a.soff[sg.subj], int32_t(a.slen[sg.subj]), int32_t(orient),
-                          a.qcode + a.qoff[sg.query], sg.s0, sg.s1, sg.q0, sg.q1, sg.flags & 3u,
-                          sg.band);
-            R = v.R;
-        }
-        const int32_t Rw = warp_max(R);
-        const int32_t j0 = s * kStripW;
-        const bool full = !active || dp_strip_full(v, j0, kStripW);
-        const int32_t wlast = active ? dp_strip_wlast(v, j0, kStripW) : -1;
-        const bool wfull = __all_sync(0xffffffffu, full);
-        const bool wleft = __any_sync(0xffffffffu, wlast >= 0);
-        // whole-band fast path: every segment of the warp inside its band and all
-        // with the same align-left column (the shape key makes it so)
-        const int32_t wl = active ? dp_left_col<kStripW>(v) : -2;
-        const int32_t wl0 = warp_max(wl);
-        const bool whole = a.whole &&
-                           __all_sync(0xffffffffu, !active || (dp_whole_band(v) && wl == wl0));
-        if (whole) {
-            if (wl0 >= 0) {
-                wave_whole<AFFINE, true>(v, active, R, Rw, G, s, lane, wl0, tb, tab);
-            } else {
-                wave_whole<AFFINE, false>(v, active, R, Rw, G, s, lane, -1, tb, tab);
-            }
-        } else if (wfull) {
-            if (wleft) {
-                wave_fill<AFFINE, true, true>(v, active, R, Rw, G, s, lane, wlast, tb);
-            } else {
-                wave_fill<AFFINE, true, false>(v, active, R, Rw, G, s, lane, wlast, tb);
-            }
-        } else {
-            if (wleft) {
-                wave_fill<AFFINE, false, true>(v, active, R, Rw, G, s, lane, wlast, tb);
-            } else {
-                wave_fill<AFFINE, false, false>(v, active, R, Rw, G, s, lane, wlast, tb);
-            }
-        }
-        __syncwarp();
-        // Traceback.  When the ops fit in the group's strip tables in shared
-        // memory (free once the fill is done), every lane of the group walks a
-        // chunk of rows (dp_walk_span) from a guessed start; a start is right
-        // once it equals the end of the lane before, and each round makes at
-        // least one more lane right (mostly one round in all).  The verified
-        // chunks then write their ops at their offsets.  Otherwise lane s = 0
-        // walks the whole path.
-        uint32_t *const stage =
-            reinterpret_cast<uint32_t *>(wave_smem) + (size_t(wib) * 32u + size_t(g) * G) * kTabWords;
-        const bool staged = a.stride <= uint32_t(G) * kTabWords;
-        struct SmemCodes {
-            const uint16_t *tb;
-            int base;
-            __device__ __forceinline__ uint32_t tb_get(int32_t st, int32_t i) const {
-                return tb[size_t(i - 1) * 32u + base + st];
-            }
-        } sc{tb, g * G};
-        int32_t n = 0;
-        if (staged && !kChunkWalk) {
-            if (active && s == 0) {
-                OpsWriter w{stage, int32_t(a.stride * 16u)};
-                n = dp_walk<kStripW>(v, sc, w);
-                w.flush();
-            }
-            n = __shfl_sync(0xffffffffu, n, (g * G) & 31);
-        } else if (staged) {
-            if (active)
-                for (uint32_t k = uint32_t(s); k < a.stride; k += uint32_t(G)) stage[k] = 0u;
-            int32_t rtop = 0, rbot = 0, c = 0, e = 0, cnt = 0;
-            if (active) {
-                dp_chunk_rows(v.R, G, s, rtop, rbot);
-                c = s == 0 ? v.C : dp_chunk_guess(v, rtop);
-            }
-            const uint32_t gbits = G >= 32 ? 0xffffffffu : (1u << G) - 1u;
-            bool todo = active;
-            for (int round = 0; round <= 32; round++) {  // at most G rounds
-                if (todo) {
-                    int32_t jj = c;
-                    cnt = dp_walk_span<kStripW>(sc, rtop, jj, rbot);
-                    e = jj;
-                }
-                const int32_t pe = __shfl_up_sync(0xffffffffu, e, 1);
-                const bool wrong = active && s > 0 && c != pe;
-                const uint32_t gm = (__ballot_sync(0xffffffffu, wrong) >> (g * G)) & gbits;
-                if (!__any_sync(0xffffffffu, gm != 0u)) break;
-                // lanes from the first wrong one on start again where the lane
-                // before them ended (right for the first wrong lane, whose
-                // predecessor is right; a good guess for the rest)
-                const int32_t f = gm ? __ffs(int(gm)) - 1 : G;
-                todo = active && s >= f;
-                if (todo) c = pe;
-            }
-            int32_t before = cnt;  // ops of the lanes before this one (exclusive scan)
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int32_t y = __shfl_up_sync(0xffffffffu, before, d);
-                if (s >= d) before += y;
-            }
-            n = __shfl_sync(0xffffffffu, before, (g * G + G - 1) & 31);  // the group's total
-            before -= cnt;
-            __syncwarp();  // stage zeroed
-            if (active && cnt > 0) {
-                struct Put {
-                    uint32_t *stage;
-                    int32_t p;
-                    int32_t q;
-                    uint32_t acc;
-                    __device__ __forceinline__ void operator()(uint32_t op) {
-                        p--;
-                        if ((p >> 4) != q) {
-                            atomicOr(stage + q, acc);
-                            acc = 0u;
-                            q = p >> 4;
-                        }
-                        acc |= op << (2 * (p & 15));
-                    }
-                };
-                const int32_t p0 = int32_t(a.stride * 16u) - before;
-                Put put{stage, p0, (p0 - 1) >> 4, 0u};
-                dp_walk_span_ops<kStripW>(sc, dp_op_lut(v), rtop, c, rbot, put);
-                atomicOr(stage + put.q, put.acc);
-            }
-        } else if (active && s == 0) {
-            uint32_t *words = a.ops + uint64_t(si) * a.stride;
-            OpsWriter w{words, int32_t(a.stride * 16u)};
+// Per-warp shared memory of k_dp_wave: the lanes' strip tables (32 x
+// tab_stride words: kTabWords, or kTabWords2 when pairs run), then rmax rows of
+// traceback codes, 32 lanes wide (16 bits a lane for single segments, 32 for
+// pairs: tb_bytes per lane-row).
+__host__ __device__ constexpr uint32_t tab_stride(uint32_t tb_bytes) {
+    return tb_bytes == 4u ? uint32_t(kTabWords2) : uint32_t(kTabWords);
+}
+
+// codes of one segment of a group: a 16-bit word per (row, strip), or one half
+// of a pair's 32-bit word
+struct SmemCodes {
+    const uint16_t *tb;
+    int base;
+    __device__ __forceinline__ uint32_t tb_get(int32_t st, int32_t i) const {
+        return tb[size_t(i - 1) * 32u + base + st];
+    }
+};
+struct SmemCodesPair {
+    const uint32_t *tb;
+    int base, shift;
+    __device__ __forceinline__ uint32_t tb_get(int32_t st, int32_t i) const {
+        return (tb[size_t(i - 1) * 32u + base + st] >> shift) & 0xffffu;
+    }
+};
+
+// Traceback of the group's segment.  When the ops fit in the group's strip
+// tables in shared memory (free once the fill is done), every lane of the group
+// walks a chunk of rows (dp_walk_span) from a guessed start; a start is right
+// once it equals the end of the lane before, and each round makes at least one
+// more lane right (mostly one round in all).  The verified chunks then write
+// their ops at their offsets.  Otherwise lane s = 0 walks the whole path.  Then
+// the segment's DpSum, its reference cells and its ops go out.
+template <class Codes>
+__device__ __forceinline__ void group_traceback(const DpLaunch &a, const Codes &sc,
+                                                const SegView &v, bool active, uint32_t si,
+                                                int G, int g, int s, uint32_t *stage,
+                                                uint32_t stage_words) {
+    const bool staged = a.stride <= stage_words;
+    const bool chunk = pair_strips(a.chunk_mask, G);  // bit G of the mask
+    int32_t n = 0;
+    if (staged && !chunk) {
+        if (active && s == 0) {
+            OpsWriter w{stage, int32_t(a.stride * 16u)};
             n = dp_walk<kStripW>(v, sc, w);
             w.flush();
         }
-        __syncwarp();
-        if (active && s == 0) {
-            DpSum sum;
-            ops_summary(staged ? stage : a.ops + uint64_t(si) * a.stride,
-                        a.stride * 16u - uint32_t(n), uint32_t(n), sum);
-            a.sums[si] = sum;
-            if (a.cells) {
-                const uint64_t cl = band_cells(v.R, v.C, v.band);
-                a.cells[si] = uint32_t(cl > 0xffffffffull ? 0xffffffffull : cl);
+        n = __shfl_sync(0xffffffffu, n, (g * G) & 31);
+    } else if (staged) {
+        if (active)
+            for (uint32_t k = uint32_t(s); k < a.stride; k += uint32_t(G)) stage[k] = 0u;
+        int32_t rtop = 0, rbot = 0, c = 0, e = 0, cnt = 0;
+        if (active) {
+            dp_chunk_rows(v.R, G, s, rtop, rbot);
+            c = s == 0 ? v.C : dp_chunk_guess(v, rtop);
+        }
+        const uint32_t gbits = G >= 32 ? 0xffffffffu : (1u << G) - 1u;
+        bool todo = active;
+        for (int round = 0; round <= 32; round++) {  // at most G rounds
+            if (todo) {
+                int32_t jj = c;
+                cnt = dp_walk_span<kStripW>(sc, rtop, jj, rbot);
+                e = jj;
             }
+            const int32_t pe = __shfl_up_sync(0xffffffffu, e, 1);
+            const bool wrong = active && s > 0 && c != pe;
+            const uint32_t gm = (__ballot_sync(0xffffffffu, wrong) >> (g * G)) & gbits;
+            if (!__any_sync(0xffffffffu, gm != 0u)) break;
+            // lanes from the first wrong one on start again where the lane
+            // before them ended (right for the first wrong lane, whose
+            // predecessor is right; a good guess for the rest)
+            const int32_t f = gm ? __ffs(int(gm)) - 1 : G;
+            todo = active && s >= f;
+            if (todo) c = pe;
         }
-        if (staged && active) {  // the group's lanes copy the ops out together
-            uint32_t *out = a.ops + uint64_t(si) * a.stride;
-            for (uint32_t k = ((a.stride * 16u - uint32_t(n)) >> 4) + uint32_t(s); k < a.stride;
-                 k += uint32_t(G))
-                out[k] = stage[k];
+        int32_t before = cnt;  // ops of the lanes before this one (exclusive scan)
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, before, d);
+            if (s >= d) before += y;
         }
-        __syncwarp();
+        n = __shfl_sync(0xffffffffu, before, (g * G + G - 1) & 31);  // the group's total
+        before -= cnt;
+        __syncwarp();  // stage zeroed
+        if (active && cnt > 0) {
+            struct Put {
+                uint32_t *stage;
+                int32_t p;
+                int32_t q;
+                uint32_t acc;
+                __device__ __forceinline__ void operator()(uint32_t op) {
+                    p--;
+                    if ((p >> 4) != q) {
+                        atomicOr(stage + q, acc);
+                        acc = 0u;
+                        q = p >> 4;
+                    }
+                    acc |= op << (2 * (p & 15));
+                }
+            };
+            const int32_t p0 = int32_t(a.stride * 16u) - before;
+            Put put{stage, p0, (p0 - 1) >> 4, 0u};
+            dp_walk_span_ops<kStripW>(sc, dp_op_lut(v), rtop, c, rbot, put);
+            atomicOr(stage + put.q, put.acc);
+        }
+    } else if (active && s == 0) {
+        uint32_t *words = a.ops + uint64_t(si) * a.stride;
+        OpsWriter w{words, int32_t(a.stride * 16u)};
+        n = dp_walk<kStripW>(v, sc, w);
+        w.flush();
+    }
+    __syncwarp();
+    if (active && s == 0) {
+        DpSum sum;
+        ops_summary(staged ? stage : a.ops + uint64_t(si) * a.stride, a.stride * 16u - uint32_t(n),
+                    uint32_t(n), sum);
+        a.sums[si] = sum;
+        if (a.cells) {
+            const uint64_t cl = band_cells(v.R, v.C, v.band);
+            a.cells[si] = uint32_t(cl > 0xffffffffull ? 0xffffffffull : cl);
+        }
+    }
+    if (staged && active) {  // the group's lanes copy the ops out together
+        uint32_t *out = a.ops + uint64_t(si) * a.stride;
+        for (uint32_t k = ((a.stride * 16u - uint32_t(n)) >> 4) + uint32_t(s); k < a.stride;
+             k += uint32_t(G))
+            out[k] = stage[k];
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ SegView seg_view(const DpLaunch &a, uint32_t si) {
+    const DpSeg sg = a.segs[si];
+    const uint32_t orient = (sg.flags >> kSegOrientShift) & 1u;
+    return make_view(a.scode + a.soff[sg.subj], int32_t(a.slen[sg.subj]), int32_t(orient),
+                     a.qcode + a.qoff[sg.query], sg.s0, sg.s1, sg.q0, sg.q1, sg.flags & 3u,
+                     sg.band);
+}
+
+// One task of single segments: group g (G lanes) takes the sorted segment
+// first + g * step, if below end.
+template <bool AFFINE>
+__device__ __forceinline__ void task_single(const DpLaunch a, uint64_t first, uint64_t step,
+                                         uint64_t end, int G, int lane, uint16_t *tb,
+                                         uint32_t *tabs) {
+    const int S = 32 / G, g = lane / G, s = lane % G;
+    const bool active = g < S && first + uint64_t(g) * step < end;
+    uint32_t si = 0;
+    SegView v{};
+    int32_t R = 0;
+    if (active) {
+        si = a.perm[first + uint64_t(g) * step];
+        v = seg_view(a, si);
+        R = v.R;
+    }
+    const int32_t Rw = warp_max(R);
+    const int32_t j0 = s * kStripW;
+    const bool full = !active || dp_strip_full(v, j0, kStripW);
+    const int32_t wlast = active ? dp_strip_wlast(v, j0, kStripW) : -1;
+    const bool wfull = __all_sync(0xffffffffu, full);
+    const bool wleft = __any_sync(0xffffffffu, wlast >= 0);
+    // whole-band fast path: every segment of the warp inside its band and all
+    // with the same align-left column (the shape key makes it so)
+    const int32_t wl = active ? dp_left_col<kStripW>(v) : -2;
+    const int32_t wl0 = warp_max(wl);
+    const bool whole =
+        a.whole && __all_sync(0xffffffffu, !active || (dp_whole_band(v) && wl == wl0));
+    const uint32_t TS = tab_stride(a.tb_bytes);
+    int32_t *tab = reinterpret_cast<int32_t *>(tabs + size_t(lane) * TS);
+    if (whole) {
+        if (wl0 >= 0) {
+            wave_whole<AFFINE, true>(v, active, R, Rw, G, s, lane, wl0, tb, tab);
+        } else {
+            wave_whole<AFFINE, false>(v, active, R, Rw, G, s, lane, -1, tb, tab);
+        }
+    } else if (wfull) {
+        if (wleft) {
+            wave_fill<AFFINE, true, true>(v, active, R, Rw, G, s, lane, wlast, tb);
+        } else {
+            wave_fill<AFFINE, true, false>(v, active, R, Rw, G, s, lane, wlast, tb);
+        }
+    } else {
+        if (wleft) {
+            wave_fill<AFFINE, false, true>(v, active, R, Rw, G, s, lane, wlast, tb);
+        } else {
+            wave_fill<AFFINE, false, false>(v, active, R, Rw, G, s, lane, wlast, tb);
+        }
+    }
+    __syncwarp();
+    group_traceback(a, SmemCodes{tb, g * G}, v, active, si, G, g, s,
+                    tabs + size_t(g) * G * TS, uint32_t(G) * TS);
+}
+
+// the wavefront over one warp's pairs of whole-band segments (dp_pair_row):
+// group lanes hold segment A in the low halves and B in the high halves
+template <bool LEFT>
+__device__ __noinline__ void wave_pair(const SegView va, const SegView vb, bool active, int32_t R,
+                                       int32_t Rw, int G, int s, int lane, int32_t wl,
+                                       uint32_t *tb, uint32_t *tab) {
+    const int32_t j0 = s * kStripW;
+    uint32_t f[kStripW], x[kStripW], m[kStripW];
+    uint32_t pm = 0, c0f = 0, c0y = 0, mul = 0;
+    const uint8_t *rpa = va.row_base, *rpb = vb.row_base;
+    uint32_t cha = 0, chb = 0;
+    if (active) {
+        dp_pair_table<kStripW>(va, vb, j0, tab);
+        dp_pair_init<kStripW>(va, vb, j0, f, x, m, pm);
+        int32_t ca[3], cb[3];
+        dp_whole_col0<true>(va, ca);
+        dp_whole_col0<true>(vb, cb);
+        mul = pack2(ca[0], cb[0]);
+        c0f = pack2(ca[0] + ca[1], cb[0] + cb[1]);  // row 1
+        c0y = pack2(ca[0] + ca[2], cb[0] + cb[2]);
+        cha = (rpa[0] ^ va.row_xor) & 3u;
+        chb = (rpb[0] ^ vb.row_xor) & 3u;
+    }
+    const bool holds_c = LEFT && s == G - 1;
+    const uint32_t neg = pack2(kNEG16, kNEG16);
+    uint32_t pf = neg, py = neg, pmv = neg;  // FM, IY, M published to lane s+1
+    uint32_t *tp = tb + lane;
+    const uint16_t *sc16 = reinterpret_cast<const uint16_t *>(tab);
+#pragma unroll 1
+    for (int32_t t = 0; t < Rw + G - 1; t++) {
+        const uint32_t inf = __shfl_up_sync(0xffffffffu, pf, 1);
+        const uint32_t iny = __shfl_up_sync(0xffffffffu, py, 1);
+        const uint32_t inm = __shfl_up_sync(0xffffffffu, pmv, 1);
+        const int32_t i = t - s + 1;
+        if (active && uint32_t(i - 1) < uint32_t(R)) {
+            const uint32_t ba = cha, bb = chb;
+            if (i < R) {  // next row's bases, loaded a step early
+                rpa += va.row_dir;
+                rpb += vb.row_dir;
+                cha = (rpa[0] ^ va.row_xor) & 3u;
+                chb = (rpb[0] ^ vb.row_xor) & 3u;
+            }
+            uint32_t lf = s == 0 ? c0f : inf;
+            uint32_t ly = s == 0 ? c0y : iny;
+            const uint4 A = reinterpret_cast<const uint4 *>(sc16 + ba * kStripW)[0];
+            const uint4 B = reinterpret_cast<const uint4 *>(sc16 + (4u + bb) * kStripW)[0];
+            const uint32_t sc[kStripW] = {__byte_perm(A.x, B.x, 0x5410), __byte_perm(A.x, B.x, 0x7632),
+                                          __byte_perm(A.y, B.y, 0x5410), __byte_perm(A.y, B.y, 0x7632),
+                                          __byte_perm(A.z, B.z, 0x5410), __byte_perm(A.z, B.z, 0x7632),
+                                          __byte_perm(A.w, B.w, 0x5410), __byte_perm(A.w, B.w, 0x7632)};
+            if (LEFT) dp_pair_left<kStripW>(wl, holds_c, f, x);
+            const uint32_t bits =
+                dp_pair_row<kStripW>(sc, tab[32 + ba], tab[36 + bb], f, x, m, lf, ly, pm);
+            *tp = bits;
+            tp += 32;
+            pf = lf;
+            py = ly;
+            pmv = m[kStripW - 1];
+            pm = s == 0 ? c0f : inm;
+            c0f = add2(c0f, mul);
+            c0y = add2(c0y, mul);
+        }
+    }
+}
+
+// One task of pairs: group g takes the sorted segments first + 2g (A, low
+// halves) and first + 2g + 1 (B, high halves).  Warps whose pairs are not all
+// whole-band (or too long for 16-bit scores) run their A segments, then their
+// B segments, as two tasks of single segments.
+__device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint64_t end, int G,
+                                       int lane, uint32_t *tb, uint32_t *tabs) {
+    const int S = 32 / G, g = lane / G, s = lane % G;
+    const uint64_t ia = first + 2u * uint64_t(g), ib = ia + 1u;
+    const bool active = g < S && ia < end;
+    const bool has_b = active && ib < end;
+    uint32_t sa = 0, sb = 0;
+    SegView va{}, vb{};
+    int32_t R = 0;
+    bool ok = true;
+    int32_t wl = -2;
+    if (active) {
+        sa = a.perm[ia];
+        va = seg_view(a, sa);
+        sb = has_b ? a.perm[ib] : sa;
+        vb = has_b ? seg_view(a, sb) : va;
+        R = va.R;
+        wl = dp_left_col<kStripW>(va);
+        ok = dp_whole_band(va) && dp_whole_band(vb) && va.R == vb.R &&
+             dp_left_col<kStripW>(vb) == wl && va.R + va.C <= kPairMaxSide &&
+             vb.R + vb.C <= kPairMaxSide;
+    }
+    const int32_t wl0 = warp_max(wl);
+    if (!(a.whole && __all_sync(0xffffffffu, !active || (ok && wl == wl0)))) {
+        uint16_t *tb16 = reinterpret_cast<uint16_t *>(tb);
+        task_single<true>(a, first, 2, end, G, lane, tb16, tabs);
+        task_single<true>(a, first + 1, 2, end, G, lane, tb16, tabs);
+        return;
+    }
+    const int32_t Rw = warp_max(R);
+    const uint32_t TS = kTabWords2;
+    uint32_t *tab = tabs + size_t(lane) * TS;
+    if (wl0 >= 0) {
+        wave_pair<true>(va, vb, active, R, Rw, G, s, lane, wl0, tb, tab);
+    } else {
+        wave_pair<false>(va, vb, active, R, Rw, G, s, lane, -1, tb, tab);
+    }
+    __syncwarp();
+    uint32_t *stage = tabs + size_t(g) * G * TS;
+    group_traceback(a, SmemCodesPair{tb, g * G, 0}, va, active, sa, G, g, s, stage,
+                    uint32_t(G) * TS);
+    group_traceback(a, SmemCodesPair{tb, g * G, 16}, vb, has_b, sb, G, g, s, stage,
+                    uint32_t(G) * TS);
+}
+
+template <bool AFFINE, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS))
+    k_dp_wave(DpLaunch a, uint64_t *tasks) {
+    extern __shared__ int4 wave_smem[];
+    const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
+    const uint32_t TS = tab_stride(a.tb_bytes);
+    uint32_t *tabs = reinterpret_cast<uint32_t *>(wave_smem) + size_t(wib) * 32u * TS;
+    uint8_t *tbw = reinterpret_cast<uint8_t *>(wave_smem) + size_t(WARPS) * 32u * TS * 4u +
+                   size_t(wib) * size_t(a.rmax) * 32u * a.tb_bytes;
+    // a persistent grid fed by a work queue: each warp takes the next task, the
+    // largest shapes first (tasks are sorted by strips, then rows)
+    const uint64_t ntask = tasks[33];
+    for (;;) {
+        unsigned long long q = 0;
+        if (lane == 0) q = atomicAdd(reinterpret_cast<unsigned long long *>(tasks + kTaskQueue), 1ull);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= ntask) break;
+        const uint64_t task = ntask - 1 - q;
+        int G = 1;
+        while (G < 32 && tasks[G + 1] <= task) G++;
+        const bool pair = AFFINE && pair_strips(a.pair_mask, G);
+        const uint64_t per = uint64_t(32 / G) * (pair ? 2u : 1u);  // segments per task
+        const uint64_t first = tasks[34 + G] + (task - tasks[G]) * per;
+        const uint64_t end = tasks[68 + G];
+        if (pair) {
+            task_pair(a, first, end, G, lane, reinterpret_cast<uint32_t *>(tbw), tabs);
+        } else {
+            task_single<AFFINE>(a, first, 1, end, G, lane, reinterpret_cast<uint16_t *>(tbw), tabs);
+        }
     }
 }
 
@@ -1642,16 +1816,21 @@ uint64_t dp_threads(int device) {
 }
 
 // shared memory of a wavefront block: per warp, the lanes' strip tables and
-// rmax rows of 2-bit codes (32 lanes x 16 bits)
-static size_t wave_smem(int32_t rmax) {
-    return size_t(kWaveWarps) * (32u * kTabWords * 4u + size_t(rmax) * 64u);
+// rmax rows of 2-bit codes (32 lanes x 16 bits, or x 32 bits for pairs)
+static size_t wave_smem(int32_t rmax, uint32_t tb_bytes, int warps) {
+    return size_t(warps) * (32u * tab_stride(tb_bytes) * 4u + size_t(rmax) * 32u * tb_bytes);
 }
 
-bool dp_wave_fits(int32_t rmax) { return wave_smem(rmax) <= 200u * 1024u; }
+bool dp_wave_fits(int32_t rmax) { return wave_smem(rmax, 2, kWaveWarps) <= 200u * 1024u; }
 
-void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int32_t cmax,
+void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, int32_t cmax,
                cudaStream_t st) {
-    if (!a.nd) return;
+    if (!a_in.nd) return;
+    DpLaunch a = a_in;
+    if (a.warps != 2) a.warps = 4;
+    // pairs need 32-bit code rows; without the room (or for the global aligner) none run
+    if (!a.affine || wave_smem(a.rmax, 4, a.warps) > 200u * 1024u) a.pair_mask = 0;
+    a.tb_bytes = a.pair_mask ? 4u : 2u;
     if (!dp_wave_fits(a.rmax)) {  // rows too long for the shared-memory codes
         const unsigned g = unsigned(a.threads / kDpThreads);
         counted();
@@ -1663,28 +1842,37 @@ void launch_dp(const DpLaunch &a, const uint64_t *bin_off, uint64_t *tasks, int3
         return;
     }
     counted();
-    k_dp_tasks<<<1, 32, 0, st>>>(bin_off, tasks);
+    k_dp_tasks<<<1, 32, 0, st>>>(bin_off, tasks, a.pair_mask);
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = wave_smem(a.rmax);
-    const unsigned g = unsigned(sms) * 8u;
+    const size_t smem = wave_smem(a.rmax, a.tb_bytes, a.warps);
+    // a persistent grid: twice the blocks that fit for registers (the work queue
+    // stops the extra ones at once)
+    const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps));
     // the opt-in is set once per size increase (never while a graph is being captured
     // for a size not seen before: the eager round that precedes a capture sets it)
-    static size_t opted[2] = {0, 0};
-    if (smem > 48u * 1024u && smem > opted[a.affine ? 1 : 0]) {
-        if (a.affine) {
-            cudaFuncSetAttribute(k_dp_wave<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        } else {
-            cudaFuncSetAttribute(k_dp_wave<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        }
-        opted[a.affine ? 1 : 0] = smem;
+    static size_t opted[2][2] = {{0, 0}, {0, 0}};
+    const int ai = a.affine ? 1 : 0, wi = a.warps == 2 ? 0 : 1;
+    if (smem > 48u * 1024u && smem > opted[ai][wi]) {
+        const void *fn = a.affine ? (a.warps == 2 ? (const void *)k_dp_wave<true, 2> : (const void *)k_dp_wave<true, 4>)
+                                  : (a.warps == 2 ? (const void *)k_dp_wave<false, 2> : (const void *)k_dp_wave<false, 4>);
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        opted[ai][wi] = smem;
     }
     counted();
     if (a.affine) {
-        k_dp_wave<true><<<g, kWaveWarps * 32, smem, st>>>(a, tasks);
+        if (a.warps == 2) {
+            k_dp_wave<true, 2><<<g, 64, smem, st>>>(a, tasks);
+        } else {
+            k_dp_wave<true, 4><<<g, 128, smem, st>>>(a, tasks);
+        }
     } else {
-        k_dp_wave<false><<<g, kWaveWarps * 32, smem, st>>>(a, tasks);
+        if (a.warps == 2) {
+            k_dp_wave<false, 2><<<g, 64, smem, st>>>(a, tasks);
+        } else {
+            k_dp_wave<false, 4><<<g, 128, smem, st>>>(a, tasks);
+        }
     }
     if (cmax > 32 * kStripW) {
         const unsigned gw = unsigned(a.threads / kDpThreads);

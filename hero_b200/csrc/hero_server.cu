@@ -62,6 +62,8 @@ struct hero_server {
     uint64_t next_id = 1, rounds = 0, submitted = 0, done = 0, failed = 0, bases_done = 0;
     uint64_t max_jobs = 0;   // jobs a key can tell apart (k-mer bits leave room for the job)
     uint64_t cap_jobs = 0;   // jobs per round after a round ran out of memory (0: no cap)
+    std::vector<hero_dp_tuning> tuning;  // DP kernel shapes to apply before the next round
+    bool tuning_new = false;
     double busy_ms = 0;
 
     double now_ms() const {
@@ -107,7 +109,14 @@ void hero_server::run() {
             jobs[id].state = HERO_JOB_RUNNING;
             jobs[id].start_ms = t;
         }
+        std::vector<hero_dp_tuning> tun;
+        const bool retune = tuning_new;
+        if (retune) {
+            tun = tuning;
+            tuning_new = false;
+        }
         lk.unlock();
+        if (retune) hero_set_dp_tuning(ctx, tun.data(), uint32_t(tun.size()));
         run_round(ids);
         lk.lock();
         cv_done.notify_all();
@@ -258,6 +267,16 @@ extern "C" void hero_server_destroy(hero_server *s) {
     if (s->worker.joinable()) s->worker.join();
     hero_destroy(s->ctx);
     delete s;
+}
+
+extern "C" int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t, uint32_t n) {
+    if (!s || (n && !t)) return HERO_E_INPUT;
+    for (uint32_t i = 0; i < n; i++)
+        if (t[i].warps_per_block != 2 && t[i].warps_per_block != 4) return HERO_E_INPUT;
+    std::lock_guard<std::mutex> g(s->mu);
+    s->tuning.assign(t, t + n);
+    s->tuning_new = true;
+    return HERO_OK;
 }
 
 extern "C" int hero_job_submit(hero_server *s, const uint8_t *seq, const uint64_t *off,

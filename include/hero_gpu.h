@@ -137,6 +137,23 @@ int hero_get_votes(hero_ctx *ctx, uint32_t *cov);
 
 int hero_get_stats(hero_ctx *ctx, hero_stats *out);
 
+/* Shapes of the banded-DP kernel per class of subject batch, chosen by the
+ * project's autotuner (hero_b200/autotune.py: it times each candidate on a
+ * sample of a workload and records the fastest per class in a JSON file that
+ * the Python binding loads).  A batch whose longest DP side is at most
+ * rows_max takes the first such class; batches no class covers, and contexts
+ * without a table, use 4 warps a block, no pairs and row-chunk walks for every
+ * strip count.  No reference counterpart (the reference has one CPU aligner). */
+typedef struct {
+    int32_t rows_max;          /* class bound on the longest DP side of a batch */
+    int32_t warps_per_block;   /* 2 or 4 */
+    uint32_t pair_strips;      /* bit n: n-strip segments run as 16-bit pairs (affine) */
+    uint32_t chunk_strips;     /* bit n: n-strip tracebacks walk in row chunks */
+} hero_dp_tuning;
+
+/* Replaces the context's tuning table (n = 0 clears it). */
+int hero_set_dp_tuning(hero_ctx *ctx, const hero_dp_tuning *t, uint32_t n);
+
 /* Aligns an explicit list of DP segments on the device (test and tooling entry
  * point).  subj/query: concatenated reads (same layout as above); per segment
  * the subject read index, its orientation (0 forward, 1 reverse complement),
@@ -243,6 +260,9 @@ const char *hero_job_error(hero_server *s, uint64_t job_id);
 /* Frees a finished job's results. */
 int hero_job_release(hero_server *s, uint64_t job_id);
 int hero_server_get_stats(hero_server *s, hero_server_stats *out);
+
+/* DP kernel shapes (hero_set_dp_tuning) for the rounds the server runs next. */
+int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t, uint32_t n);
 
 /* Admission estimate: device bytes a job of `bases` bases in `reads` reads adds
  * to a round (read copies, vote matrix, k-mer table, consensus outputs). */

@@ -310,7 +310,119 @@ void emu_whole_any(int wl, const SegView &v, int G, std::vector<uint16_t> &tb) {
         emu_whole<AFFINE, false>(v, G, -1, tb);
     }
 }
+
+// two segments of one shape as a 16-bit pair (the kernel's wave_pair), lanes in turn
+template <bool LEFT>
+void emu_pair(const SegView &va, const SegView &vb, int G, int32_t wl, std::vector<uint32_t> &tb) {
+    constexpr int W = 8;
+    struct Lane {
+        uint32_t f[W], x[W], m[W], tab[kTabWords2];
+        uint32_t pm, pf, py, pmv, c0f, c0y, mul;
+        const uint8_t *rpa, *rpb;
+        uint32_t cha, chb;
+    };
+    std::vector<Lane> L(G);
+    for (int s = 0; s < G; s++) {
+        Lane &x = L[s];
+        dp_pair_table<W>(va, vb, s * W, x.tab);
+        dp_pair_init<W>(va, vb, s * W, x.f, x.x, x.m, x.pm);
+        int32_t ca[3], cb[3];
+        dp_whole_col0<true>(va, ca);
+        dp_whole_col0<true>(vb, cb);
+        x.mul = pack2(ca[0], cb[0]);
+        x.c0f = pack2(ca[0] + ca[1], cb[0] + cb[1]);
+        x.c0y = pack2(ca[0] + ca[2], cb[0] + cb[2]);
+        x.rpa = va.row_base;
+        x.rpb = vb.row_base;
+        x.cha = (x.rpa[0] ^ va.row_xor) & 3u;
+        x.chb = (x.rpb[0] ^ vb.row_xor) & 3u;
+        x.pf = x.py = x.pmv = pack2(kNEG16, kNEG16);
+    }
+    std::vector<uint32_t> inf(G), iny(G), inm(G);
+    for (int t = 0; t < va.R + G - 1; t++) {
+        for (int s = 0; s < G; s++) {
+            inf[s] = s > 0 ? L[s - 1].pf : 0;
+            iny[s] = s > 0 ? L[s - 1].py : 0;
+            inm[s] = s > 0 ? L[s - 1].pmv : 0;
+        }
+        for (int s = 0; s < G; s++) {
+            const int32_t i = t - s + 1;
+            if (i < 1 || i > va.R) continue;
+            Lane &x = L[s];
+            const uint32_t ba = x.cha, bb = x.chb;
+            if (i < va.R) {
+                x.rpa += va.row_dir;
+                x.rpb += vb.row_dir;
+                x.cha = (x.rpa[0] ^ va.row_xor) & 3u;
+                x.chb = (x.rpb[0] ^ vb.row_xor) & 3u;
+            }
+            uint32_t lf = s == 0 ? x.c0f : inf[s];
+            uint32_t ly = s == 0 ? x.c0y : iny[s];
+            const uint16_t *sc16 = reinterpret_cast<const uint16_t *>(x.tab);
+            uint32_t sc[W];
+            for (int w = 0; w < W; w++) sc[w] = uint32_t(sc16[ba * W + w]) | (uint32_t(sc16[(4 + bb) * W + w]) << 16);
+            if (LEFT) dp_pair_left<W>(wl, s == G - 1, x.f, x.x);
+            const uint32_t bits = dp_pair_row<W>(sc, x.tab[32 + ba], x.tab[36 + bb], x.f, x.x, x.m, lf, ly, x.pm);
+            tb[size_t(i - 1) * 32 + s] = bits;
+            x.pf = lf;
+            x.py = ly;
+            x.pmv = x.m[W - 1];
+            x.pm = s == 0 ? x.c0f : inm[s];
+            x.c0f = add2(x.c0f, x.mul);
+            x.c0y = add2(x.c0y, x.mul);
+        }
+    }
+}
 }  // extern "C++"
+
+
+// A pair of segments with equal lengths (same rows, strips and align-left
+// column) through the 16-bit pair rows; each half's ops are walked and returned
+// (ops_a / ops_b, capacity cap each).  Returns 0, or -1 if the pair does not
+// qualify or a path does not fit.
+int emu_align_pair(const uint8_t *sa, const uint8_t *qa, const uint8_t *sb, const uint8_t *qb,
+                   int32_t ls, int32_t lq, int64_t band_a, int64_t band_b, int flags_a,
+                   int flags_b, uint8_t *ops_a, int32_t *na, uint8_t *ops_b, int32_t *nb,
+                   int32_t cap) {
+    constexpr int W = 8;
+    std::vector<uint8_t> sca(ls), qca(lq), scb(ls), qcb(lq);
+    for (int i = 0; i < ls; i++) {
+        sca[i] = base_code(sa[i]);
+        scb[i] = base_code(sb[i]);
+    }
+    for (int i = 0; i < lq; i++) {
+        qca[i] = base_code(qa[i]);
+        qcb[i] = base_code(qb[i]);
+    }
+    const SegView va = make_view(sca.data(), ls, 0, qca.data(), 0, ls, 0, lq, uint32_t(flags_a), band_a);
+    const SegView vb = make_view(scb.data(), ls, 0, qcb.data(), 0, ls, 0, lq, uint32_t(flags_b), band_b);
+    if (!dp_whole_band(va) || !dp_whole_band(vb) || dp_left_col<W>(va) != dp_left_col<W>(vb) ||
+        va.R + va.C > kPairMaxSide)
+        return -1;
+    const int G = (va.C + W - 1) / W;
+    std::vector<uint32_t> tb(size_t(va.R) * 32, 0);
+    const int32_t wl = dp_left_col<W>(va);
+    if (wl >= 0) {
+        emu_pair<true>(va, vb, G, wl, tb);
+    } else {
+        emu_pair<false>(va, vb, G, -1, tb);
+    }
+    for (int h = 0; h < 2; h++) {
+        struct Codes {
+            const uint32_t *tb;
+            int shift;
+            uint32_t tb_get(int32_t st, int32_t i) const { return (tb[size_t(i - 1) * 32 + st] >> shift) & 0xffffu; }
+        } sc{tb.data(), 16 * h};
+        std::vector<uint8_t> rev;
+        auto emit = [&](uint8_t op) { rev.push_back(op); };
+        const int n = dp_walk<W>(h ? vb : va, sc, emit);
+        if (n > cap) return -1;
+        uint8_t *out = h ? ops_b : ops_a;
+        for (int k = 0; k < n; k++) out[k] = rev[size_t(n - 1 - k)];
+        (h ? *nb : *na) = n;
+    }
+    return 0;
+}
 
 int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *query, int32_t lq,
                    int64_t band, int align_right, int align_left, uint8_t *ops, int32_t cap) {

@@ -38,3 +38,17 @@ def test_sass_is_sm100a():
     out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", lib],
                          capture_output=True, text=True).stdout
     assert "sm_100a" in out
+
+
+def test_tuning_record_parses(tmp_path):
+    import json
+
+    from hero_b200 import autotune
+    from hero_b200._lib import load_tuning
+    assert len(list(autotune.candidates())) == 12
+    p = tmp_path / "t.json"
+    p.write_text(json.dumps({"classes": [{"rows_max": 168, "warps_per_block": 2, "pair_strips": 0,
+                                          "chunk_strips": autotune.ALL}]}))
+    assert load_tuning(str(p)) == [{"rows_max": 168, "warps_per_block": 2, "pair_strips": 0,
+                                    "chunk_strips": autotune.ALL}]
+    assert load_tuning(str(tmp_path / "missing.json")) == []

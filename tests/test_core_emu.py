@@ -121,3 +121,44 @@ def test_rolling_kmers_match_direct(emu):
     codes = rng.integers(0, 4, 400).astype(np.uint8)
     for k in (1, 2, 15, 21, 31, 32, 33, 39, 47, 63):
         assert f(codes.ctypes.data, len(codes), k) == -1, k
+
+
+def test_pair_rows_match_oracle(oracle, emu):
+    """Two segments of one shape in the 16-bit halves of the pair rows: each
+    half's path equals the oracle's affine path (flags may differ in align-right,
+    share align-left)."""
+    import ctypes as C
+    f = emu.lib.emu_align_pair
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p] * 4 + [C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int, C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    rng = np.random.default_rng(77)
+    done = 0
+    for _ in range(400):
+        ls = int(rng.integers(1, 200))
+        lq = int(rng.integers(1, 200))
+        seqs = []
+        for _h in range(2):
+            s = ACGT[rng.integers(0, 4, ls)]
+            if rng.random() < 0.7:
+                q = _indels(rng, synth.substitute(rng, np.resize(s, lq).copy(), 0.03), 0.01)
+                q = np.resize(q, lq).astype(np.uint8)
+            else:
+                q = ACGT[rng.integers(0, 4, lq)]
+            seqs.append((bytes(s), bytes(q)))
+        left = int(rng.integers(0, 2))
+        fa = (int(rng.integers(0, 2)) | (left << 1))
+        fb = (int(rng.integers(0, 2)) | (left << 1))
+        band_a, band_b = int(rng.choice([400, 1000])), int(rng.choice([400, 1000]))
+        cap = ls + lq + 1
+        oa, ob = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
+        na, nb = C.c_int32(), C.c_int32()
+        bufs = [np.frombuffer(x, np.uint8).copy() for x in (seqs[0][0], seqs[0][1], seqs[1][0], seqs[1][1])]
+        rc = f(*[b.ctypes.data for b in bufs], ls, lq, band_a, band_b, fa, fb,
+               oa.ctypes.data, C.byref(na), ob.ctypes.data, C.byref(nb), cap)
+        assert rc == 0
+        for (s, q), band, fl, ops, n in ((seqs[0], band_a, fa, oa, na), (seqs[1], band_b, fb, ob, nb)):
+            want, _ = oracle.align(1, s, q, band, bool(fl & 1), bool(fl & 2))
+            assert np.array_equal(want, ops[:n.value]), (ls, lq, band, fl)
+        done += 1
+    assert done == 400
