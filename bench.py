@@ -286,12 +286,12 @@ def run_served(jobs, reads, dev: int, busy_target: float = 0.85, check: int = 3)
     srv = HeroServer(aligner="affine", device=dev)
     try:
         # warm-up (the server's context sizes its device buffers), then capacity:
-        # jobs submitted all at once, back to back (closed loop)
+        # every job of the stream submitted at once, back to back (closed loop)
         for i in range(min(2, len(jobs))):
             j = srv.submit(*reads[i])
             srv.wait(j)
             srv.release(j)
-        cal = list(range(min(16, len(jobs))))
+        cal = list(range(len(jobs)))  # the whole stream, so the load below is a true fraction
         t0 = time.perf_counter()
         ids = [srv.submit(*reads[i]) for i in cal]
         for j in ids:

@@ -142,6 +142,27 @@ void hero_server::run_round(std::vector<uint64_t> ids) {
         std::lock_guard<std::mutex> g(mu);
         for (uint64_t id : ids) js.push_back(&jobs[id]);
     }
+    // jobs in order of their longest read: subject batches then hold reads of
+    // similar length (a job's reads only meet its own), so each batch's DP
+    // launch is shaped for its own segments rather than the round's longest
+    auto longest = [](const Job *j) {
+        uint64_t m = 0;
+        for (size_t i = 0; i + 1 < j->off.size(); i++) m = std::max(m, j->off[i + 1] - j->off[i]);
+        return m;
+    };
+    std::vector<std::pair<uint64_t, size_t>> order;
+    for (size_t t = 0; t < js.size(); t++) order.push_back({longest(js[t]), t});
+    std::stable_sort(order.begin(), order.end());
+    {
+        std::vector<Job *> js2;
+        std::vector<uint64_t> ids2;
+        for (const auto &o : order) {
+            js2.push_back(js[o.second]);
+            ids2.push_back(ids[o.second]);
+        }
+        js.swap(js2);
+        ids.swap(ids2);
+    }
     uint64_t n = 0, nb = 0;
     for (Job *j : js) {
         n += j->n();
