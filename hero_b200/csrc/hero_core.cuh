@@ -791,7 +791,9 @@ HERO_HD uint32_t dp_whole_row(const int32_t (&sc)[W], uint32_t diag, int32_t (&f
         const int32_t dx = kDX;
         if (AFFINE) {
             const int32_t ex = kEX;
-            const int32_t yv = add_max(lf, kDY, ly + kEX);    // BandAligner.cpp:180-188
+            // BandAligner.cpp:180-188: max(FM + dy, IY + ex) of the cell to the left,
+            // with the add on FM off the IY chain (one dependent op per column)
+            const int32_t yv = add_max(ly, kEX, lf + kDY);
             const int32_t xv = add_max(f[w], dx, x[w] + ex);  // BandAligner.cpp:189-201
             const int32_t fv = dm + sc[w];                    // BandAligner.cpp:203-207
             dm = m[w];
@@ -945,7 +947,7 @@ HERO_HD uint32_t dp_pair_row(const uint32_t (&sc)[W], uint32_t diag_a, uint32_t 
     uint32_t da = 0, db = 0, la = 0, lb = 0;
 #pragma unroll
     for (int32_t w = 0; w < W; w++) {
-        const uint32_t yv = add_max2(lf, DY2, add2(ly, EX2));      // BandAligner.cpp:180-188
+        const uint32_t yv = add_max2(ly, EX2, add2(lf, DY2));      // BandAligner.cpp:180-188
         const uint32_t xv = add_max2(f[w], DX2, add2(x[w], EX2));  // BandAligner.cpp:189-201
         const uint32_t fv = add2(dm, sc[w]);                       // BandAligner.cpp:203-207
         dm = m[w];

@@ -762,18 +762,35 @@ __device__ __forceinline__ uint32_t shape_key(const DpSeg &g) {
     return (uint32_t(nst) << kShapeStripShift) | (wl << 10) | uint32_t(r > 1023 ? 1023 : r);
 }
 
+// Counting sort by shape.  Segments of a chain mostly share a few shapes, so
+// the lanes of a warp with equal keys (__match_any_sync) add their count with
+// one atomic by the lowest of them; in the scatter each lane then takes its
+// rank among them.  The order inside a bin is free: every segment writes its
+// results to its own slot.
 __global__ void k_dp_hist(const DpSeg *segs, uint64_t nd, uint32_t *bins) {
-    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nd;
-         i += uint64_t(gridDim.x) * blockDim.x)
-        atomicAdd(&bins[shape_key(segs[i])], 1u);
+    const uint32_t lane = lane_id();
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) & ~uint64_t(31); b < nd;
+         b += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i = b + lane;
+        const uint32_t key = i < nd ? shape_key(segs[i]) : 0xffffffffu;
+        const uint32_t same = __match_any_sync(0xffffffffu, key);
+        if (i < nd && lane == uint32_t(__ffs(int(same))) - 1u) atomicAdd(&bins[key], uint32_t(__popc(same)));
+    }
 }
 
 __global__ void k_dp_scatter(const DpSeg *segs, uint64_t nd, uint32_t *cursor,
                              const uint64_t *bin_off, uint32_t *perm) {
-    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nd;
-         i += uint64_t(gridDim.x) * blockDim.x) {
-        const uint32_t key = shape_key(segs[i]);
-        perm[bin_off[key] + atomicAdd(&cursor[key], 1u)] = uint32_t(i);
+    const uint32_t lane = lane_id();
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) & ~uint64_t(31); b < nd;
+         b += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i = b + lane;
+        const uint32_t key = i < nd ? shape_key(segs[i]) : 0xffffffffu;
+        const uint32_t same = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = uint32_t(__ffs(int(same))) - 1u;
+        uint32_t base = 0;
+        if (i < nd && lane == leader) base = atomicAdd(&cursor[key], uint32_t(__popc(same)));
+        base = __shfl_sync(0xffffffffu, base, int(leader));
+        if (i < nd) perm[bin_off[key] + base + __popc(same & ((1u << lane) - 1u))] = uint32_t(i);
     }
 }
 
