@@ -175,6 +175,29 @@ def cpu_sample(args):
     return rs, flags, desc
 
 
+CLI_BIN = os.path.join(ROOT, "hero_b200", "bin", "hero_b200")
+
+
+def measure_file_e2e(rs, flags: list[str]) -> dict | None:
+    """The drop-in program file to file: FASTQ in, .fasta and .info out, with the
+    reference's flags (parsing, upload, correction, download and writing)."""
+    if not os.path.exists(CLI_BIN):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        fq = os.path.join(d, "in.fq")
+        rs.write_fastq(fq)
+        out = os.path.join(d, "out")
+        t0 = time.perf_counter()
+        r = subprocess.run([CLI_BIN, "-q", fq, "-s", fq, "-o", out] + flags,
+                           stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        return {"error": r.stdout[-300:]}
+    return {"seconds": wall, "bases_per_s": rs.total_bases / wall,
+            "command": "hero_b200/bin/hero_b200 -q in.fq -s in.fq -o out " + " ".join(flags),
+            "includes": "process start, FASTQ parse, device setup, correction, .fasta/.info writing"}
+
+
 def measure_cpu_baseline(args) -> dict:
     if not os.path.exists(REF_BIN):
         return {"value": None, "unit": "bases/s", "cores": 0, "kind": "reference",
@@ -521,6 +544,7 @@ def bench_hero(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = measure_cpu_baseline(args)
+    file_e2e = measure_file_e2e(rs, flags) if rank == 0 and world == 1 and not args.profile else None
 
     if rank == 0:
         line = {
@@ -552,6 +576,7 @@ def bench_hero(args):
             "plain_form": {"value": plain_value, "ms_per_step": 1e3 * t_plain / plain_steps,
                            "stage_ms_per_step": per},
             "cpu_baseline": cpu,
+            "file_e2e": file_e2e,
             "clocks": clocks,
             "gpu_launches": launches,
             "work_per_step": {"dp_cells": cells // steps,

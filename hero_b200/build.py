@@ -79,7 +79,7 @@ def build_cli(verbose: bool = False, force: bool = False) -> str | None:
         return CLI
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
     cxx = shutil.which("g++") or "g++"
-    _run([cxx, "-std=c++17", "-O3", "-fopenmp", "-I", os.path.join(ROOT, "include"), "-o", CLI]
+    _run([cxx, "-std=c++17", "-O3", "-pthread", "-I", os.path.join(ROOT, "include"), "-o", CLI]
          + srcs + ["-L", HERE, "-lhero_b200", "-Wl,-rpath,$ORIGIN/.."], verbose)
     return CLI
 

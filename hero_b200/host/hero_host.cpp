@@ -9,6 +9,10 @@
 #include <fstream>
 #include <iostream>
 #include <sstream>
+#include <algorithm>
+#include <string_view>
+#include <thread>
+#include <vector>
 
 namespace herohost {
 
@@ -137,67 +141,135 @@ bool Config::parse(int argc, char **argv) {
 // header line then everything up to the next '>' with newlines removed; names
 // lose a leading '>' or '@'; bases are upper-cased; id = atoi(name).
 // ---------------------------------------------------------------------------
+// host threads for parsing and formatting
+static unsigned host_threads() {
+    const unsigned t = std::thread::hardware_concurrency();
+    return t ? (t > 64 ? 64 : t) : 4;
+}
+
+// runs fn(begin, end) over [0, n) in one contiguous piece per thread
+template <class Fn>
+static void parallel_ranges(uint64_t n, Fn fn) {
+    const unsigned T = n < 4096 ? 1 : host_threads();
+    if (T == 1) {
+        fn(uint64_t(0), n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t++) {
+        const uint64_t a = n * t / T, b = n * (t + 1) / T;
+        th.emplace_back([=] { fn(a, b); });
+    }
+    for (std::thread &x : th) x.join();
+}
+
+// One pass finds each record's name line and sequence span (the reference's
+// line rules: QueryDataset.cpp:246-391); threads then parse the ids, count and
+// copy the uppercased bases into place.
 bool load_reads(const std::string &path, ReadSet &out, std::string *err) {
-    std::ifstream f(path.c_str(), std::ios::binary);
-    if (!f.is_open()) {
+    std::FILE *fp = std::fopen(path.c_str(), "rb");
+    if (!fp) {
         if (err) *err = "Unable to open file: " + path;
         return false;
     }
-    std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    std::string data;
+    if (std::fseek(fp, 0, SEEK_END) == 0) {
+        const long sz = std::ftell(fp);
+        if (sz > 0) {
+            data.resize(size_t(sz));
+            std::rewind(fp);
+            data.resize(std::fread(&data[0], 1, size_t(sz), fp));
+        }
+    }
+    std::fclose(fp);
     if (data.empty()) return true;
     const bool fasta = data[0] == '>';
     if (!fasta && data[0] != '@') {
         if (err) *err = "Unknown input file format: " + path;
         return false;
     }
+    struct Rec {
+        size_t name, nlen, seq, slen;  // spans in data; FASTA sequences may hold newlines
+    };
+    std::vector<Rec> recs;
+    recs.reserve(data.size() / 256 + 16);
     size_t p = 0;
     const size_t n = data.size();
-    auto line = [&](std::string_view &v) -> bool {
+    const char *d = data.data();
+    auto line = [&](size_t &b, size_t &len) -> bool {
         if (p >= n) return false;
-        size_t e = data.find('\n', p);
-        if (e == std::string::npos) e = n;
-        v = std::string_view(data.data() + p, e - p);
+        const void *q = std::memchr(d + p, '\n', n - p);
+        const size_t e = q ? size_t(static_cast<const char *>(q) - d) : n;
+        b = p;
+        len = e - p;
         p = e < n ? e + 1 : n;
         return true;
     };
-    auto add = [&](std::string_view name, const char *s, size_t len, bool skip_newlines) {
-        if (!name.empty() && (name[0] == '>' || name[0] == '@')) name.remove_prefix(1);
-        std::string nm(name);
-        out.uid.push_back(int64_t(std::atoi(nm.c_str())));
-        for (size_t i = 0; i < len; i++) {
-            const char c = s[i];
-            if (skip_newlines && c == '\n') continue;
-            out.seq.push_back(char(std::toupper(static_cast<unsigned char>(c))));
-        }
-        out.off.push_back(out.seq.size());
-    };
     if (!fasta) {
-        std::string_view l0, l1, l2, l3;
-        while (line(l0)) {
-            if (!line(l1)) {
-                if (!l0.empty()) {  // a lone header line at the end
+        size_t b0, n0, b1, n1, b2, n2, b3, n3;
+        while (line(b0, n0)) {
+            if (!line(b1, n1)) {
+                if (n0) {  // a lone header line at the end
                     if (err) *err = "truncated FASTQ record in " + path;
                     return false;
                 }
                 break;
             }
-            line(l2);
-            line(l3);
-            if (l0.empty() && l1.empty()) continue;  // trailing blank lines
-            add(l0, l1.data(), l1.size(), false);
+            line(b2, n2);
+            line(b3, n3);
+            if (!n0 && !n1) continue;  // trailing blank lines
+            recs.push_back({b0, n0, b1, n1});
         }
     } else {
         while (p < n) {
-            std::string_view l0;
-            line(l0);
-            size_t e = data.find('>', p);
-            if (e == std::string::npos) e = n;
+            size_t b0, n0;
+            line(b0, n0);
+            const void *q = std::memchr(d + p, '>', n - p);
+            const size_t e = q ? size_t(static_cast<const char *>(q) - d) : n;
             const size_t b = p;
             p = e < n ? e + 1 : n;
-            if (l0.empty() && e == b) continue;  // blank trailing record
-            add(l0, data.data() + b, e - b, true);
+            if (!n0 && e == b) continue;  // blank trailing record
+            recs.push_back({b0, n0, b, e - b});
         }
     }
+    const uint64_t nr = recs.size(), base_reads = out.uid.size();
+    const uint64_t base = out.seq.size();
+    std::vector<uint64_t> len(nr);
+    out.uid.resize(base_reads + nr);
+    parallel_ranges(nr, [&](uint64_t a, uint64_t b) {
+        std::string nm;
+        for (uint64_t r = a; r < b; r++) {
+            const Rec &x = recs[r];
+            size_t nb = x.name, nl = x.nlen;
+            if (nl && (d[nb] == '>' || d[nb] == '@')) {
+                nb++;
+                nl--;
+            }
+            nm.assign(d + nb, nl);
+            out.uid[base_reads + r] = int64_t(std::atoi(nm.c_str()));
+            uint64_t l = x.slen;
+            if (fasta) l -= uint64_t(std::count(d + x.seq, d + x.seq + x.slen, '\n'));
+            len[r] = l;
+        }
+    });
+    out.off.resize(base_reads + nr + 1);
+    uint64_t tot = base;
+    for (uint64_t r = 0; r < nr; r++) {
+        tot += len[r];
+        out.off[base_reads + r + 1] = tot;
+    }
+    out.seq.resize(tot);
+    parallel_ranges(nr, [&](uint64_t a, uint64_t b) {
+        for (uint64_t r = a; r < b; r++) {
+            const Rec &x = recs[r];
+            char *o = &out.seq[out.off[base_reads + r]];
+            for (size_t i = 0; i < x.slen; i++) {
+                const char c = d[x.seq + i];
+                if (fasta && c == '\n') continue;
+                *o++ = char(std::toupper(static_cast<unsigned char>(c)));
+            }
+        }
+    });
     return true;
 }
 
@@ -207,35 +279,59 @@ bool QueryDataset::build(const Config &c, std::string *err) {
     return true;
 }
 
+// QueryDataset::writeQueryOut (QueryDataset.cpp:414-537): records formatted by
+// threads in contiguous pieces, appended in order.  A double prints as an
+// ostream prints it by default (precision 6, the %g conversion).
 bool QueryDataset::write(const Config &c, std::string *err) const {
     const uint64_t n = reads.n();
     if (!c.single_reads && (n % 2)) {
         if (err) *err = "an odd number of reads needs --singleReads (the paired writer reads past the end)";
         return false;
     }
+    const unsigned T = n < 4096 ? 1 : host_threads();
+    std::vector<std::string> fa_parts(T), info_parts(T);
+    auto piece = [&](unsigned t) {
+        const uint64_t a = n * t / T, b = n * (t + 1) / T;
+        std::string &fa = fa_parts[t], &fi = info_parts[t];
+        fa.reserve(size_t(reads.off[b] - reads.off[a]) + size_t(b - a) * 24);
+        char buf[160];
+        for (uint64_t i = a; i < b; i++) {
+            const uint64_t L = reads.off[i + 1] - reads.off[i];
+            int k = std::snprintf(buf, sizeof(buf), ">%lld\n", static_cast<long long>(reads.uid[i]));
+            fa.append(buf, size_t(k));
+            fa.append(corrected.data() + reads.off[i], size_t(L));
+            fa.push_back('\n');
+            if (c.covinfo) {
+                k = std::snprintf(buf, sizeof(buf), "%lld\t%u\t%u\t%u\t%llu\t%g\t%g\n",
+                                  static_cast<long long>(reads.uid[i]), imin[i], imed[i], imax[i],
+                                  static_cast<unsigned long long>(L), mismatch_rate[i], gc[i]);
+                fi.append(buf, size_t(k));
+            }
+        }
+    };
+    if (T == 1) {
+        piece(0);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < T; t++) th.emplace_back(piece, t);
+        for (std::thread &x : th) x.join();
+    }
     // both files are opened in append mode, as the reference does
-    std::ofstream fa((c.out + ".fasta").c_str(), std::ios_base::app);
-    if (!fa.is_open()) {
+    auto put = [&](const std::string &path, const std::vector<std::string> &parts) {
+        std::FILE *f = std::fopen(path.c_str(), "ab");
+        if (!f) return false;
+        bool good = true;
+        for (const std::string &x : parts)
+            if (!x.empty() && std::fwrite(x.data(), 1, x.size(), f) != x.size()) good = false;
+        return std::fclose(f) == 0 && good;
+    };
+    if (!put(c.out + ".fasta", fa_parts)) {
         if (err) *err = "cannot write " + c.out + ".fasta";
         return false;
     }
-    for (uint64_t i = 0; i < n; i++) {
-        fa << ">" << reads.uid[i] << std::endl;
-        fa.write(corrected.data() + reads.off[i], std::streamsize(reads.off[i + 1] - reads.off[i]));
-        fa << std::endl;
-    }
-    fa.close();
-    if (c.covinfo) {
-        std::ofstream fi((c.out + ".info").c_str(), std::ios_base::app);
-        if (!fi.is_open()) {
-            if (err) *err = "cannot write " + c.out + ".info";
-            return false;
-        }
-        for (uint64_t i = 0; i < n; i++) {
-            fi << reads.uid[i] << "\t" << imin[i] << "\t" << imed[i] << "\t" << imax[i] << "\t"
-               << (reads.off[i + 1] - reads.off[i]) << "\t" << mismatch_rate[i] << "\t" << gc[i]
-               << std::endl;
-        }
+    if (c.covinfo && !put(c.out + ".info", info_parts)) {
+        if (err) *err = "cannot write " + c.out + ".info";
+        return false;
     }
     return true;
 }
