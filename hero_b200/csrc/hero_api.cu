@@ -60,6 +60,7 @@ struct hero_ctx {
     DBuf ch_subj, ch_query, ch_key_off, ch_seg_off, ch_nkeys, ch_nseg, ch_orient, ch_status,
         ch_win, ch_rate, ch_len;
     DBuf keys, segs, sums, cells, ops, perm, bins, bin_off, tb, bnd, dp_tasks, winners;
+    DBuf win_sorted, win_bins;  // winners sorted by chain shape, and the sort's bins
     DBuf scan_tmp, counters;
     // index build temporaries (kept between builds)
     DBuf x_cnt, x_koff, x_klo, x_khi, x_kval, x_owner, x_count, x_slot_of, x_start, x_fill, x_tmp;
@@ -94,7 +95,7 @@ struct hero_ctx {
                         &ch_win, &ch_rate, &ch_len, &keys, &segs, &sums, &cells, &ops, &perm,
                         &bins, &bin_off, &tb, &bnd, &dp_tasks, &winners, &scan_tmp, &counters, &x_cnt, &x_koff,
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
-                        &x_fill, &x_tmp, &q_job};
+                        &x_fill, &x_tmp, &q_job, &win_sorted, &win_bins};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -566,10 +567,13 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         launch_assemble(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSum>(c->sums),
                         P_<uint32_t>(c->cells), ctr, c->st);
         if ((r = c->ensure(c->winners, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
+        if ((r = c->ensure(c->win_sorted, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
+        if ((r = c->ensure(c->win_bins, kWinScratch * 4, "winners"))) break;
         launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
                       P_<uint32_t>(c->winners), ctr, c->st);
         rec(5);
-        launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->keys), subj, q,
+        launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->win_sorted),
+                    P_<uint32_t>(c->win_bins), P_<uint32_t>(c->keys), subj, q,
                     P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov),
                     P_<int32_t>(c->mdiff), ctr, c->st);
         if ((r = c->check_launch("record/vote"))) break;

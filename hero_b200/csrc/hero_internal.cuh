@@ -173,10 +173,11 @@ void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
 // Votes.  A mismatch votes the subject base into cov[pos][4]; a run of matches
 // votes the query's own base, recorded as +1/-1 at the run's ends in mdiff
 // (a per-read difference array, summed by the consensus).
+constexpr uint32_t kWinScratch = 3 * 512;  // uint32 bins, offsets and cursors of the winner sort
 void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,
-                 const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
-                 uint32_t stride, const DpSum *sums, uint32_t *cov, int32_t *mdiff,
-                 unsigned long long *counters, cudaStream_t st);
+                 uint32_t *sorted, uint32_t *win_bins, const uint32_t *keys, ReadsView subj,
+                 ReadsView q, const uint32_t *ops, uint32_t stride, const DpSum *sums,
+                 uint32_t *cov, int32_t *mdiff, unsigned long long *counters, cudaStream_t st);
 void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, const int32_t *mdiff,
                       uint8_t *out, uint32_t *colsum, uint32_t *imin, uint32_t *imed,
                       uint32_t *imax, double *mis, cudaStream_t st);

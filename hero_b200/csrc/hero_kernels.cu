@@ -1532,6 +1532,61 @@ struct VoteVisitor {
     __device__ void finish() { close(); }
 };
 
+// Winners sorted by chain shape (DP pieces, keys) before the votes: a warp then
+// walks chains of one shape, and its lanes stay together (a counting sort over
+// kWinBins shapes; order inside a shape is free, votes commute).
+constexpr uint32_t kWinBins = 512;
+
+__device__ __forceinline__ uint32_t win_key(const ChainArrays &ch, uint32_t c) {
+    const uint32_t ns = ch.nseg[c], nk = ch.nkeys[c];
+    return ((ns < 31u ? ns : 31u) << 4) | (nk < 15u ? nk : 15u);
+}
+
+__global__ void k_win_hist(const unsigned long long *counters, ChainArrays ch,
+                           const uint32_t *winners, uint32_t *bins) {
+    __shared__ uint32_t h[kWinBins];
+    for (uint32_t i = threadIdx.x; i < kWinBins; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const uint64_t nw = counters[C_WIN];
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nw;
+         i += uint64_t(gridDim.x) * blockDim.x)
+        atomicAdd(&h[win_key(ch, winners[i])], 1u);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kWinBins; i += blockDim.x)
+        if (h[i]) atomicAdd(&bins[i], h[i]);
+}
+
+// bins -> first slot of each shape (exclusive scan); cursors start at zero
+__global__ void k_win_offsets(const uint32_t *bins, uint32_t *off, uint32_t *cursor) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        uint32_t t = 0;
+        for (uint32_t i = 0; i < kWinBins; i++) {
+            off[i] = t;
+            t += bins[i];
+            cursor[i] = 0;
+        }
+    }
+}
+
+__global__ void k_win_scatter(const unsigned long long *counters, ChainArrays ch,
+                              const uint32_t *winners, const uint32_t *off, uint32_t *cursor,
+                              uint32_t *sorted) {
+    const uint32_t lane = lane_id();
+    const uint64_t nw = counters[C_WIN];
+    for (uint64_t b = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) & ~uint64_t(31); b < nw;
+         b += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i = b + lane;
+        const uint32_t w = i < nw ? winners[i] : 0u;
+        const uint32_t key = i < nw ? win_key(ch, w) : 0xffffffffu;
+        const uint32_t same = __match_any_sync(0xffffffffu, key);
+        const uint32_t leader = uint32_t(__ffs(int(same))) - 1u;
+        uint32_t base = 0;
+        if (i < nw && lane == leader) base = atomicAdd(&cursor[key], uint32_t(__popc(same)));
+        base = __shfl_sync(0xffffffffu, base, int(leader));
+        if (i < nw) sorted[off[key] + base + __popc(same & ((1u << lane) - 1u))] = w;
+    }
+}
+
 __global__ void k_vote(Params p, const unsigned long long *counters_in, ChainArrays ch,
                        const uint32_t *winners, const uint32_t *keys, ReadsView subj, ReadsView q,
                        const uint32_t *ops, uint32_t stride, const DpSum *sums, uint32_t *cov,
@@ -1922,12 +1977,21 @@ void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
 }
 
 void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,
-                 const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
-                 uint32_t stride, const DpSum *sums, uint32_t *cov, int32_t *mdiff,
-                 unsigned long long *counters, cudaStream_t st) {
+                 uint32_t *sorted, uint32_t *win_bins, const uint32_t *keys, ReadsView subj,
+                 ReadsView q, const uint32_t *ops, uint32_t stride, const DpSum *sums,
+                 uint32_t *cov, int32_t *mdiff, unsigned long long *counters, cudaStream_t st) {
     if (!max_winners) return;
+    uint32_t *bins = win_bins, *off = win_bins + kWinBins, *cursor = win_bins + 2 * kWinBins;
+    cudaMemsetAsync(bins, 0, kWinBins * sizeof(uint32_t), st);
+    const unsigned g = grid_1d(max_winners, 256, 148u * 8u);
     counted();
-    k_vote<<<grid_1d(max_winners, 128), 128, 0, st>>>(p, counters, ch, winners, keys, subj, q, ops,
+    k_win_hist<<<g, 256, 0, st>>>(counters, ch, winners, bins);
+    counted();
+    k_win_offsets<<<1, 32, 0, st>>>(bins, off, cursor);
+    counted();
+    k_win_scatter<<<g, 256, 0, st>>>(counters, ch, winners, off, cursor, sorted);
+    counted();
+    k_vote<<<grid_1d(max_winners, 128), 128, 0, st>>>(p, counters, ch, sorted, keys, subj, q, ops,
                                                       stride, sums, cov, mdiff, counters);
 }
 
