@@ -22,6 +22,19 @@ slowest rank's time.
 --impl reference times the reference itself (oracle/_ref/hero_ref, built
 from the reference sources) on the host cores, on a bounded sample of the same
 workload (same generator, smaller genome, same coverage/read length/errors).
+
+The default line also carries:
+  roofline          the DP kernel against the measured int32 add+max peak
+  seeding_roofline  probes + hit sort against the measured HBM bandwidth
+  served            a stream of independent jobs through a hero_server
+                    (Poisson arrivals at 85 % of its closed-loop capacity):
+                    p50/p99 job latency, aggregate bases/s, served == alone
+  file_e2e          the drop-in program, FASTQ file to .fasta/.info files
+  cpu_baseline      the reference on the host cores (bounded sample)
+
+Other workloads (--workload): config1 (plain/global, 300 k x 100 bp),
+config3 (mixed lengths 75-250 bp, 12.3 M reads), config5 (diploid, 20 M
+reads), config4 (the serving stream alone: p50/p99 job latency).
 """
 from __future__ import annotations
 

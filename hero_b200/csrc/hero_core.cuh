@@ -1248,19 +1248,26 @@ HERO_HD int32_t dp_traceback(const SegView &v, Scratch &sc, Emit &emit, DpSum &s
 // c[] already includes the read's own vote.  Returns the new code, or -1 to
 // keep the base.
 // ---------------------------------------------------------------------------
+// The reference divides every count by the sum and keeps the largest fraction
+// and the one it replaced.  For sum > 0 the fractions compare as the counts do
+// (two different counts differ by at least 1/sum, far above the rounding), so
+// the scan runs on the counts and only the two kept fractions are divided, with
+// the same operands and rounding.  With sum == 0 no fraction is ever larger.
 HERO_HD int32_t column_consensus(const uint32_t c[4], double thr) {
     double sum = 0;
     for (int j = 0; j < 4; j++) sum = HERO_DADD(sum, double(c[j]));
     int32_t id = -1;
-    double fLargest = 0, fLarger = 0;
+    uint32_t largest = 0, larger = 0;  // counts behind fLargest, fLarger
     for (int j = 0; j < 4; j++) {
-        const double f = HERO_DDIV(double(c[j]), sum);
-        if (fLargest < f) {
-            fLarger = fLargest;
-            fLargest = f;
+        if (largest < c[j]) {
+            larger = largest;
+            largest = c[j];
             id = j;
         }
     }
+    if (id < 0) return -1;  // no count above 0: the reference keeps id -1 too
+    const double fLargest = HERO_DDIV(double(largest), sum);
+    const double fLarger = HERO_DDIV(double(larger), sum);
     if (HERO_DSUB(fLargest, fLarger) >= thr) return id;
     return -1;
 }

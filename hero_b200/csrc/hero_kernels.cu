@@ -1620,9 +1620,12 @@ __global__ void k_vote(Params p, const unsigned long long *counters_in, ChainArr
 // consensus: QueryRead::callConsensus + calculateCoverageStatistic
 // (QueryRead.cpp:148-212); one warp per query read
 // ---------------------------------------------------------------------------
-__global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, const int32_t *mdiff,
-                            uint8_t *out, uint32_t *colsum, uint32_t *imin, uint32_t *imed,
-                            uint32_t *imax, double *mis) {
+constexpr uint32_t kConsWarps = 8, kConsSmem = 1024;  // column sums of reads up to 1024 bases
+
+__global__ void __launch_bounds__(kConsWarps * 32)
+    k_consensus(Params p, ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint8_t *out,
+                uint32_t *colsum, uint32_t *imin, uint32_t *imed, uint32_t *imax, double *mis) {
+    __shared__ uint32_t sums[kConsWarps][kConsSmem];
     const uint32_t lane = lane_id();
     const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
     for (uint64_t r = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < q.n;
@@ -1638,6 +1641,8 @@ __global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, const in
         }
         const uint64_t b = q.off[r];
         const uint32_t L = q.len[r];
+        // the read's column sums, in shared memory when they fit
+        uint32_t *cs = L <= kConsSmem ? sums[threadIdx.x >> 5] : colsum + b;
         uint32_t changed = 0, mn = 0xffffffffu, mx = 0;
         int32_t carry = 0;  // match-run coverage entering the current chunk
         for (uint32_t c0 = 0; c0 < L; c0 += 32) {
@@ -1659,7 +1664,7 @@ __global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, const in
                 }
                 out[b + i] = uint8_t(code_base(nb));
                 const uint32_t sm = c[0] + c[1] + c[2] + c[3];
-                colsum[b + i] = sm;
+                cs[i] = sm;
                 mn = sm < mn ? sm : mn;
                 mx = sm > mx ? sm : mx;
             }
@@ -1673,10 +1678,10 @@ __global__ void k_consensus(Params p, ReadsView q, const uint32_t *cov, const in
         uint32_t v_hi = 0, v_lo = 0;
         bool f_hi = false, f_lo = false;
         for (uint32_t i = lane; i < L; i += 32) {
-            const uint32_t x = colsum[b + i];
+            const uint32_t x = cs[i];
             uint32_t lt = 0, le = 0;
             for (uint32_t j = 0; j < L; j++) {
-                const uint32_t y = colsum[b + j];
+                const uint32_t y = cs[j];
                 lt += y < x;
                 le += y <= x;
             }
