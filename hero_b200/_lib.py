@@ -59,7 +59,8 @@ _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record"
 
 class HeroStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
-                [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64)])
+                [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64),
+                 ("dp_rows_max", C.c_uint64)])
 
 
 class DpTuning(C.Structure):

@@ -1,12 +1,16 @@
 """Autotuner of the banded-DP kernel shapes.
 
-For each class of subject batch (by the longest DP side, which follows the read
-length) it builds a sample correction job with reads of that length, runs the
-DP kernel under every candidate shape -- warps per block, 16-bit pairs of
-segments, row-chunk or one-lane tracebacks -- and records the fastest per
-class, with every candidate's time, in a JSON file (hero_b200/tuning.json by
-default), which hero_b200.Hero loads.  Shapes never change results: the tests
-check every candidate against the default on the same reads.
+For each sample read length it builds a correction job with reads of that
+length, runs the DP kernel under every candidate shape -- warps per block,
+16-bit pairs of segments, row-chunk or one-lane tracebacks -- and records the
+fastest, with every candidate's time, in a JSON file (hero_b200/tuning.json by
+default), which hero_b200.Hero loads.  A class is keyed on the longest DP side
+the sample's batches showed (read length - k for reads that share a k-mer
+anchor, not the read length): its bound ``rows_max`` is the midpoint to the
+next sample's longest side, so a batch takes the class of the nearest sample
+at or above it, and the last class covers every longer batch.  Shapes never
+change results: the tests check every candidate against the default on the
+same reads.
 
     python -m hero_b200.autotune [--out PATH] [--genome-bp N]
 """
@@ -21,8 +25,10 @@ import time
 ALL = 0xFFFFFFFE  # bit n = n strips, n = 1..31
 FROM3 = ALL & ~0x7  # 3 strips and more
 
-# (read length of the sample, class bound on the longest DP side)
-CLASSES = [(100, 112), (150, 168), (200, 224), (250, 1023)]
+# read lengths of the samples, one class each
+READ_LENGTHS = [100, 150, 200, 250]
+# bound of the last class: every batch the shared-memory kernel takes
+ROWS_LAST = 1023
 
 
 def candidates():
@@ -35,9 +41,9 @@ def sample(read_len: int, genome_bp: int, seed: int = 91):
     return synth.Job(0, 0.0, seed + read_len, genome_bp, read_len, 40.0).reads()
 
 
-def time_dp(h, reads, shape: dict, rows_max: int, rounds: int = 2) -> float:
+def time_dp(h, reads, shape: dict, rounds: int = 2) -> float:
     """Device time of the DP kernels of one correction under a shape (ms, best of rounds)."""
-    h.set_tuning([dict(shape, rows_max=rows_max)])
+    h.set_tuning([dict(shape, rows_max=ROWS_LAST)])
     best = None
     for _ in range(rounds):
         s0 = h.stats()
@@ -49,7 +55,12 @@ def time_dp(h, reads, shape: dict, rows_max: int, rounds: int = 2) -> float:
     return best
 
 
-def tune(genome_bp: int = 60_000, device: int = 0, classes=CLASSES, log=print) -> dict:
+def class_bounds(rows: list[int]) -> list[int]:
+    """rows_max of each class from the samples' longest DP sides (ascending)."""
+    return [(a + b) // 2 for a, b in zip(rows, rows[1:])] + [ROWS_LAST]
+
+
+def tune(genome_bp: int = 60_000, device: int = 0, read_lengths=READ_LENGTHS, log=print) -> dict:
     from hero_b200 import Hero
     out = {"device": None, "genome_bp": genome_bp, "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
            "classes": []}
@@ -58,19 +69,22 @@ def tune(genome_bp: int = 60_000, device: int = 0, classes=CLASSES, log=print) -
         out["device"] = torch.cuda.get_device_name(device)
     except Exception:  # noqa: BLE001 - the name is informational
         pass
-    for read_len, rows_max in classes:
+    for read_len in sorted(read_lengths):
         reads = sample(read_len, genome_bp)
         with Hero(aligner="affine", device=device, tuning=[]) as h:
             h.set_queries(reads.seq, reads.off, reads.names)
             timings = []
             for shape in candidates():
-                ms = time_dp(h, reads, shape, rows_max)
+                ms = time_dp(h, reads, shape)
                 timings.append((ms, shape))
                 log(f"  L={read_len} {shape} {ms:.2f} ms")
+            rows = int(h.stats()["dp_rows_max"])
         ms, best = min(timings, key=lambda x: x[0])
-        out["classes"].append(dict(best, rows_max=rows_max, read_len=read_len, ms=round(ms, 3),
+        out["classes"].append(dict(best, rows_seen=rows, read_len=read_len, ms=round(ms, 3),
                                    candidates=[dict(s, ms=round(t, 3)) for t, s in timings]))
-        log(f"L={read_len}: {best} ({ms:.2f} ms)")
+        log(f"L={read_len} (longest DP side {rows}): {best} ({ms:.2f} ms)")
+    for c, bound in zip(out["classes"], class_bounds([c["rows_seen"] for c in out["classes"]])):
+        c["rows_max"] = bound
     return out
 
 

@@ -831,6 +831,7 @@ extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
     s.dp_segments_ref = c->ctr[C_DP_REF];
     s.dp_cells = c->ctr[C_CELLS];
     s.dp_cells_computed = c->ctr[C_CELLS_ALL];
+    s.dp_rows_max = c->ctr[C_MAXR];
     s.vote_anomalies = c->ctr[C_ANOMALY];
     s.device_bytes_peak = c->bytes_peak;
     s.kernel_launches = kernel_launches();

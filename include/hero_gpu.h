@@ -81,6 +81,8 @@ typedef struct {
     double ms_align_wall;      /* host wall time inside the align calls */
     uint64_t graph_rounds;     /* rounds replayed from a CUDA graph */
     uint64_t dp_cells_computed; /* band cells of every DP segment computed on the device */
+    uint64_t dp_rows_max;      /* longest DP side (the row count of a segment) seen so far;
+                                  the key of hero_dp_tuning classes */
 } hero_stats;
 
 /* Returns the default parameters of the reference's Config. */

@@ -52,3 +52,10 @@ def test_tuning_record_parses(tmp_path):
     assert load_tuning(str(p)) == [{"rows_max": 168, "warps_per_block": 2, "pair_strips": 0,
                                     "chunk_strips": autotune.ALL}]
     assert load_tuning(str(tmp_path / "missing.json")) == []
+
+
+def test_tuning_class_bounds_meet_halfway():
+    from hero_b200 import autotune
+    # samples whose batches showed longest DP sides 61, 111, 161, 211
+    assert autotune.class_bounds([61, 111, 161, 211]) == [86, 136, 186, autotune.ROWS_LAST]
+    assert autotune.class_bounds([111]) == [autotune.ROWS_LAST]

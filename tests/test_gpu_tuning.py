@@ -43,9 +43,15 @@ def test_every_candidate_shape_gives_the_same_result(name):
 
 
 def test_tuner_records_the_fastest_candidate(tmp_path):
-    rec = autotune.tune(genome_bp=20_000, classes=[(150, 168)], log=lambda *a: None)
+    rec = autotune.tune(genome_bp=20_000, read_lengths=[150], log=lambda *a: None)
     (cls,) = rec["classes"]
-    assert cls["rows_max"] == 168 and len(cls["candidates"]) == len(list(autotune.candidates()))
+    # the class key is the longest DP side of the sample, as the oracle's segments give it
+    from hero_testlib import Oracle
+    seg = Oracle().correct(upper(autotune.sample(150, 20_000)), aligner="affine",
+                           keep_segments=True)["segments"]
+    rows = int(np.maximum(seg["s1"] - seg["s0"], seg["q1"] - seg["q0"]).max())
+    assert cls["rows_seen"] == rows and cls["rows_max"] == autotune.ROWS_LAST
+    assert len(cls["candidates"]) == len(list(autotune.candidates()))
     assert cls["ms"] == min(c["ms"] for c in cls["candidates"])
     p = tmp_path / "tuning.json"
     p.write_text(json.dumps(rec))
