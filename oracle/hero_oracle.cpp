@@ -32,6 +32,7 @@ const char ADNA[4] = {'A', 'C', 'T', 'G'};  // QueryRead.cpp:11
 struct Params {
     int64_t k, l;
     bool affine, keep_segments;
+    bool aln;  // alignment output (no -c): SubjectReadAligner::writeToFile
     double mis_rate, indel_rate, thr;
 };
 
@@ -304,7 +305,8 @@ struct Band {
 // -------------------------------------------------------------------------
 struct Record {
     uint32_t orient = 0;
-    uint32_t query = 0;              // iQueryReadUniqueId = inner id in consensus mode
+    uint32_t query = 0;              // inner id of the query read
+    uint64_t key = 0;                // iQueryReadUniqueId: inner id with -c, else atoi(name)
     int64_t pos = 0;                 // iPositionOfQueryOnSubject
     std::vector<char> type;
     std::vector<int> count;
@@ -442,6 +444,7 @@ struct Table {
 
 struct Outputs {
     std::vector<Record> kept;                 // SubjectRead::vAlignment
+    std::vector<std::pair<uint32_t, std::string>> aln;  // SubjectRead::sAlignment per subject
     std::vector<Segment> segments;
     hero_oracle_stats st{};
 };
@@ -453,6 +456,7 @@ struct Corrector {
     const Table &T;
     std::vector<uint32_t> *votes;  // per query: L*4 (atomic adds)
     std::vector<uint64_t> qoff;
+    const std::vector<std::string> *qrc = nullptr;  // query reverse complements (alignment output)
 
     Corrector(const Params &p_, const Reads &q, const Reads &s, const Table &t,
               std::vector<uint32_t> *v, std::vector<uint64_t> off)
@@ -516,7 +520,9 @@ struct Corrector {
     // getAlignment2 (SubjectReadAligner.cpp:197-389)
     bool getAlignment2(Outputs &o, Band &b, uint32_t subject, const std::string &Sseq,
                        uint32_t orient, const std::vector<Key> &keys, Record &rec) {
-        const std::string &Qs = Q.seq[keys[0].q];
+        // SubjectReadAligner.cpp:199-210: without -c the reverse-complement pass
+        // aligns the query's reverse complement to the forward subject
+        const std::string &Qs = (p.aln && orient == 1) ? (*qrc)[keys[0].q] : Q.seq[keys[0].q];
         const int64_t k = p.k;
         int64_t posQ = keys[0].posQ, posS = keys[0].posS;
         int64_t Lq = int64_t(Qs.size()), Ls = int64_t(Sseq.size());
@@ -530,6 +536,8 @@ struct Corrector {
         rec = Record();
         rec.orient = orient;
         rec.query = keys[0].q;
+        // SubjectReadAligner.cpp:230-235 (UINT64 field)
+        rec.key = p.aln ? uint64_t(Q.uid[keys[0].q]) : uint64_t(keys[0].q);
         b.m_band = extra * 2;  // setBand
         const uint32_t qid = keys[0].q;
         if (posQ != 0 && posS != 0) {
@@ -644,7 +652,7 @@ struct Corrector {
         return true;
     }
 
-    // SubjectRead::addAlignment (SubjectRead.cpp:25-79); consensus mode, no -v
+    // SubjectRead::addAlignment (SubjectRead.cpp:25-79), without -v
     static void addAlignment(std::vector<Record> &v, uint64_t &largest, Record &&r) {
         auto better_in_place = [](Record &cur, Record &&r) {
             double a = cur.indel_rate + cur.mis_rate, b = r.indel_rate + r.mis_rate;
@@ -657,23 +665,23 @@ struct Corrector {
             cur = std::move(r);
         };
         if (v.empty()) {
-            largest = r.query;
+            largest = r.key;
             v.push_back(std::move(r));
             return;
         }
-        if (v.back().query == r.query) {
+        if (v.back().key == r.key) {
             better_in_place(v.back(), std::move(r));
         } else if (largest >= r.query) {
             for (size_t i = 0; i < v.size(); i++) {
-                if (v[i].query > r.query) break;
-                if (v[i].query == r.query) {
+                if (v[i].key > r.key) break;
+                if (v[i].key == r.key) {
                     better_in_place(v[i], std::move(r));
                     return;
                 }
             }
             v.push_back(std::move(r));
         } else {
-            largest = r.query;
+            largest = r.key;
             v.push_back(std::move(r));
         }
     }
@@ -718,8 +726,41 @@ struct Corrector {
     }
 
     // SubjectReadAligner::start loop body (SubjectReadAligner.cpp:523-562) for one subject
+    // AlignmentRecord::getCigar (AlignmentRecord.cpp:102-149), storeOverhang off:
+    // id,orientation,position,CIGAR,inserted bases of the inner I entries,
+    static void cigarText(const Record &r, const std::string &qs, std::string &t) {
+        t += std::to_string(r.key);
+        t += ',';
+        t += std::to_string(r.orient);
+        t += ',';
+        t += std::to_string(r.pos);
+        t += ',';
+        for (size_t i = 0; i < r.type.size(); i++) {
+            t += std::to_string(r.count[i]);
+            t += r.type[i];
+        }
+        t += ',';
+        size_t index = 0;
+        for (size_t i = 0; i < r.type.size(); i++) {
+            if (r.type[i] == 'I') {
+                for (int j = 0; j < r.count[i]; j++) {
+                    if (i != 0 && i != r.count.size() - 1) t += qs.at(index);
+                    index++;
+                }
+                continue;
+            }
+            if (r.type[i] == 'D') continue;
+            index += size_t(r.count[i]);
+        }
+        t += ',';
+    }
+
     void processSubject(uint32_t s, Outputs &o, Band &b) {
-        if (!S.good[s]) return;
+        if (!S.good[s]) {
+            // SubjectReadAligner::writeToFile (SubjectReadAligner.cpp:898-902): no alignment string
+            if (p.aln) o.aln.push_back({s, ">" + std::to_string(S.uid[s]) + "\n\n"});
+            return;
+        }
         const std::string &fwd = S.seq[s];
         std::string rc = revcomp(fwd);
         std::vector<Record> vAlignment;
@@ -737,6 +778,14 @@ struct Corrector {
                 if (it == T.map.end()) continue;
                 for (auto &e : it->second) {
                     if (Q.uid[e.first] == S.uid[s]) continue;
+                    if (p.aln && orient == 1) {
+                        // SubjectReadAligner.cpp:477-481: positions flipped onto the
+                        // forward subject and the query's reverse complement
+                        const int64_t lq = int64_t(Q.seq[e.first].size());
+                        hits.push_back(Key{e.first, int64_t(seq.size()) - (i + p.k),
+                                           lq - (e.second + p.k)});
+                        continue;
+                    }
                     hits.push_back(Key{e.first, i, e.second});
                 }
             }
@@ -776,7 +825,9 @@ struct Corrector {
                     if (kl[c] != best) continue;
                     o.st.chains_kept++;
                     Record rec;
-                    if (getAlignment2(o, b, s, seq, orient, chains[c], rec)) {
+                    // processOneSubjectRead2 (SubjectReadAligner.cpp:808-812): without
+                    // -c the subject stays forward in both passes
+                    if (getAlignment2(o, b, s, p.aln ? fwd : seq, orient, chains[c], rec)) {
                         o.st.records_accepted++;
                         addAlignment(vAlignment, largest, std::move(rec));
                     }
@@ -785,7 +836,16 @@ struct Corrector {
             }
         }
         o.st.records_kept += vAlignment.size();
-        applyVotes(vAlignment, fwd, rc);
+        if (p.aln) {
+            // SubjectRead::writeAlignment (SubjectRead.cpp:179-193): records in list order
+            std::string t = ">" + std::to_string(S.uid[s]) + "\n";
+            for (const Record &r : vAlignment)
+                cigarText(r, r.orient == 1 ? (*qrc)[r.query] : Q.seq[r.query], t);
+            t += "\n";
+            o.aln.push_back({s, std::move(t)});
+        } else {
+            applyVotes(vAlignment, fwd, rc);
+        }
         std::sort(vAlignment.begin(), vAlignment.end(),
                   [](const Record &a, const Record &c) { return a.query < c.query; });
         for (auto &r : vAlignment) o.kept.push_back(std::move(r));
@@ -797,6 +857,8 @@ struct Corrector {
 struct hero_oracle_run_s {
     Params p;
     Reads Q;
+    std::vector<std::string> qrc;
+    std::string aln;  // the .aln file (alignment output)
     std::vector<uint64_t> qoff;
     std::vector<uint32_t> votes;
     std::vector<uint32_t> subj_of_kept;
@@ -834,6 +896,7 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
     p.mis_rate = pp->mis_rate;
     p.indel_rate = pp->indel_rate;
     p.thr = pp->consensus_thr;
+    p.aln = pp->aln_mode != 0;
 
     load(run->Q, nq, qseq, qoff, quid);
     Reads S;
@@ -857,6 +920,11 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
     std::vector<Outputs> outs(nt);
     std::vector<std::vector<uint32_t>> subj_ids(nt);
     Corrector cor(p, run->Q, S, T, &run->votes, run->qoff);
+    if (p.aln) {  // QueryRead::setSequence (QueryRead.cpp:36-43) without -c
+        run->qrc.resize(nq);
+        for (uint64_t i = 0; i < nq; i++) run->qrc[i] = revcomp(run->Q.seq[i]);
+        cor.qrc = &run->qrc;
+    }
 #pragma omp parallel num_threads(nt)
     {
         int t = 0;
@@ -887,6 +955,13 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
         a.records_kept += c.records_kept;
         a.dp_segments += c.dp_segments;
         a.dp_cells += c.dp_cells;
+    }
+    if (p.aln) {  // SubjectReadAligner::writeToFile (SubjectReadAligner.cpp:854-906): subject order
+        std::vector<std::pair<uint32_t, std::pair<int, size_t>>> ao;
+        for (int t = 0; t < nt; t++)
+            for (size_t i = 0; i < outs[t].aln.size(); i++) ao.push_back({outs[t].aln[i].first, {t, i}});
+        std::sort(ao.begin(), ao.end());
+        for (auto &a : ao) run->aln += outs[a.second.first].aln[a.second.second].second;
     }
     std::stable_sort(order.begin(), order.end(), [&](const auto &a, const auto &b) {
         if (a.first != b.first) return a.first < b.first;
@@ -982,6 +1057,12 @@ extern "C" void hero_oracle_consensus(const hero_oracle_run *r, uint8_t *seq_out
         if (gc) gc[q] = r->gc[q];
         if (good) good[q] = r->Q.good[q];
     }
+}
+
+extern "C" uint64_t hero_oracle_aln_size(const hero_oracle_run *r) { return r->aln.size(); }
+
+extern "C" void hero_oracle_aln(const hero_oracle_run *r, uint8_t *out) {
+    std::memcpy(out, r->aln.data(), r->aln.size());
 }
 
 extern "C" void hero_oracle_votes(const hero_oracle_run *r, uint32_t *cov) {

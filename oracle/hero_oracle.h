@@ -2,9 +2,10 @@
  * hero_oracle.h -- TEST INFRASTRUCTURE ONLY.
  *
  * CPU restatement of the HERO read-correction path (guo-xuan/Hero, consensus
- * mode `-c`).  Only the test suite, the smoke check and the benchmark's CPU
- * baseline use it, and only as the checker: the product path never links or
- * calls anything in oracle/.
+ * mode `-c`, and the alignment-output mode that writes the .aln file).  Only
+ * the test suite, the smoke check and the benchmark's CPU baseline use it, and
+ * only as the checker: the product path never links or calls anything in
+ * oracle/.
  *
  * Parity pin: the restatement is checked byte-for-byte against the reference
  * itself (oracle/_ref/hero_ref, built from the reference sources by
@@ -27,6 +28,7 @@ typedef struct {
     double mis_rate;        /* Config::dMaxMismatchRate = atof(-m)/100 (default 1) */
     double indel_rate;      /* Config::dMaxIndelRate = atof(-i)/100 (default 1) */
     double consensus_thr;   /* Config::dMinFrequencyCallConsensus (default 0.6) */
+    int32_t aln_mode;       /* 1 = alignment output (no -c): the .aln file, no votes */
 } hero_oracle_params;
 
 typedef struct {
@@ -64,6 +66,13 @@ void hero_oracle_stats_get(const hero_oracle_run *r, hero_oracle_stats *out);
 void hero_oracle_consensus(const hero_oracle_run *r, uint8_t *seq_out, uint32_t *imin,
                            uint32_t *imed, uint32_t *imax, double *mismatch_rate,
                            double *gc, uint8_t *good);
+
+/* The .aln file of the alignment-output mode (aln_mode = 1): per subject read,
+ * ">id\n", its records as "query,orientation,position,CIGAR,inserted bases,",
+ * then "\n" (SubjectReadAligner::writeToFile, SubjectRead::writeAlignment,
+ * AlignmentRecord::getCigar). */
+uint64_t hero_oracle_aln_size(const hero_oracle_run *r);
+void hero_oracle_aln(const hero_oracle_run *r, uint8_t *out);
 
 /* Vote matrix after every subject's votes and before the self vote:
  * uint32 [total query bases][4], column index (c>>1)&3 (A,C,T,G). */

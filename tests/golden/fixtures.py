@@ -58,6 +58,18 @@ def upper(rs: synth.ReadSet) -> synth.ReadSet:
     return synth.ReadSet(seq, rs.off, rs.names, rs.qual, dict(rs.meta))
 
 
+def aln_flags(flags: list[str]) -> list[str]:
+    """The flags of the alignment-output mode: the consensus threshold (-c x) dropped."""
+    out, i = [], 0
+    while i < len(flags):
+        if flags[i] == "-c":
+            i += 2
+            continue
+        out += flags[i:i + 2]
+        i += 2
+    return out
+
+
 def params(flags: list[str]) -> dict:
     """Reference flags -> keyword arguments of hero_b200.Hero (Config::setConfig)."""
     p = dict(k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,

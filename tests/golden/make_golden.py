@@ -2,8 +2,9 @@
 
 Runs the unmodified reference (oracle/_ref/hero_ref, built from the reference
 sources by oracle/Makefile) on every fixture input and records md5 sums of the
-input FASTQ and of the reference .fasta/.info; the outputs of the fixtures in
-STORED are kept gzipped.  Usage:  python tests/golden/make_golden.py
+input FASTQ, of the reference .fasta/.info (consensus mode, -c) and of its .aln
+(alignment-output mode: the same flags without -c); the .fasta/.info of the
+fixtures in STORED are kept gzipped.  Usage:  python tests/golden/make_golden.py
 
     python tests/golden/make_golden.py --full NAME...
 
@@ -23,7 +24,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from fixtures import FIXTURES, STORED  # noqa: E402
+from fixtures import FIXTURES, STORED, aln_flags  # noqa: E402
 
 from hero_b200 import synth  # noqa: E402
 
@@ -57,6 +58,17 @@ def run_reference(fq: str, flags: list[str], workdir: str) -> tuple[bytes, bytes
     with open(out + ".info", "rb") as f:
         info = f.read()
     return fa, info
+
+
+def run_reference_aln(fq: str, flags: list[str], workdir: str) -> bytes:
+    """The .aln of the alignment-output mode (no -c; SubjectReadAligner::writeToFile)."""
+    out = os.path.join(workdir, "aln")
+    if os.path.exists(out + ".aln"):  # opened in append mode
+        os.remove(out + ".aln")
+    subprocess.run([REF, "-q", fq, "-s", fq, "--singleReads", "-t", str(os.cpu_count() or 1),
+                    "-o", out] + aln_flags(flags), stdout=subprocess.DEVNULL, check=True)
+    with open(out + ".aln", "rb") as f:
+        return f.read()
 
 
 def main_full(names: list[str]):
@@ -95,8 +107,10 @@ def main():
             with open(fq, "wb") as f:
                 f.write(fqb)
             fa, info = run_reference(fq, flags, d)
+            aln = run_reference_aln(fq, flags, d)
             manifest[name] = dict(flags=flags, reads=rs.n, fastq_md5=md5(fqb),
-                                  fasta_md5=md5(fa), info_md5=md5(info))
+                                  fasta_md5=md5(fa), info_md5=md5(info), aln_md5=md5(aln),
+                                  aln_bytes=len(aln))
             if name in STORED:
                 for ext, data in ((".fasta.gz", fa), (".info.gz", info)):
                     with gzip.GzipFile(os.path.join(HERE, name + ext), "wb", mtime=0) as g:

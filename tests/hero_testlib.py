@@ -41,7 +41,8 @@ def build_emu():
 class OracleParams(C.Structure):
     _fields_ = [("k", C.c_int32), ("min_overlap", C.c_int32), ("affine", C.c_int32),
                 ("keep_segments", C.c_int32), ("mis_rate", C.c_double),
-                ("indel_rate", C.c_double), ("consensus_thr", C.c_double)]
+                ("indel_rate", C.c_double), ("consensus_thr", C.c_double),
+                ("aln_mode", C.c_int32)]
 
 
 class OracleStats(C.Structure):
@@ -76,15 +77,19 @@ class Oracle:
         lib.hero_oracle_align.argtypes = [C.c_int, vp, C.c_int32, vp, C.c_int32, C.c_int64,
                                           C.c_int, C.c_int, vp, C.c_int32, C.POINTER(C.c_int64)]
         lib.hero_oracle_quality_filter.argtypes = [vp, C.c_uint64]
+        lib.hero_oracle_aln_size.argtypes = [vp]
+        lib.hero_oracle_aln_size.restype = C.c_uint64
+        lib.hero_oracle_aln.argtypes = [vp, vp]
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
                 max_mismatch_rate=1.0, max_indel_rate=1.0, consensus_threshold=0.6,
-                keep_segments=False, threads=8):
+                keep_segments=False, threads=8, aln=False):
+        """aln=True: the alignment-output mode (no -c); res["aln"] holds the .aln bytes."""
         subj = subjects if subjects is not None else reads
         p = OracleParams(k, min_overlap, 1 if aligner in ("a", "affine") else 0,
                          1 if keep_segments else 0, max_mismatch_rate, max_indel_rate,
-                         consensus_threshold)
+                         consensus_threshold, 1 if aln else 0)
         qs, qo, qu = reads.seq, reads.off.astype(np.uint64), reads.names.astype(np.int64)
         ss, so, su = subj.seq, subj.off.astype(np.uint64), subj.names.astype(np.int64)
         h = self.lib.hero_oracle_correct(C.byref(p), threads, reads.n, _vp(qs), _vp(qo), _vp(qu),
@@ -101,6 +106,10 @@ class Oracle:
             cov = np.zeros(nb * 4, np.uint32)
             self.lib.hero_oracle_votes(h, _vp(cov))
             res["votes"] = cov
+            if aln:
+                buf = np.zeros(max(1, self.lib.hero_oracle_aln_size(h)), np.uint8)
+                self.lib.hero_oracle_aln(h, _vp(buf))
+                res["aln"] = buf[:self.lib.hero_oracle_aln_size(h)].tobytes()
             st = OracleStats()
             self.lib.hero_oracle_stats_get(h, C.byref(st))
             res["stats"] = {f: getattr(st, f) for f, _ in st._fields_}

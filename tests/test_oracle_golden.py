@@ -5,7 +5,7 @@ import json
 import os
 
 import pytest
-from fixtures import FIXTURES, STORED, params, upper
+from fixtures import FIXTURES, STORED, aln_flags, params, upper
 from hero_testlib import format_outputs
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -31,6 +31,18 @@ def test_oracle_matches_reference(oracle, name):
         assert info == gzip.open(os.path.join(HERE, name + ".info.gz")).read()
     assert md5(fa) == m["fasta_md5"]
     assert md5(info) == m["info_md5"]
+
+
+@pytest.mark.parametrize("name", sorted(FIXTURES))
+def test_oracle_alignment_output_matches_reference(oracle, name):
+    """Alignment-output mode (no -c): the .aln bytes of the reference."""
+    gen, flags = FIXTURES[name]
+    m = MANIFEST[name]
+    kw = params(aln_flags(flags))
+    kw.pop("consensus_threshold")
+    r = oracle.correct(upper(gen()), aln=True, **kw)
+    assert len(r["aln"]) == m["aln_bytes"]
+    assert md5(r["aln"]) == m["aln_md5"]
 
 
 def test_quality_filter(oracle):
