@@ -9,6 +9,8 @@ record selection, consensus) behind a C ABI (include/hero_gpu.h).
         h.align_self()
         out = h.consensus()
 """
-from ._lib import EXPORTS, Hero, HeroError, HeroServer, correct, load_library  # noqa: F401
+from ._lib import (EXPORTS, Hero, HeroError, HeroServer, align_output, correct,  # noqa: F401
+                   load_library)
 
-__all__ = ["Hero", "HeroError", "HeroServer", "correct", "load_library", "EXPORTS"]
+__all__ = ["Hero", "HeroError", "HeroServer", "align_output", "correct", "load_library",
+           "EXPORTS"]

@@ -28,8 +28,11 @@ EXPORTS = [
     "hero_set_query_jobs", "hero_server_create", "hero_server_destroy", "hero_job_submit",
     "hero_job_poll", "hero_job_wait", "hero_job_result", "hero_job_error", "hero_job_release",
     "hero_server_get_stats", "hero_job_bytes", "hero_round_admit", "hero_set_dp_tuning",
-    "hero_server_set_dp_tuning",
+    "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
 ]
+
+# hero_params.flags: the alignment-output mode (HERO without -c)
+FLAG_ALIGNMENT_OUTPUT = 1
 
 # the autotuner's record (hero_b200.autotune); loaded by every Hero unless told otherwise
 TUNING_PATH = os.path.join(HERE, "tuning.json")
@@ -121,6 +124,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_fetch.argtypes = [vp] * 8
     lib.hero_consensus.argtypes = [vp] * 8
     lib.hero_get_votes.argtypes = [vp, vp]
+    lib.hero_alignments_size.argtypes = [vp, C.POINTER(C.c_uint64)]
+    lib.hero_alignments_take.argtypes = [vp, vp, C.c_uint64]
     lib.hero_get_stats.argtypes = [vp, C.POINTER(HeroStats)]
     lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          C.c_uint64] + [vp] * 12)
@@ -174,7 +179,9 @@ class Hero:
                  max_mismatch_rate: float = 1.0, max_indel_rate: float = 1.0,
                  consensus_threshold: float = 0.6, device: int = 0, subject_batch: int = 0,
                  device_memory_budget: int = 0, stream: int | None = None,
-                 tuning: list[dict] | str | None = None):
+                 tuning: list[dict] | str | None = None, alignment_output: bool = False):
+        """alignment_output=True: HERO without -c -- the .aln records of every
+        subject (alignments()) instead of votes and a consensus."""
         self.lib = load_library()
         p = HeroParams()
         self.lib.hero_default_params(C.byref(p))
@@ -188,6 +195,7 @@ class Hero:
         p.subject_batch = subject_batch
         p.device_memory_budget = device_memory_budget
         p.stream = stream
+        p.flags = FLAG_ALIGNMENT_OUTPUT if alignment_output else 0
         self.params = p
         h = C.c_void_p()
         rc = self.lib.hero_create(C.byref(p), C.byref(h))
@@ -304,6 +312,14 @@ class Hero:
             self.h, _ptr(res["seq"]), _ptr(res["imin"]), _ptr(res["imed"]), _ptr(res["imax"]),
             _ptr(res["mismatch_rate"]), _ptr(res["gc"]), _ptr(res["good"])), "consensus")
         return res
+
+    def alignments(self) -> bytes:
+        """The .aln text of every subject aligned since the last call (and drops it)."""
+        n = C.c_uint64()
+        self._check(self.lib.hero_alignments_size(self.h, C.byref(n)), "alignments")
+        buf = np.empty(max(1, n.value), np.uint8)
+        self._check(self.lib.hero_alignments_take(self.h, _ptr(buf), n.value), "alignments")
+        return buf[:n.value].tobytes()
 
     def votes(self):
         cov = np.empty(self.nqb * 4, np.uint32)
@@ -441,3 +457,12 @@ def correct(reads, **kw):
         res = h.consensus()
         res["stats"] = h.stats()
         return res
+
+
+def align_output(reads, **kw) -> bytes:
+    """The .aln file of HERO run without -c (-q X -s X): every read's records."""
+    with Hero(alignment_output=True, **kw) as h:
+        h.set_queries(reads.seq, reads.off, reads.names)
+        h.build_index()
+        h.align_self()
+        return h.alignments()

@@ -62,6 +62,9 @@ struct hero_ctx {
     DBuf keys, segs, sums, cells, ops, perm, bins, bin_off, tb, bnd, dp_tasks, winners;
     DBuf win_sorted, win_bins;  // winners sorted by chain shape, and the sort's bins
     DBuf scan_tmp, counters;
+    // alignment output: record lists, text units and the batch's text
+    DBuf a_list, a_n, a_roff, a_unit, a_len, a_pre, a_cig, a_uoff, a_text;
+    std::vector<uint8_t> aln_host;  // .aln text of every subject aligned since the last take
     // index build temporaries (kept between builds)
     DBuf x_cnt, x_koff, x_klo, x_khi, x_kval, x_owner, x_count, x_slot_of, x_start, x_fill, x_tmp;
     uint64_t dp_T = 0;
@@ -95,7 +98,8 @@ struct hero_ctx {
                         &ch_win, &ch_rate, &ch_len, &keys, &segs, &sums, &cells, &ops, &perm,
                         &bins, &bin_off, &tb, &bnd, &dp_tasks, &winners, &scan_tmp, &counters, &x_cnt, &x_koff,
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
-                        &x_fill, &x_tmp, &q_job, &win_sorted, &win_bins};
+                        &x_fill, &x_tmp, &q_job, &win_sorted, &win_bins, &a_list, &a_n,
+                        &a_roff, &a_unit, &a_len, &a_pre, &a_cig, &a_uoff, &a_text};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -208,6 +212,7 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
     if (!p || !out) return HERO_E_INPUT;
     *out = nullptr;
     if (p->k < 1 || p->k > 63) return HERO_E_INPUT;
+    if (p->flags & ~HERO_FLAG_ALIGNMENT_OUTPUT) return HERO_E_INPUT;
     hero_ctx *c = new hero_ctx();
     c->P = *p;
     c->p.k = p->k;
@@ -216,6 +221,7 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
     c->p.mis_rate = p->max_mismatch_rate;
     c->p.indel_rate = p->max_indel_rate;
     c->p.thr = p->consensus_threshold;
+    c->p.aln = (p->flags & HERO_FLAG_ALIGNMENT_OUTPUT) ? 1 : 0;
     c->dev = p->device;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -451,6 +457,55 @@ extern "C" int hero_build_index(hero_ctx *c) {
     return r;
 }
 
+// Alignment output of one batch (after the records are scored): the kept
+// records per subject (SubjectRead::addAlignment by query uniqueId), the text
+// units, their sizes, a scan, the text; appended to the context's host text.
+static int aln_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, ReadsView q,
+                     const ChainArrays &ch, uint64_t NC, uint32_t stride) {
+    unsigned long long *ctr = P_<unsigned long long>(c->counters);
+    if (NC >= uint64_t(kUnitChainLimit) || nsub >= uint64_t(kUnitChainLimit))
+        return c->fail(HERO_E_INPUT, "too many chains or subjects in a batch");
+    HERO_TRY(c->ensure(c->a_list, std::max<uint64_t>(NC, 1) * 4, "alignment lists"));
+    HERO_TRY(c->ensure(c->a_n, nsub * 4 + 4, "alignment lists"));
+    HERO_TRY(c->ensure(c->a_roff, (nsub + 1) * 8, "alignment lists"));
+    launch_aln_list(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch, q,
+                    P_<uint32_t>(c->a_list), P_<uint32_t>(c->a_n), ctr, c->st);
+    launch_scan_u32(P_<uint32_t>(c->a_n), P_<uint64_t>(c->a_roff), nsub, c->scan_tmp.p, c->st);
+    HERO_TRY(c->check_launch("alignment lists"));
+    uint64_t R = 0;
+    HERO_TRY(c->cuda(cudaMemcpyAsync(&R, P_<uint64_t>(c->a_roff) + nsub, 8, cudaMemcpyDeviceToHost, c->st), "alignment lists"));
+    HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "alignment lists"));
+    const uint64_t U = R + 2 * nsub;  // units: header, records, closing newline per subject
+    HERO_TRY(c->ensure(c->a_unit, U * 4, "alignment text"));
+    HERO_TRY(c->ensure(c->a_len, U * 4, "alignment text"));
+    HERO_TRY(c->ensure(c->a_pre, U * 4, "alignment text"));
+    HERO_TRY(c->ensure(c->a_cig, U * 4, "alignment text"));
+    HERO_TRY(c->ensure(c->a_uoff, (U + 1) * 8, "alignment text"));
+    HERO_TRY(c->ensure(c->scan_tmp, scan_tmp_bytes(std::max<uint64_t>(U + 1, std::max<uint64_t>(2 * nsub + 1, kDpBins + 1))), "scan"));
+    launch_aln_units(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount),
+                     P_<uint32_t>(c->a_list), P_<uint32_t>(c->a_n), P_<uint64_t>(c->a_roff), subj,
+                     P_<uint32_t>(c->a_unit), P_<uint32_t>(c->a_len), c->st);
+    launch_aln_size(c->p, U, P_<uint32_t>(c->a_unit), ch, P_<uint32_t>(c->keys), subj, q,
+                    P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->a_len),
+                    P_<uint32_t>(c->a_pre), P_<uint32_t>(c->a_cig), c->st);
+    launch_scan_u32(P_<uint32_t>(c->a_len), P_<uint64_t>(c->a_uoff), U, c->scan_tmp.p, c->st);
+    HERO_TRY(c->check_launch("alignment text"));
+    uint64_t B = 0;
+    HERO_TRY(c->cuda(cudaMemcpyAsync(&B, P_<uint64_t>(c->a_uoff) + U, 8, cudaMemcpyDeviceToHost, c->st), "alignment text"));
+    HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "alignment text"));
+    HERO_TRY(c->ensure(c->a_text, B, "alignment text"));
+    launch_aln_write(c->p, U, P_<uint32_t>(c->a_unit), P_<uint64_t>(c->a_uoff), ch,
+                     P_<uint32_t>(c->keys), subj, q, P_<uint32_t>(c->ops), stride,
+                     P_<DpSum>(c->sums), P_<uint32_t>(c->a_pre), P_<uint32_t>(c->a_cig),
+                     P_<char>(c->a_text), c->st);
+    HERO_TRY(c->check_launch("alignment text"));
+    const size_t o = c->aln_host.size();
+    c->aln_host.resize(o + B);
+    if (B)
+        HERO_TRY(c->cuda(cudaMemcpyAsync(c->aln_host.data() + o, c->a_text.p, B, cudaMemcpyDeviceToHost, c->st), "alignment text"));
+    return c->cuda(cudaStreamSynchronize(c->st), "alignment text");
+}
+
 // runs every stage for subjects [0, nsub) of the given reads
 static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6]) {
     const uint64_t nseg = 2 * nsub;
@@ -476,7 +531,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         if ((r = c->cuda(cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st), "batch: counters"))) break;
         static_assert(C_WIN == C_OVERFLOW + 1, "overflow flag and winner count are cleared together");
         if ((r = c->cuda(cudaMemsetAsync(ctr + C_OVERFLOW, 0, 2 * sizeof(unsigned long long), c->st), "batch: counters"))) break;
-        launch_probe(false, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
+        launch_probe(false, c->p.aln != 0, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
         launch_scan_u32(P_<uint32_t>(c->seg_hits), P_<uint64_t>(c->hit_off), nseg, c->scan_tmp.p, c->st);
         uint64_t H = 0;
         if (cap) {
@@ -488,7 +543,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         }
         const uint64_t Hc = std::max<uint64_t>(H, 1);
         if ((r = c->ensure(c->hits, Hc * 8, "hits"))) break;
-        launch_probe(true, subj, nsub, q, t, c->p.k, nullptr, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), ctr, c->st);
+        launch_probe(true, c->p.aln != 0, subj, nsub, q, t, c->p.k, nullptr, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), ctr, c->st);
         launch_sort_hits(nseg, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), c->st);
         if ((r = c->check_launch("seed"))) break;
         rec(1);
@@ -566,16 +621,21 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         if (cap) launch_stamp(P_<unsigned long long>(c->stamps) + 2 * c->batch_idx + 1, c->st);
         launch_assemble(c->p, NC, ch, P_<uint32_t>(c->keys), subj, q, P_<DpSum>(c->sums),
                         P_<uint32_t>(c->cells), ctr, c->st);
-        if ((r = c->ensure(c->winners, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
-        if ((r = c->ensure(c->win_sorted, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
-        if ((r = c->ensure(c->win_bins, kWinScratch * 4, "winners"))) break;
-        launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
-                      P_<uint32_t>(c->winners), ctr, c->st);
-        rec(5);
-        launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->win_sorted),
-                    P_<uint32_t>(c->win_bins), P_<uint32_t>(c->keys), subj, q,
-                    P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov),
-                    P_<int32_t>(c->mdiff), ctr, c->st);
+        if (c->p.aln) {
+            rec(5);
+            if ((r = aln_batch(c, subj, nsub, q, ch, NC, stride))) break;
+        } else {
+            if ((r = c->ensure(c->winners, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
+            if ((r = c->ensure(c->win_sorted, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
+            if ((r = c->ensure(c->win_bins, kWinScratch * 4, "winners"))) break;
+            launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
+                          P_<uint32_t>(c->winners), ctr, c->st);
+            rec(5);
+            launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->win_sorted),
+                        P_<uint32_t>(c->win_bins), P_<uint32_t>(c->keys), subj, q,
+                        P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov),
+                        P_<int32_t>(c->mdiff), ctr, c->st);
+        }
         if ((r = c->check_launch("record/vote"))) break;
         if (cap) break;
         rec(6);
@@ -661,6 +721,7 @@ extern "C" int hero_consensus(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uin
                               uint8_t *good_out) {
     if (!c) return HERO_E_INPUT;
     if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (c->p.aln) return c->fail(HERO_E_STATE, "an alignment-output context has no consensus");
     cudaSetDevice(c->dev);
     const uint64_t n = c->nq, nb = c->nqb;
     cudaEvent_t e0, e1;
@@ -735,6 +796,7 @@ static int round_body(hero_ctx *c) {
 extern "C" int hero_round(hero_ctx *c, uint32_t flags) {
     if (!c) return HERO_E_INPUT;
     if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (c->p.aln) return c->fail(HERO_E_STATE, "rounds are correction rounds (consensus mode)");
     cudaSetDevice(c->dev);
     const bool graph = (flags & HERO_ROUND_GRAPH) != 0;
     if (graph && c->gexec && c->plan_ok && c->plan_fp == c->qfp) {
@@ -792,6 +854,23 @@ extern "C" int hero_fetch(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uint32_
     if (gc_content && n) cudaMemcpyAsync(gc_content, c->q_gc.p, n * 8, cudaMemcpyDeviceToHost, c->st);
     if (good_out && n) cudaMemcpyAsync(good_out, c->q_good.p, n, cudaMemcpyDeviceToHost, c->st);
     return c->cuda(cudaStreamSynchronize(c->st), "fetch");
+}
+
+extern "C" int hero_alignments_size(hero_ctx *c, uint64_t *bytes) {
+    if (!c || !bytes) return HERO_E_INPUT;
+    if (!c->p.aln) return c->fail(HERO_E_STATE, "not an alignment-output context");
+    *bytes = c->aln_host.size();
+    return HERO_OK;
+}
+
+extern "C" int hero_alignments_take(hero_ctx *c, uint8_t *out, uint64_t cap) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->p.aln) return c->fail(HERO_E_STATE, "not an alignment-output context");
+    const uint64_t n = c->aln_host.size();
+    if (cap < n || (n && !out)) return c->fail(HERO_E_INPUT, "output buffer too small");
+    if (n) std::memcpy(out, c->aln_host.data(), n);
+    std::vector<uint8_t>().swap(c->aln_host);
+    return HERO_OK;
 }
 
 extern "C" int hero_get_votes(hero_ctx *c, uint32_t *cov) {

@@ -59,7 +59,7 @@ struct Params {
     int32_t k;          // Config::iKmer
     int32_t l;          // Config::minimumOverlapLength
     int32_t affine;     // Config::iAlignerType == IAFFINE
-    int32_t pad;
+    int32_t aln;        // !Config::bCallConsensus: alignment output (the .aln file)
     double mis_rate;    // Config::dMaxMismatchRate
     double indel_rate;  // Config::dMaxIndelRate
     double thr;         // Config::dMinFrequencyCallConsensus
@@ -141,6 +141,18 @@ HERO_HD uint64_t hit_pack(uint32_t q, uint32_t posQ, uint32_t posS) {
     return (uint64_t(q) << 32) | (uint64_t(posQ) << 16) | uint64_t(posS);
 }
 HERO_HD uint32_t hit_q(uint64_t h) { return uint32_t(h >> 32); }
+
+// A hit of subject window f (forward) against query position posQ, found in
+// pass o (0 forward, 1 reverse complement) of a subject of length Ls.  With -c
+// the reverse pass keeps positions on the reverse-complemented subject; the
+// alignment-output mode flips them onto the forward subject and the query's
+// reverse complement (SubjectReadAligner.cpp:477-481).
+HERO_HD uint64_t seed_hit(bool aln, int o, uint32_t q, uint32_t posQ, int32_t f, int32_t Ls,
+                          int32_t Lq, int32_t k) {
+    if (o == 0) return hit_pack(q, posQ, uint32_t(f));
+    if (aln) return hit_pack(q, uint32_t(Lq - (int32_t(posQ) + k)), uint32_t(f));
+    return hit_pack(q, posQ, uint32_t(Ls - k - f));
+}
 HERO_HD int32_t hit_posQ(uint64_t h) { return int32_t((h >> 16) & 0xffff); }
 HERO_HD int32_t hit_posS(uint64_t h) { return int32_t(h & 0xffff); }
 
@@ -451,6 +463,153 @@ HERO_HD bool record_better(double rs_new, double len_new, double rs_cur, double 
     return true;
 }
 
+// SubjectRead::addAlignment (SubjectRead.cpp:25-79) as the list it keeps, for
+// the alignment output, where the order of the list is the order of the .aln
+// records.  Records are ids; key(id) is iQueryReadUniqueId (UINT64: the
+// query's atoi(name)); better(a, b) is record_better of a over b.  A record
+// equal in key to the last one competes with it; otherwise, if its key is not
+// above the largest key seen, the list is scanned up to the first larger key
+// for an equal one (which it may replace) and else appended; a key above the
+// largest is appended.  list.get(i) / list.set(i, id) address slot i.
+// Returns the new length.
+template <class List, class Key, class Better>
+HERO_HD uint32_t list_add(List &list, uint32_t n, uint64_t &largest, uint32_t id, const Key &key,
+                          const Better &better) {
+    const uint64_t k = key(id);
+    if (n == 0) {
+        largest = k;
+        list.set(0, id);
+        return 1;
+    }
+    const uint32_t last = list.get(n - 1);
+    if (key(last) == k) {
+        if (better(id, last)) list.set(n - 1, id);
+        return n;
+    }
+    if (largest >= k) {
+        for (uint32_t i = 0; i < n; i++) {
+            const uint32_t e = list.get(i);
+            const uint64_t ke = key(e);
+            if (ke > k) break;
+            if (ke == k) {
+                if (better(id, e)) list.set(i, id);
+                return n;
+            }
+        }
+        list.set(n, id);
+        return n + 1;
+    }
+    largest = k;
+    list.set(n, id);
+    return n + 1;
+}
+
+// decimal text of integers, as ostream prints them
+HERO_HD uint32_t dec_len(uint64_t v) {
+    uint32_t n = 1;
+    while (v >= 10) {
+        v /= 10;
+        n++;
+    }
+    return n;
+}
+HERO_HD uint32_t dec_len_signed(int64_t v) {
+    return v < 0 ? 1u + dec_len(uint64_t(0) - uint64_t(v)) : dec_len(uint64_t(v));
+}
+HERO_HD char *dec_put(char *o, uint64_t v) {
+    const uint32_t n = dec_len(v);
+    for (uint32_t i = n; i > 0; i--) {
+        o[i - 1] = char('0' + v % 10);
+        v /= 10;
+    }
+    return o + n;
+}
+HERO_HD char *dec_put_signed(char *o, int64_t v) {
+    if (v < 0) {
+        *o++ = '-';
+        return dec_put(o, uint64_t(0) - uint64_t(v));
+    }
+    return dec_put(o, uint64_t(v));
+}
+
+// Text of one alignment record, AlignmentRecord::getCigar (AlignmentRecord.cpp:
+// 102-149) with storeOverhang off:  "id,orientation,position,CIGAR,inserted,".
+// The CIGAR is the run-length form of the per-base types -- M, I, D, or the
+// query's base at a mismatch (BandAligner.cpp:258-419) -- because
+// AlignmentRecord::addCigar (AlignmentRecord.cpp:35-48) merges every equal
+// neighbour, whichever piece it came from.  "inserted" holds the query bases
+// of every I entry except the first and the last entry.  Driven by walk_chain
+// through a piece source: src.each(piece, f) calls f(op) for the ops of DP
+// piece `piece` in order.  Count mode (cig == nullptr) only sizes the text.
+template <class Src>
+struct AlnText {
+    Src src;
+    const uint8_t *qc;  // query codes, forward
+    int32_t Lq;
+    bool qrc;           // the query's reverse complement is aligned
+    char *cig = nullptr, *ins = nullptr;  // write cursors (write mode)
+    uint32_t cig_len = 0, ins_len = 0;
+    uint32_t entries = 0, piece = 0;
+    char t = 0;
+    int64_t c = 0, q0 = 0, pq = 0;
+    int64_t pos = 0;  // iPositionOfQueryOnSubject
+
+    // the query's base letter at i (a position past the read, which only a record
+    // that also votes past the read could reach, reads as N)
+    HERO_HD char qbase(int64_t i) const {
+        if (i < 0 || i >= Lq) return 'N';
+        return code_base(qrc ? uint8_t((qc[Lq - 1 - i] ^ 2u) & 3u) : uint8_t(qc[i] & 3u));
+    }
+    HERO_HD void flush(bool last) {
+        cig_len += dec_len(uint64_t(c)) + 1u;
+        if (cig) {
+            cig = dec_put(cig, uint64_t(c));
+            *cig++ = t;
+        }
+        if (t == 'I' && entries != 1u && !last) {
+            ins_len += uint32_t(c);
+            if (ins)
+                for (int64_t i = 0; i < c; i++) *ins++ = qbase(q0 + i);
+        }
+    }
+    HERO_HD void add(char type, int64_t n) {  // AlignmentRecord::addCigar
+        if (entries && type == t) {
+            c += n;
+        } else {
+            if (entries) flush(false);
+            t = type;
+            c = n;
+            q0 = pq;
+            entries++;
+        }
+        if (type != 'D') pq += n;
+    }
+    HERO_HD void op(uint8_t o) {
+        if (o == OP_M) {
+            add('M', 1);
+        } else if (o == OP_X) {
+            add(qbase(pq), 1);
+        } else {
+            add(o == OP_I ? 'I' : 'D', 1);
+        }
+    }
+    HERO_HD void begin(int64_t, int64_t, int64_t) {}
+    HERO_HD void position(int64_t p) { pos = p; }
+    HERO_HD void run(uint8_t o, int64_t n) { add(o == OP_M ? 'M' : o == OP_I ? 'I' : 'D', n); }
+    HERO_HD void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
+        src.each(piece++, [this](uint8_t o) { op(o); });
+    }
+    HERO_HD bool check(int64_t, int64_t) { return true; }
+    HERO_HD void finish() {
+        if (entries) flush(true);  // the open entry is the last one
+    }
+};
+
+// length of a record's "id,orientation,position," prefix
+HERO_HD uint32_t aln_prefix_len(uint64_t key, uint32_t orient, int64_t pos) {
+    return dec_len(key) + 1u + dec_len(orient) + 1u + dec_len_signed(pos) + 1u;
+}
+
 // ---------------------------------------------------------------------------
 // banded DP: BandAligner::bandedAlign / bandedAlignAffineGap (BandAligner.cpp:56-239)
 //
@@ -476,10 +635,12 @@ struct SegView {  // a DP segment after setSequences (rows = longer side)
 };
 
 // builds the view of segment [s0,s1) of the subject (orientation rc when
-// orient=1) against [q0,q1) of the query, as BandAligner::setSequences does
+// orient=1) against [q0,q1) of the query (of the query's reverse complement
+// when qrc, for the alignment output's reverse pass; Lq = query length), as
+// BandAligner::setSequences does
 HERO_HD SegView make_view(const uint8_t *subj, int32_t Ls, int32_t orient, const uint8_t *qry,
                           int32_t s0, int32_t s1, int32_t q0, int32_t q1, uint32_t flags,
-                          int64_t band_in) {
+                          int64_t band_in, int32_t Lq = 0, bool qrc = false) {
     SegView v;
     const uint8_t *sb;
     int32_t sdir;
@@ -493,21 +654,24 @@ HERO_HD SegView make_view(const uint8_t *subj, int32_t Ls, int32_t orient, const
         sdir = 1;
         sx = 0;
     }
+    const uint8_t *qb = qrc ? qry + (Lq - 1 - q0) : qry + q0;
+    const int32_t qdir = qrc ? -1 : 1;
+    const uint8_t qx = qrc ? 2 : 0;
     const int32_t ls = s1 - s0, lq = q1 - q0;
     if (lq <= ls) {
         v.row_base = sb;
         v.row_dir = sdir;
         v.row_xor = sx;
-        v.col_base = qry + q0;
-        v.col_dir = 1;
-        v.col_xor = 0;
+        v.col_base = qb;
+        v.col_dir = qdir;
+        v.col_xor = qx;
         v.R = ls;
         v.C = lq;
         v.reversed = false;
     } else {
-        v.row_base = qry + q0;
-        v.row_dir = 1;
-        v.row_xor = 0;
+        v.row_base = qb;
+        v.row_dir = qdir;
+        v.row_xor = qx;
         v.col_base = sb;
         v.col_dir = sdir;
         v.col_xor = sx;

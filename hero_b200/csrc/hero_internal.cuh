@@ -22,10 +22,23 @@ struct __align__(16) DpSeg {
     uint16_t s0, s1;  // subject range, subject orientation coordinates
     uint16_t q0, q1;  // query range
     int32_t band;     // band held by the aligner before the call
-    uint32_t flags;   // DPF_RIGHT | DPF_LEFT | orient << 2
+    uint32_t flags;   // DPF_RIGHT | DPF_LEFT | orient << 2 (subject reverse complement)
+                      // | qrc << 3 (query reverse complement: alignment output)
     uint32_t pad;
 };
 constexpr uint32_t kSegOrientShift = 2;
+constexpr uint32_t kSegQrcShift = 3;
+
+// the BandAligner view of a DP segment; qoff has n+1 entries
+HERO_HD SegView dpseg_view(const DpSeg &g, const uint8_t *scode, const uint64_t *soff,
+                           const uint32_t *slen, const uint8_t *qcode, const uint64_t *qoff) {
+    const uint32_t orient = (g.flags >> kSegOrientShift) & 1u;
+    const bool qrc = ((g.flags >> kSegQrcShift) & 1u) != 0;
+    const uint64_t qo = qoff[g.query];
+    const int32_t Lq = qrc ? int32_t(qoff[g.query + 1] - qo) : 0;
+    return make_view(scode + soff[g.subj], int32_t(slen[g.subj]), int32_t(orient), qcode + qo,
+                     g.s0, g.s1, g.q0, g.q1, g.flags & 3u, g.band, Lq, qrc);
+}
 
 // reads resident on the device (queries, or one batch of subjects)
 struct ReadsView {
@@ -111,7 +124,8 @@ void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint3
                            const uint32_t *count, const uint64_t *start, uint64_t nslots,
                            Slot *slots, cudaStream_t st);
 
-void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
+// aln: the alignment output's positions (seed_hit)
+void launch_probe(bool emit, bool aln, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
                   uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
                   unsigned long long *counters, cudaStream_t st);
 void launch_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits, cudaStream_t st);
@@ -174,6 +188,27 @@ void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
 // votes the query's own base, recorded as +1/-1 at the run's ends in mdiff
 // (a per-read difference array, summed by the consensus).
 constexpr uint32_t kWinScratch = 3 * 512;  // uint32 bins, offsets and cursors of the winner sort
+constexpr uint32_t kUnitSubject = 0x80000000u;  // header unit: kUnitSubject | subject
+constexpr uint32_t kUnitEnd = 0xffffffffu;      // closing newline of a subject
+constexpr uint32_t kUnitChainLimit = kUnitSubject;  // chains and subjects of a batch stay below
+// alignment output (HERO without -c): per subject the list of kept records
+// (alist: slots in the subject's chain ranges, alist_n: lengths), then the .aln
+// text in units (unit: kUnitSubject | subject, a chain index, or the closing
+// newline; sizes ulen, prefix and CIGAR lengths upre / ucig; offsets uoff)
+void launch_aln_list(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
+                     ChainArrays ch, ReadsView q, uint32_t *alist, uint32_t *alist_n,
+                     unsigned long long *counters, cudaStream_t st);
+void launch_aln_units(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
+                      const uint32_t *alist, const uint32_t *alist_n, const uint64_t *rec_off,
+                      ReadsView subj, uint32_t *unit, uint32_t *ulen, cudaStream_t st);
+void launch_aln_size(const Params &p, uint64_t nunit, const uint32_t *unit, ChainArrays ch,
+                     const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
+                     uint32_t stride, const DpSum *sums, uint32_t *ulen, uint32_t *upre,
+                     uint32_t *ucig, cudaStream_t st);
+void launch_aln_write(const Params &p, uint64_t nunit, const uint32_t *unit, const uint64_t *uoff,
+                      ChainArrays ch, const uint32_t *keys, ReadsView subj, ReadsView q,
+                      const uint32_t *ops, uint32_t stride, const DpSum *sums,
+                      const uint32_t *upre, const uint32_t *ucig, char *text, cudaStream_t st);
 void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,
                  uint32_t *sorted, uint32_t *win_bins, const uint32_t *keys, ReadsView subj,
                  ReadsView q, const uint32_t *ops, uint32_t stride, const DpSum *sums,

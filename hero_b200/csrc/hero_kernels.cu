@@ -307,7 +307,7 @@ constexpr int kProbeWarps = 8;
 
 template <bool EMIT>
 __global__ void __launch_bounds__(kProbeWarps * 32)
-    k_probe(ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
+    k_probe(ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k, bool aln,
             uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
             unsigned long long *counters) {
     __shared__ uint32_t fill[kProbeWarps][2];
@@ -359,14 +359,15 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
                 for (int o = 0; o < 2; o++) {
                     uint32_t st = 0, cnt = 0;
                     if (!table_find(t, o ? rm : fm, st, cnt)) continue;
-                    const uint32_t posS = o ? uint32_t(L - k - f) : uint32_t(f);
                     for (uint32_t e = 0; e < cnt; e++) {
                         const uint64_t v = __ldg(&t.vals[st + e]);
                         const uint32_t qq = uint32_t(v >> 32);
                         if (__ldg(&q.uid[qq]) == su) continue;  // self hit (SubjectReadAligner.cpp:463-465)
                         if (EMIT) {
                             const uint32_t slot = atomicAdd(&fill[wib][o], 1u);
-                            hits[(o ? o1 : o0) + slot] = hit_pack(qq, uint32_t(v & 0xffffffffu), posS);
+                            const int32_t lq = (aln && o) ? int32_t(__ldg(&q.len[qq])) : 0;
+                            hits[(o ? o1 : o0) + slot] =
+                                seed_hit(aln, o, qq, uint32_t(v & 0xffffffffu), f, L, lq, k);
                         } else {
                             if (o) {
                                 c1++;
@@ -513,6 +514,7 @@ struct CountDp {
 struct EmitDp {
     DpSeg *out;
     uint32_t subj, query, orient;
+    uint32_t orient_shift;  // the subject's orientation (-c), or the query's (alignment output)
     uint32_t n = 0;
     int32_t maxr = 0, maxc = 0;
     HERO_HD void begin(int64_t, int64_t, int64_t) {}
@@ -528,7 +530,7 @@ struct EmitDp {
         g.q1 = uint16_t(q1);
         // any band >= 65535 covers every cell of a segment of reads below 65536 bases
         g.band = int32_t(band > 65535 ? 65535 : band);
-        g.flags = flags | (orient << kSegOrientShift);
+        g.flags = flags | (orient << orient_shift);
         g.pad = 0;
         out[n++] = g;
         const int32_t ls = int32_t(s1 - s0), lq = int32_t(q1 - q0);
@@ -680,6 +682,7 @@ __global__ void __launch_bounds__(256)
                     ev.subj = s;
                     ev.query = qid;
                     ev.orient = orient;
+                    ev.orient_shift = p.aln ? kSegQrcShift : kSegOrientShift;
                     walk_chain(p, Lq, Ls, key, sz, ev);
                     if (ev.maxr > maxr) maxr = ev.maxr;
                     if (ev.maxc > maxc) maxc = ev.maxc;
@@ -804,12 +807,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
     for (uint64_t idx = t; idx < a.nd; idx += T) {
         const uint32_t si = a.perm ? a.perm[idx] : uint32_t(idx);
         const DpSeg g = a.segs[si];
-        const uint32_t orient = (g.flags >> kSegOrientShift) & 1u;
-        const uint8_t *sb = a.scode + a.soff[g.subj];
-        const int32_t Ls = int32_t(a.slen[g.subj]);
-        const uint8_t *qb = a.qcode + a.qoff[g.query];
-        const SegView v = make_view(sb, Ls, int32_t(orient), qb, g.s0, g.s1, g.q0, g.q1,
-                                    g.flags & 3u, g.band);
+        const SegView v = dpseg_view(g, a.scode, a.soff, a.slen, a.qcode, a.qoff);
         dp_fill<kStripW, AFFINE>(v, sc);
         OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
         DpSum sum;
@@ -1086,11 +1084,7 @@ __device__ __forceinline__ void group_traceback(const DpLaunch &a, const Codes &
 }
 
 __device__ __forceinline__ SegView seg_view(const DpLaunch &a, uint32_t si) {
-    const DpSeg sg = a.segs[si];
-    const uint32_t orient = (sg.flags >> kSegOrientShift) & 1u;
-    return make_view(a.scode + a.soff[sg.subj], int32_t(a.slen[sg.subj]), int32_t(orient),
-                     a.qcode + a.qoff[sg.query], sg.s0, sg.s1, sg.q0, sg.q1, sg.flags & 3u,
-                     sg.band);
+    return dpseg_view(a.segs[si], a.scode, a.soff, a.slen, a.qcode, a.qoff);
 }
 
 // One task of single segments: group g (G lanes) takes the sorted segment
@@ -1302,10 +1296,7 @@ __global__ void __launch_bounds__(kDpThreads) k_dp_wide(DpLaunch a, const uint64
     for (uint64_t idx = tasks[0] + t; idx < a.nd; idx += T) {
         const uint32_t si = a.perm[idx];
         const DpSeg g = a.segs[si];
-        const uint32_t orient = (g.flags >> kSegOrientShift) & 1u;
-        const SegView v = make_view(a.scode + a.soff[g.subj], int32_t(a.slen[g.subj]),
-                                    int32_t(orient), a.qcode + a.qoff[g.query], g.s0, g.s1, g.q0,
-                                    g.q1, g.flags & 3u, g.band);
+        const SegView v = dpseg_view(g, a.scode, a.soff, a.slen, a.qcode, a.qoff);
         dp_fill<kStripW, AFFINE>(v, sc);
         OpsWriter w{a.ops + uint64_t(si) * a.stride, int32_t(a.stride * 16u)};
         DpSum sum;
@@ -1422,6 +1413,159 @@ __global__ void k_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
     }
     kept = warp_sum(kept);
     if (lane_id() == 0) atomicAdd(&counters[C_KEPT], kept);
+}
+
+// ---------------------------------------------------------------------------
+// alignment output (HERO without -c): SubjectRead::addAlignment's list keyed by
+// the query's uniqueId (list_add), then the batch's .aln text
+// (SubjectReadAligner::writeToFile, SubjectRead::writeAlignment,
+// AlignmentRecord::getCigar).  The text is cut into units -- per subject its
+// header ">id\n", its records in list order and its closing "\n" -- that one
+// kernel sizes, a scan places and another writes, one thread per unit.
+// ---------------------------------------------------------------------------
+// the list slots of a subject: its forward chains' range, then its reverse range
+struct ChainSlots {
+    uint32_t *a;
+    uint32_t s0, n0, s1;
+    __device__ __forceinline__ uint32_t slot(uint32_t i) const { return i < n0 ? s0 + i : s1 + (i - n0); }
+    __device__ __forceinline__ uint32_t get(uint32_t i) const { return a[slot(i)]; }
+    __device__ __forceinline__ void set(uint32_t i, uint32_t v) { a[slot(i)] = v; }
+};
+
+// one thread per subject: its accepted records in arrival order (forward
+// chains, then reverse-complement chains, each in (query, chain) order)
+__global__ void k_aln_list(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
+                           ChainArrays ch, ReadsView q, uint32_t *alist, uint32_t *alist_n,
+                           unsigned long long *counters) {
+    unsigned long long kept = 0;
+    for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nsub;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        ChainSlots L{alist, cstart[2 * s], ccount[2 * s], cstart[2 * s + 1]};
+        auto key = [&](uint32_t c) { return uint64_t(q.uid[ch.query[c]]); };
+        auto better = [&](uint32_t a, uint32_t b) {
+            return record_better(ch.rate[a], ch.len[a], ch.rate[b], ch.len[b]);
+        };
+        uint32_t n = 0;
+        uint64_t largest = 0;
+        for (int o = 0; o < 2; o++) {
+            const uint32_t b = cstart[2 * s + o], e = b + ccount[2 * s + o];
+            for (uint32_t c = b; c < e; c++)
+                if (ch.status[c] == CH_ACCEPTED) n = list_add(L, n, largest, c, key, better);
+        }
+        alist_n[s] = n;
+        kept += n;
+    }
+    kept = warp_sum(kept);
+    if (lane_id() == 0) atomicAdd(&counters[C_KEPT], kept);
+}
+
+// one thread per subject: its units (rec_off = exclusive scan of alist_n)
+__global__ void k_aln_units(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
+                            const uint32_t *alist, const uint32_t *alist_n,
+                            const uint64_t *rec_off, ReadsView subj, uint32_t *unit,
+                            uint32_t *ulen) {
+    for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nsub;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        const ChainSlots L{const_cast<uint32_t *>(alist), cstart[2 * s], ccount[2 * s],
+                           cstart[2 * s + 1]};
+        const uint64_t u0 = rec_off[s] + 2 * s;
+        const uint32_t n = alist_n[s];
+        unit[u0] = kUnitSubject | uint32_t(s);
+        ulen[u0] = 2u + dec_len_signed(subj.uid[s]);
+        for (uint32_t i = 0; i < n; i++) unit[u0 + 1 + i] = L.get(i);
+        unit[u0 + 1 + n] = kUnitEnd;
+        ulen[u0 + 1 + n] = 1u;
+    }
+}
+
+// the DP pieces of a chain: ops of segment seg0 + piece, packed 2 bits a step at
+// the end of the segment's stride words
+struct DevPieces {
+    const uint32_t *ops;
+    uint32_t stride;
+    const DpSum *sums;
+    uint32_t seg0;
+    template <class F>
+    __device__ void each(uint32_t piece, F f) const {
+        const uint32_t si = seg0 + piece;
+        const DpSum sm = sums[si];
+        const uint32_t P = uint32_t(sm.tot[0]) + sm.tot[1] + sm.tot[2] + sm.tot[3];
+        const uint32_t *w = ops + uint64_t(si) * stride;
+        const uint32_t end = stride * 16u;
+        for (uint32_t pos = end - P; pos < end; pos++) f(uint8_t((w[pos >> 4] >> (2 * (pos & 15u))) & 3u));
+    }
+};
+
+struct AlnRec {
+    AlnText<DevPieces> t;
+    KeyAt ka;
+    int32_t nkeys;
+    int64_t Ls;
+    uint64_t key;
+    uint32_t orient;
+};
+
+__device__ __forceinline__ AlnRec aln_rec(uint32_t c, ChainArrays ch, const uint32_t *keys,
+                                          ReadsView subj, ReadsView q, const uint32_t *ops,
+                                          uint32_t stride, const DpSum *sums) {
+    const uint32_t s = ch.subj[c], qid = ch.query[c];
+    AlnRec r{AlnText<DevPieces>{DevPieces{ops, stride, sums, ch.seg_off[c]}, q.code + q.off[qid],
+                                int32_t(q.len[qid]), ch.orient[c] != 0},
+             KeyAt{keys + ch.key_off[c]}, int32_t(ch.nkeys[c]), int64_t(subj.len[s]),
+             uint64_t(q.uid[qid]), uint32_t(ch.orient[c])};
+    return r;
+}
+
+// one thread per unit: text length of each record (and of its prefix and CIGAR)
+__global__ void k_aln_size(Params p, uint64_t nunit, const uint32_t *unit, ChainArrays ch,
+                           const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
+                           uint32_t stride, const DpSum *sums, uint32_t *ulen, uint32_t *upre,
+                           uint32_t *ucig) {
+    for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < nunit;
+         u += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t c = unit[u];
+        if (c & kUnitSubject) continue;
+        AlnRec r = aln_rec(c, ch, keys, subj, q, ops, stride, sums);
+        walk_chain(p, int64_t(r.t.Lq), r.Ls, r.ka, r.nkeys, r.t);
+        const uint32_t pre = aln_prefix_len(r.key, r.orient, r.t.pos);
+        upre[u] = pre;
+        ucig[u] = r.t.cig_len;
+        ulen[u] = pre + r.t.cig_len + 1u + r.t.ins_len + 1u;
+    }
+}
+
+// one thread per unit: the text at its offset
+__global__ void k_aln_write(Params p, uint64_t nunit, const uint32_t *unit, const uint64_t *uoff,
+                            ChainArrays ch, const uint32_t *keys, ReadsView subj, ReadsView q,
+                            const uint32_t *ops, uint32_t stride, const DpSum *sums,
+                            const uint32_t *upre, const uint32_t *ucig, char *text) {
+    for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < nunit;
+         u += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t c = unit[u];
+        char *o = text + uoff[u];
+        if (c == kUnitEnd) {
+            *o = '\n';
+            continue;
+        }
+        if (c & kUnitSubject) {
+            *o++ = '>';
+            o = dec_put_signed(o, subj.uid[c & ~kUnitSubject]);
+            *o = '\n';
+            continue;
+        }
+        AlnRec r = aln_rec(c, ch, keys, subj, q, ops, stride, sums);
+        r.t.cig = o + upre[u];
+        r.t.ins = r.t.cig + ucig[u] + 1;
+        walk_chain(p, int64_t(r.t.Lq), r.Ls, r.ka, r.nkeys, r.t);
+        o = dec_put(o, r.key);
+        *o++ = ',';
+        o = dec_put(o, r.orient);
+        *o++ = ',';
+        o = dec_put_signed(o, r.t.pos);
+        *o = ',';
+        *r.t.cig = ',';
+        *r.t.ins = ',';
+    }
 }
 
 // SubjectRead::updateQueryCoverage (SubjectRead.cpp:208-330): M votes the
@@ -1837,17 +1981,17 @@ void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint3
     k_table_finalize<<<grid_1d(nslots, 256), 256, 0, st>>>(klo, khi, owner, count, start, nslots, slots);
 }
 
-void launch_probe(bool emit, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
+void launch_probe(bool emit, bool aln, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
                   uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
                   unsigned long long *counters, cudaStream_t st) {
     if (!nsub) return;
     const unsigned g = grid_1d(nsub, kProbeWarps, 148u * 16u);
     if (emit) {
         counted();
-        k_probe<true><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, seg_hits, hit_off, hits, counters);
+        k_probe<true><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, aln, seg_hits, hit_off, hits, counters);
     } else {
         counted();
-        k_probe<false><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, seg_hits, hit_off, hits, counters);
+        k_probe<false><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, aln, seg_hits, hit_off, hits, counters);
     }
 }
 
@@ -1979,6 +2123,44 @@ void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
         k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch,
                                                      winners, counters);
     }
+}
+
+void launch_aln_list(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
+                     ChainArrays ch, ReadsView q, uint32_t *alist, uint32_t *alist_n,
+                     unsigned long long *counters, cudaStream_t st) {
+    if (!nsub) return;
+    counted();
+    k_aln_list<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, cstart, ccount, ch, q, alist, alist_n,
+                                                   counters);
+}
+
+void launch_aln_units(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
+                      const uint32_t *alist, const uint32_t *alist_n, const uint64_t *rec_off,
+                      ReadsView subj, uint32_t *unit, uint32_t *ulen, cudaStream_t st) {
+    if (!nsub) return;
+    counted();
+    k_aln_units<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, cstart, ccount, alist, alist_n, rec_off,
+                                                    subj, unit, ulen);
+}
+
+void launch_aln_size(const Params &p, uint64_t nunit, const uint32_t *unit, ChainArrays ch,
+                     const uint32_t *keys, ReadsView subj, ReadsView q, const uint32_t *ops,
+                     uint32_t stride, const DpSum *sums, uint32_t *ulen, uint32_t *upre,
+                     uint32_t *ucig, cudaStream_t st) {
+    if (!nunit) return;
+    counted();
+    k_aln_size<<<grid_1d(nunit, 128), 128, 0, st>>>(p, nunit, unit, ch, keys, subj, q, ops, stride,
+                                                    sums, ulen, upre, ucig);
+}
+
+void launch_aln_write(const Params &p, uint64_t nunit, const uint32_t *unit, const uint64_t *uoff,
+                      ChainArrays ch, const uint32_t *keys, ReadsView subj, ReadsView q,
+                      const uint32_t *ops, uint32_t stride, const DpSum *sums,
+                      const uint32_t *upre, const uint32_t *ucig, char *text, cudaStream_t st) {
+    if (!nunit) return;
+    counted();
+    k_aln_write<<<grid_1d(nunit, 128), 128, 0, st>>>(p, nunit, unit, uoff, ch, keys, subj, q, ops,
+                                                     stride, sums, upre, ucig, text);
 }
 
 void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,

@@ -21,8 +21,9 @@ namespace herohost {
 // refused with a message instead of being silently ignored.
 // ---------------------------------------------------------------------------
 void Config::help() {
-    std::cout << "Usage: hero_b200 -q <query[,query...]> -s <subject[,subject...]> -c [thr]\n"
-                 "  -o/--out      output prefix (default: query) -> <out>.fasta, <out>.info\n"
+    std::cout << "Usage: hero_b200 -q <query[,query...]> -s <subject[,subject...]> [-c [thr]]\n"
+                 "  -o/--out      output prefix (default: query) -> <out>.fasta, <out>.info with -c,\n"
+                 "                else <out>.aln (every subject read's alignment records)\n"
                  "  -c [thr]      call the consensus (default threshold 0.6)\n"
                  "  --covinfo     write <out>.info (coverage min/median/max, rates)\n"
                  "  --singleReads inputs are unpaired reads\n"
@@ -113,7 +114,7 @@ bool Config::parse(int argc, char **argv) {
             subject_batch = uint32_t(std::strtoul(v.c_str(), nullptr, 10));
         } else if (a == "-v" || a == "--mapping" || a == "--merge" || a == "--covfilter" ||
                    a == "--suffix" || a == "--size" || a == "--notification") {
-            std::cerr << a << ": not part of the consensus path this build replaces\n";
+            std::cerr << a << ": not part of the path this build replaces\n";
             return false;
         } else {
             std::cerr << "unknown flag " << a << "\n";
@@ -123,10 +124,6 @@ bool Config::parse(int argc, char **argv) {
     }
     if (subject_files.empty() || query_files.empty()) {
         std::cerr << "missed -subject or -query input files!\n";
-        return false;
-    }
-    if (!consensus) {
-        std::cerr << "only the consensus mode (-c) is provided; the .aln alignment output is not\n";
         return false;
     }
     if (k < 1 || k > 63) {
@@ -381,6 +378,7 @@ bool HashTableGpu::createHashTables(const Config &c, QueryDataset *q, std::strin
     p.consensus_threshold = c.consensus_thr;
     p.device = c.device;
     p.subject_batch = c.subject_batch;
+    p.flags = c.consensus ? 0u : HERO_FLAG_ALIGNMENT_OUTPUT;
     if (!ok(nullptr, hero_create(&p, &ctx), "hero_create", err)) return false;
     const ReadSet &r = q->reads;
     return ok(ctx, hero_set_queries(ctx, reinterpret_cast<const uint8_t *>(r.seq.data()),
@@ -396,13 +394,30 @@ HashTableGpu::~HashTableGpu() {
     if (ctx) hero_destroy(ctx);
 }
 
+// SubjectReadAligner::writeToFile (SubjectReadAligner.cpp:854-906): after each
+// chunk the chunk's alignment text is appended to <out>.aln
+static bool write_alignments(const Config &c, hero_ctx *ctx, std::string *err) {
+    uint64_t n = 0;
+    if (!ok(ctx, hero_alignments_size(ctx, &n), "hero_alignments_size", err)) return false;
+    std::vector<uint8_t> buf(n ? n : 1);
+    if (!ok(ctx, hero_alignments_take(ctx, buf.data(), n), "hero_alignments_take", err)) return false;
+    const std::string path = c.out + ".aln";
+    std::FILE *f = std::fopen(path.c_str(), "ab");
+    if (!f) {
+        if (err) *err = "Unable to open file: " + path;
+        return false;
+    }
+    const bool good = std::fwrite(buf.data(), 1, n, f) == n;
+    return (std::fclose(f) == 0) && good;
+}
+
 bool SubjectReadAligner::start(const Config &c, std::string *err) {
     using clk = std::chrono::steady_clock;
     if (c.subject_files == c.query_files) {  // -q X -s X: the resident query set
         const auto t0 = clk::now();
         const bool r = ok(table->ctx, hero_align_self(table->ctx), "hero_align_self", err);
         seconds_aligning += std::chrono::duration<double>(clk::now() - t0).count();
-        return r;
+        return r && (c.consensus || write_alignments(c, table->ctx, err));
     }
     SubjectDataset sd(c);
     ReadSet chunk;
@@ -417,6 +432,7 @@ bool SubjectReadAligner::start(const Config &c, std::string *err) {
                                                 chunk.off.data(), chunk.uid.data(), chunk.n()),
                 "hero_align_subjects", err))
             return false;
+        if (!c.consensus && !write_alignments(c, table->ctx, err)) return false;
         seconds_aligning += std::chrono::duration<double>(clk::now() - t1).count();
     }
     return true;

@@ -1,5 +1,6 @@
-// main.cpp -- drop-in replacement of HERO's correction driver (main.cpp:26-106
-// of the reference): same flags, same sequence, same .fasta/.info output.
+// main.cpp -- drop-in replacement of HERO's driver (main.cpp:26-106 of the
+// reference): same flags, same sequence, same .fasta/.info output with -c and
+// the same .aln output without it.
 #include <chrono>
 #include <iostream>
 
@@ -39,12 +40,12 @@ int main(int argc, char **argv) {
         return 1;
     }
     const auto t3 = clk::now();
-    if (!call_consensus(table, query, &err)) {
+    if (cfg.consensus && !call_consensus(table, query, &err)) {
         std::cerr << "Error: " << err << std::endl;
         return 1;
     }
     const auto t4 = clk::now();
-    if (!query.write(cfg, &err)) {
+    if (cfg.consensus && !query.write(cfg, &err)) {
         std::cerr << "Error: " << err << std::endl;
         return 1;
     }

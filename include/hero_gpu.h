@@ -52,6 +52,15 @@ extern "C" {
 
 typedef struct hero_ctx hero_ctx;
 
+/* Alignment-output mode: HERO run without -c.  The aligner keeps one record per
+ * (subject, query uniqueId) and writes them as the .aln file
+ * (SubjectReadAligner::writeToFile, SubjectReadAligner.cpp:854-906); the
+ * reverse-complement pass aligns the query's reverse complement to the forward
+ * subject (SubjectReadAligner.cpp:199-210, 477-481).  No votes, no consensus:
+ * hero_align_subjects / hero_align_self append each subject's text, and
+ * hero_alignments_size / hero_alignments_take return it. */
+#define HERO_FLAG_ALIGNMENT_OUTPUT 1u
+
 typedef struct {
     int32_t k;              /* k-mer length, 1..63 (Config::iKmer, -k; default 39) */
     int32_t min_overlap;    /* Config::minimumOverlapLength, -l (default 40) */
@@ -62,7 +71,7 @@ typedef struct {
     double consensus_threshold; /* Config::dMinFrequencyCallConsensus, -c (default 0.6) */
     uint64_t device_memory_budget; /* bytes this context may hold; 0 = no limit */
     uint32_t subject_batch; /* subject reads per device batch; 0 = default */
-    uint32_t flags;         /* reserved, 0 */
+    uint32_t flags;         /* HERO_FLAG_* (0 = consensus mode, -c) */
     void *stream;           /* cudaStream_t to run on; NULL = a private stream */
 } hero_params;
 
@@ -133,6 +142,14 @@ int hero_round(hero_ctx *ctx, uint32_t flags);
 /* Results of the last round (same outputs as hero_consensus). */
 int hero_fetch(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *imed, uint32_t *imax,
                double *mismatch_rate, double *gc_content, uint8_t *good_out);
+
+/* Alignment-output mode: bytes of .aln text held (every subject aligned since the
+ * last take, in subject order: ">uniqueId\n", its records
+ * "queryUniqueId,orientation,position,CIGAR,inserted bases," (AlignmentRecord::
+ * getCigar, AlignmentRecord.cpp:102-149), "\n"). */
+int hero_alignments_size(hero_ctx *ctx, uint64_t *bytes);
+/* Copies the held text to out (cap >= hero_alignments_size) and drops it. */
+int hero_alignments_take(hero_ctx *ctx, uint8_t *out, uint64_t cap);
 
 /* Vote matrix before the self vote: uint32 [total query bases][4] (A,C,T,G). */
 int hero_get_votes(hero_ctx *ctx, uint32_t *cov);

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <string>
 #include <unordered_map>
 #include <vector>
 
@@ -570,6 +571,168 @@ int emu_align_wave(int affine, const uint8_t *subj, int32_t ls, const uint8_t *q
     if (n > cap) return -1;
     for (int i = 0; i < n; i++) ops[i] = uint8_t(ops_field(wv.data(), words * 16 - n + i));
     return n;
+}
+
+// alignment output (no -c), sequentially, through the same core functions as
+// the kernels: seed_hit, make_view with the query reverse complement,
+// list_add, AlnText.  out receives the .aln text; returns its length, or -1 if
+// cap is too small.
+extern "C++" {
+struct EmuPieces {
+    const SegRec *segs;
+    template <class F>
+    void each(uint32_t piece, F f) const {
+        for (uint8_t o : segs[piece].ops) f(o);
+    }
+};
+}  // extern "C++"
+
+int64_t emu_align_output(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate,
+                         uint64_t nq, const uint8_t *qseq, const uint64_t *qoff,
+                         const int64_t *quid, uint8_t *out, uint64_t cap) {
+    Params p{k, l, affine, 1, mis_rate, indel_rate, 0.6};
+    Reads Q;
+    load(Q, nq, qseq, qoff, quid, l);
+    std::unordered_map<std::pair<uint64_t, uint64_t>, std::vector<uint64_t>, KeyHash> table;
+    for (uint64_t r = 0; r < nq; r++) {
+        if (!Q.gq[r]) continue;
+        const int64_t L = Q.len[r];
+        const int32_t nk = query_key_count(L, k);
+        for (int32_t i = 0; i < nk; i++) {
+            const int64_t pos = query_key_pos(L, k, i);
+            Kmer m{0, 0};
+            for (int32_t t = 0; t < k; t++) kmer_push(m, Q.code[Q.off[r] + pos + t] & 3u, k);
+            table[{m.lo, m.hi}].push_back((uint64_t(r) << 32) | uint64_t(pos));
+        }
+    }
+    std::string text;
+    for (uint64_t s = 0; s < nq; s++) {
+        text += '>';
+        text += std::to_string(Q.uid[s]);
+        text += '\n';
+        if (!Q.gs[s]) {
+            text += '\n';
+            continue;
+        }
+        const int32_t L = int32_t(Q.len[s]);
+        const uint8_t *c = Q.code.data() + Q.off[s];
+        std::vector<uint64_t> hits[2];
+        if (L >= k) {
+            for (int32_t f = 0; f + k <= L; f++) {
+                Kmer fm{0, 0}, rm{0, 0};
+                bool bad = false;
+                for (int32_t i = 0; i < k; i++) {
+                    bad |= c[f + i] >= 4;
+                    kmer_push(fm, c[f + i] & 3u, k);
+                }
+                if (bad) continue;
+                for (int32_t i = k - 1; i >= 0; i--) kmer_push(rm, (c[f + i] & 3u) ^ 2u, k);
+                for (int o = 0; o < 2; o++) {
+                    Kmer m = o ? rm : fm;
+                    auto it = table.find({m.lo, m.hi});
+                    if (it == table.end()) continue;
+                    for (uint64_t v : it->second) {
+                        uint32_t qq = uint32_t(v >> 32);
+                        if (Q.uid[qq] == Q.uid[s]) continue;
+                        hits[o].push_back(seed_hit(true, o, qq, uint32_t(v), f, L, int32_t(Q.len[qq]), k));
+                    }
+                }
+            }
+        }
+        struct Cand {
+            uint32_t q;
+            int orient;
+            std::vector<SegRec> segs;
+            std::vector<uint64_t> keys;
+            bool accepted;
+            double rate, len;
+        };
+        std::vector<Cand> cands;
+        for (int o = 0; o < 2; o++) {
+            auto &H = hits[o];
+            std::sort(H.begin(), H.end());
+            size_t g0 = 0;
+            for (size_t i = 0; i < H.size(); i++) {
+                if (i + 1 != H.size() && hit_q(H[i]) == hit_q(H[i + 1])) continue;
+                const int32_t gn = int32_t(i + 1 - g0);
+                const uint64_t *G = H.data() + g0;
+                auto hit = [G](int32_t h) { return G[h]; };
+                std::vector<uint32_t> chain_of(gn);
+                std::vector<int32_t> first(gn), last(gn), prev(gn);
+                std::vector<int64_t> kl(gn);
+                int32_t nch = chain_group(p, hit, gn, chain_of.data(), first.data(), last.data());
+                int64_t best = chain_key_lengths(p, hit, gn, chain_of.data(), nch, kl.data(), prev.data());
+                const uint32_t qid = hit_q(G[0]);
+                const int32_t Lq = int32_t(Q.len[qid]);
+                for (int32_t ch = 0; ch < nch; ch++) {
+                    if (kl[ch] != best) continue;
+                    Cand cd;
+                    cd.q = qid;
+                    cd.orient = o;
+                    for (int32_t h = 0; h < gn; h++)
+                        if (chain_of[h] == uint32_t(ch)) cd.keys.push_back(G[h]);
+                    auto key = [&cd](int32_t t) { return cd.keys[t]; };
+                    Collect col{&cd.segs};
+                    walk_chain(p, Lq, L, key, int32_t(cd.keys.size()), col);
+                    for (SegRec &sr : cd.segs) {
+                        SegView v = make_view(c, L, 0, Q.code.data() + Q.off[qid], int32_t(sr.s0),
+                                              int32_t(sr.s1), int32_t(sr.q0), int32_t(sr.q1),
+                                              sr.flags, sr.band, Lq, o == 1);
+                        run_dp<8>(v, affine != 0, sr.ops, sr.sum);
+                    }
+                    Asm as;
+                    as.segs = cd.segs.data();
+                    bool ok = walk_chain(p, Lq, L, key, int32_t(cd.keys.size()), as);
+                    cd.accepted = as.built && ok && as.st.good_rates(p, cd.rate, cd.len);
+                    cands.push_back(std::move(cd));
+                }
+                g0 = i + 1;
+            }
+        }
+        struct Slots {
+            std::vector<uint32_t> v;
+            uint32_t get(uint32_t i) const { return v[i]; }
+            void set(uint32_t i, uint32_t x) {
+                if (i >= v.size()) v.resize(i + 1);
+                v[i] = x;
+            }
+        } list;
+        auto key = [&](uint32_t i) { return uint64_t(Q.uid[cands[i].q]); };
+        auto better = [&](uint32_t a, uint32_t b) {
+            return record_better(cands[a].rate, cands[a].len, cands[b].rate, cands[b].len);
+        };
+        uint32_t n = 0;
+        uint64_t largest = 0;
+        for (uint32_t i = 0; i < cands.size(); i++)
+            if (cands[i].accepted) n = list_add(list, n, largest, i, key, better);
+        for (uint32_t e = 0; e < n; e++) {
+            const Cand &w = cands[list.get(e)];
+            const int32_t Lq = int32_t(Q.len[w.q]);
+            auto kk = [&w](int32_t t) { return w.keys[t]; };
+            AlnText<EmuPieces> sz{EmuPieces{w.segs.data()}, Q.code.data() + Q.off[w.q], Lq, w.orient == 1};
+            walk_chain(p, Lq, L, kk, int32_t(w.keys.size()), sz);
+            const uint32_t pre = aln_prefix_len(key(list.get(e)), uint32_t(w.orient), sz.pos);
+            std::string rec(pre + sz.cig_len + 1 + sz.ins_len + 1, '?');
+            AlnText<EmuPieces> wr{EmuPieces{w.segs.data()}, Q.code.data() + Q.off[w.q], Lq, w.orient == 1};
+            wr.cig = &rec[pre];
+            wr.ins = wr.cig + sz.cig_len + 1;
+            walk_chain(p, Lq, L, kk, int32_t(w.keys.size()), wr);
+            char *o = &rec[0];
+            o = dec_put(o, key(list.get(e)));
+            *o++ = ',';
+            o = dec_put(o, uint32_t(w.orient));
+            *o++ = ',';
+            o = dec_put_signed(o, wr.pos);
+            *o = ',';
+            *wr.cig = ',';
+            *wr.ins = ',';
+            text += rec;
+        }
+        text += '\n';
+    }
+    if (text.size() > cap) return -1;
+    std::memcpy(out, text.data(), text.size());
+    return int64_t(text.size());
 }
 
 // whole path, sequentially, through the core item functions

@@ -152,7 +152,25 @@ class Emu:
                                        C.c_int, vp, C.c_int32]
         lib.emu_correct.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                      C.c_double, C.c_uint64] + [vp] * 11)
+        lib.emu_align_output.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                          C.c_uint64, vp, vp, vp, vp, C.c_uint64])
+        lib.emu_align_output.restype = C.c_int64
         self.lib = lib
+
+    def align_output(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
+                     max_indel_rate=1.0, cap=None):
+        """The .aln text of the alignment-output mode (reads against themselves)."""
+        cap = cap or (len(reads.seq) * 64 + reads.n * 64 + 1024)
+        out = np.zeros(cap, np.uint8)
+        off = reads.off.astype(np.uint64)
+        uid = reads.names.astype(np.int64)
+        n = self.lib.emu_align_output(k, min_overlap, 1 if aligner in ("a", "affine") else 0,
+                                      max_mismatch_rate, max_indel_rate, reads.n, _vp(reads.seq),
+                                      _vp(off), _vp(uid), _vp(out), cap)
+        if n < 0:
+            return self.align_output(reads, k, min_overlap, aligner, max_mismatch_rate,
+                                     max_indel_rate, cap * 4)
+        return out[:n].tobytes()
 
     def align(self, affine, subj: bytes, query: bytes, band, right=False, left=False, strip16=False):
         s = np.frombuffer(subj, np.uint8).copy()

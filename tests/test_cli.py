@@ -29,15 +29,16 @@ def test_requires_inputs(cli):
     assert r.returncode == 1 and "missed -subject or -query" in r.stderr
 
 
-def test_requires_consensus_mode(cli):
-    r = run(cli, "-q", "a.fq", "-s", "a.fq")
-    assert r.returncode == 1 and "consensus mode" in r.stderr
+def test_alignment_output_mode_without_c(cli, tmp_path):
+    # no -c: the .aln mode; the flags parse and the run stops at the missing input
+    r = run(cli, "-q", str(tmp_path / "nope.fq"), "-s", str(tmp_path / "nope.fq"))
+    assert r.returncode == 1 and "Unable to open file" in r.stderr
 
 
 @pytest.mark.parametrize("flag", ["-v", "--mapping", "--merge"])
 def test_refuses_modes_outside_the_path(cli, flag):
     r = run(cli, "-q", "a.fq", "-s", "a.fq", "-c", flag)
-    assert r.returncode == 1 and "not part of the consensus path" in r.stderr
+    assert r.returncode == 1 and "not part of the path" in r.stderr
 
 
 def test_missing_file(cli, tmp_path):

@@ -162,3 +162,23 @@ def test_pair_rows_match_oracle(oracle, emu):
             assert np.array_equal(want, ops[:n.value]), (ls, lq, band, fl)
         done += 1
     assert done == 400
+
+
+@pytest.mark.parametrize("name", ["c1_20k", "c1_20k_affine", "mix", "mix_affine", "mix_i0",
+                                  "mix_k21_l60", "c1_20k_narrow"])
+def test_emulated_alignment_output_matches_reference(emu, name):
+    """The device item logic of the alignment-output mode (flipped seeds, the
+    query's reverse complement in the DP, the record list, the record text),
+    driven sequentially on the host: the reference's .aln bytes."""
+    import hashlib
+    import json
+    import os
+    from fixtures import FIXTURES, aln_flags, params, upper
+    m = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                    "manifest.json")))[name]
+    gen, flags = FIXTURES[name]
+    kw = params(aln_flags(flags))
+    kw.pop("consensus_threshold")
+    a = emu.align_output(upper(gen()), **kw)
+    assert len(a) == m["aln_bytes"]
+    assert hashlib.md5(a).hexdigest() == m["aln_md5"]
