@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--cpu-sample-bp", type=int, default=60000,
                     help="genome size of the bounded sample the CPU reference runs on")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-alignment-output", action="store_true",
+                    help="skip the alignment-output (.aln) line")
     ap.add_argument("--profile", action="store_true",
                     help="run --warmup then --steps device-resident steps and exit (for ncu)")
     return ap.parse_args()
@@ -554,6 +556,10 @@ def bench_hero(args):
                               f"0.5-20 Mbp x {args.jobs_scale or 0.02}, L in {{100,150,250}}, "
                               "coverage U(20,80), affine/indel errors")
 
+    aln = None
+    if rank == 0 and world == 1 and not args.profile and not args.no_alignment_output:
+        aln = measure_alignment_output(rs, kw, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = measure_cpu_baseline(args)
@@ -595,10 +601,34 @@ def bench_hero(args):
             "work_per_step": {"dp_cells": cells // steps,
                               "dp_segments": (s1["dp_segments"] - s0["dp_segments"]) // steps},
             "served": served,
+            "alignment_output": aln,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def measure_alignment_output(rs, kw, dev):
+    """The alignment-output mode (HERO without -c) on the same reads: host reads
+    in, the whole .aln text in host memory out; wall time of the second of two
+    runs (table, seeding, chaining, DP, record lists, text, copy out)."""
+    from hero_b200 import Hero
+    walls, size = [], 0
+    with Hero(alignment_output=True, device=dev, **kw) as h:
+        for _ in range(2):
+            t0 = time.perf_counter()
+            h.set_queries(rs.seq, rs.off, rs.names)
+            h.build_index()
+            h.align_self()
+            text = h.alignments()
+            walls.append(time.perf_counter() - t0)
+            size = len(text)
+            del text
+        st = h.stats()
+    return {"metric": "aligned bases/s (.aln text in host memory)",
+            "value": rs.total_bases / walls[-1], "unit": "bases/s", "seconds": walls[-1],
+            "aln_bytes": size, "records": st["records_kept"] // 2,
+            "flags": "as the main line without -c"}
 
 
 def main():
