@@ -54,10 +54,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM traffic (read + write) of the affine DP kernel per band cell, from one ncu
-# capture of a whole launch (profiles/k_dp_wave_affine_100kbp.md: 2.200 GB for
+# capture of a whole launch (profiles/k_dp_wave_affine_100kbp.md: 2.226 GB for
 # 23.19 G cells); the traffic is per segment (codes in, ops and summaries out),
 # so it scales with the cells of a launch
-DP_DRAM_BYTES_PER_CELL = 2.199761e9 / 23_186_600_877
+DP_DRAM_BYTES_PER_CELL = 2.225526e9 / 23_186_600_877
 
 
 def log(*a):
