@@ -82,6 +82,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-alignment-output", action="store_true",
                     help="skip the alignment-output (.aln) line")
+    ap.add_argument("--shard", action="store_true",
+                    help="one job split across the ranks by subject reads (strong scaling; "
+                         "votes summed by one NCCL all-reduce) instead of one job per rank")
     ap.add_argument("--profile", action="store_true",
                     help="run --warmup then --steps device-resident steps and exit (for ncu)")
     return ap.parse_args()
@@ -419,7 +422,7 @@ def bench_hero(args):
     import torch
     import torch.distributed as dist
 
-    from hero_b200 import Hero, build
+    from hero_b200 import Hero, build, shard
     if not os.environ.get("HERO_B200_LIB"):
         build.build_library()
 
@@ -437,11 +440,7 @@ def bench_hero(args):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, device="cuda")
 
     served_in = None
     if args.served_jobs and world == 1 and not args.profile and args.workload == "config2":
@@ -631,12 +630,120 @@ def measure_alignment_output(rs, kw, dev):
             "flags": "as the main line without -c"}
 
 
+def bench_sharded(args):
+    """One correction split across the ranks by subject reads (hero_b200.shard):
+    every rank holds the whole query set and table, aligns its range of subject
+    reads, the vote states are summed by one all-reduce (NCCL over NVLink), and
+    every rank calls the consensus.  Strong scaling: value = the job's bases
+    over the slowest rank's device time of a step."""
+    import torch
+    import torch.distributed as dist
+
+    from hero_b200 import Hero, build, shard
+    if not os.environ.get("HERO_B200_LIB"):
+        build.build_library()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900),
+                                device_id=torch.device("cuda", dev))
+    rs, kw, flags, desc = make_workload(args.workload, args.genome_bp)
+    n, nb = rs.n, rs.total_bases
+    a, b = shard.shard_range(n, rank, world)
+    seq_p = torch.from_numpy(rs.seq).pin_memory()
+    off_p = torch.from_numpy(rs.off.view(np.int64)).pin_memory()
+    uid_p = torch.from_numpy(rs.names.astype(np.int64)).pin_memory()
+    out_seq = torch.empty(nb, dtype=torch.uint8).pin_memory()
+    out_u32 = [torch.empty(n, dtype=torch.int32).pin_memory() for _ in range(3)]
+    out_f64 = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(2)]
+    stream = torch.cuda.Stream(device=dev)
+    h = Hero(device=dev, stream=stream.cuda_stream, **kw)
+    h.set_queries_ptr(seq_p.data_ptr(), off_p.data_ptr(), uid_p.data_ptr(), n, nb)
+
+    def device_step():
+        h.reset_votes()
+        h.build_index()
+        h.align_self_range(a, b - a)
+        shard.exchange_votes(h, dev)
+        h.consensus_ptr()
+
+    def e2e_step():
+        h.set_queries_ptr(seq_p.data_ptr(), off_p.data_ptr(), uid_p.data_ptr(), n, nb)
+        h.build_index()
+        h.align_self_range(a, b - a)
+        shard.exchange_votes(h, dev)
+        h.consensus_ptr(out_seq.data_ptr(), out_u32[0].data_ptr(), out_u32[1].data_ptr(),
+                        out_u32[2].data_ptr(), out_f64[0].data_ptr(), out_f64[1].data_ptr())
+
+    def timed(fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for e0, e1 in ev:
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return shard.max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in ev) / 1e3, "cuda")
+
+    for _ in range(args.warmup):
+        device_step()
+    s0 = h.stats()
+    with ClockSampler(dev) as clk:
+        t_dev = timed(device_step, args.steps)
+    s1 = h.stats()
+    t_e2e = timed(e2e_step, args.steps)
+    cells = s1["dp_cells"] - s0["dp_cells"]
+    dp_ms = s1["ms_dp_kernel"] - s0["ms_dp_kernel"]
+    ops_per_cell = 10 if kw["aligner"] == "affine" else 6
+    achieved = cells * ops_per_cell / (dp_ms / 1e3) / 1e12 if dp_ms > 0 else None
+    peak = int_peak_tops(dev)
+    launches = s1["kernel_launches"] - s0["kernel_launches"]
+    h.close()
+    if rank == 0:
+        line = {
+            "metric": "corrected bases/s", "value": nb * args.steps / t_dev, "unit": "bases/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded generator, no public dataset)",
+            "config": {"workload": desc, "reads": n, "bases": nb, "flags": " ".join(flags),
+                       "parallelism": f"one job, subject reads sharded x{world}, votes summed "
+                                      "by one all-reduce",
+                       "l2": f"inputs larger than L2 ({nb / 1e6:.0f} Mbp reads, "
+                             f"{20 * nb / 1e9:.1f} GB vote state)"},
+            "e2e": {"value": nb * args.steps / t_e2e, "unit": "bases/s",
+                    "h2d_bytes_per_step": nb + 8 * (n + 1) + 8 * n,
+                    "d2h_bytes_per_step": nb + 3 * 4 * n + 2 * 8 * n},
+            "roofline": {"bound": "alu", "kernel": "k_dp (rank 0's DP launches)",
+                         "achieved": achieved, "peak": peak, "unit": "Tops/s",
+                         "frac": (achieved / peak) if (achieved and peak) else None,
+                         "traffic": None, "ops_per_cell": ops_per_cell},
+            "cpu_baseline": None,
+            "exchange_bytes_per_rank": 20 * nb,
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         bench_reference(args)
     elif args.workload == "config4":
         bench_served(args)
+    elif args.shard:
+        bench_sharded(args)
     else:
         bench_hero(args)
 

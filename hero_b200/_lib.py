@@ -29,6 +29,7 @@ EXPORTS = [
     "hero_job_poll", "hero_job_wait", "hero_job_result", "hero_job_error", "hero_job_release",
     "hero_server_get_stats", "hero_job_bytes", "hero_round_admit", "hero_set_dp_tuning",
     "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
+    "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
 ]
 
 # hero_params.flags: the alignment-output mode (HERO without -c)
@@ -126,6 +127,10 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_get_votes.argtypes = [vp, vp]
     lib.hero_alignments_size.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_alignments_take.argtypes = [vp, vp, C.c_uint64]
+    lib.hero_align_self_range.argtypes = [vp, C.c_uint64, C.c_uint64]
+    lib.hero_votes_words.argtypes = [vp, C.POINTER(C.c_uint64)]
+    lib.hero_votes_save.argtypes = [vp, vp]
+    lib.hero_votes_load.argtypes = [vp, vp]
     lib.hero_get_stats.argtypes = [vp, C.POINTER(HeroStats)]
     lib.hero_align_segments.argtypes = ([vp, C.c_int, vp, vp, C.c_uint64, vp, vp, C.c_uint64,
                                          C.c_uint64] + [vp] * 12)
@@ -312,6 +317,25 @@ class Hero:
             self.h, _ptr(res["seq"]), _ptr(res["imin"]), _ptr(res["imed"]), _ptr(res["imax"]),
             _ptr(res["mismatch_rate"]), _ptr(res["gc"]), _ptr(res["good"])), "consensus")
         return res
+
+    def align_self_range(self, first: int, count: int):
+        """The query reads [first, first + count) as subjects (one shard of align_self)."""
+        self._check(self.lib.hero_align_self_range(self.h, int(first), int(count)),
+                    "align_self_range")
+
+    def votes_words(self) -> int:
+        """Size of the additive vote state in 32-bit words (5 per query base)."""
+        n = C.c_uint64()
+        self._check(self.lib.hero_votes_words(self.h, C.byref(n)), "votes_words")
+        return n.value
+
+    def votes_save(self, dev_ptr: int):
+        """Copies the vote state into a device buffer (e.g. a CUDA tensor's data_ptr())."""
+        self._check(self.lib.hero_votes_save(self.h, C.c_void_p(dev_ptr)), "votes_save")
+
+    def votes_load(self, dev_ptr: int):
+        """Replaces the vote state from a device buffer (the shards' sum)."""
+        self._check(self.lib.hero_votes_load(self.h, C.c_void_p(dev_ptr)), "votes_load")
 
     def alignments(self) -> bytes:
         """The .aln text of every subject aligned since the last call (and drops it)."""

@@ -693,6 +693,50 @@ extern "C" int hero_align_self(hero_ctx *c) {
     return align_reads(c, v, c->nq);
 }
 
+extern "C" int hero_align_self_range(hero_ctx *c, uint64_t first, uint64_t count) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_index) return c->fail(HERO_E_STATE, "index not built");
+    if (first > c->nq || count > c->nq - first) return c->fail(HERO_E_INPUT, "range outside the query set");
+    if (count == 0) return HERO_OK;
+    cudaSetDevice(c->dev);
+    const uint32_t *job = job_tags(c);
+    ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off) + first, P_<uint32_t>(c->q_len) + first,
+                P_<int64_t>(c->q_uid) + first, P_<uint8_t>(c->q_sgood) + first, count,
+                job ? job + first : nullptr};
+    return align_reads(c, v, count);
+}
+
+extern "C" int hero_votes_words(hero_ctx *c, uint64_t *words) {
+    if (!c || !words) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    *words = c->nqb * 5;
+    return HERO_OK;
+}
+
+extern "C" int hero_votes_save(hero_ctx *c, void *dst) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (!c->nqb) return HERO_OK;
+    if (!dst) return c->fail(HERO_E_INPUT, "null vote buffer");
+    cudaSetDevice(c->dev);
+    uint8_t *d = static_cast<uint8_t *>(dst);
+    HERO_TRY(c->cuda(cudaMemcpyAsync(d, c->cov.p, c->nqb * 16, cudaMemcpyDeviceToDevice, c->st), "votes save"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(d + c->nqb * 16, c->mdiff.p, c->nqb * 4, cudaMemcpyDeviceToDevice, c->st), "votes save"));
+    return c->cuda(cudaStreamSynchronize(c->st), "votes save");
+}
+
+extern "C" int hero_votes_load(hero_ctx *c, const void *src) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (!c->nqb) return HERO_OK;
+    if (!src) return c->fail(HERO_E_INPUT, "null vote buffer");
+    cudaSetDevice(c->dev);
+    const uint8_t *s = static_cast<const uint8_t *>(src);
+    HERO_TRY(c->cuda(cudaMemcpyAsync(c->cov.p, s, c->nqb * 16, cudaMemcpyDeviceToDevice, c->st), "votes load"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(c->mdiff.p, s + c->nqb * 16, c->nqb * 4, cudaMemcpyDeviceToDevice, c->st), "votes load"));
+    return c->cuda(cudaStreamSynchronize(c->st), "votes load");
+}
+
 extern "C" int hero_align_subjects(hero_ctx *c, const uint8_t *seq, const uint64_t *off,
                                    const int64_t *uid, uint64_t n) {
     if (!c) return HERO_E_INPUT;

@@ -117,6 +117,24 @@ int hero_align_subjects(hero_ctx *ctx, const uint8_t *seq, const uint64_t *off,
 /* The query set itself as the subject set, without a second upload. */
 int hero_align_self(hero_ctx *ctx);
 
+/* The query reads [first, first + count) as the subject set: one shard of
+ * hero_align_self, for a correction split across devices by subject reads
+ * (each device aligns its range against the whole query table; the votes of
+ * all ranges add up to hero_align_self's). */
+int hero_align_self_range(hero_ctx *ctx, uint64_t first, uint64_t count);
+
+/* Vote state for the exchange between contexts that aligned different subject
+ * reads against the same query set: hero_votes_words gives its size in 32-bit
+ * words (5 per query base: mismatch votes [bases][4], then the match-run
+ * difference array [bases]); it is additive -- the element-wise sum of the
+ * shards' states (integer addition mod 2^32) is the state of the whole run.
+ * hero_votes_save copies it to, and hero_votes_load replaces it from, a
+ * buffer in this context's device memory owned by the caller (e.g. the
+ * buffer of an NCCL all-reduce); both return once the copy is done. */
+int hero_votes_words(hero_ctx *ctx, uint64_t *words);
+int hero_votes_save(hero_ctx *ctx, void *dev_dst);
+int hero_votes_load(hero_ctx *ctx, const void *dev_src);
+
 /* Clears the vote matrix for a new correction of the same query set, as
  * QueryRead::initilizeCoverageMatrix zeroes it at load (QueryRead.cpp:100-115). */
 int hero_reset_votes(hero_ctx *ctx);
