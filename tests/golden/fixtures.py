@@ -3,7 +3,8 @@
 Each fixture's input is regenerated from its seed (hero_b200.synth); the
 reference outputs recorded by make_golden.py are stored beside this file
 (manifest.json: md5 of the FASTQ and of the reference .fasta/.info; the
-smallest outputs are also kept gzipped).  Read names are 1..N.
+smallest outputs are also kept gzipped).  Read names are 1..N, except in
+c2_20k_names (shuffled, duplicated and negative names).
 """
 from __future__ import annotations
 
@@ -32,6 +33,22 @@ def _mix(seed: int = 11) -> synth.ReadSet:
     return rs
 
 
+def _names(seed: int = 23) -> synth.ReadSet:
+    """Affine workload reads under shuffled names, 3 % of them repeating another
+    read's name (such reads never align to each other: the self-hit test compares
+    names) and 1 % negative (atoi keeps the sign; the .aln prints a query's id as
+    UINT64)."""
+    rs = synth.config2(seed=seed, genome_bp=20000, n_repeats=4)
+    rng = np.random.default_rng(seed + 2000)
+    names = rng.permutation(np.arange(1, rs.n + 1, dtype=np.int64))
+    dup = rng.random(rs.n) < 0.03
+    names[dup] = names[rng.integers(0, rs.n, int(dup.sum()))]
+    neg = rng.random(rs.n) < 0.01
+    names[neg] = -names[neg]
+    rs.names = names
+    return rs
+
+
 # name -> (input generator, reference flags)
 FIXTURES = {
     "c1_20k": (lambda: synth.config1(genome_bp=20000), []),
@@ -46,6 +63,7 @@ FIXTURES = {
     "mix_affine": (_mix, ["-a", "a"]),
     "mix_k21_l60": (_mix, ["-k", "21", "-l", "60"]),
     "mix_i0": (_mix, ["-i", "0", "-m", "4"]),
+    "c2_20k_names": (_names, ["-a", "a"]),
 }
 
 # fixtures whose reference outputs are stored in full (gzipped)

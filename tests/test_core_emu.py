@@ -52,7 +52,7 @@ def test_dp_edge_shapes(oracle, emu):
 
 
 @pytest.mark.parametrize("name", ["c1_20k", "c1_20k_narrow", "mix_affine", "mix_k21_l60",
-                                  "mix_i0"])
+                                  "mix_i0", "c2_20k_names"])
 def test_pipeline_matches_oracle(oracle, emu, name):
     gen, flags = FIXTURES[name]
     rs = upper(gen())
@@ -165,7 +165,7 @@ def test_pair_rows_match_oracle(oracle, emu):
 
 
 @pytest.mark.parametrize("name", ["c1_20k", "c1_20k_affine", "mix", "mix_affine", "mix_i0",
-                                  "mix_k21_l60", "c1_20k_narrow"])
+                                  "mix_k21_l60", "c1_20k_narrow", "c2_20k_names"])
 def test_emulated_alignment_output_matches_reference(emu, name):
     """The device item logic of the alignment-output mode (flipped seeds, the
     query's reverse complement in the DP, the record list, the record text),
