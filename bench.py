@@ -17,7 +17,9 @@ chaining, banded affine DP, record selection, votes and consensus.
           (D2H).
 Multi-GPU (torchrun): each rank corrects its own copy of the job (independent
 jobs, no data-path collective, weak scaling); value = all ranks' bases / the
-slowest rank's time.
+slowest rank's time.  --shard instead splits one job's subject reads over the
+ranks and sums the vote states in one NCCL all-reduce (strong scaling; value =
+the job's bases / the slowest rank's time).
 
 --impl reference times the reference itself (oracle/_ref/hero_ref, built
 from the reference sources) on the host cores, on a bounded sample of the same
@@ -30,6 +32,8 @@ The default line also carries:
                     (Poisson arrivals at 85 % of its closed-loop capacity):
                     p50/p99 job latency, aggregate bases/s, served == alone
   file_e2e          the drop-in program, FASTQ file to .fasta/.info files
+  alignment_output  the same reads without -c: the whole .aln text in host
+                    memory (aligned bases/s)
   cpu_baseline      the reference on the host cores (bounded sample)
 
 Other workloads (--workload): config1 (plain/global, 300 k x 100 bp),
