@@ -33,6 +33,7 @@ struct Params {
     int64_t k, l;
     bool affine, keep_segments;
     bool aln;  // alignment output (no -c): SubjectReadAligner::writeToFile
+    bool merge;  // --merge: overhang votes and paired-read merging
     double mis_rate, indel_rate, thr;
 };
 
@@ -455,6 +456,7 @@ struct Corrector {
     const Reads &S;
     const Table &T;
     std::vector<uint32_t> *votes;  // per query: L*4 (atomic adds)
+    std::vector<uint32_t> *extra = nullptr;  // --merge: per query 20*4 overhang votes
     std::vector<uint64_t> qoff;
     const std::vector<std::string> *qrc = nullptr;  // query reverse complements (alignment output)
 
@@ -722,6 +724,18 @@ struct Corrector {
                     }
                 }
             }
+            // --merge: SubjectRead::updateQueryCoverageConsiderMerging
+            // (SubjectRead.cpp:332-462) votes like the loop above, and a record of
+            // more than one entry also votes the subject bases past its end into
+            // the query's overhang matrix (QueryRead::updateExtraCoverageMatrix,
+            // QueryRead.cpp:352-369: at most 20 columns)
+            if (extra && r.type.size() > 1) {
+                uint32_t *m = &(*extra)[size_t(r.query) * 80];
+                for (int idx = 0; idx < 20 && ps < ss.size(); idx++, ps++) {
+#pragma omp atomic
+                    m[idx * 4 + ((ss[ps] >> 1) & 3)]++;
+                }
+            }
         }
     }
 
@@ -859,6 +873,8 @@ struct hero_oracle_run_s {
     Reads Q;
     std::vector<std::string> qrc;
     std::string aln;  // the .aln file (alignment output)
+    std::vector<uint32_t> extra;    // --merge: overhang votes, 20*4 per query
+    std::vector<uint32_t> merged_len;  // --merge: per pair, length of the merged read (0: not merged)
     std::vector<uint64_t> qoff;
     std::vector<uint32_t> votes;
     std::vector<uint32_t> subj_of_kept;
@@ -870,6 +886,73 @@ struct hero_oracle_run_s {
     std::vector<uint32_t> imin, imed, imax;
     std::vector<double> mis, gc;
 };
+
+// QueryRead::getComplementBase (QueryRead.cpp:375-382): C<->G by bit 2, A<->T by 0x15
+static char complementBase(char c) { return (c & 0x02) ? char(c ^ 0x04) : char(c ^ 0x15); }
+
+// QueryRead::getExtendSequence (QueryRead.cpp:384-403): per overhang column the
+// strictly largest count (first of equals), aDNA letter; stop at a column of zeros
+static std::string extendSequence(const uint32_t *m) {
+    std::string out;
+    for (int i = 0; i < 20; i++) {
+        int id = -1;
+        double largest = 0;
+        for (int j = 0; j < 4; j++) {
+            const double f = double(m[i * 4 + j]);
+            if (largest < f) {
+                largest = f;
+                id = j;
+            }
+        }
+        if (largest < 1) break;
+        out.push_back(ADNA[id]);
+    }
+    return out;
+}
+
+// QueryDataset::mergePairedReads (QueryDataset.cpp:539-558) ->
+// QueryRead::mergingPairedReads (QueryRead.cpp:268-319) on reads (2i, 2i+1), after
+// the consensus.  isGoodRead() is always true (QueryRead.cpp:214-216), so every
+// pair is tried.  The left read grows by the right read's complement bases; the
+// right read becomes empty.
+static void mergePairs(hero_oracle_run_s &run) {
+    const size_t n = run.corrected.size();
+    run.merged_len.assign(n / 2, 0);
+    for (size_t i = 0; i + 1 < n; i += 2) {
+        std::string &left = run.corrected[i];
+        std::string &right = run.corrected[i + 1];
+        const std::string seqL = extendSequence(&run.extra[i * 80]);
+        std::string seqR = extendSequence(&run.extra[(i + 1) * 80]);
+        for (char &c : seqR) c = complementBase(c);  // getExtendComplementSequence
+        const int lenL = int(run.Q.seq[i].size()), lenR = int(run.Q.seq[i + 1].size());
+        int pl = 0;
+        bool match = true;
+        for (; pl < lenL; pl++) {
+            const int old = pl;
+            int pr = lenR - 1;
+            match = true;
+            for (; pr >= 0 && pl < lenL; pr--, pl++) {
+                if (left.at(size_t(pl)) != complementBase(right[size_t(pr)])) {
+                    match = false;
+                    break;
+                }
+            }
+            pl = old;
+            if (match) break;
+        }
+        if (!(match && pl < lenL)) continue;
+        if (int(seqL.size() + seqR.size()) + (lenL - pl) < 40) continue;
+        int mism = 0;
+        for (int a = lenR - lenL + pl - 1, j = 0; a >= 0 && j < int(seqL.size()); j++, a--)
+            if (complementBase(right[size_t(a)]) != seqL.at(size_t(j))) mism++;
+        for (int a = pl - 1, j = 0; a >= 0 && j < int(seqR.size()); j++, a--)
+            if (left.at(size_t(a)) != seqR.at(size_t(j))) mism++;
+        if (mism > 0) continue;
+        for (int a = lenR - lenL + pl - 1; a >= 0; a--) left.push_back(complementBase(right[size_t(a)]));
+        right.clear();
+        run.merged_len[i / 2] = uint32_t(left.size());
+    }
+}
 
 static void load(Reads &r, uint64_t n, const uint8_t *seq, const uint64_t *off,
                  const int64_t *uid) {
@@ -887,6 +970,8 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
                                                 uint64_t ns, const uint8_t *sseq,
                                                 const uint64_t *soff, const int64_t *suid) {
     if (!pp || pp->k <= 0) return nullptr;
+    // --merge pairs reads (i, i+1): with an odd count the reference reads past the end
+    if (pp->merge_pairs && (nq % 2)) return nullptr;
     hero_oracle_run *run = new hero_oracle_run_s();
     Params &p = run->p;
     p.k = pp->k;
@@ -897,6 +982,7 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
     p.indel_rate = pp->indel_rate;
     p.thr = pp->consensus_thr;
     p.aln = pp->aln_mode != 0;
+    p.merge = pp->merge_pairs != 0;
 
     load(run->Q, nq, qseq, qoff, quid);
     Reads S;
@@ -920,6 +1006,10 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
     std::vector<Outputs> outs(nt);
     std::vector<std::vector<uint32_t>> subj_ids(nt);
     Corrector cor(p, run->Q, S, T, &run->votes, run->qoff);
+    if (p.merge) {
+        run->extra.assign(size_t(nq) * 80, 0);
+        cor.extra = &run->extra;
+    }
     if (p.aln) {  // QueryRead::setSequence (QueryRead.cpp:36-43) without -c
         run->qrc.resize(nq);
         for (uint64_t i = 0; i < nq; i++) run->qrc[i] = revcomp(run->Q.seq[i]);
@@ -1036,6 +1126,7 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
             run->imed[q] = sums[(L - 1) / 2];
         }
     }
+    if (p.merge) mergePairs(*run);
     return run;
 }
 
@@ -1057,6 +1148,20 @@ extern "C" void hero_oracle_consensus(const hero_oracle_run *r, uint8_t *seq_out
         if (gc) gc[q] = r->gc[q];
         if (good) good[q] = r->Q.good[q];
     }
+}
+
+extern "C" void hero_oracle_merged(const hero_oracle_run *r, uint8_t *seq_out, uint32_t *merged_len) {
+    for (size_t p = 0; p < r->merged_len.size(); p++) {
+        merged_len[p] = r->merged_len[p];
+        const std::string &a = r->corrected[2 * p], &b = r->corrected[2 * p + 1];
+        uint8_t *o = seq_out + r->qoff[2 * p];
+        std::memcpy(o, a.data(), a.size());
+        if (!r->merged_len[p]) std::memcpy(seq_out + r->qoff[2 * p + 1], b.data(), b.size());
+    }
+}
+
+extern "C" void hero_oracle_overhang(const hero_oracle_run *r, uint32_t *out) {
+    std::memcpy(out, r->extra.data(), r->extra.size() * sizeof(uint32_t));
 }
 
 extern "C" uint64_t hero_oracle_aln_size(const hero_oracle_run *r) { return r->aln.size(); }

@@ -29,6 +29,8 @@ typedef struct {
     double indel_rate;      /* Config::dMaxIndelRate = atof(-i)/100 (default 1) */
     double consensus_thr;   /* Config::dMinFrequencyCallConsensus (default 0.6) */
     int32_t aln_mode;       /* 1 = alignment output (no -c): the .aln file, no votes */
+    int32_t merge_pairs;    /* 1 = --merge: overhang votes, reads (2i, 2i+1) merged after
+                               the consensus (an odd read count is refused) */
 } hero_oracle_params;
 
 typedef struct {
@@ -73,6 +75,14 @@ void hero_oracle_consensus(const hero_oracle_run *r, uint8_t *seq_out, uint32_t 
  * AlignmentRecord::getCigar). */
 uint64_t hero_oracle_aln_size(const hero_oracle_run *r);
 void hero_oracle_aln(const hero_oracle_run *r, uint8_t *out);
+
+/* --merge: per read pair p (reads 2p, 2p+1), merged_len[p] = length of the
+ * merged read (0: not merged); seq_out has the query layout with pair p's
+ * merged read written from offset off[2p] (it fits in the pair's bases), else
+ * both corrected reads.  hero_oracle_overhang: the overhang votes, uint32
+ * [reads][20][4]. */
+void hero_oracle_merged(const hero_oracle_run *r, uint8_t *seq_out, uint32_t *merged_len);
+void hero_oracle_overhang(const hero_oracle_run *r, uint32_t *out);
 
 /* Vote matrix after every subject's votes and before the self vote:
  * uint32 [total query bases][4], column index (c>>1)&3 (A,C,T,G). */

@@ -49,6 +49,27 @@ def _names(seed: int = 23) -> synth.ReadSet:
     return rs
 
 
+def _pairs(seed: int = 31) -> synth.ReadSet:
+    """Read pairs for --merge: per fragment of 160-290 bases (either strand of a
+    20 kbp genome) the first 150 bases and the reverse complement of the last
+    150, stored as reads 2i and 2i+1, with 0.5 % substitutions."""
+    rng = np.random.default_rng(seed)
+    g = synth.random_genome(rng, 20000)
+    reads = []
+    for _ in range(2700):
+        flen = int(rng.integers(160, 291))
+        a = int(rng.integers(0, len(g) - flen))
+        frag = g[a:a + flen]
+        if rng.random() < 0.5:
+            frag = synth.revcomp(frag)
+        reads.append(synth.substitute(rng, frag[:150], 0.005))
+        reads.append(synth.substitute(rng, synth.revcomp(frag[flen - 150:]), 0.005))
+    off = np.zeros(len(reads) + 1, np.uint64)
+    off[1:] = np.cumsum([len(r) for r in reads])
+    return synth.ReadSet(np.concatenate(reads).astype(np.uint8), off,
+                         np.arange(1, len(reads) + 1, dtype=np.int64))
+
+
 # name -> (input generator, reference flags)
 FIXTURES = {
     "c1_20k": (lambda: synth.config1(genome_bp=20000), []),
@@ -64,6 +85,14 @@ FIXTURES = {
     "mix_k21_l60": (_mix, ["-k", "21", "-l", "60"]),
     "mix_i0": (_mix, ["-i", "0", "-m", "4"]),
     "c2_20k_names": (_names, ["-a", "a"]),
+}
+
+# --merge fixtures: name -> (input generator, reference flags besides
+# -c --covinfo --merge; paired input, no --singleReads)
+MERGE_FIXTURES = {
+    "merge_pairs": (_pairs, []),
+    "merge_pairs_affine": (_pairs, ["-a", "a"]),
+    "merge_c1_20k": (lambda: synth.config1(genome_bp=20000), []),
 }
 
 # fixtures whose reference outputs are stored in full (gzipped)

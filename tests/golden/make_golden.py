@@ -4,7 +4,9 @@ Runs the unmodified reference (oracle/_ref/hero_ref, built from the reference
 sources by oracle/Makefile) on every fixture input and records md5 sums of the
 input FASTQ, of the reference .fasta/.info (consensus mode, -c) and of its .aln
 (alignment-output mode: the same flags without -c); the .fasta/.info of the
-fixtures in STORED are kept gzipped.  Usage:  python tests/golden/make_golden.py
+fixtures in STORED are kept gzipped.  The MERGE_FIXTURES (paired input) get
+the md5 and size of the reference's _merged.fasta, _unmerged.fasta and .info
+with -c --covinfo --merge.  Usage:  python tests/golden/make_golden.py
 
     python tests/golden/make_golden.py --full NAME...
 
@@ -24,7 +26,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from fixtures import FIXTURES, STORED, aln_flags  # noqa: E402
+from fixtures import FIXTURES, MERGE_FIXTURES, STORED, aln_flags  # noqa: E402
 
 from hero_b200 import synth  # noqa: E402
 
@@ -71,6 +73,26 @@ def run_reference_aln(fq: str, flags: list[str], workdir: str) -> bytes:
         return f.read()
 
 
+def run_reference_merge(fq: str, flags: list[str], workdir: str) -> dict:
+    """--merge (paired input): md5 and size of _merged.fasta, _unmerged.fasta, .info."""
+    out = os.path.join(workdir, "merge")
+    exts = ("_merged.fasta", "_unmerged.fasta", ".info")
+    for e in exts:  # opened in append mode
+        if os.path.exists(out + e):
+            os.remove(out + e)
+    subprocess.run([REF, "-q", fq, "-s", fq, "-c", "--covinfo", "--merge", "-t",
+                    str(os.cpu_count() or 1), "-o", out] + flags,
+                   stdout=subprocess.DEVNULL, check=True)
+    res = {}
+    for e in exts:
+        with open(out + e, "rb") as f:
+            b = f.read()
+        key = e.strip("._").replace(".", "_")
+        res[key + "_md5"] = md5(b)
+        res[key + "_bytes"] = len(b)
+    return res
+
+
 def main_full(names: list[str]):
     import time
     path = os.path.join(HERE, "manifest_full.json")
@@ -115,6 +137,15 @@ def main():
                 for ext, data in ((".fasta.gz", fa), (".info.gz", info)):
                     with gzip.GzipFile(os.path.join(HERE, name + ext), "wb", mtime=0) as g:
                         g.write(data)
+            print(name, manifest[name], flush=True)
+        for name, (gen, flags) in MERGE_FIXTURES.items():
+            rs = gen()
+            fqb = rs.to_fastq()
+            fq = os.path.join(d, "in.fq")
+            with open(fq, "wb") as f:
+                f.write(fqb)
+            manifest[name] = dict(flags=flags, reads=rs.n, fastq_md5=md5(fqb),
+                                  **run_reference_merge(fq, flags, d))
             print(name, manifest[name], flush=True)
     with open(os.path.join(HERE, "manifest.json"), "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)

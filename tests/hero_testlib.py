@@ -42,7 +42,7 @@ class OracleParams(C.Structure):
     _fields_ = [("k", C.c_int32), ("min_overlap", C.c_int32), ("affine", C.c_int32),
                 ("keep_segments", C.c_int32), ("mis_rate", C.c_double),
                 ("indel_rate", C.c_double), ("consensus_thr", C.c_double),
-                ("aln_mode", C.c_int32)]
+                ("aln_mode", C.c_int32), ("merge_pairs", C.c_int32)]
 
 
 class OracleStats(C.Structure):
@@ -80,16 +80,19 @@ class Oracle:
         lib.hero_oracle_aln_size.argtypes = [vp]
         lib.hero_oracle_aln_size.restype = C.c_uint64
         lib.hero_oracle_aln.argtypes = [vp, vp]
+        lib.hero_oracle_merged.argtypes = [vp, vp, vp]
+        lib.hero_oracle_overhang.argtypes = [vp, vp]
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
                 max_mismatch_rate=1.0, max_indel_rate=1.0, consensus_threshold=0.6,
-                keep_segments=False, threads=8, aln=False):
-        """aln=True: the alignment-output mode (no -c); res["aln"] holds the .aln bytes."""
+                keep_segments=False, threads=8, aln=False, merge=False):
+        """aln=True: the alignment-output mode (no -c); res["aln"] holds the .aln bytes.
+        merge=True: --merge; res["merged_seq"], res["merged_len"], res["overhang"]."""
         subj = subjects if subjects is not None else reads
         p = OracleParams(k, min_overlap, 1 if aligner in ("a", "affine") else 0,
                          1 if keep_segments else 0, max_mismatch_rate, max_indel_rate,
-                         consensus_threshold, 1 if aln else 0)
+                         consensus_threshold, 1 if aln else 0, 1 if merge else 0)
         qs, qo, qu = reads.seq, reads.off.astype(np.uint64), reads.names.astype(np.int64)
         ss, so, su = subj.seq, subj.off.astype(np.uint64), subj.names.astype(np.int64)
         h = self.lib.hero_oracle_correct(C.byref(p), threads, reads.n, _vp(qs), _vp(qo), _vp(qu),
@@ -106,6 +109,12 @@ class Oracle:
             cov = np.zeros(nb * 4, np.uint32)
             self.lib.hero_oracle_votes(h, _vp(cov))
             res["votes"] = cov
+            if merge:
+                res["merged_seq"] = np.zeros(nb, np.uint8)
+                res["merged_len"] = np.zeros(n // 2, np.uint32)
+                res["overhang"] = np.zeros(n * 80, np.uint32)
+                self.lib.hero_oracle_merged(h, _vp(res["merged_seq"]), _vp(res["merged_len"]))
+                self.lib.hero_oracle_overhang(h, _vp(res["overhang"]))
             if aln:
                 buf = np.zeros(max(1, self.lib.hero_oracle_aln_size(h)), np.uint8)
                 self.lib.hero_oracle_aln(h, _vp(buf))
@@ -237,6 +246,21 @@ def format_outputs(uid, seq, off, imin, imed, imax, mis, gc):
             int(uid[i]), int(imin[i]), int(imed[i]), int(imax[i]), int(off[i + 1] - off[i]),
             _g(mis[i]), _g(gc[i])))
     return b"".join(fa), b"".join(info)
+
+
+def format_merged(uid, merged_seq, off, merged_len):
+    """QueryDataset::writeQueryOut with --merge (QueryDataset.cpp:417-459): per
+    pair (2p, 2p+1), the merged read into _merged.fasta, else both reads into
+    _unmerged.fasta (isGoodRead() is always true)."""
+    merged, unmerged = [], []
+    for p in range(len(merged_len)):
+        a = int(off[2 * p])
+        if merged_len[p]:
+            merged.append(b">%d\n%s\n" % (int(uid[2 * p]), bytes(merged_seq[a:a + int(merged_len[p])])))
+        else:
+            for r in (2 * p, 2 * p + 1):
+                unmerged.append(b">%d\n%s\n" % (int(uid[r]), bytes(merged_seq[int(off[r]):int(off[r + 1])])))
+    return b"".join(merged), b"".join(unmerged)
 
 
 def _g(x: float) -> bytes:

@@ -5,7 +5,7 @@ import json
 import os
 
 import pytest
-from fixtures import FIXTURES, STORED, aln_flags, params, upper
+from fixtures import FIXTURES, MERGE_FIXTURES, STORED, aln_flags, params, upper
 from hero_testlib import format_outputs
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -43,6 +43,23 @@ def test_oracle_alignment_output_matches_reference(oracle, name):
     r = oracle.correct(upper(gen()), aln=True, **kw)
     assert len(r["aln"]) == m["aln_bytes"]
     assert md5(r["aln"]) == m["aln_md5"]
+
+
+@pytest.mark.parametrize("name", sorted(MERGE_FIXTURES))
+def test_oracle_merge_matches_reference(oracle, name):
+    """--merge on paired input: the reference's _merged.fasta, _unmerged.fasta, .info."""
+    from hero_testlib import format_merged
+    gen, flags = MERGE_FIXTURES[name]
+    rs = gen()
+    m = MANIFEST[name]
+    assert md5(rs.to_fastq()) == m["fastq_md5"], "synthetic generator drifted"
+    r = oracle.correct(upper(rs), merge=True, **params(flags))
+    merged, unmerged = format_merged(rs.names, r["merged_seq"], rs.off, r["merged_len"])
+    _, info = format_outputs(rs.names, r["seq"], rs.off, r["imin"], r["imed"], r["imax"],
+                             r["mismatch_rate"], r["gc"])
+    assert md5(merged) == m["merged_fasta_md5"]
+    assert md5(unmerged) == m["unmerged_fasta_md5"]
+    assert md5(info) == m["info_md5"]
 
 
 def test_quality_filter(oracle):
