@@ -605,6 +605,108 @@ struct AlnText {
     }
 };
 
+// ---------------------------------------------------------------------------
+// --merge: overhang votes and paired-read merging
+// ---------------------------------------------------------------------------
+constexpr int kOverhang = 20;  // QueryRead::iLength4ExtraMatrix (QueryRead.cpp:225)
+
+// Where a kept record ends on its subject, and whether its CIGAR has more than
+// one entry (SubjectRead::updateQueryCoverageConsiderMerging,
+// SubjectRead.cpp:332-462, votes the subject bases past the record's end into
+// the query's overhang matrix only then).  A CIGAR has a single entry exactly
+// when every step is a match (I, D and mismatch letters differ from M), so the
+// DP pieces' totals decide it: sums(piece) gives a piece's DpSum.
+template <class Sums>
+struct OverhangWalk {
+    Sums sums;
+    uint32_t piece = 0;
+    int64_t ps = 0;
+    bool other = false;
+    HERO_HD void begin(int64_t, int64_t, int64_t) {}
+    HERO_HD void position(int64_t p) { ps = p; }
+    HERO_HD void run(uint8_t t, int64_t c) {
+        if (t != OP_M) other = true;
+        if (t != OP_I) ps += c;
+    }
+    HERO_HD void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
+        const DpSum s = sums(piece++);
+        const uint32_t P = uint32_t(s.tot[0]) + s.tot[1] + s.tot[2] + s.tot[3];
+        if (s.tot[OP_M] != P) other = true;
+        ps += int64_t(s.tot[OP_M]) + s.tot[OP_X] + s.tot[OP_D];
+    }
+    HERO_HD bool check(int64_t, int64_t) { return true; }
+    HERO_HD void finish() {}
+};
+
+// QueryRead::getComplementBase (QueryRead.cpp:375-382), on the ASCII letter:
+// bit 2 set (C, G) flips C<->G, else A<->T by xor 0x15
+HERO_HD char complement_char(char c) { return (c & 0x02) ? char(c ^ 0x04) : char(c ^ 0x15); }
+
+// QueryRead::getExtendSequence (QueryRead.cpp:384-403): per overhang column the
+// strictly largest count (the first of equal counts), as an aDNA letter; stops
+// at a column without votes.  Returns the length (at most kOverhang).
+HERO_HD int overhang_letters(const uint32_t *m, char *out) {
+    int n = 0;
+    for (int i = 0; i < kOverhang; i++) {
+        int id = -1;
+        uint32_t best = 0;
+        for (int j = 0; j < 4; j++) {
+            const uint32_t v = m[i * 4 + j];
+            if (best < v) {
+                best = v;
+                id = j;
+            }
+        }
+        if (best < 1) break;
+        out[n++] = code_base(uint8_t(id));
+    }
+    return n;
+}
+
+// QueryRead::mergingPairedReads (QueryRead.cpp:268-319) for one pair after the
+// consensus: left and right are the corrected reads (raw lengths lenL, lenR),
+// extL / extR their overhang votes.  The first left offset at which the whole
+// rest of the left read equals the right read's complement read backwards is
+// the overlap; the pair merges if the overlap plus both extensions reach 40
+// bases and both extensions agree with the other read.  The merged read -- the
+// left read, then the right read's complement bases backwards from where the
+// overlap leaves off -- goes to out (room for lenL + lenR); returns its length,
+// or 0 when the pair does not merge.
+HERO_HD uint32_t merge_pair(const char *left, int lenL, const char *right, int lenR,
+                            const uint32_t *extL, const uint32_t *extR, char *out) {
+    char seqL[kOverhang], seqR[kOverhang];
+    const int nL = overhang_letters(extL, seqL);
+    const int nR = overhang_letters(extR, seqR);
+    for (int i = 0; i < nR; i++) seqR[i] = complement_char(seqR[i]);  // getExtendComplementSequence
+    int pl = 0;
+    bool match = true;
+    for (; pl < lenL; pl++) {
+        const int old = pl;
+        int pr = lenR - 1;
+        match = true;
+        for (; pr >= 0 && pl < lenL; pr--, pl++) {
+            if (left[pl] != complement_char(right[pr])) {
+                match = false;
+                break;
+            }
+        }
+        pl = old;
+        if (match) break;
+    }
+    if (!(match && pl < lenL)) return 0;
+    if (nL + nR + (lenL - pl) < 40) return 0;
+    int mism = 0;
+    for (int a = lenR - lenL + pl - 1, j = 0; a >= 0 && j < nL; j++, a--)
+        if (complement_char(right[a]) != seqL[j]) mism++;
+    for (int a = pl - 1, j = 0; a >= 0 && j < nR; j++, a--)
+        if (left[a] != seqR[j]) mism++;
+    if (mism > 0) return 0;
+    int n = 0;
+    for (int i = 0; i < lenL; i++) out[n++] = left[i];
+    for (int a = lenR - lenL + pl - 1; a >= 0; a--) out[n++] = complement_char(right[a]);
+    return uint32_t(n);
+}
+
 // length of a record's "id,orientation,position," prefix
 HERO_HD uint32_t aln_prefix_len(uint64_t key, uint32_t orient, int64_t pos) {
     return dec_len(key) + 1u + dec_len(orient) + 1u + dec_len_signed(pos) + 1u;

@@ -736,11 +736,14 @@ int64_t emu_align_output(int32_t k, int32_t l, int32_t affine, double mis_rate, 
 }
 
 // whole path, sequentially, through the core item functions
-int emu_correct(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate,
-                double thr, uint64_t nq, const uint8_t *qseq, const uint64_t *qoff,
-                const int64_t *quid, uint8_t *out_seq, uint32_t *imin, uint32_t *imed,
-                uint32_t *imax, double *mis, double *gc, uint32_t *cov_out, uint64_t *counters) {
+// ext: NULL, or the overhang votes of --merge (uint32 [reads][20][4], zeroed here)
+int emu_correct_ext(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate,
+                    double thr, uint64_t nq, const uint8_t *qseq, const uint64_t *qoff,
+                    const int64_t *quid, uint8_t *out_seq, uint32_t *imin, uint32_t *imed,
+                    uint32_t *imax, double *mis, double *gc, uint32_t *cov_out, uint64_t *counters,
+                    uint32_t *ext) {
     Params p{k, l, affine, 0, mis_rate, indel_rate, thr};
+    if (ext) std::memset(ext, 0, size_t(nq) * kOverhang * 4 * sizeof(uint32_t));
     Reads Q;
     load(Q, nq, qseq, qoff, quid, l);
     // table: exact multimap
@@ -872,6 +875,18 @@ int emu_correct(int32_t k, int32_t l, int32_t affine, double mis_rate, double in
                 auto key = [&w](int32_t t) { return w.keys[t]; };
                 walk_chain(p, vt.Lq, vt.Ls, key, int32_t(w.keys.size()), vt);
                 anomalies += vt.anomalies;
+                if (ext) {  // the device's overhang pass over the same record
+                    const SegRec *sr = w.segs.data();
+                    auto sums = [sr](uint32_t i) { return sr[i].sum; };
+                    OverhangWalk<decltype(sums)> ow{sums};
+                    walk_chain(p, vt.Lq, vt.Ls, key, int32_t(w.keys.size()), ow);
+                    uint32_t *m = ext + size_t(w.q) * kOverhang * 4;
+                    for (int64_t i = 0; ow.other && i < kOverhang && ow.ps + i < L; i++) {
+                        const int64_t x = ow.ps + i;
+                        const uint8_t code = w.orient ? uint8_t(c[L - 1 - x] ^ 2u) : c[x];
+                        if (code < 4) m[i * 4 + code]++;
+                    }
+                }
             }
             a = b;
         }
@@ -915,6 +930,37 @@ int emu_correct(int32_t k, int32_t l, int32_t affine, double mis_rate, double in
         counters[2] = kept_total;
         counters[3] = dpseg;
         counters[4] = anomalies;
+    }
+    return 0;
+}
+
+int emu_correct(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate,
+                double thr, uint64_t nq, const uint8_t *qseq, const uint64_t *qoff,
+                const int64_t *quid, uint8_t *out_seq, uint32_t *imin, uint32_t *imed,
+                uint32_t *imax, double *mis, double *gc, uint32_t *cov_out, uint64_t *counters) {
+    return emu_correct_ext(k, l, affine, mis_rate, indel_rate, thr, nq, qseq, qoff, quid, out_seq,
+                           imin, imed, imax, mis, gc, cov_out, counters, nullptr);
+}
+
+// --merge after the emulated correction: merge_pair on reads (2p, 2p+1) of the
+// corrected reads.  merged_seq has the read layout (pair p's merged read from
+// off[2p], else both corrected reads); merged_len[p] = 0 when not merged.
+int emu_merge(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate, double thr,
+              uint64_t nq, const uint8_t *qseq, const uint64_t *qoff, const int64_t *quid,
+              uint8_t *corrected, uint8_t *merged_seq, uint32_t *merged_len, uint32_t *ext) {
+    if (nq % 2) return -1;
+    std::vector<uint32_t> imin(nq), imed(nq), imax(nq);
+    std::vector<double> mis(nq), gc(nq);
+    emu_correct_ext(k, l, affine, mis_rate, indel_rate, thr, nq, qseq, qoff, quid, corrected,
+                    imin.data(), imed.data(), imax.data(), mis.data(), gc.data(), nullptr, nullptr,
+                    ext);
+    std::memcpy(merged_seq, corrected, qoff[nq]);
+    for (uint64_t pr = 0; pr < nq / 2; pr++) {
+        const uint64_t a = qoff[2 * pr], b = qoff[2 * pr + 1], e = qoff[2 * pr + 2];
+        merged_len[pr] = merge_pair(reinterpret_cast<const char *>(corrected + a), int(b - a),
+                                    reinterpret_cast<const char *>(corrected + b), int(e - b),
+                                    ext + 2 * pr * kOverhang * 4, ext + (2 * pr + 1) * kOverhang * 4,
+                                    reinterpret_cast<char *>(merged_seq + a));
     }
     return 0;
 }

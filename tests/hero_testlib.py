@@ -164,7 +164,27 @@ class Emu:
         lib.emu_align_output.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                           C.c_uint64, vp, vp, vp, vp, C.c_uint64])
         lib.emu_align_output.restype = C.c_int64
+        lib.emu_merge.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                   C.c_double, C.c_uint64] + [vp] * 7)
+        lib.emu_merge.restype = C.c_int
         self.lib = lib
+
+    def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
+              max_indel_rate=1.0, consensus_threshold=0.6):
+        """--merge: the corrected reads, the merged pairs and the overhang votes."""
+        n, nb = reads.n, len(reads.seq)
+        res = dict(seq=np.zeros(nb, np.uint8), merged_seq=np.zeros(nb, np.uint8),
+                   merged_len=np.zeros(n // 2, np.uint32), overhang=np.zeros(n * 80, np.uint32))
+        off = reads.off.astype(np.uint64)
+        uid = reads.names.astype(np.int64)
+        rc = self.lib.emu_merge(k, min_overlap, 1 if aligner in ("a", "affine") else 0,
+                                max_mismatch_rate, max_indel_rate, consensus_threshold, n,
+                                _vp(reads.seq), _vp(off), _vp(uid), _vp(res["seq"]),
+                                _vp(res["merged_seq"]), _vp(res["merged_len"]),
+                                _vp(res["overhang"]))
+        if rc != 0:
+            raise ValueError("an odd number of reads cannot be paired")
+        return res
 
     def align_output(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
                      max_indel_rate=1.0, cap=None):

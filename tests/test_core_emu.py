@@ -182,3 +182,25 @@ def test_emulated_alignment_output_matches_reference(emu, name):
     a = emu.align_output(upper(gen()), **kw)
     assert len(a) == m["aln_bytes"]
     assert hashlib.md5(a).hexdigest() == m["aln_md5"]
+
+
+@pytest.mark.parametrize("name", ["merge_pairs", "merge_pairs_affine", "merge_c1_20k"])
+def test_emulated_merge_matches_reference(oracle, emu, name):
+    """--merge through the device item logic (overhang walk, extension letters,
+    pair merge) on the host: the oracle's overhang votes and the reference's
+    _merged.fasta / _unmerged.fasta."""
+    import hashlib
+    import json
+    import os
+    from fixtures import MERGE_FIXTURES
+    from hero_testlib import format_merged
+    m = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                    "manifest.json")))[name]
+    gen, flags = MERGE_FIXTURES[name]
+    rs = gen()
+    got = emu.merge(upper(rs), **params(flags))
+    want = oracle.correct(upper(rs), merge=True, **params(flags))
+    assert np.array_equal(got["overhang"], want["overhang"])
+    merged, unmerged = format_merged(rs.names, got["merged_seq"], rs.off, got["merged_len"])
+    assert hashlib.md5(merged).hexdigest() == m["merged_fasta_md5"]
+    assert hashlib.md5(unmerged).hexdigest() == m["unmerged_fasta_md5"]
