@@ -30,10 +30,12 @@ EXPORTS = [
     "hero_server_get_stats", "hero_job_bytes", "hero_round_admit", "hero_set_dp_tuning",
     "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
     "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
+    "hero_merge_pairs", "hero_get_overhang",
 ]
 
-# hero_params.flags: the alignment-output mode (HERO without -c)
+# hero_params.flags: the alignment-output mode (HERO without -c); --merge
 FLAG_ALIGNMENT_OUTPUT = 1
+FLAG_MERGE_PAIRS = 2
 
 # the autotuner's record (hero_b200.autotune); loaded by every Hero unless told otherwise
 TUNING_PATH = os.path.join(HERE, "tuning.json")
@@ -128,6 +130,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_alignments_size.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_alignments_take.argtypes = [vp, vp, C.c_uint64]
     lib.hero_align_self_range.argtypes = [vp, C.c_uint64, C.c_uint64]
+    lib.hero_merge_pairs.argtypes = [vp, vp, vp]
+    lib.hero_get_overhang.argtypes = [vp, vp]
     lib.hero_votes_words.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_votes_save.argtypes = [vp, vp]
     lib.hero_votes_load.argtypes = [vp, vp]
@@ -184,9 +188,12 @@ class Hero:
                  max_mismatch_rate: float = 1.0, max_indel_rate: float = 1.0,
                  consensus_threshold: float = 0.6, device: int = 0, subject_batch: int = 0,
                  device_memory_budget: int = 0, stream: int | None = None,
-                 tuning: list[dict] | str | None = None, alignment_output: bool = False):
+                 tuning: list[dict] | str | None = None, alignment_output: bool = False,
+                 merge_pairs: bool = False):
         """alignment_output=True: HERO without -c -- the .aln records of every
-        subject (alignments()) instead of votes and a consensus."""
+        subject (alignments()) instead of votes and a consensus.
+        merge_pairs=True: --merge -- overhang votes, then merge_pairs() after
+        the consensus."""
         self.lib = load_library()
         p = HeroParams()
         self.lib.hero_default_params(C.byref(p))
@@ -200,7 +207,8 @@ class Hero:
         p.subject_batch = subject_batch
         p.device_memory_budget = device_memory_budget
         p.stream = stream
-        p.flags = FLAG_ALIGNMENT_OUTPUT if alignment_output else 0
+        p.flags = ((FLAG_ALIGNMENT_OUTPUT if alignment_output else 0) |
+                   (FLAG_MERGE_PAIRS if merge_pairs else 0))
         self.params = p
         h = C.c_void_p()
         rc = self.lib.hero_create(C.byref(p), C.byref(h))
@@ -336,6 +344,23 @@ class Hero:
     def votes_load(self, dev_ptr: int):
         """Replaces the vote state from a device buffer (the shards' sum)."""
         self._check(self.lib.hero_votes_load(self.h, C.c_void_p(dev_ptr)), "votes_load")
+
+    def merge_pairs(self) -> dict:
+        """--merge after the consensus: merged_seq (read layout, pair p's merged read
+        from its first base) and merged_len (per pair, 0 = not merged)."""
+        res = dict(merged_seq=np.empty(max(1, self.nqb), np.uint8),
+                   merged_len=np.empty(max(1, self.nq // 2), np.uint32))
+        self._check(self.lib.hero_merge_pairs(self.h, _ptr(res["merged_seq"]),
+                                              _ptr(res["merged_len"])), "merge_pairs")
+        res["merged_seq"] = res["merged_seq"][:self.nqb]
+        res["merged_len"] = res["merged_len"][:self.nq // 2]
+        return res
+
+    def overhang(self):
+        """--merge: the overhang votes, uint32 [reads * 20 * 4]."""
+        out = np.empty(max(1, self.nq * 80), np.uint32)
+        self._check(self.lib.hero_get_overhang(self.h, _ptr(out)), "overhang")
+        return out[:self.nq * 80]
 
     def alignments(self) -> bytes:
         """The .aln text of every subject aligned since the last call (and drops it)."""

@@ -64,6 +64,10 @@ struct hero_ctx {
     DBuf scan_tmp, counters;
     // alignment output: record lists, text units and the batch's text
     DBuf a_list, a_n, a_roff, a_unit, a_len, a_pre, a_cig, a_uoff, a_text;
+    // --merge: overhang votes per query read, merged pairs
+    DBuf q_ext, m_seq, m_len;
+    bool merge = false;
+    bool consensus_done = false;  // out_seq holds the consensus of the current votes
     std::vector<uint8_t> aln_host;  // .aln text of every subject aligned since the last take
     // index build temporaries (kept between builds)
     DBuf x_cnt, x_koff, x_klo, x_khi, x_kval, x_owner, x_count, x_slot_of, x_start, x_fill, x_tmp;
@@ -99,7 +103,8 @@ struct hero_ctx {
                         &bins, &bin_off, &tb, &bnd, &dp_tasks, &winners, &scan_tmp, &counters, &x_cnt, &x_koff,
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
                         &x_fill, &x_tmp, &q_job, &win_sorted, &win_bins, &a_list, &a_n,
-                        &a_roff, &a_unit, &a_len, &a_pre, &a_cig, &a_uoff, &a_text};
+                        &a_roff, &a_unit, &a_len, &a_pre, &a_cig, &a_uoff, &a_text, &q_ext,
+                        &m_seq, &m_len};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -212,7 +217,9 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
     if (!p || !out) return HERO_E_INPUT;
     *out = nullptr;
     if (p->k < 1 || p->k > 63) return HERO_E_INPUT;
-    if (p->flags & ~HERO_FLAG_ALIGNMENT_OUTPUT) return HERO_E_INPUT;
+    if (p->flags & ~(HERO_FLAG_ALIGNMENT_OUTPUT | HERO_FLAG_MERGE_PAIRS)) return HERO_E_INPUT;
+    if ((p->flags & HERO_FLAG_ALIGNMENT_OUTPUT) && (p->flags & HERO_FLAG_MERGE_PAIRS))
+        return HERO_E_INPUT;  // --merge is part of the consensus mode
     hero_ctx *c = new hero_ctx();
     c->P = *p;
     c->p.k = p->k;
@@ -222,6 +229,7 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
     c->p.indel_rate = p->max_indel_rate;
     c->p.thr = p->consensus_threshold;
     c->p.aln = (p->flags & HERO_FLAG_ALIGNMENT_OUTPUT) ? 1 : 0;
+    c->merge = (p->flags & HERO_FLAG_MERGE_PAIRS) != 0;
     c->dev = p->device;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -319,6 +327,7 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     c->nq = n;
     c->nqb = n ? off[n] : 0;
     c->have_index = false;
+    c->consensus_done = false;
     c->tagged = false;
     HERO_TRY(upload_reads(c, seq, n ? off : nullptr, uid, n, c->q_raw, c->q_code, c->q_off,
                           c->q_len, c->q_uid, &c->q_good, &c->q_sgood, &c->q_gc));
@@ -329,6 +338,10 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     HERO_TRY(c->ensure(c->mdiff, c->nqb * 4, "vote matrix"));
     HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "memset"));
     HERO_TRY(c->cuda(cudaMemsetAsync(c->mdiff.p, 0, c->nqb * 4, c->st), "memset"));
+    if (c->merge) {
+        HERO_TRY(c->ensure(c->q_ext, n * kOverhang * 16, "overhang votes"));
+        if (n) HERO_TRY(c->cuda(cudaMemsetAsync(c->q_ext.p, 0, n * kOverhang * 16, c->st), "memset"));
+    }
     cudaEventRecord(e1, c->st);
     HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "set queries"));
     c->stats.ms_upload += elapsed(e0, e1);
@@ -635,6 +648,9 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
                         P_<uint32_t>(c->win_bins), P_<uint32_t>(c->keys), subj, q,
                         P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums), P_<uint32_t>(c->cov),
                         P_<int32_t>(c->mdiff), ctr, c->st);
+            if (c->merge)
+                launch_vote_overhang(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->keys),
+                                     subj, q, P_<DpSum>(c->sums), P_<uint32_t>(c->q_ext), ctr, c->st);
         }
         if ((r = c->check_launch("record/vote"))) break;
         if (cap) break;
@@ -654,6 +670,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
 }
 
 static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
+    c->consensus_done = false;
     const auto wall0 = std::chrono::steady_clock::now();
     uint64_t B = c->P.subject_batch ? c->P.subject_batch : 131072;
     double ms[6] = {0, 0, 0, 0, 0, 0};
@@ -732,6 +749,7 @@ extern "C" int hero_votes_load(hero_ctx *c, const void *src) {
     if (!src) return c->fail(HERO_E_INPUT, "null vote buffer");
     cudaSetDevice(c->dev);
     const uint8_t *s = static_cast<const uint8_t *>(src);
+    c->consensus_done = false;
     HERO_TRY(c->cuda(cudaMemcpyAsync(c->cov.p, s, c->nqb * 16, cudaMemcpyDeviceToDevice, c->st), "votes load"));
     HERO_TRY(c->cuda(cudaMemcpyAsync(c->mdiff.p, s + c->nqb * 16, c->nqb * 4, cudaMemcpyDeviceToDevice, c->st), "votes load"));
     return c->cuda(cudaStreamSynchronize(c->st), "votes load");
@@ -793,6 +811,7 @@ extern "C" int hero_consensus(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uin
     if (gc_content && n) cudaMemcpyAsync(gc_content, c->q_gc.p, n * 8, cudaMemcpyDeviceToHost, c->st);
     if (good_out && n) cudaMemcpyAsync(good_out, c->q_good.p, n, cudaMemcpyDeviceToHost, c->st);
     HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "consensus"));
+    c->consensus_done = true;
     c->stats.ms_consensus += elapsed(e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -803,8 +822,11 @@ extern "C" int hero_reset_votes(hero_ctx *c) {
     if (!c) return HERO_E_INPUT;
     if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
     cudaSetDevice(c->dev);
+    c->consensus_done = false;
     if (c->nqb) HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "reset votes"));
     if (c->nqb) HERO_TRY(c->cuda(cudaMemsetAsync(c->mdiff.p, 0, c->nqb * 4, c->st), "reset votes"));
+    if (c->merge && c->nq)
+        HERO_TRY(c->cuda(cudaMemsetAsync(c->q_ext.p, 0, c->nq * kOverhang * 16, c->st), "reset votes"));
     return c->cuda(cudaStreamSynchronize(c->st), "reset votes");
 }
 
@@ -821,6 +843,7 @@ static int consensus_device(hero_ctx *c) {
     launch_consensus(c->p, query_view(c), P_<uint32_t>(c->cov), P_<int32_t>(c->mdiff),
                      P_<uint8_t>(c->out_seq), P_<uint32_t>(c->colsum), P_<uint32_t>(c->o_imin),
                      P_<uint32_t>(c->o_imed), P_<uint32_t>(c->o_imax), P_<double>(c->o_mis), c->st);
+    c->consensus_done = true;
     return c->check_launch("consensus");
 }
 
@@ -830,6 +853,8 @@ static int round_body(hero_ctx *c) {
         HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "round: clear votes"));
         HERO_TRY(c->cuda(cudaMemsetAsync(c->mdiff.p, 0, c->nqb * 4, c->st), "round: clear votes"));
     }
+    if (c->merge && c->nq)
+        HERO_TRY(c->cuda(cudaMemsetAsync(c->q_ext.p, 0, c->nq * kOverhang * 16, c->st), "round: clear votes"));
     HERO_TRY(hero_build_index(c));
     ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
                 P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq, job_tags(c)};
@@ -856,6 +881,7 @@ extern "C" int hero_round(hero_ctx *c, uint32_t flags) {
         }
         c->stats.subjects += c->nq;
         c->stats.graph_rounds++;
+        c->consensus_done = true;
         return HERO_OK;
     }
     // eager round: runs the work and records the per-batch plan
@@ -898,6 +924,36 @@ extern "C" int hero_fetch(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uint32_
     if (gc_content && n) cudaMemcpyAsync(gc_content, c->q_gc.p, n * 8, cudaMemcpyDeviceToHost, c->st);
     if (good_out && n) cudaMemcpyAsync(good_out, c->q_good.p, n, cudaMemcpyDeviceToHost, c->st);
     return c->cuda(cudaStreamSynchronize(c->st), "fetch");
+}
+
+extern "C" int hero_merge_pairs(hero_ctx *c, uint8_t *seq_out, uint32_t *merged_len) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->merge) return c->fail(HERO_E_STATE, "the context was not created with HERO_FLAG_MERGE_PAIRS");
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (c->nq % 2) return c->fail(HERO_E_INPUT, "an odd number of reads cannot be paired");
+    if (!c->consensus_done) return c->fail(HERO_E_STATE, "no consensus of the current votes yet");
+    if (c->nq && (!seq_out || !merged_len)) return c->fail(HERO_E_INPUT, "null output buffer");
+    cudaSetDevice(c->dev);
+    const uint64_t np = c->nq / 2;
+    if (!np) return HERO_OK;
+    HERO_TRY(c->ensure(c->m_seq, c->nqb, "merged reads"));
+    HERO_TRY(c->ensure(c->m_len, np * 4, "merged reads"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(c->m_seq.p, c->out_seq.p, c->nqb, cudaMemcpyDeviceToDevice, c->st), "merge"));
+    launch_merge_pairs(np, P_<uint64_t>(c->q_off), P_<uint8_t>(c->out_seq), P_<uint32_t>(c->q_ext),
+                       P_<uint8_t>(c->m_seq), P_<uint32_t>(c->m_len), c->st);
+    HERO_TRY(c->check_launch("merge"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(seq_out, c->m_seq.p, c->nqb, cudaMemcpyDeviceToHost, c->st), "merge"));
+    HERO_TRY(c->cuda(cudaMemcpyAsync(merged_len, c->m_len.p, np * 4, cudaMemcpyDeviceToHost, c->st), "merge"));
+    return c->cuda(cudaStreamSynchronize(c->st), "merge");
+}
+
+extern "C" int hero_get_overhang(hero_ctx *c, uint32_t *out) {
+    if (!c || !out) return HERO_E_INPUT;
+    if (!c->merge) return c->fail(HERO_E_STATE, "the context was not created with HERO_FLAG_MERGE_PAIRS");
+    if (!c->nq) return HERO_OK;
+    cudaSetDevice(c->dev);
+    HERO_TRY(c->cuda(cudaMemcpyAsync(out, c->q_ext.p, c->nq * kOverhang * 16, cudaMemcpyDeviceToHost, c->st), "overhang"));
+    return c->cuda(cudaStreamSynchronize(c->st), "overhang");
 }
 
 extern "C" int hero_alignments_size(hero_ctx *c, uint64_t *bytes) {

@@ -209,6 +209,15 @@ void launch_aln_write(const Params &p, uint64_t nunit, const uint32_t *unit, con
                       ChainArrays ch, const uint32_t *keys, ReadsView subj, ReadsView q,
                       const uint32_t *ops, uint32_t stride, const DpSum *sums,
                       const uint32_t *upre, const uint32_t *ucig, char *text, cudaStream_t st);
+// --merge: overhang votes of the batch's winners (after launch_vote; ext is
+// uint32 [query reads][kOverhang][4]), and the pair merge after the consensus
+void launch_vote_overhang(const Params &p, uint64_t max_winners, ChainArrays ch,
+                          const uint32_t *winners, const uint32_t *keys, ReadsView subj,
+                          ReadsView q, const DpSum *sums, uint32_t *ext,
+                          const unsigned long long *counters, cudaStream_t st);
+void launch_merge_pairs(uint64_t npairs, const uint64_t *off, const uint8_t *corrected,
+                        const uint32_t *ext, uint8_t *merged, uint32_t *merged_len,
+                        cudaStream_t st);
 void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const uint32_t *winners,
                  uint32_t *sorted, uint32_t *win_bins, const uint32_t *keys, ReadsView subj,
                  ReadsView q, const uint32_t *ops, uint32_t stride, const DpSum *sums,

@@ -1760,6 +1760,53 @@ __global__ void k_vote(Params p, const unsigned long long *counters_in, ChainArr
     if (lane_id() == 0 && anomalies) atomicAdd(&counters[C_ANOMALY], anomalies);
 }
 
+// --merge: per kept record, the subject bases past its end voted into the
+// query's overhang matrix (SubjectRead::updateQueryCoverageConsiderMerging,
+// SubjectRead.cpp:332-462; QueryRead::updateExtraCoverageMatrix,
+// QueryRead.cpp:352-369).  A second, light walk of each winner (positions and
+// DP totals only); k_vote is unchanged.
+__global__ void k_vote_overhang(Params p, const unsigned long long *counters_in, ChainArrays ch,
+                                const uint32_t *winners, const uint32_t *keys, ReadsView subj,
+                                ReadsView q, const DpSum *sums, uint32_t *ext) {
+    const uint64_t nw = counters_in[C_WIN];
+    for (uint64_t wi = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; wi < nw;
+         wi += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t ci = winners[wi];
+        const uint32_t s = ch.subj[ci], qid = ch.query[ci];
+        const DpSum *sm = sums + ch.seg_off[ci];
+        auto piece = [sm](uint32_t i) { return sm[i]; };
+        OverhangWalk<decltype(piece)> w{piece};
+        const int64_t Ls = subj.len[s];
+        walk_chain(p, int64_t(q.len[qid]), Ls, KeyAt{keys + ch.key_off[ci]}, int32_t(ch.nkeys[ci]), w);
+        if (!w.other) continue;
+        const uint8_t *sc = subj.code + subj.off[s];
+        const bool rc = ch.orient[ci] != 0;
+        uint32_t *m = ext + uint64_t(qid) * (kOverhang * 4);
+        for (int64_t i = 0; i < kOverhang && w.ps + i < Ls; i++) {
+            const int64_t x = w.ps + i;
+            const uint8_t code = rc ? uint8_t(sc[Ls - 1 - x] ^ 2u) : sc[x];
+            if (code < 4) atomicAdd(&m[i * 4 + code], 1u);
+        }
+    }
+}
+
+// --merge after the consensus: QueryDataset::mergePairedReads (QueryDataset.cpp:
+// 539-558) -> merge_pair on reads (2p, 2p+1), one thread per pair; the merged
+// read is written from the pair's first base in `merged` (a copy of the
+// corrected reads), its length to merged_len[p] (0: not merged)
+__global__ void k_merge_pairs(uint64_t npairs, const uint64_t *off, const uint8_t *corrected,
+                              const uint32_t *ext, uint8_t *merged, uint32_t *merged_len) {
+    for (uint64_t pr = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; pr < npairs;
+         pr += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t a = off[2 * pr], b = off[2 * pr + 1], e = off[2 * pr + 2];
+        merged_len[pr] = merge_pair(reinterpret_cast<const char *>(corrected + a), int(b - a),
+                                    reinterpret_cast<const char *>(corrected + b), int(e - b),
+                                    ext + 2 * pr * (kOverhang * 4),
+                                    ext + (2 * pr + 1) * (kOverhang * 4),
+                                    reinterpret_cast<char *>(merged + a));
+    }
+}
+
 // ---------------------------------------------------------------------------
 // consensus: QueryRead::callConsensus + calculateCoverageStatistic
 // (QueryRead.cpp:148-212); one warp per query read
@@ -2180,6 +2227,25 @@ void launch_vote(const Params &p, uint64_t max_winners, ChainArrays ch, const ui
     counted();
     k_vote<<<grid_1d(max_winners, 128), 128, 0, st>>>(p, counters, ch, sorted, keys, subj, q, ops,
                                                       stride, sums, cov, mdiff, counters);
+}
+
+void launch_vote_overhang(const Params &p, uint64_t max_winners, ChainArrays ch,
+                          const uint32_t *winners, const uint32_t *keys, ReadsView subj,
+                          ReadsView q, const DpSum *sums, uint32_t *ext,
+                          const unsigned long long *counters, cudaStream_t st) {
+    if (!max_winners) return;
+    counted();
+    k_vote_overhang<<<grid_1d(max_winners, 128), 128, 0, st>>>(p, counters, ch, winners, keys, subj,
+                                                               q, sums, ext);
+}
+
+void launch_merge_pairs(uint64_t npairs, const uint64_t *off, const uint8_t *corrected,
+                        const uint32_t *ext, uint8_t *merged, uint32_t *merged_len,
+                        cudaStream_t st) {
+    if (!npairs) return;
+    counted();
+    k_merge_pairs<<<grid_1d(npairs, 128), 128, 0, st>>>(npairs, off, corrected, ext, merged,
+                                                        merged_len);
 }
 
 void launch_consensus(const Params &p, ReadsView q, const uint32_t *cov, const int32_t *mdiff,

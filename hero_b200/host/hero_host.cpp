@@ -26,6 +26,8 @@ void Config::help() {
                  "                else <out>.aln (every subject read's alignment records)\n"
                  "  -c [thr]      call the consensus (default threshold 0.6)\n"
                  "  --covinfo     write <out>.info (coverage min/median/max, rates)\n"
+                 "  --merge       with -c: merge read pairs (2i, 2i+1) -> <out>_merged.fasta,\n"
+                 "                <out>_unmerged.fasta instead of <out>.fasta\n"
                  "  --singleReads inputs are unpaired reads\n"
                  "  -k            k-mer length (default 39, at most 63)\n"
                  "  -m / -i       maximum mismatch / indel rate in percent (default 100)\n"
@@ -112,7 +114,9 @@ bool Config::parse(int argc, char **argv) {
         } else if (a == "--batch") {
             if (!next(v)) return false;
             subject_batch = uint32_t(std::strtoul(v.c_str(), nullptr, 10));
-        } else if (a == "-v" || a == "--mapping" || a == "--merge" || a == "--covfilter" ||
+        } else if (a == "--merge") {
+            merge = true;
+        } else if (a == "-v" || a == "--mapping" || a == "--covfilter" ||
                    a == "--suffix" || a == "--size" || a == "--notification") {
             std::cerr << a << ": not part of the path this build replaces\n";
             return false;
@@ -281,7 +285,7 @@ bool QueryDataset::build(const Config &c, std::string *err) {
 // ostream prints it by default (precision 6, the %g conversion).
 bool QueryDataset::write(const Config &c, std::string *err) const {
     const uint64_t n = reads.n();
-    if (!c.single_reads && (n % 2)) {
+    if ((!c.single_reads || c.merge) && (n % 2)) {
         if (err) *err = "an odd number of reads needs --singleReads (the paired writer reads past the end)";
         return false;
     }
@@ -322,7 +326,34 @@ bool QueryDataset::write(const Config &c, std::string *err) const {
             if (!x.empty() && std::fwrite(x.data(), 1, x.size(), f) != x.size()) good = false;
         return std::fclose(f) == 0 && good;
     };
-    if (!put(c.out + ".fasta", fa_parts)) {
+    if (c.merge) {
+        // QueryDataset::writeQueryOut with --merge (QueryDataset.cpp:417-459): a
+        // merged pair goes to _merged.fasta as the left read's id and the merged
+        // read, any other pair to _unmerged.fasta as both reads
+        // (isGoodRead() is always true, QueryRead.cpp:214-216)
+        std::string mg, um;
+        char buf[32];
+        for (uint64_t p = 0; 2 * p + 1 < n; p++) {
+            const uint64_t a = reads.off[2 * p];
+            if (merged_len[p]) {
+                int k = std::snprintf(buf, sizeof(buf), ">%lld\n", static_cast<long long>(reads.uid[2 * p]));
+                mg.append(buf, size_t(k));
+                mg.append(merged.data() + a, merged_len[p]);
+                mg.push_back('\n');
+            } else {
+                for (uint64_t r = 2 * p; r < 2 * p + 2; r++) {
+                    int k = std::snprintf(buf, sizeof(buf), ">%lld\n", static_cast<long long>(reads.uid[r]));
+                    um.append(buf, size_t(k));
+                    um.append(merged.data() + reads.off[r], size_t(reads.off[r + 1] - reads.off[r]));
+                    um.push_back('\n');
+                }
+            }
+        }
+        if (!put(c.out + "_merged.fasta", {mg}) || !put(c.out + "_unmerged.fasta", {um})) {
+            if (err) *err = "cannot write " + c.out + "_merged.fasta / _unmerged.fasta";
+            return false;
+        }
+    } else if (!put(c.out + ".fasta", fa_parts)) {
         if (err) *err = "cannot write " + c.out + ".fasta";
         return false;
     }
@@ -378,7 +409,7 @@ bool HashTableGpu::createHashTables(const Config &c, QueryDataset *q, std::strin
     p.consensus_threshold = c.consensus_thr;
     p.device = c.device;
     p.subject_batch = c.subject_batch;
-    p.flags = c.consensus ? 0u : HERO_FLAG_ALIGNMENT_OUTPUT;
+    p.flags = c.consensus ? (c.merge ? HERO_FLAG_MERGE_PAIRS : 0u) : HERO_FLAG_ALIGNMENT_OUTPUT;
     if (!ok(nullptr, hero_create(&p, &ctx), "hero_create", err)) return false;
     const ReadSet &r = q->reads;
     return ok(ctx, hero_set_queries(ctx, reinterpret_cast<const uint8_t *>(r.seq.data()),
@@ -450,6 +481,14 @@ bool call_consensus(HashTableGpu &t, QueryDataset &q, std::string *err) {
                                     q.imin.data(), q.imed.data(), q.imax.data(),
                                     q.mismatch_rate.data(), q.gc.data(), nullptr),
               "hero_consensus", err);
+}
+
+bool merge_pairs(HashTableGpu &t, QueryDataset &q, std::string *err) {
+    q.merged.assign(q.reads.seq.size(), 0);
+    q.merged_len.assign(q.reads.n() / 2, 0);
+    return ok(t.ctx, hero_merge_pairs(t.ctx, reinterpret_cast<uint8_t *>(&q.merged[0]),
+                                      q.merged_len.data()),
+              "hero_merge_pairs", err);
 }
 
 }  // namespace herohost

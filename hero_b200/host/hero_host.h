@@ -21,6 +21,7 @@ struct Config {
     int32_t k = 39, min_overlap = 40, threads = 1;
     double mis_rate = 1.0, indel_rate = 1.0, consensus_thr = 0.6;
     bool affine = false, consensus = false, covinfo = false, single_reads = false;
+    bool merge = false;  // --merge: paired reads (2i, 2i+1) merged after the consensus
     uint64_t stream_chunk = 400, query_chunk = 800;
     int device = 0;
     uint32_t subject_batch = 0;
@@ -48,6 +49,9 @@ class QueryDataset {
     std::string corrected;
     std::vector<uint32_t> imin, imed, imax;
     std::vector<double> mismatch_rate, gc;
+    // --merge: per pair the merged read (from the pair's first base) and its length
+    std::string merged;
+    std::vector<uint32_t> merged_len;
     bool build(const Config &c, std::string *err);
     // QueryDataset::writeQueryOut (QueryDataset.cpp:414-537): append mode
     bool write(const Config &c, std::string *err) const;
@@ -89,5 +93,8 @@ class SubjectReadAligner {
 
 // QueryDataset::callConsensus (QueryDataset.cpp:393-412) on the device
 bool call_consensus(HashTableGpu &t, QueryDataset &q, std::string *err);
+
+// QueryDataset::mergePairedReads (QueryDataset.cpp:539-558) on the device (--merge)
+bool merge_pairs(HashTableGpu &t, QueryDataset &q, std::string *err);
 
 }  // namespace herohost

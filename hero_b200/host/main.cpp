@@ -44,6 +44,10 @@ int main(int argc, char **argv) {
         std::cerr << "Error: " << err << std::endl;
         return 1;
     }
+    if (cfg.consensus && cfg.merge && !merge_pairs(table, query, &err)) {
+        std::cerr << "Error: " << err << std::endl;
+        return 1;
+    }
     const auto t4 = clk::now();
     if (cfg.consensus && !query.write(cfg, &err)) {
         std::cerr << "Error: " << err << std::endl;

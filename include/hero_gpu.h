@@ -61,6 +61,14 @@ typedef struct hero_ctx hero_ctx;
  * hero_alignments_size / hero_alignments_take return it. */
 #define HERO_FLAG_ALIGNMENT_OUTPUT 1u
 
+/* --merge (consensus mode only): the votes also fill each query read's
+ * overhang matrix -- the subject bases past the end of every kept record of
+ * more than one CIGAR entry, 20 columns (SubjectRead::
+ * updateQueryCoverageConsiderMerging, SubjectRead.cpp:332-462) -- and after the
+ * consensus hero_merge_pairs merges reads (2i, 2i+1) as
+ * QueryDataset::mergePairedReads does (QueryDataset.cpp:539-558). */
+#define HERO_FLAG_MERGE_PAIRS 2u
+
 typedef struct {
     int32_t k;              /* k-mer length, 1..63 (Config::iKmer, -k; default 39) */
     int32_t min_overlap;    /* Config::minimumOverlapLength, -l (default 40) */
@@ -160,6 +168,15 @@ int hero_round(hero_ctx *ctx, uint32_t flags);
 /* Results of the last round (same outputs as hero_consensus). */
 int hero_fetch(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *imed, uint32_t *imax,
                double *mismatch_rate, double *gc_content, uint8_t *good_out);
+
+/* --merge, after hero_consensus (or hero_round): merges every pair of query
+ * reads (2p, 2p+1) (QueryRead::mergingPairedReads, QueryRead.cpp:268-319).
+ * seq_out has the query layout: pair p's merged read is written from the pair's
+ * first base and merged_len[p] is its length; a pair that does not merge keeps
+ * both corrected reads and merged_len[p] = 0.  An odd read count is refused. */
+int hero_merge_pairs(hero_ctx *ctx, uint8_t *seq_out, uint32_t *merged_len);
+/* --merge: the overhang votes, uint32 [query reads][20][4] (A,C,T,G). */
+int hero_get_overhang(hero_ctx *ctx, uint32_t *out);
 
 /* Alignment-output mode: bytes of .aln text held (every subject aligned since the
  * last take, in subject order: ">uniqueId\n", its records
