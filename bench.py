@@ -34,6 +34,8 @@ The default line also carries:
   file_e2e          the drop-in program, FASTQ file to .fasta/.info files
   alignment_output  the same reads without -c: the whole .aln text in host
                     memory (aligned bases/s)
+  merge             -c --merge on paired reads of the same size (corrected and
+                    merged bases/s)
   cpu_baseline      the reference on the host cores (bounded sample)
 
 Other workloads (--workload): config1 (plain/global, 300 k x 100 bp),
@@ -86,6 +88,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-alignment-output", action="store_true",
                     help="skip the alignment-output (.aln) line")
+    ap.add_argument("--no-merge", action="store_true", help="skip the --merge line")
     ap.add_argument("--shard", action="store_true",
                     help="one job split across the ranks by subject reads (strong scaling; "
                          "votes summed by one NCCL all-reduce) instead of one job per rank")
@@ -570,6 +573,9 @@ def bench_hero(args):
     aln = None
     if rank == 0 and world == 1 and not args.profile and not args.no_alignment_output:
         aln = measure_alignment_output(rs, kw, dev)
+    merge = None
+    if rank == 0 and world == 1 and not args.profile and not args.no_merge:
+        merge = measure_merge(dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -613,6 +619,7 @@ def bench_hero(args):
                               "dp_segments": (s1["dp_segments"] - s0["dp_segments"]) // steps},
             "served": served,
             "alignment_output": aln,
+            "merge": merge,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -746,6 +753,31 @@ def bench_sharded(args):
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def measure_merge(dev):
+    """-c --merge on paired reads of the same size as the main workload (5 Mbp
+    genome, fragments 160-290 bases read from both ends, 150 bp, 50x, 0.5 %
+    substitutions): host reads in, corrected and merged reads out; wall time of
+    the second of two runs (table, seeding, DP, votes with overhang votes,
+    consensus, pair merge, copies)."""
+    from hero_b200 import Hero, synth
+    rs = synth.paired()
+    walls = []
+    with Hero(aligner="affine", device=dev, merge_pairs=True) as h:
+        for _ in range(2):
+            t0 = time.perf_counter()
+            h.set_queries(rs.seq, rs.off, rs.names)
+            h.build_index()
+            h.align_self()
+            h.consensus()
+            mg = h.merge_pairs()
+            walls.append(time.perf_counter() - t0)
+    return {"metric": "corrected and merged bases/s (-c --merge, paired reads)",
+            "value": rs.total_bases / walls[-1], "unit": "bases/s", "seconds": walls[-1],
+            "reads": rs.n, "pairs_merged": int((mg["merged_len"] > 0).sum()),
+            "workload": "5 Mbp genome, fragments U{160..290} read from both ends, 150 bp, "
+                        "50x, 0.5 % substitutions, affine"}
 
 
 def main():

@@ -297,6 +297,34 @@ def config5(seed: int = 5, genome_bp: int = 100_000_000, coverage: float = 30.0,
     return rs
 
 
+def paired(seed: int = 6, genome_bp: int = 5_000_000, coverage: float = 50.0,
+           read_len: int = 150, frag_min: int = 160, frag_max: int = 290,
+           sub_rate: float = 0.005) -> ReadSet:
+    """Read pairs for --merge: per fragment (length U{frag_min..frag_max}, either
+    strand) its first read_len bases and the reverse complement of its last
+    read_len, stored as reads 2i and 2i+1, with iid substitutions."""
+    rng = np.random.default_rng(seed)
+    g = random_genome(rng, genome_bp)
+    npairs = max(1, int(coverage * genome_bp / (2 * read_len)))
+    flen = rng.integers(frag_min, frag_max + 1, size=npairs)
+    start = rng.integers(0, genome_bp - flen)
+    cols = np.arange(read_len)
+    head = g[start[:, None] + cols]                           # forward first bases
+    tail = _COMP[g[(start + flen)[:, None] - 1 - cols]]       # reverse complement of the end
+    flip = rng.random(npairs) < 0.5                          # fragment from the other strand
+    left = np.where(flip[:, None], tail, head)
+    right = np.where(flip[:, None], head, tail)
+    reads = np.empty((2 * npairs, read_len), np.uint8)
+    reads[0::2] = left
+    reads[1::2] = right
+    reads = substitute(rng, reads, sub_rate)
+    off = np.arange(2 * npairs + 1, dtype=np.uint64) * np.uint64(read_len)
+    rs = ReadSet(reads.reshape(-1), off, np.arange(1, 2 * npairs + 1, dtype=np.int64))
+    rs.meta.update(config="paired", genome_bp=genome_bp, coverage=coverage, read_len=read_len,
+                   fragments=(frag_min, frag_max), seed=seed)
+    return rs
+
+
 @dataclass
 class Job:
     """One correction job of the serving stream."""
