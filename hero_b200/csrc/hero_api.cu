@@ -733,6 +733,7 @@ extern "C" int hero_votes_words(hero_ctx *c, uint64_t *words) {
 extern "C" int hero_votes_save(hero_ctx *c, void *dst) {
     if (!c) return HERO_E_INPUT;
     if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (c->merge) return c->fail(HERO_E_STATE, "the overhang votes of --merge are not part of the exchanged state");
     if (!c->nqb) return HERO_OK;
     if (!dst) return c->fail(HERO_E_INPUT, "null vote buffer");
     cudaSetDevice(c->dev);
@@ -745,6 +746,7 @@ extern "C" int hero_votes_save(hero_ctx *c, void *dst) {
 extern "C" int hero_votes_load(hero_ctx *c, const void *src) {
     if (!c) return HERO_E_INPUT;
     if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (c->merge) return c->fail(HERO_E_STATE, "the overhang votes of --merge are not part of the exchanged state");
     if (!c->nqb) return HERO_OK;
     if (!src) return c->fail(HERO_E_INPUT, "null vote buffer");
     cudaSetDevice(c->dev);

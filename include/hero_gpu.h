@@ -138,7 +138,9 @@ int hero_align_self_range(hero_ctx *ctx, uint64_t first, uint64_t count);
  * shards' states (integer addition mod 2^32) is the state of the whole run.
  * hero_votes_save copies it to, and hero_votes_load replaces it from, a
  * buffer in this context's device memory owned by the caller (e.g. the
- * buffer of an NCCL all-reduce); both return once the copy is done. */
+ * buffer of an NCCL all-reduce); both return once the copy is done.  Contexts
+ * created with HERO_FLAG_MERGE_PAIRS refuse both (HERO_E_STATE): their overhang
+ * votes are not part of this state. */
 int hero_votes_words(hero_ctx *ctx, uint64_t *words);
 int hero_votes_save(hero_ctx *ctx, void *dev_dst);
 int hero_votes_load(hero_ctx *ctx, const void *dev_src);
