@@ -673,7 +673,7 @@ struct Corrector {
         }
         if (v.back().key == r.key) {
             better_in_place(v.back(), std::move(r));
-        } else if (largest >= r.query) {
+        } else if (largest >= r.key) {
             for (size_t i = 0; i < v.size(); i++) {
                 if (v[i].key > r.key) break;
                 if (v[i].key == r.key) {
@@ -915,16 +915,13 @@ static std::string extendSequence(const uint32_t *m) {
 // the consensus.  isGoodRead() is always true (QueryRead.cpp:214-216), so every
 // pair is tried.  The left read grows by the right read's complement bases; the
 // right read becomes empty.
-static void mergePairs(hero_oracle_run_s &run) {
-    const size_t n = run.corrected.size();
-    run.merged_len.assign(n / 2, 0);
-    for (size_t i = 0; i + 1 < n; i += 2) {
-        std::string &left = run.corrected[i];
-        std::string &right = run.corrected[i + 1];
-        const std::string seqL = extendSequence(&run.extra[i * 80]);
-        std::string seqR = extendSequence(&run.extra[(i + 1) * 80]);
+// one pair: merges right into left in place (right emptied); returns whether merged
+static bool mergePair(std::string &left, std::string &right, int lenL, int lenR,
+                      const uint32_t *extL, const uint32_t *extR) {
+    {
+        const std::string seqL = extendSequence(extL);
+        std::string seqR = extendSequence(extR);
         for (char &c : seqR) c = complementBase(c);  // getExtendComplementSequence
-        const int lenL = int(run.Q.seq[i].size()), lenR = int(run.Q.seq[i + 1].size());
         int pl = 0;
         bool match = true;
         for (; pl < lenL; pl++) {
@@ -940,17 +937,27 @@ static void mergePairs(hero_oracle_run_s &run) {
             pl = old;
             if (match) break;
         }
-        if (!(match && pl < lenL)) continue;
-        if (int(seqL.size() + seqR.size()) + (lenL - pl) < 40) continue;
+        if (!(match && pl < lenL)) return false;
+        if (int(seqL.size() + seqR.size()) + (lenL - pl) < 40) return false;
         int mism = 0;
         for (int a = lenR - lenL + pl - 1, j = 0; a >= 0 && j < int(seqL.size()); j++, a--)
             if (complementBase(right[size_t(a)]) != seqL.at(size_t(j))) mism++;
         for (int a = pl - 1, j = 0; a >= 0 && j < int(seqR.size()); j++, a--)
             if (left.at(size_t(a)) != seqR.at(size_t(j))) mism++;
-        if (mism > 0) continue;
+        if (mism > 0) return false;
         for (int a = lenR - lenL + pl - 1; a >= 0; a--) left.push_back(complementBase(right[size_t(a)]));
         right.clear();
-        run.merged_len[i / 2] = uint32_t(left.size());
+        return true;
+    }
+}
+
+static void mergePairs(hero_oracle_run_s &run) {
+    const size_t n = run.corrected.size();
+    run.merged_len.assign(n / 2, 0);
+    for (size_t i = 0; i + 1 < n; i += 2) {
+        if (mergePair(run.corrected[i], run.corrected[i + 1], int(run.Q.seq[i].size()),
+                      int(run.Q.seq[i + 1].size()), &run.extra[i * 80], &run.extra[(i + 1) * 80]))
+            run.merged_len[i / 2] = uint32_t(run.corrected[i].size());
     }
 }
 
@@ -1158,6 +1165,34 @@ extern "C" void hero_oracle_merged(const hero_oracle_run *r, uint8_t *seq_out, u
         std::memcpy(o, a.data(), a.size());
         if (!r->merged_len[p]) std::memcpy(seq_out + r->qoff[2 * p + 1], b.data(), b.size());
     }
+}
+
+extern "C" int hero_oracle_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *right,
+                                      int32_t lenR, const uint32_t *extL, const uint32_t *extR,
+                                      uint8_t *out) {
+    std::string l(reinterpret_cast<const char *>(left), size_t(lenL));
+    std::string r(reinterpret_cast<const char *>(right), size_t(lenR));
+    if (!mergePair(l, r, lenL, lenR, extL, extR)) return 0;
+    std::memcpy(out, l.data(), l.size());
+    return int(l.size());
+}
+
+extern "C" int32_t hero_oracle_record_list(uint32_t n, const uint64_t *key, const double *rate_sum,
+                                           const double *len, uint32_t *out) {
+    // SubjectRead::addAlignment's list over records 0..n-1 in arrival order
+    std::vector<Record> v;
+    uint64_t largest = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        Record r;
+        r.query = i;
+        r.key = key[i];
+        r.mis_rate = rate_sum[i];
+        r.indel_rate = 0;
+        r.len = len[i];
+        Corrector::addAlignment(v, largest, std::move(r));
+    }
+    for (size_t i = 0; i < v.size(); i++) out[i] = v[i].query;
+    return int32_t(v.size());
 }
 
 extern "C" void hero_oracle_overhang(const hero_oracle_run *r, uint32_t *out) {

@@ -84,6 +84,16 @@ void hero_oracle_aln(const hero_oracle_run *r, uint8_t *out);
 void hero_oracle_merged(const hero_oracle_run *r, uint8_t *seq_out, uint32_t *merged_len);
 void hero_oracle_overhang(const hero_oracle_run *r, uint32_t *out);
 
+/* Item checks: QueryRead::mergingPairedReads on one pair (extL / extR: 20x4
+ * overhang votes; out: room for lenL + lenR; returns the merged length or 0),
+ * and SubjectRead::addAlignment's list over n records in arrival order (keys =
+ * query uniqueIds, rate sums, lengths; out: the kept record indices in list
+ * order; returns their count). */
+int hero_oracle_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *right, int32_t lenR,
+                           const uint32_t *extL, const uint32_t *extR, uint8_t *out);
+int32_t hero_oracle_record_list(uint32_t n, const uint64_t *key, const double *rate_sum,
+                                const double *len, uint32_t *out);
+
 /* Vote matrix after every subject's votes and before the self vote:
  * uint32 [total query bases][4], column index (c>>1)&3 (A,C,T,G). */
 void hero_oracle_votes(const hero_oracle_run *r, uint32_t *cov);

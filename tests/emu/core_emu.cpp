@@ -942,6 +942,32 @@ int emu_correct(int32_t k, int32_t l, int32_t affine, double mis_rate, double in
                            imin, imed, imax, mis, gc, cov_out, counters, nullptr);
 }
 
+// item checks of the shared core: merge_pair on one pair, and list_add over
+// records in arrival order (record_better as the comparison)
+int emu_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *right, int32_t lenR,
+                   const uint32_t *extL, const uint32_t *extR, uint8_t *out) {
+    return int(merge_pair(reinterpret_cast<const char *>(left), lenL,
+                          reinterpret_cast<const char *>(right), lenR, extL, extR,
+                          reinterpret_cast<char *>(out)));
+}
+
+int32_t emu_record_list(uint32_t n, const uint64_t *key, const double *rate_sum, const double *len,
+                        uint32_t *out) {
+    struct Slots {
+        uint32_t *o;
+        uint32_t get(uint32_t i) const { return o[i]; }
+        void set(uint32_t i, uint32_t x) { o[i] = x; }
+    } list{out};
+    auto k = [key](uint32_t i) { return key[i]; };
+    auto better = [rate_sum, len](uint32_t a, uint32_t b) {
+        return record_better(rate_sum[a], len[a], rate_sum[b], len[b]);
+    };
+    uint32_t m = 0;
+    uint64_t largest = 0;
+    for (uint32_t i = 0; i < n; i++) m = list_add(list, m, largest, i, k, better);
+    return int32_t(m);
+}
+
 // --merge after the emulated correction: merge_pair on reads (2p, 2p+1) of the
 // corrected reads.  merged_seq has the read layout (pair p's merged read from
 // off[2p], else both corrected reads); merged_len[p] = 0 when not merged.

@@ -82,6 +82,10 @@ class Oracle:
         lib.hero_oracle_aln.argtypes = [vp, vp]
         lib.hero_oracle_merged.argtypes = [vp, vp, vp]
         lib.hero_oracle_overhang.argtypes = [vp, vp]
+        lib.hero_oracle_merge_pair.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, vp, vp]
+        lib.hero_oracle_merge_pair.restype = C.c_int
+        lib.hero_oracle_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
+        lib.hero_oracle_record_list.restype = C.c_int32
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -167,6 +171,10 @@ class Emu:
         lib.emu_merge.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
                                    C.c_double, C.c_uint64] + [vp] * 7)
         lib.emu_merge.restype = C.c_int
+        lib.emu_merge_pair.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, vp, vp]
+        lib.emu_merge_pair.restype = C.c_int
+        lib.emu_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
+        lib.emu_record_list.restype = C.c_int32
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
@@ -288,3 +296,25 @@ def _g(x: float) -> bytes:
     if x != x:
         return b"nan" if np.copysign(1.0, x) > 0 else b"-nan"
     return (b"%g" % x)
+
+
+def merge_pair(lib, prefix, left: bytes, right: bytes, extL, extR):
+    """One pair through <prefix>_merge_pair (oracle or emulator): merged bytes or None."""
+    l = np.frombuffer(left, np.uint8).copy()
+    r = np.frombuffer(right, np.uint8).copy()
+    eL = np.ascontiguousarray(extL, np.uint32)
+    eR = np.ascontiguousarray(extR, np.uint32)
+    out = np.zeros(len(l) + len(r) + 1, np.uint8)
+    n = getattr(lib, prefix + "_merge_pair")(_vp(l), len(l), _vp(r), len(r), _vp(eL), _vp(eR),
+                                             _vp(out))
+    return out[:n].tobytes() if n else None
+
+
+def record_list(lib, prefix, key, rate_sum, length):
+    """Record indices kept by SubjectRead::addAlignment's list, in list order."""
+    k = np.ascontiguousarray(key, np.uint64)
+    r = np.ascontiguousarray(rate_sum, np.float64)
+    ln = np.ascontiguousarray(length, np.float64)
+    out = np.zeros(max(1, len(k)), np.uint32)
+    n = getattr(lib, prefix + "_record_list")(len(k), _vp(k), _vp(r), _vp(ln), _vp(out))
+    return out[:n].tolist()

@@ -1,0 +1,64 @@
+"""Randomised differential checks of two items whose rules are subtle, each
+through the shared device logic (hero_core.cuh, host build) and through the
+oracle's independent restatement: the --merge pair merge
+(QueryRead::mergingPairedReads) and the alignment output's record list
+(SubjectRead::addAlignment keyed by query uniqueId)."""
+import numpy as np
+from hero_testlib import merge_pair, record_list
+
+COMP = bytes.maketrans(b"ACGTN", b"TGCAJ")
+
+
+def _ext(rng, seq: bytes, n: int, noise: float):
+    """Overhang votes that spell seq's first n letters (with noise votes)."""
+    m = np.zeros((20, 4), np.uint32)
+    code = {ord("A"): 0, ord("C"): 1, ord("T"): 2, ord("G"): 3}
+    for i in range(min(n, 20, len(seq))):
+        m[i, code.get(seq[i], 0)] += rng.integers(1, 6)
+        if rng.random() < noise:
+            m[i, rng.integers(4)] += rng.integers(1, 6)  # ties and other letters
+    return m.reshape(-1)
+
+
+def test_pair_merge_agrees(oracle, emu):
+    rng = np.random.default_rng(17)
+    bases = np.frombuffer(b"ACGT", np.uint8)
+    merged = 0
+    for t in range(3000):
+        flen = int(rng.integers(60, 320))
+        frag = bases[rng.integers(0, 4, flen)].tobytes()
+        la, lb = int(rng.integers(20, 160)), int(rng.integers(20, 160))
+        left = frag[:la]
+        right = frag[max(0, flen - lb):][::-1].translate(COMP)  # reverse complement of the end
+        if rng.random() < 0.3:  # a substitution somewhere
+            b = bytearray(left if rng.random() < 0.5 else right)
+            if b:
+                b[int(rng.integers(len(b)))] = int(bases[rng.integers(4)])
+            left, right = (bytes(b), right) if len(b) == len(left) and rng.random() < 0.5 else (left, bytes(b) if len(b) == len(right) else right)
+        if rng.random() < 0.05:
+            left = left[:-1] + b"N"
+        # extensions: what lies past each read's end on the fragment (or noise)
+        extL = _ext(rng, frag[la:], int(rng.integers(0, 21)), 0.2)
+        tail = frag[:max(0, flen - lb)][::-1].translate(COMP)
+        extR = _ext(rng, tail, int(rng.integers(0, 21)), 0.2)
+        a = merge_pair(oracle.lib, "hero_oracle", left, right, extL, extR)
+        b = merge_pair(emu.lib, "emu", left, right, extL, extR)
+        assert a == b, (t, left, right)
+        merged += a is not None
+    assert 300 < merged < 2900  # both outcomes are exercised
+
+
+def test_record_list_agrees(oracle, emu):
+    rng = np.random.default_rng(19)
+    for t in range(2000):
+        n = int(rng.integers(0, 40))
+        # few distinct keys in arbitrary order (repeats, descending runs), few rate
+        # values and lengths (ties on both)
+        key = rng.integers(0, 12, n).astype(np.uint64)
+        if rng.random() < 0.3:
+            key = np.sort(key)
+        rate = rng.integers(0, 4, n) / 8.0
+        length = rng.integers(40, 44, n).astype(np.float64)
+        a = record_list(oracle.lib, "hero_oracle", key, rate, length)
+        b = record_list(emu.lib, "emu", key, rate, length)
+        assert a == b, (t, key.tolist(), rate.tolist(), length.tolist())
