@@ -887,6 +887,26 @@ struct hero_oracle_run_s {
     std::vector<double> mis, gc;
 };
 
+// QueryRead::callConsensus per column (QueryRead.cpp:151-177): fractions of the
+// sum in column order, the largest and the one it replaced; the letter is
+// called when their difference reaches the threshold.  Returns the column's
+// row (A,C,T,G) or -1.
+static int consensusColumn(const uint32_t *c, double thr) {
+    int largest_id = -1;
+    double fLargest = 0, fLarger = 0, sum = 0, f;
+    for (int j = 0; j < 4; j++) sum += c[j];
+    for (int j = 0; j < 4; j++) {
+        f = double(c[j]) / sum;
+        if (fLargest < f) {
+            fLarger = fLargest;
+            fLargest = f;
+            largest_id = j;
+        }
+    }
+    if (largest_id >= 0 && fLargest - fLarger >= thr) return largest_id;
+    return -1;
+}
+
 // QueryRead::getComplementBase (QueryRead.cpp:375-382): C<->G by bit 2, A<->T by 0x15
 static char complementBase(char c) { return (c & 0x02) ? char(c ^ 0x04) : char(c ^ 0x15); }
 
@@ -1101,18 +1121,8 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
         std::string &out = run->corrected[q];
         double changed = 0;
         for (size_t i = 0; i < L; i++) {
-            int largest_id = -1;
-            double fLargest = 0, fLarger = 0, sum = 0, f;
-            for (int j = 0; j < 4; j++) sum += m[i * 4 + j];
-            for (int j = 0; j < 4; j++) {
-                f = double(m[i * 4 + j]) / sum;
-                if (fLargest < f) {
-                    fLarger = fLargest;
-                    fLargest = f;
-                    largest_id = j;
-                }
-            }
-            if (fLargest - fLarger >= p.thr) {
+            const int largest_id = consensusColumn(&m[i * 4], p.thr);
+            if (largest_id >= 0) {
                 if (out[i] != ADNA[largest_id]) changed++;
                 out[i] = ADNA[largest_id];
             }
@@ -1175,6 +1185,10 @@ extern "C" int hero_oracle_merge_pair(const uint8_t *left, int32_t lenL, const u
     if (!mergePair(l, r, lenL, lenR, extL, extR)) return 0;
     std::memcpy(out, l.data(), l.size());
     return int(l.size());
+}
+
+extern "C" void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = consensusColumn(counts + 4 * i, thr);
 }
 
 extern "C" int32_t hero_oracle_record_list(uint32_t n, const uint64_t *key, const double *rate_sum,

@@ -93,6 +93,9 @@ int hero_oracle_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *rig
                            const uint32_t *extL, const uint32_t *extR, uint8_t *out);
 int32_t hero_oracle_record_list(uint32_t n, const uint64_t *key, const double *rate_sum,
                                 const double *len, uint32_t *out);
+/* QueryRead::callConsensus on n columns of counts [n][4] (A,C,T,G): the called
+ * row per column, or -1. */
+void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out);
 
 /* Vote matrix after every subject's votes and before the self vote:
  * uint32 [total query bases][4], column index (c>>1)&3 (A,C,T,G). */

@@ -951,6 +951,10 @@ int emu_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *right, int3
                           reinterpret_cast<char *>(out)));
 }
 
+void emu_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = column_consensus(counts + 4 * i, thr);
+}
+
 int32_t emu_record_list(uint32_t n, const uint64_t *key, const double *rate_sum, const double *len,
                         uint32_t *out) {
     struct Slots {

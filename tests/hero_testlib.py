@@ -86,6 +86,7 @@ class Oracle:
         lib.hero_oracle_merge_pair.restype = C.c_int
         lib.hero_oracle_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
         lib.hero_oracle_record_list.restype = C.c_int32
+        lib.hero_oracle_columns.argtypes = [C.c_uint64, vp, C.c_double, vp]
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -175,6 +176,7 @@ class Emu:
         lib.emu_merge_pair.restype = C.c_int
         lib.emu_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
         lib.emu_record_list.restype = C.c_int32
+        lib.emu_columns.argtypes = [C.c_uint64, vp, C.c_double, vp]
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
@@ -318,3 +320,11 @@ def record_list(lib, prefix, key, rate_sum, length):
     out = np.zeros(max(1, len(k)), np.uint32)
     n = getattr(lib, prefix + "_record_list")(len(k), _vp(k), _vp(r), _vp(ln), _vp(out))
     return out[:n].tolist()
+
+
+def columns(lib, prefix, counts, thr):
+    """Called row per consensus column (counts [n][4], A,C,T,G), -1 where none."""
+    c = np.ascontiguousarray(counts, np.uint32)
+    out = np.zeros(max(1, len(c)), np.int32)
+    getattr(lib, prefix + "_columns")(len(c), _vp(c), float(thr), _vp(out))
+    return out[:len(c)]

@@ -1,10 +1,11 @@
-"""Randomised differential checks of two items whose rules are subtle, each
-through the shared device logic (hero_core.cuh, host build) and through the
-oracle's independent restatement: the --merge pair merge
-(QueryRead::mergingPairedReads) and the alignment output's record list
-(SubjectRead::addAlignment keyed by query uniqueId)."""
+"""Randomised differential checks of items whose rules are subtle, each through
+the shared device logic (hero_core.cuh, host build) and through the oracle's
+independent restatement: the --merge pair merge (QueryRead::mergingPairedReads),
+the alignment output's record list (SubjectRead::addAlignment keyed by query
+uniqueId) and the consensus call of a column (QueryRead::callConsensus, whose
+device form scans integer counts and divides only the two kept ones)."""
 import numpy as np
-from hero_testlib import merge_pair, record_list
+from hero_testlib import columns, merge_pair, record_list
 
 COMP = bytes.maketrans(b"ACGTN", b"TGCAJ")
 
@@ -62,3 +63,24 @@ def test_record_list_agrees(oracle, emu):
         a = record_list(oracle.lib, "hero_oracle", key, rate, length)
         b = record_list(emu.lib, "emu", key, rate, length)
         assert a == b, (t, key.tolist(), rate.tolist(), length.tolist())
+
+
+def test_consensus_columns_agree(oracle, emu):
+    rng = np.random.default_rng(23)
+    parts = [rng.integers(0, 6, (20000, 4)),                      # small counts: ties
+             rng.integers(0, 200, (20000, 4)),
+             rng.integers(0, 2 ** 20, (5000, 4)),                 # deep columns
+             np.array([[0, 0, 0, 0], [1, 0, 0, 0], [3, 2, 0, 0], [2, 2, 1, 0],
+                       [0, 3, 0, 2], [6, 0, 4, 0], [5, 0, 0, 0], [4, 1, 0, 0]])]
+    counts = np.concatenate(parts).astype(np.uint32)
+    # fractions exactly at the threshold: a = round(thr * s) + b
+    for s_ in (5, 10, 20, 50, 100, 1000):
+        for thr in (0.6, 0.7, 0.5):
+            a = int(round(thr * s_))
+            counts = np.concatenate([counts, np.array([[a, s_ - a, 0, 0], [0, s_ - a, a, 0]],
+                                                       np.uint32)])
+    for thr in (0.6, 0.7, 0.5, 0.0 + 1e-12, 0.99):
+        a = columns(oracle.lib, "hero_oracle", counts, thr)
+        b = columns(emu.lib, "emu", counts, thr)
+        bad = np.nonzero(a != b)[0]
+        assert bad.size == 0, (thr, counts[bad[:5]].tolist(), a[bad[:5]], b[bad[:5]])
