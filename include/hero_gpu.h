@@ -1,5 +1,6 @@
 /*
- * hero_gpu.h -- C ABI of the B200 read-correction path (HERO consensus mode).
+ * hero_gpu.h -- C ABI of the B200 read-correction path (HERO consensus mode,
+ * its alignment output and paired-read merging).
  *
  * The reference (guo-xuan/Hero) has no plugin or FFI layer: its hot path is a
  * set of C++ classes driven from main.cpp.  These entry points replace the
@@ -24,6 +25,14 @@
  *                         form replayed as a CUDA graph); hero_fetch its results
  *   hero_get_stats        the per-phase timers the reference prints
  *                         (SubjectReadAligner.cpp:635-640) and work counters
+ *   hero_alignments_size / _take
+ *                         SubjectReadAligner::writeToFile of HERO run without -c
+ *                         (SubjectReadAligner.cpp:854-906; HERO_FLAG_ALIGNMENT_OUTPUT)
+ *   hero_merge_pairs      QueryDataset::mergePairedReads of --merge
+ *                         (QueryDataset.cpp:539-558; HERO_FLAG_MERGE_PAIRS)
+ *   hero_align_self_range, hero_votes_save / _load
+ *                         one correction split across devices by subject reads
+ *                         (SubjectReadAligner::start's chunks on several GPUs)
  *
  * Conventions: plain pointers and sizes only; host buffers belong to the
  * caller and are only read during the call.  Every call returns 0 or a
