@@ -1187,6 +1187,25 @@ extern "C" int hero_oracle_merge_pair(const uint8_t *left, int32_t lenL, const u
     return int(l.size());
 }
 
+extern "C" void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
+                                         const int32_t *count, const uint8_t *letter,
+                                         int64_t *out) {
+    // AlignmentRecord::addCigar per event, then calculateScore
+    Record r;
+    for (uint32_t i = 0; i < nev; i++) {
+        const char t = type[i] == HERO_OP_M   ? 'M'
+                       : type[i] == HERO_OP_I ? 'I'
+                       : type[i] == HERO_OP_D ? 'D'
+                                              : char(letter[i]);
+        (void)piece;
+        r.addCigar(count[i], t);
+    }
+    r.calculateScore();
+    out[0] = int64_t(r.nmis);
+    out[1] = int64_t(r.nindel);
+    out[2] = int64_t(r.len);
+}
+
 extern "C" void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = consensusColumn(counts + 4 * i, thr);
 }

@@ -96,6 +96,13 @@ int32_t hero_oracle_record_list(uint32_t n, const uint64_t *key, const double *r
 /* QueryRead::callConsensus on n columns of counts [n][4] (A,C,T,G): the called
  * row per column, or -1. */
 void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out);
+/* AlignmentRecord::calculateScore of a record given as nev events in order:
+ * type (HERO_OP_*), count, and for a mismatch its letter; piece[i] = 0 for a
+ * run outside the DP, else the number of the DP piece the step belongs to
+ * (ignored here: the reference merges every equal neighbour).  out: mismatches,
+ * indels, alignment length. */
+void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
+                              const int32_t *count, const uint8_t *letter, int64_t *out);
 
 /* Vote matrix after every subject's votes and before the self vote:
  * uint32 [total query bases][4], column index (c>>1)&3 (A,C,T,G). */

@@ -951,6 +951,34 @@ int emu_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *right, int3
                           reinterpret_cast<char *>(out)));
 }
 
+// RecState over the same events: runs through add, the steps of each DP piece
+// packed as the kernel packs ops (2 bits each, at the end of the words) and
+// summarised by ops_summary for add_piece
+void emu_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
+                      const int32_t *count, const uint8_t *, int64_t *out) {
+    RecState st;
+    for (uint32_t i = 0; i < nev;) {
+        if (piece[i] == 0) {
+            st.add(type[i], count[i]);
+            i++;
+            continue;
+        }
+        uint32_t j = i;
+        while (j < nev && piece[j] == piece[i]) j++;
+        const uint32_t P = j - i, words = (P + 15) / 16 + 1, first = words * 16 - P;
+        std::vector<uint32_t> w(words, 0);
+        for (uint32_t k = 0; k < P; k++) {
+            const uint32_t f = first + k;
+            w[f >> 4] |= uint32_t(type[i + k]) << (2 * (f & 15));
+        }
+        DpSum sum;
+        ops_summary(w.data(), first, P, sum);
+        st.add_piece(sum);
+        i = j;
+    }
+    st.score(out[0], out[1], out[2]);
+}
+
 void emu_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = column_consensus(counts + 4 * i, thr);
 }

@@ -87,6 +87,7 @@ class Oracle:
         lib.hero_oracle_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
         lib.hero_oracle_record_list.restype = C.c_int32
         lib.hero_oracle_columns.argtypes = [C.c_uint64, vp, C.c_double, vp]
+        lib.hero_oracle_record_score.argtypes = [C.c_uint32, vp, vp, vp, vp, vp]
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -177,6 +178,7 @@ class Emu:
         lib.emu_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
         lib.emu_record_list.restype = C.c_int32
         lib.emu_columns.argtypes = [C.c_uint64, vp, C.c_double, vp]
+        lib.emu_record_score.argtypes = [C.c_uint32, vp, vp, vp, vp, vp]
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
@@ -328,3 +330,14 @@ def columns(lib, prefix, counts, thr):
     out = np.zeros(max(1, len(c)), np.int32)
     getattr(lib, prefix + "_columns")(len(c), _vp(c), float(thr), _vp(out))
     return out[:len(c)]
+
+
+def record_score(lib, prefix, piece, typ, count, letter):
+    """(mismatches, indels, length) of a record given as events (see the oracle header)."""
+    pc = np.ascontiguousarray(piece, np.uint32)
+    t = np.ascontiguousarray(typ, np.uint8)
+    c = np.ascontiguousarray(count, np.int32)
+    le = np.ascontiguousarray(letter, np.uint8)
+    out = np.zeros(3, np.int64)
+    getattr(lib, prefix + "_record_score")(len(t), _vp(pc), _vp(t), _vp(c), _vp(le), _vp(out))
+    return tuple(int(x) for x in out)

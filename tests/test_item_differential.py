@@ -2,10 +2,11 @@
 the shared device logic (hero_core.cuh, host build) and through the oracle's
 independent restatement: the --merge pair merge (QueryRead::mergingPairedReads),
 the alignment output's record list (SubjectRead::addAlignment keyed by query
-uniqueId) and the consensus call of a column (QueryRead::callConsensus, whose
+uniqueId), a record's score from its run ends and DP-piece summaries
+(AlignmentRecord::calculateScore) and the consensus call of a column (QueryRead::callConsensus, whose
 device form scans integer counts and divides only the two kept ones)."""
 import numpy as np
-from hero_testlib import columns, merge_pair, record_list
+from hero_testlib import columns, merge_pair, record_list, record_score
 
 COMP = bytes.maketrans(b"ACGTN", b"TGCAJ")
 
@@ -84,3 +85,31 @@ def test_consensus_columns_agree(oracle, emu):
         b = columns(emu.lib, "emu", counts, thr)
         bad = np.nonzero(a != b)[0]
         assert bad.size == 0, (thr, counts[bad[:5]].tolist(), a[bad[:5]], b[bad[:5]])
+
+
+def test_record_scores_agree(oracle, emu):
+    """Records as the chain walk builds them: k-mer runs (M, and I / D between
+    keys) and DP pieces of single steps (M, mismatch with a letter, I, D)."""
+    rng = np.random.default_rng(29)
+    letters = np.frombuffer(b"ACGT", np.uint8)
+    for t in range(3000):
+        piece, typ, count, letter = [], [], [], []
+        npc = 0
+        for _ in range(int(rng.integers(1, 7))):
+            if rng.random() < 0.5:  # a run outside the DP
+                piece.append(0)
+                typ.append(int(rng.choice([0, 0, 2, 3])))
+                count.append(int(rng.integers(1, 40)))
+                letter.append(0)
+            else:  # a DP piece: steps with runs of equal ops
+                npc += 1
+                for _ in range(int(rng.integers(1, 6))):
+                    op = int(rng.choice([0, 0, 1, 2, 3]))
+                    for _ in range(int(rng.integers(1, 5))):
+                        piece.append(npc)
+                        typ.append(op)
+                        count.append(1)
+                        letter.append(int(letters[rng.integers(4)]))
+        a = record_score(oracle.lib, "hero_oracle", piece, typ, count, letter)
+        b = record_score(emu.lib, "emu", piece, typ, count, letter)
+        assert a == b, (t, list(zip(piece, typ, count)))
