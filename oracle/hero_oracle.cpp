@@ -1206,6 +1206,41 @@ extern "C" void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, co
     out[2] = int64_t(r.len);
 }
 
+extern "C" int32_t hero_oracle_chain(int32_t k, double indel_rate, uint32_t n, const int64_t *posQ,
+                                     const int64_t *posS, uint32_t *chain_of, uint8_t *kept) {
+    // processOneSubjectRead2's chaining of one query group (hits sorted by posQ,
+    // posS) and markTheBestPossibleAlignment
+    Params p{};
+    p.k = k;
+    p.indel_rate = indel_rate;
+    Reads none;
+    Table t;
+    Corrector cor(p, none, none, t, nullptr, {});
+    std::vector<std::vector<Key>> chains;
+    std::vector<std::vector<uint32_t>> ids;
+    for (uint32_t h = 0; h < n; h++) {
+        const Key x{0, posS[h], posQ[h]};
+        size_t c = 0;
+        for (; c < chains.size(); c++)
+            if (cor.sameAlignment(x, chains[c].front(), chains[c].back())) break;
+        if (c == chains.size()) {
+            chains.push_back({});
+            ids.push_back({});
+        }
+        chains[c].push_back(x);
+        ids[c].push_back(h);
+        chain_of[h] = uint32_t(c);
+    }
+    int64_t best = 0;
+    std::vector<int64_t> kl(chains.size());
+    for (size_t c = 0; c < chains.size(); c++) {
+        kl[c] = cor.keyLength(chains[c]);
+        if (kl[c] > best) best = kl[c];
+    }
+    for (size_t c = 0; c < chains.size(); c++) kept[c] = kl[c] == best ? 1 : 0;
+    return int32_t(chains.size());
+}
+
 extern "C" void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = consensusColumn(counts + 4 * i, thr);
 }

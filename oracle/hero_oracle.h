@@ -101,6 +101,11 @@ void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t
  * run outside the DP, else the number of the DP piece the step belongs to
  * (ignored here: the reference merges every equal neighbour).  out: mismatches,
  * indels, alignment length. */
+/* Chaining of one query group: hits sorted by (posQ, posS); chain_of[h] = the
+ * chain of hit h, kept[c] = 1 for the chains of the largest key length (room
+ * for n); returns the number of chains. */
+int32_t hero_oracle_chain(int32_t k, double indel_rate, uint32_t n, const int64_t *posQ,
+                          const int64_t *posS, uint32_t *chain_of, uint8_t *kept);
 void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
                               const int32_t *count, const uint8_t *letter, int64_t *out);
 

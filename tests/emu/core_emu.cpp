@@ -979,6 +979,20 @@ void emu_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
     st.score(out[0], out[1], out[2]);
 }
 
+int32_t emu_chain(int32_t k, double indel_rate, uint32_t n, const int64_t *posQ,
+                  const int64_t *posS, uint32_t *chain_of, uint8_t *kept) {
+    Params p{k, 0, 0, 0, 1.0, indel_rate, 0.6};
+    std::vector<uint64_t> hits(n);
+    for (uint32_t h = 0; h < n; h++) hits[h] = hit_pack(0, uint32_t(posQ[h]), uint32_t(posS[h]));
+    auto hit = [&hits](int32_t h) { return hits[size_t(h)]; };
+    std::vector<int32_t> first(n + 1), last(n + 1), prev(n + 1);
+    std::vector<int64_t> kl(n + 1);
+    const int32_t nch = chain_group(p, hit, int32_t(n), chain_of, first.data(), last.data());
+    const int64_t best = chain_key_lengths(p, hit, int32_t(n), chain_of, nch, kl.data(), prev.data());
+    for (int32_t c = 0; c < nch; c++) kept[c] = kl[size_t(c)] == best ? 1 : 0;
+    return nch;
+}
+
 void emu_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = column_consensus(counts + 4 * i, thr);
 }

@@ -88,6 +88,8 @@ class Oracle:
         lib.hero_oracle_record_list.restype = C.c_int32
         lib.hero_oracle_columns.argtypes = [C.c_uint64, vp, C.c_double, vp]
         lib.hero_oracle_record_score.argtypes = [C.c_uint32, vp, vp, vp, vp, vp]
+        lib.hero_oracle_chain.argtypes = [C.c_int32, C.c_double, C.c_uint32, vp, vp, vp, vp]
+        lib.hero_oracle_chain.restype = C.c_int32
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -179,6 +181,8 @@ class Emu:
         lib.emu_record_list.restype = C.c_int32
         lib.emu_columns.argtypes = [C.c_uint64, vp, C.c_double, vp]
         lib.emu_record_score.argtypes = [C.c_uint32, vp, vp, vp, vp, vp]
+        lib.emu_chain.argtypes = [C.c_int32, C.c_double, C.c_uint32, vp, vp, vp, vp]
+        lib.emu_chain.restype = C.c_int32
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
@@ -341,3 +345,14 @@ def record_score(lib, prefix, piece, typ, count, letter):
     out = np.zeros(3, np.int64)
     getattr(lib, prefix + "_record_score")(len(t), _vp(pc), _vp(t), _vp(c), _vp(le), _vp(out))
     return tuple(int(x) for x in out)
+
+
+def chain(lib, prefix, k, indel_rate, posQ, posS):
+    """Chain of each hit and the kept chains of one query group (hits sorted)."""
+    q = np.ascontiguousarray(posQ, np.int64)
+    s_ = np.ascontiguousarray(posS, np.int64)
+    chain_of = np.zeros(max(1, len(q)), np.uint32)
+    kept = np.zeros(max(1, len(q)), np.uint8)
+    nch = getattr(lib, prefix + "_chain")(k, float(indel_rate), len(q), _vp(q), _vp(s_),
+                                          _vp(chain_of), _vp(kept))
+    return chain_of[:len(q)].tolist(), kept[:nch].tolist()

@@ -3,10 +3,12 @@ the shared device logic (hero_core.cuh, host build) and through the oracle's
 independent restatement: the --merge pair merge (QueryRead::mergingPairedReads),
 the alignment output's record list (SubjectRead::addAlignment keyed by query
 uniqueId), a record's score from its run ends and DP-piece summaries
-(AlignmentRecord::calculateScore) and the consensus call of a column (QueryRead::callConsensus, whose
+(AlignmentRecord::calculateScore), the chaining of a query group
+(isFromTheSameAlignment's ratio test, markTheBestPossibleAlignment) and the
+consensus call of a column (QueryRead::callConsensus, whose
 device form scans integer counts and divides only the two kept ones)."""
 import numpy as np
-from hero_testlib import columns, merge_pair, record_list, record_score
+from hero_testlib import chain, columns, merge_pair, record_list, record_score
 
 COMP = bytes.maketrans(b"ACGTN", b"TGCAJ")
 
@@ -113,3 +115,26 @@ def test_record_scores_agree(oracle, emu):
         a = record_score(oracle.lib, "hero_oracle", piece, typ, count, letter)
         b = record_score(emu.lib, "emu", piece, typ, count, letter)
         assert a == b, (t, list(zip(piece, typ, count)))
+
+
+def test_chaining_agrees(oracle, emu):
+    """Groups of hits sorted by (posQ, posS); indel rates include ratios that a
+    candidate hit meets exactly (the test is a strict >)."""
+    rng = np.random.default_rng(31)
+    for t in range(3000):
+        k = int(rng.choice([21, 31, 39]))
+        n = int(rng.integers(1, 25))
+        q = rng.integers(0, 120, n)
+        d = rng.integers(-6, 7, n) * (rng.random(n) < 0.5)  # near-diagonal and off-diagonal hits
+        s_ = np.clip(q + 10 + d + rng.integers(0, 3, n) * 40, 0, 300)
+        order = np.lexsort((s_, q))
+        q, s_ = q[order], s_[order]
+        if rng.random() < 0.5:  # a ratio some pair meets exactly
+            i, j = sorted(rng.choice(n, 2)) if n > 1 else (0, 0)
+            lq, ls = abs(int(q[j]) - int(q[i])), abs(int(s_[j]) - int(s_[i]))
+            rate = abs(lq - ls) / (max(lq, ls) + k)
+        else:
+            rate = float(rng.choice([0.0, 0.01, 0.02, 0.05, 0.2, 1.0]))
+        a = chain(oracle.lib, "hero_oracle", k, rate, q, s_)
+        b = chain(emu.lib, "emu", k, rate, q, s_)
+        assert a == b, (t, k, rate, q.tolist(), s_.tolist())
