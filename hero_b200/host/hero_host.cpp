@@ -1,6 +1,11 @@
 // hero_host.cpp -- host side of the drop-in (see hero_host.h).
 #include "hero_host.h"
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <cctype>
 #include <chrono>
 #include <cstdio>
@@ -164,68 +169,138 @@ static void parallel_ranges(uint64_t n, Fn fn) {
     for (std::thread &x : th) x.join();
 }
 
-// One pass finds each record's name line and sequence span (the reference's
-// line rules: QueryDataset.cpp:246-391); threads then parse the ids, count and
-// copy the uppercased bases into place.
+// The file is mapped, not copied.  FASTQ: a record is four lines (the
+// reference reads them with four getline calls, QueryDataset.cpp:246-391), so
+// the threads count the line breaks of their slices, a scan numbers the lines,
+// and record r is lines 4r..4r+3; FASTA: one pass from '>' to '>'.  Threads then
+// parse the ids and copy the uppercased bases into place.
+namespace {
+
+struct Mapped {
+    const char *d = nullptr;
+    size_t n = 0;
+    int fd = -1;
+    ~Mapped() {
+        if (d && n) munmap(const_cast<char *>(d), n);
+        if (fd >= 0) close(fd);
+    }
+};
+
+char upper_ascii(char c) { return (c >= 'a' && c <= 'z') ? char(c - 32) : c; }
+
+}  // namespace
+
 bool load_reads(const std::string &path, ReadSet &out, std::string *err) {
-    std::FILE *fp = std::fopen(path.c_str(), "rb");
-    if (!fp) {
+    Mapped m;
+    m.fd = open(path.c_str(), O_RDONLY);
+    if (m.fd < 0) {
         if (err) *err = "Unable to open file: " + path;
         return false;
     }
-    std::string data;
-    if (std::fseek(fp, 0, SEEK_END) == 0) {
-        const long sz = std::ftell(fp);
-        if (sz > 0) {
-            data.resize(size_t(sz));
-            std::rewind(fp);
-            data.resize(std::fread(&data[0], 1, size_t(sz), fp));
-        }
+    struct stat st;
+    if (fstat(m.fd, &st) != 0) {
+        if (err) *err = "Unable to open file: " + path;
+        return false;
     }
-    std::fclose(fp);
-    if (data.empty()) return true;
-    const bool fasta = data[0] == '>';
-    if (!fasta && data[0] != '@') {
+    m.n = size_t(st.st_size);
+    if (m.n == 0) return true;
+    void *mp = mmap(nullptr, m.n, PROT_READ, MAP_PRIVATE, m.fd, 0);
+    if (mp == MAP_FAILED) {
+        m.n = 0;
+        if (err) *err = "Unable to map file: " + path;
+        return false;
+    }
+    m.d = static_cast<const char *>(mp);
+    madvise(mp, m.n, MADV_SEQUENTIAL | MADV_WILLNEED);
+    const char *d = m.d;
+    const size_t n = m.n;
+    const bool fasta = d[0] == '>';
+    if (!fasta && d[0] != '@') {
         if (err) *err = "Unknown input file format: " + path;
         return false;
     }
     struct Rec {
-        size_t name, nlen, seq, slen;  // spans in data; FASTA sequences may hold newlines
+        size_t name, nlen, seq, slen;  // spans in the file; FASTA sequences may hold newlines
     };
     std::vector<Rec> recs;
-    recs.reserve(data.size() / 256 + 16);
-    size_t p = 0;
-    const size_t n = data.size();
-    const char *d = data.data();
-    auto line = [&](size_t &b, size_t &len) -> bool {
-        if (p >= n) return false;
-        const void *q = std::memchr(d + p, '\n', n - p);
-        const size_t e = q ? size_t(static_cast<const char *>(q) - d) : n;
-        b = p;
-        len = e - p;
-        p = e < n ? e + 1 : n;
-        return true;
-    };
     if (!fasta) {
-        size_t b0, n0, b1, n1, b2, n2, b3, n3;
-        while (line(b0, n0)) {
-            if (!line(b1, n1)) {
+        // line starts, numbered across the slices of the threads
+        const unsigned T = n < (1u << 20) ? 1 : host_threads();
+        std::vector<uint64_t> cnt(T + 1, 0);
+        auto slice = [&](unsigned t, size_t &a, size_t &b) {
+            a = n * t / T;
+            b = n * (t + 1) / T;
+        };
+        auto each_break = [&](size_t a, size_t b, auto fn) {
+            const char *q = d + a;
+            const char *e = d + b;
+            while (q < e) {
+                const void *h = std::memchr(q, '\n', size_t(e - q));
+                if (!h) break;
+                const char *x = static_cast<const char *>(h);
+                fn(size_t(x - d));
+                q = x + 1;
+            }
+        };
+        auto run = [&](auto fn) {
+            if (T == 1) {
+                fn(0u);
+                return;
+            }
+            std::vector<std::thread> th;
+            for (unsigned t = 0; t < T; t++) th.emplace_back(fn, t);
+            for (std::thread &x : th) x.join();
+        };
+        // a line starts at 0 and after every break that is not the last byte
+        run([&](unsigned t) {
+            size_t a, b;
+            slice(t, a, b);
+            uint64_t c = 0;
+            each_break(a, b, [&](size_t i) { c += i + 1 < n; });
+            cnt[t + 1] = c;
+        });
+        for (unsigned t = 0; t < T; t++) cnt[t + 1] += cnt[t];
+        const uint64_t nlines = cnt[T] + 1;
+        std::vector<uint64_t> ls(nlines + 1);
+        ls[0] = 0;
+        run([&](unsigned t) {
+            size_t a, b;
+            slice(t, a, b);
+            uint64_t j = cnt[t] + 1;
+            each_break(a, b, [&](size_t i) {
+                if (i + 1 < n) ls[j++] = i + 1;
+            });
+        });
+        // one past the end of the last line: its break, or the end of the file
+        ls[nlines] = d[n - 1] == '\n' ? n : n + 1;
+        auto span = [&](uint64_t j, size_t &b, size_t &len) {
+            b = size_t(ls[j]);
+            len = size_t(ls[j + 1]) - 1 - b;  // up to the break ending line j
+        };
+        recs.reserve(nlines / 4 + 1);
+        for (uint64_t g = 0; g < nlines; g += 4) {
+            size_t b0, n0, b1, n1;
+            span(g, b0, n0);
+            if (g + 1 >= nlines) {
                 if (n0) {  // a lone header line at the end
                     if (err) *err = "truncated FASTQ record in " + path;
                     return false;
                 }
                 break;
             }
-            line(b2, n2);
-            line(b3, n3);
-            if (!n0 && !n1) continue;  // trailing blank lines
+            span(g + 1, b1, n1);
+            if (!n0 && !n1) continue;  // blank lines
             recs.push_back({b0, n0, b1, n1});
         }
     } else {
+        size_t p = 0;
+        recs.reserve(n / 256 + 16);
         while (p < n) {
-            size_t b0, n0;
-            line(b0, n0);
-            const void *q = std::memchr(d + p, '>', n - p);
+            const void *q0 = std::memchr(d + p, '\n', n - p);
+            const size_t e0 = q0 ? size_t(static_cast<const char *>(q0) - d) : n;
+            const size_t b0 = p, n0 = e0 - p;
+            p = e0 < n ? e0 + 1 : n;
+            const void *q = p < n ? std::memchr(d + p, '>', n - p) : nullptr;
             const size_t e = q ? size_t(static_cast<const char *>(q) - d) : n;
             const size_t b = p;
             p = e < n ? e + 1 : n;
@@ -238,7 +313,8 @@ bool load_reads(const std::string &path, ReadSet &out, std::string *err) {
     std::vector<uint64_t> len(nr);
     out.uid.resize(base_reads + nr);
     parallel_ranges(nr, [&](uint64_t a, uint64_t b) {
-        std::string nm;
+        char nm[64];
+        std::string big;
         for (uint64_t r = a; r < b; r++) {
             const Rec &x = recs[r];
             size_t nb = x.name, nl = x.nlen;
@@ -246,8 +322,16 @@ bool load_reads(const std::string &path, ReadSet &out, std::string *err) {
                 nb++;
                 nl--;
             }
-            nm.assign(d + nb, nl);
-            out.uid[base_reads + r] = int64_t(std::atoi(nm.c_str()));
+            const char *s;
+            if (nl < sizeof(nm)) {
+                std::memcpy(nm, d + nb, nl);
+                nm[nl] = 0;
+                s = nm;
+            } else {
+                big.assign(d + nb, nl);
+                s = big.c_str();
+            }
+            out.uid[base_reads + r] = int64_t(std::atoi(s));
             uint64_t l = x.slen;
             if (fasta) l -= uint64_t(std::count(d + x.seq, d + x.seq + x.slen, '\n'));
             len[r] = l;
@@ -264,10 +348,14 @@ bool load_reads(const std::string &path, ReadSet &out, std::string *err) {
         for (uint64_t r = a; r < b; r++) {
             const Rec &x = recs[r];
             char *o = &out.seq[out.off[base_reads + r]];
+            if (!fasta) {
+                for (size_t i = 0; i < x.slen; i++) o[i] = upper_ascii(d[x.seq + i]);
+                continue;
+            }
             for (size_t i = 0; i < x.slen; i++) {
                 const char c = d[x.seq + i];
-                if (fasta && c == '\n') continue;
-                *o++ = char(std::toupper(static_cast<unsigned char>(c)));
+                if (c == '\n') continue;
+                *o++ = upper_ascii(c);
             }
         }
     });
