@@ -1241,6 +1241,51 @@ extern "C" int32_t hero_oracle_chain(int32_t k, double indel_rate, uint32_t n, c
     return int32_t(chains.size());
 }
 
+extern "C" int32_t hero_oracle_chain_layout(int32_t k, int32_t l, int32_t affine, double mis_rate,
+                                            double indel_rate, const uint8_t *qseq, int32_t Lq,
+                                            const uint8_t *sseq, int32_t Ls, uint32_t nkeys,
+                                            const int64_t *posQ, const int64_t *posS, int64_t *seg,
+                                            int32_t cap, int64_t *pos_out, int32_t *status) {
+    // getAlignment2 on one chain: the DP calls it makes (s0, s1, q0, q1, flags,
+    // band before the call), the record's position and its fate
+    Params p{};
+    p.k = k;
+    p.l = l;
+    p.affine = affine != 0;
+    p.keep_segments = true;
+    p.mis_rate = mis_rate;
+    p.indel_rate = indel_rate;
+    Reads Q;
+    Q.seq.push_back(std::string(reinterpret_cast<const char *>(qseq), size_t(Lq)));
+    Q.uid.push_back(1);
+    Q.good.push_back(1);
+    Table t;
+    Corrector cor(p, Q, Q, t, nullptr, {});
+    std::vector<Key> keys(nkeys);
+    for (uint32_t i = 0; i < nkeys; i++) keys[i] = Key{0, posS[i], posQ[i]};
+    Outputs o;
+    Band b;
+    b.affine = p.affine;
+    Record rec;
+    const std::string S(reinterpret_cast<const char *>(sseq), size_t(Ls));
+    const uint64_t built0 = o.st.records_built;
+    const bool ok = cor.getAlignment2(o, b, 0, S, 0, keys, rec);
+    *status = o.st.records_built == built0 ? 0 : (ok ? 2 : 1);
+    *pos_out = rec.pos;
+    const int32_t n = int32_t(o.segments.size());
+    for (int32_t i = 0; i < n && i < cap; i++) {
+        const Segment &g = o.segments[size_t(i)];
+        int64_t *x = seg + 6 * i;
+        x[0] = g.s0;
+        x[1] = g.s1;
+        x[2] = g.q0;
+        x[3] = g.q1;
+        x[4] = g.flags;
+        x[5] = g.band;
+    }
+    return n;
+}
+
 extern "C" void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = consensusColumn(counts + 4 * i, thr);
 }

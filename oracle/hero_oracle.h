@@ -106,6 +106,16 @@ void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t
  * for n); returns the number of chains. */
 int32_t hero_oracle_chain(int32_t k, double indel_rate, uint32_t n, const int64_t *posQ,
                           const int64_t *posS, uint32_t *chain_of, uint8_t *kept);
+/* getAlignment2 on one chain of keys (posQ, posS) between a query and a
+ * subject (ASCII): the DP calls it makes, 6 values each (s0, s1, q0, q1,
+ * flags 1 = align right / 2 = align left, band before the call; room for
+ * cap), *pos_out the record's position, *status 0 = no record (overlap below
+ * l), 1 = rejected, 2 = accepted.  Returns the number of DP calls. */
+int32_t hero_oracle_chain_layout(int32_t k, int32_t l, int32_t affine, double mis_rate,
+                                 double indel_rate, const uint8_t *qseq, int32_t Lq,
+                                 const uint8_t *sseq, int32_t Ls, uint32_t nkeys,
+                                 const int64_t *posQ, const int64_t *posS, int64_t *seg,
+                                 int32_t cap, int64_t *pos_out, int32_t *status);
 void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
                               const int32_t *count, const uint8_t *letter, int64_t *out);
 

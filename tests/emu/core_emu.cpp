@@ -993,6 +993,58 @@ int32_t emu_chain(int32_t k, double indel_rate, uint32_t n, const int64_t *posQ,
     return nch;
 }
 
+// walk_chain on one chain: every DP piece (Collect), each aligned (run_dp), then
+// the record replayed with getAlignment2's exits (Asm): the pieces the
+// reference computes (Asm::used), the position and the record's fate
+int32_t emu_chain_layout(int32_t k, int32_t l, int32_t affine, double mis_rate, double indel_rate,
+                         const uint8_t *qseq, int32_t Lq, const uint8_t *sseq, int32_t Ls,
+                         uint32_t nkeys, const int64_t *posQ, const int64_t *posS, int64_t *seg,
+                         int32_t cap, int64_t *pos_out, int32_t *status) {
+    Params p{k, l, affine, 0, mis_rate, indel_rate, 0.6};
+    std::vector<uint8_t> qc(static_cast<size_t>(Lq)), sc(static_cast<size_t>(Ls));
+    for (int32_t i = 0; i < Lq; i++) qc[size_t(i)] = base_code(qseq[i]);
+    for (int32_t i = 0; i < Ls; i++) sc[size_t(i)] = base_code(sseq[i]);
+    std::vector<uint64_t> keys(nkeys);
+    for (uint32_t i = 0; i < nkeys; i++) keys[i] = hit_pack(0, uint32_t(posQ[i]), uint32_t(posS[i]));
+    auto key = [&keys](int32_t t) { return keys[size_t(t)]; };
+    std::vector<SegRec> segs;
+    Collect col{&segs};
+    walk_chain(p, Lq, Ls, key, int32_t(nkeys), col);
+    for (SegRec &sr : segs) {
+        SegView v = make_view(sc.data(), Ls, 0, qc.data(), int32_t(sr.s0), int32_t(sr.s1),
+                              int32_t(sr.q0), int32_t(sr.q1), sr.flags, sr.band);
+        run_dp<8>(v, affine != 0, sr.ops, sr.sum);
+    }
+    Asm as;
+    as.segs = segs.data();
+    struct Pos {
+        int64_t pos = 0;
+        void begin(int64_t, int64_t, int64_t) {}
+        void position(int64_t q) { pos = q; }
+        void run(uint8_t, int64_t) {}
+        void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {}
+        bool check(int64_t, int64_t) { return true; }
+        void finish() {}
+    } ps;
+    walk_chain(p, Lq, Ls, key, int32_t(nkeys), ps);
+    const bool ok = walk_chain(p, Lq, Ls, key, int32_t(nkeys), as);
+    double rate = 0, len = 0;
+    *status = !as.built ? 0 : (ok && as.st.good_rates(p, rate, len)) ? 2 : 1;
+    *pos_out = ps.pos;
+    const int32_t n = int32_t(as.used);
+    for (int32_t i = 0; i < n && i < cap; i++) {
+        const SegRec &g = segs[size_t(i)];
+        int64_t *x = seg + 6 * i;
+        x[0] = g.s0;
+        x[1] = g.s1;
+        x[2] = g.q0;
+        x[3] = g.q1;
+        x[4] = g.flags;
+        x[5] = g.band;
+    }
+    return n;
+}
+
 void emu_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = column_consensus(counts + 4 * i, thr);
 }

@@ -90,6 +90,10 @@ class Oracle:
         lib.hero_oracle_record_score.argtypes = [C.c_uint32, vp, vp, vp, vp, vp]
         lib.hero_oracle_chain.argtypes = [C.c_int32, C.c_double, C.c_uint32, vp, vp, vp, vp]
         lib.hero_oracle_chain.restype = C.c_int32
+        lib.hero_oracle_chain_layout.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double,
+                                                  C.c_double, vp, C.c_int32, vp, C.c_int32,
+                                                  C.c_uint32, vp, vp, vp, C.c_int32, vp, vp])
+        lib.hero_oracle_chain_layout.restype = C.c_int32
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -183,6 +187,10 @@ class Emu:
         lib.emu_record_score.argtypes = [C.c_uint32, vp, vp, vp, vp, vp]
         lib.emu_chain.argtypes = [C.c_int32, C.c_double, C.c_uint32, vp, vp, vp, vp]
         lib.emu_chain.restype = C.c_int32
+        lib.emu_chain_layout.argtypes = ([C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                          vp, C.c_int32, vp, C.c_int32, C.c_uint32, vp, vp, vp,
+                                          C.c_int32, vp, vp])
+        lib.emu_chain_layout.restype = C.c_int32
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
@@ -356,3 +364,21 @@ def chain(lib, prefix, k, indel_rate, posQ, posS):
     nch = getattr(lib, prefix + "_chain")(k, float(indel_rate), len(q), _vp(q), _vp(s_),
                                           _vp(chain_of), _vp(kept))
     return chain_of[:len(q)].tolist(), kept[:nch].tolist()
+
+
+def chain_layout(lib, prefix, k, l, affine, mis_rate, indel_rate, query: bytes, subject: bytes,
+                 posQ, posS):
+    """(DP calls as 6-tuples, record position, status) of one chain of keys."""
+    q = np.frombuffer(query, np.uint8).copy()
+    s_ = np.frombuffer(subject, np.uint8).copy()
+    pq = np.ascontiguousarray(posQ, np.int64)
+    ps = np.ascontiguousarray(posS, np.int64)
+    cap = 2 * len(pq) + 4
+    seg = np.zeros(6 * cap, np.int64)
+    pos = C.c_int64()
+    st = C.c_int32()
+    n = getattr(lib, prefix + "_chain_layout")(k, l, int(affine), float(mis_rate),
+                                              float(indel_rate), _vp(q), len(q), _vp(s_), len(s_),
+                                              len(pq), _vp(pq), _vp(ps), _vp(seg), cap,
+                                              C.byref(pos), C.byref(st))
+    return [tuple(seg[6 * i:6 * i + 6].tolist()) for i in range(n)], pos.value, st.value

@@ -138,3 +138,46 @@ def test_chaining_agrees(oracle, emu):
         a = chain(oracle.lib, "hero_oracle", k, rate, q, s_)
         b = chain(emu.lib, "emu", k, rate, q, s_)
         assert a == b, (t, k, rate, q.tolist(), s_.tolist())
+
+
+def test_chain_layout_agrees(oracle, emu):
+    """getAlignment2 on random chains: every geometry of the start, middle and end
+    pieces (keys overlapping, adjacent, apart; diagonal shifts both ways; reads
+    of unequal length), with and without early exits: the DP calls made, the
+    record's position and its fate."""
+    from hero_testlib import chain_layout
+    rng = np.random.default_rng(37)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    fates = set()
+    for t in range(1500):
+        k = int(rng.choice([11, 21, 39]))
+        n = int(rng.integers(1, 6))
+        q0, s0 = int(rng.integers(0, 60)), int(rng.integers(0, 60))
+        if rng.random() < 0.2:
+            q0 = 0
+        if rng.random() < 0.2:
+            s0 = 0
+        pq, ps = [q0], [s0]
+        for _ in range(n - 1):
+            dq = int(rng.integers(1, 2 * k + 10))
+            ds = dq if rng.random() < 0.4 else int(rng.integers(1, 2 * k + 10))
+            pq.append(pq[-1] + dq)
+            ps.append(ps[-1] + ds)
+        Lq = pq[-1] + k + int(rng.integers(0, 60))
+        Ls = ps[-1] + k + int(rng.integers(0, 60))
+        if rng.random() < 0.15:
+            Ls = ps[-1] + k  # the last key at the subject's end
+        query = acgt[rng.integers(0, 4, Lq)].tobytes()
+        subject = bytearray(acgt[rng.integers(0, 4, Ls)].tobytes())
+        for a, b in zip(pq, ps):  # the keys match
+            subject[b:b + k] = query[a:a + k]
+        mis, ind = (1.0, 1.0) if rng.random() < 0.5 else (float(rng.choice([0.02, 0.1, 0.3])),
+                                                           float(rng.choice([0.01, 0.05, 0.2])))
+        l = int(rng.choice([20, 40, 80]))
+        affine = bool(rng.random() < 0.5)
+        a = chain_layout(oracle.lib, "hero_oracle", k, l, affine, mis, ind, query, bytes(subject),
+                         pq, ps)
+        b = chain_layout(emu.lib, "emu", k, l, affine, mis, ind, query, bytes(subject), pq, ps)
+        assert a == b, (t, k, l, affine, mis, ind, pq, ps, Lq, Ls)
+        fates.add(a[2])
+    assert fates == {0, 1, 2}
