@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 
 #include "hero_internal.cuh"
 
@@ -2120,13 +2121,19 @@ void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, i
     const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps));
     // the opt-in is set once per size increase (never while a graph is being captured
     // for a size not seen before: the eager round that precedes a capture sets it)
-    static size_t opted[2][2] = {{0, 0}, {0, 0}};
+    // (per device, and shared by the host threads of every context in the process)
+    constexpr int kOptDevices = 64;
+    static std::mutex opt_mu;
+    static size_t opted[kOptDevices][2][2] = {};
     const int ai = a.affine ? 1 : 0, wi = a.warps == 2 ? 0 : 1;
-    if (smem > 48u * 1024u && smem > opted[ai][wi]) {
-        const void *fn = a.affine ? (a.warps == 2 ? (const void *)k_dp_wave<true, 2> : (const void *)k_dp_wave<true, 4>)
-                                  : (a.warps == 2 ? (const void *)k_dp_wave<false, 2> : (const void *)k_dp_wave<false, 4>);
-        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        opted[ai][wi] = smem;
+    if (smem > 48u * 1024u) {
+        std::lock_guard<std::mutex> lock(opt_mu);
+        if (dev >= kOptDevices || smem > opted[dev][ai][wi]) {
+            const void *fn = a.affine ? (a.warps == 2 ? (const void *)k_dp_wave<true, 2> : (const void *)k_dp_wave<true, 4>)
+                                      : (a.warps == 2 ? (const void *)k_dp_wave<false, 2> : (const void *)k_dp_wave<false, 4>);
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (dev < kOptDevices) opted[dev][ai][wi] = smem;
+        }
     }
     counted();
     if (a.affine) {
