@@ -1286,6 +1286,36 @@ extern "C" int32_t hero_oracle_chain_layout(int32_t k, int32_t l, int32_t affine
     return n;
 }
 
+extern "C" int32_t hero_oracle_record_text(uint64_t key, uint32_t orient, int64_t pos, uint32_t nev,
+                                           const uint32_t *piece, const uint8_t *type,
+                                           const int32_t *count, const uint8_t *query, int32_t Lq,
+                                           int32_t qrc, uint8_t *out, int32_t cap) {
+    // the record as getAlignment2 builds it (addCigar per run and per step, a
+    // mismatch named by the query's base there), then AlignmentRecord::getCigar
+    std::string qs(reinterpret_cast<const char *>(query), size_t(Lq));
+    if (qrc) qs = revcomp(qs);
+    Record r;
+    r.key = key;
+    r.orient = orient;
+    r.pos = pos;
+    size_t pq = 0;
+    for (uint32_t i = 0; i < nev; i++) {
+        (void)piece;
+        const uint8_t t = type[i];
+        if (t == HERO_OP_X) {
+            r.addCigar(count[i], qs.at(pq));
+        } else {
+            r.addCigar(count[i], t == HERO_OP_M ? 'M' : t == HERO_OP_I ? 'I' : 'D');
+        }
+        if (t != HERO_OP_D) pq += size_t(count[i]);
+    }
+    std::string text;
+    Corrector::cigarText(r, qs, text);
+    if (int32_t(text.size()) > cap) return -1;
+    std::memcpy(out, text.data(), text.size());
+    return int32_t(text.size());
+}
+
 extern "C" void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = consensusColumn(counts + 4 * i, thr);
 }

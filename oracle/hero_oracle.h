@@ -116,6 +116,14 @@ int32_t hero_oracle_chain_layout(int32_t k, int32_t l, int32_t affine, double mi
                                  const uint8_t *sseq, int32_t Ls, uint32_t nkeys,
                                  const int64_t *posQ, const int64_t *posS, int64_t *seg,
                                  int32_t cap, int64_t *pos_out, int32_t *status);
+/* AlignmentRecord::getCigar of a record given as events (as for
+ * hero_oracle_record_score; a mismatch is a single step named by the query's
+ * base; qrc: the query's reverse complement is aligned).  Returns the text's
+ * length, or -1 if cap is too small. */
+int32_t hero_oracle_record_text(uint64_t key, uint32_t orient, int64_t pos, uint32_t nev,
+                                const uint32_t *piece, const uint8_t *type, const int32_t *count,
+                                const uint8_t *query, int32_t Lq, int32_t qrc, uint8_t *out,
+                                int32_t cap);
 void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
                               const int32_t *count, const uint8_t *letter, int64_t *out);
 

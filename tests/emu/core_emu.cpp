@@ -1045,6 +1045,61 @@ int32_t emu_chain_layout(int32_t k, int32_t l, int32_t affine, double mis_rate, 
     return n;
 }
 
+// AlnText driven by the same events: runs through run(), each DP piece through
+// dp() with its steps from a vector source; sized, then written, as the kernels do
+extern "C++" {
+struct VecPieces {
+    const std::vector<std::vector<uint8_t>> *p;
+    template <class F>
+    void each(uint32_t i, F f) const {
+        for (uint8_t o : (*p)[i]) f(o);
+    }
+};
+}  // extern "C++"
+
+int32_t emu_record_text(uint64_t key, uint32_t orient, int64_t pos, uint32_t nev,
+                        const uint32_t *piece, const uint8_t *type, const int32_t *count,
+                        const uint8_t *query, int32_t Lq, int32_t qrc, uint8_t *out, int32_t cap) {
+    std::vector<uint8_t> qc(static_cast<size_t>(Lq));
+    for (int32_t i = 0; i < Lq; i++) qc[size_t(i)] = base_code(query[i]);
+    std::vector<std::vector<uint8_t>> pieces;
+    for (uint32_t i = 0; i < nev; i++) {
+        if (!piece[i]) continue;
+        if (i == 0 || piece[i - 1] != piece[i]) pieces.emplace_back();
+        pieces.back().push_back(type[i]);
+    }
+    auto drive = [&](AlnText<VecPieces> &t) {
+        t.position(pos);
+        for (uint32_t i = 0; i < nev; i++) {
+            if (!piece[i]) {
+                t.run(type[i], count[i]);
+            } else if (i == 0 || piece[i - 1] != piece[i]) {
+                t.dp(0, 0, 0, 0, 0, 0);
+            }
+        }
+        t.finish();
+    };
+    AlnText<VecPieces> sz{VecPieces{&pieces}, qc.data(), Lq, qrc != 0};
+    drive(sz);
+    const uint32_t pre = aln_prefix_len(key, orient, sz.pos);
+    const uint32_t total = pre + sz.cig_len + 1 + sz.ins_len + 1;
+    if (int32_t(total) > cap) return -1;
+    AlnText<VecPieces> wr{VecPieces{&pieces}, qc.data(), Lq, qrc != 0};
+    char *o = reinterpret_cast<char *>(out);
+    wr.cig = o + pre;
+    wr.ins = wr.cig + sz.cig_len + 1;
+    drive(wr);
+    o = dec_put(o, key);
+    *o++ = ',';
+    o = dec_put(o, orient);
+    *o++ = ',';
+    o = dec_put_signed(o, wr.pos);
+    *o = ',';
+    *wr.cig = ',';
+    *wr.ins = ',';
+    return int32_t(total);
+}
+
 void emu_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = column_consensus(counts + 4 * i, thr);
 }

@@ -94,6 +94,9 @@ class Oracle:
                                                   C.c_double, vp, C.c_int32, vp, C.c_int32,
                                                   C.c_uint32, vp, vp, vp, C.c_int32, vp, vp])
         lib.hero_oracle_chain_layout.restype = C.c_int32
+        lib.hero_oracle_record_text.argtypes = ([C.c_uint64, C.c_uint32, C.c_int64, C.c_uint32, vp,
+                                                 vp, vp, vp, C.c_int32, C.c_int32, vp, C.c_int32])
+        lib.hero_oracle_record_text.restype = C.c_int32
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -191,6 +194,9 @@ class Emu:
                                           vp, C.c_int32, vp, C.c_int32, C.c_uint32, vp, vp, vp,
                                           C.c_int32, vp, vp])
         lib.emu_chain_layout.restype = C.c_int32
+        lib.emu_record_text.argtypes = ([C.c_uint64, C.c_uint32, C.c_int64, C.c_uint32, vp, vp, vp,
+                                         vp, C.c_int32, C.c_int32, vp, C.c_int32])
+        lib.emu_record_text.restype = C.c_int32
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,
@@ -382,3 +388,17 @@ def chain_layout(lib, prefix, k, l, affine, mis_rate, indel_rate, query: bytes, 
                                               len(pq), _vp(pq), _vp(ps), _vp(seg), cap,
                                               C.byref(pos), C.byref(st))
     return [tuple(seg[6 * i:6 * i + 6].tolist()) for i in range(n)], pos.value, st.value
+
+
+def record_text(lib, prefix, key, orient, pos, piece, typ, count, query: bytes, qrc):
+    """One .aln record's text from events (see the oracle header)."""
+    pc = np.ascontiguousarray(piece, np.uint32)
+    t = np.ascontiguousarray(typ, np.uint8)
+    c = np.ascontiguousarray(count, np.int32)
+    q = np.frombuffer(query, np.uint8).copy()
+    cap = 64 + 16 * len(t) + 2 * len(q)
+    out = np.zeros(cap, np.uint8)
+    n = getattr(lib, prefix + "_record_text")(key, orient, pos, len(t), _vp(pc), _vp(t), _vp(c),
+                                              _vp(q), len(q), int(qrc), _vp(out), cap)
+    assert n >= 0
+    return out[:n].tobytes()

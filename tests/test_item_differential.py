@@ -8,7 +8,7 @@ uniqueId), a record's score from its run ends and DP-piece summaries
 consensus call of a column (QueryRead::callConsensus, whose
 device form scans integer counts and divides only the two kept ones)."""
 import numpy as np
-from hero_testlib import chain, columns, merge_pair, record_list, record_score
+from hero_testlib import chain, columns, merge_pair, record_list, record_score, record_text
 
 COMP = bytes.maketrans(b"ACGTN", b"TGCAJ")
 
@@ -181,3 +181,38 @@ def test_chain_layout_agrees(oracle, emu):
         assert a == b, (t, k, l, affine, mis, ind, pq, ps, Lq, Ls)
         fates.add(a[2])
     assert fates == {0, 1, 2}
+
+
+def test_record_text_agrees(oracle, emu):
+    """.aln record text: run-length entries across runs and DP pieces, mismatch
+    letters from the (reverse-complemented) query, inserted bases of inner I
+    entries only; ids above 2^63 print unsigned, positions signed."""
+    rng = np.random.default_rng(41)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    for t in range(2000):
+        piece, typ, count = [], [], []
+        npc, qlen = 0, 0
+        for _ in range(int(rng.integers(1, 7))):
+            if rng.random() < 0.5:
+                op = int(rng.choice([0, 0, 2, 3]))
+                c = int(rng.integers(1, 30))
+                piece.append(0)
+                typ.append(op)
+                count.append(c)
+                qlen += c if op != 3 else 0
+            else:
+                npc += 1
+                for _ in range(int(rng.integers(1, 8))):
+                    op = int(rng.choice([0, 1, 1, 2, 3]))
+                    piece.append(npc)
+                    typ.append(op)
+                    count.append(1)
+                    qlen += 1 if op != 3 else 0
+        query = acgt[rng.integers(0, 4, qlen + int(rng.integers(0, 5)))].tobytes()
+        key = int(rng.choice([0, 7, 12345, 2 ** 64 - 5]))
+        orient = int(rng.integers(0, 2))
+        pos = int(rng.integers(0, 300))
+        qrc = bool(rng.random() < 0.5)
+        a = record_text(oracle.lib, "hero_oracle", key, orient, pos, piece, typ, count, query, qrc)
+        b = record_text(emu.lib, "emu", key, orient, pos, piece, typ, count, query, qrc)
+        assert a == b, (t, a, b)
