@@ -1316,6 +1316,16 @@ extern "C" int32_t hero_oracle_record_text(uint64_t key, uint32_t orient, int64_
     return int32_t(text.size());
 }
 
+extern "C" int32_t hero_oracle_key_positions(int64_t L, int64_t k, int64_t *out) {
+    // HashTableLongKey::insertQueryDataset (HashTableLongKey.cpp:279-289): keys at
+    // 0, k, 2k, ... while i <= L - k, then one at L - k if i < L
+    int32_t n = 0;
+    int64_t i = 0;
+    for (i = 0; i <= L - k; i += k) out[n++] = i;
+    if (i < L) out[n++] = L - k;
+    return n;
+}
+
 extern "C" void hero_oracle_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = consensusColumn(counts + 4 * i, thr);
 }

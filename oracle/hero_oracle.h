@@ -124,6 +124,8 @@ int32_t hero_oracle_record_text(uint64_t key, uint32_t orient, int64_t pos, uint
                                 const uint32_t *piece, const uint8_t *type, const int32_t *count,
                                 const uint8_t *query, int32_t Lq, int32_t qrc, uint8_t *out,
                                 int32_t cap);
+/* Positions of the k-mers a query read of length L puts in the table. */
+int32_t hero_oracle_key_positions(int64_t L, int64_t k, int64_t *out);
 void hero_oracle_record_score(uint32_t nev, const uint32_t *piece, const uint8_t *type,
                               const int32_t *count, const uint8_t *letter, int64_t *out);
 

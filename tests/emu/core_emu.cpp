@@ -1100,6 +1100,12 @@ int32_t emu_record_text(uint64_t key, uint32_t orient, int64_t pos, uint32_t nev
     return int32_t(total);
 }
 
+int32_t emu_key_positions(int64_t L, int64_t k, int64_t *out) {
+    const int32_t n = L >= k ? query_key_count(L, int32_t(k)) : 0;
+    for (int32_t i = 0; i < n; i++) out[i] = query_key_pos(L, k, i);
+    return n;
+}
+
 void emu_columns(uint64_t n, const uint32_t *counts, double thr, int32_t *out) {
     for (uint64_t i = 0; i < n; i++) out[i] = column_consensus(counts + 4 * i, thr);
 }

@@ -97,6 +97,8 @@ class Oracle:
         lib.hero_oracle_record_text.argtypes = ([C.c_uint64, C.c_uint32, C.c_int64, C.c_uint32, vp,
                                                  vp, vp, vp, C.c_int32, C.c_int32, vp, C.c_int32])
         lib.hero_oracle_record_text.restype = C.c_int32
+        lib.hero_oracle_key_positions.argtypes = [C.c_int64, C.c_int64, vp]
+        lib.hero_oracle_key_positions.restype = C.c_int32
         self.lib = lib
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
@@ -197,6 +199,8 @@ class Emu:
         lib.emu_record_text.argtypes = ([C.c_uint64, C.c_uint32, C.c_int64, C.c_uint32, vp, vp, vp,
                                          vp, C.c_int32, C.c_int32, vp, C.c_int32])
         lib.emu_record_text.restype = C.c_int32
+        lib.emu_key_positions.argtypes = [C.c_int64, C.c_int64, vp]
+        lib.emu_key_positions.restype = C.c_int32
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,

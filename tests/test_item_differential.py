@@ -216,3 +216,16 @@ def test_record_text_agrees(oracle, emu):
         a = record_text(oracle.lib, "hero_oracle", key, orient, pos, piece, typ, count, query, qrc)
         b = record_text(emu.lib, "emu", key, orient, pos, piece, typ, count, query, qrc)
         assert a == b, (t, a, b)
+
+
+def test_query_key_positions_agree(oracle, emu):
+    """The k-mers a query read puts in the table (every k-th, then the tail).
+    Reads shorter than k are outside the reference's domain (its substr throws)."""
+    import ctypes as C
+    out_a = np.zeros(2048, np.int64)
+    out_b = np.zeros(2048, np.int64)
+    for k in range(1, 64):
+        for L in range(k, 400):
+            na = oracle.lib.hero_oracle_key_positions(L, k, out_a.ctypes.data_as(C.c_void_p))
+            nb = emu.lib.emu_key_positions(L, k, out_b.ctypes.data_as(C.c_void_p))
+            assert na == nb and np.array_equal(out_a[:na], out_b[:nb]), (L, k)
