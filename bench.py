@@ -296,16 +296,6 @@ def int_peak_tops(device: int) -> float | None:
     return v if v > 0 else None
 
 
-def dpx_peak_tops(device: int) -> float | None:
-    import ctypes as C
-    from hero_b200 import build
-    lib = C.CDLL(build.build_peak())
-    lib.hero_dpx_peak_tops.restype = C.c_double
-    lib.hero_dpx_peak_tops.argtypes = [C.c_int, C.c_int]
-    v = lib.hero_dpx_peak_tops(device, 5)
-    return v if v > 0 else None
-
-
 def _job_reads(job):
     rs = job.reads()
     return job.job_id, rs.seq, rs.off, rs.names
