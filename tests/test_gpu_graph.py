@@ -1,6 +1,5 @@
 """The batched form: a correction round captured as one CUDA graph and replayed
 gives the same bytes as the plain form, and re-plans when the reads change."""
-import numpy as np
 import pytest
 from fixtures import FIXTURES, params, upper
 from hero_testlib import assert_same_consensus
