@@ -34,6 +34,7 @@ struct Params {
     bool affine, keep_segments;
     bool aln;  // alignment output (no -c): SubjectReadAligner::writeToFile
     bool merge;  // --merge: overhang votes and paired-read merging
+    bool mapping;  // --mapping: the best covering record per subject, a coverage histogram
     double mis_rate, indel_rate, thr;
 };
 
@@ -740,6 +741,57 @@ struct Corrector {
     }
 
     // SubjectReadAligner::start loop body (SubjectReadAligner.cpp:523-562) for one subject
+    // AlignmentRecord::isSubjectCoveredByQuery (AlignmentRecord.cpp:343-370)
+    static bool coversSubject(const Record &r, int64_t Ls) {
+        if (r.pos != 0) return false;
+        int64_t len = 0;
+        if (r.type.at(0) == 'D') return false;
+        if (r.type.at(0) != 'I') len += r.count.at(0);
+        if (r.type.size() > 1) {
+            for (size_t i = 1; i < r.type.size() - 1; i++)
+                if (r.type[i] != 'I') len += r.count[i];
+            if (r.type.back() == 'D') return false;
+            if (r.type.back() != 'I') len += r.count.back();
+        }
+        return len >= Ls;
+    }
+
+    // SubjectRead::chooseQueryWithBestAlignment (SubjectRead.cpp:463-500): no
+    // record covering the subject clears the list; two or more keep the one of
+    // fewest substitutions (AlignmentRecord::getAccuracy, AlignmentRecord.cpp:
+    // 372-381; the first of equals in list order); exactly one keeps the list.
+    static void chooseBest(std::vector<Record> &v, int64_t Ls) {
+        if (v.empty()) return;
+        std::vector<size_t> q;
+        for (size_t i = 0; i < v.size(); i++)
+            if (coversSubject(v[i], Ls)) q.push_back(i);
+        if (q.empty()) {
+            v.clear();
+            return;
+        }
+        if (q.size() == 1) return;
+        int64_t best = -1;
+        double least = double(Ls);
+        for (size_t i : q) {
+            double subs = 0;
+            for (size_t j = 0; j < v[i].type.size(); j++) {
+                const char t = v[i].type[j];
+                if (t != 'I' && t != 'D' && t != 'M') subs += v[i].count[j];
+            }
+            if (subs < least) {
+                least = subs;
+                best = int64_t(i);
+            }
+        }
+        if (best < 0) {  // the reference prints an error and then indexes -1; kept empty here
+            v.clear();
+            return;
+        }
+        Record keep = std::move(v[size_t(best)]);
+        v.clear();
+        v.push_back(std::move(keep));
+    }
+
     // AlignmentRecord::getCigar (AlignmentRecord.cpp:102-149), storeOverhang off:
     // id,orientation,position,CIGAR,inserted bases of the inner I entries,
     static void cigarText(const Record &r, const std::string &qs, std::string &t) {
@@ -858,6 +910,7 @@ struct Corrector {
             t += "\n";
             o.aln.push_back({s, std::move(t)});
         } else {
+            if (p.mapping) chooseBest(vAlignment, int64_t(fwd.size()));
             applyVotes(vAlignment, fwd, rc);
         }
         std::sort(vAlignment.begin(), vAlignment.end(),
@@ -1010,6 +1063,7 @@ extern "C" hero_oracle_run *hero_oracle_correct(const hero_oracle_params *pp, in
     p.thr = pp->consensus_thr;
     p.aln = pp->aln_mode != 0;
     p.merge = pp->merge_pairs != 0;
+    p.mapping = pp->mapping != 0;
 
     load(run->Q, nq, qseq, qoff, quid);
     Reads S;
@@ -1314,6 +1368,26 @@ extern "C" int32_t hero_oracle_record_text(uint64_t key, uint32_t orient, int64_
     if (int32_t(text.size()) > cap) return -1;
     std::memcpy(out, text.data(), text.size());
     return int32_t(text.size());
+}
+
+// QueryDataset::getCoverageAndWriteResults (QueryDataset.cpp:560-599): per
+// query base the sum of its four vote counts (no self vote), a histogram of
+// those sums, "COV\tFRE" and one "coverage\tbases" line per non-empty bin
+extern "C" uint64_t hero_oracle_mapping_histogram(const hero_oracle_run *r, uint8_t *out, uint64_t cap) {
+    uint32_t maxc = 0;
+    const size_t nb = r->votes.size() / 4;
+    for (size_t i = 0; i < nb; i++) {
+        const uint32_t c = r->votes[4 * i] + r->votes[4 * i + 1] + r->votes[4 * i + 2] + r->votes[4 * i + 3];
+        if (c > maxc) maxc = c;
+    }
+    std::vector<uint32_t> hist(size_t(maxc) + 1, 0);
+    for (size_t i = 0; i < nb; i++)
+        hist[r->votes[4 * i] + r->votes[4 * i + 1] + r->votes[4 * i + 2] + r->votes[4 * i + 3]]++;
+    std::string t = "COV\tFRE\n";
+    for (size_t i = 0; i < hist.size(); i++)
+        if (hist[i] > 0) t += std::to_string(i) + "\t" + std::to_string(hist[i]) + "\n";
+    if (out && t.size() <= cap) std::memcpy(out, t.data(), t.size());
+    return t.size();
 }
 
 extern "C" int32_t hero_oracle_key_positions(int64_t L, int64_t k, int64_t *out) {

@@ -31,6 +31,8 @@ typedef struct {
     int32_t aln_mode;       /* 1 = alignment output (no -c): the .aln file, no votes */
     int32_t merge_pairs;    /* 1 = --merge: overhang votes, reads (2i, 2i+1) merged after
                                the consensus (an odd read count is refused) */
+    int32_t mapping;        /* 1 = -c --mapping: per subject the best record covering it
+                               (query uids are then the inner ids: pass 0..n-1) */
 } hero_oracle_params;
 
 typedef struct {
@@ -83,6 +85,10 @@ void hero_oracle_aln(const hero_oracle_run *r, uint8_t *out);
  * [reads][20][4]. */
 void hero_oracle_merged(const hero_oracle_run *r, uint8_t *seq_out, uint32_t *merged_len);
 void hero_oracle_overhang(const hero_oracle_run *r, uint32_t *out);
+
+/* --mapping: the coverage histogram file (QueryDataset::
+ * getCoverageAndWriteResults): its length; copied to out when cap suffices. */
+uint64_t hero_oracle_mapping_histogram(const hero_oracle_run *r, uint8_t *out, uint64_t cap);
 
 /* Item checks: QueryRead::mergingPairedReads on one pair (extL / extR: 20x4
  * overhang votes; out: room for lenL + lenR; returns the merged length or 0),

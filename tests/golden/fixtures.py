@@ -95,6 +95,10 @@ MERGE_FIXTURES = {
     "merge_c1_20k": (lambda: synth.config1(genome_bp=20000), []),
 }
 
+# -c --mapping (--singleReads, one query file): the coverage histogram of the
+# best record covering each subject; name -> the FIXTURES entry it runs on
+MAPPING_FIXTURES = ("c1_20k", "c2_30k", "mix_affine", "c2_20k_names")
+
 # fixtures whose reference outputs are stored in full (gzipped)
 STORED = ("c1_20k", "mix_affine")
 

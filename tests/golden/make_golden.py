@@ -6,7 +6,8 @@ input FASTQ, of the reference .fasta/.info (consensus mode, -c) and of its .aln
 (alignment-output mode: the same flags without -c); the .fasta/.info of the
 fixtures in STORED are kept gzipped.  The MERGE_FIXTURES (paired input) get
 the md5 and size of the reference's _merged.fasta, _unmerged.fasta and .info
-with -c --covinfo --merge.  Usage:  python tests/golden/make_golden.py
+with -c --covinfo --merge; the MAPPING_FIXTURES the md5 of the coverage
+histogram of -c --mapping.  Usage:  python tests/golden/make_golden.py
 
     python tests/golden/make_golden.py --full NAME...
 
@@ -26,7 +27,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from fixtures import FIXTURES, MERGE_FIXTURES, STORED, aln_flags  # noqa: E402
+from fixtures import FIXTURES, MAPPING_FIXTURES, MERGE_FIXTURES, STORED, aln_flags  # noqa: E402
 
 from hero_b200 import synth  # noqa: E402
 
@@ -93,6 +94,18 @@ def run_reference_merge(fq: str, flags: list[str], workdir: str) -> dict:
     return res
 
 
+def run_reference_mapping(fq: str, flags: list[str], workdir: str) -> bytes:
+    """-c --mapping: the coverage histogram file (written to the output name as given)."""
+    out = os.path.join(workdir, "mapping")
+    if os.path.exists(out):  # opened in append mode
+        os.remove(out)
+    subprocess.run([REF, "-q", fq, "-s", fq, "-c", "--mapping", "--singleReads", "-t",
+                    str(os.cpu_count() or 1), "-o", out] + aln_flags(flags),
+                   stdout=subprocess.DEVNULL, check=True)
+    with open(out, "rb") as f:
+        return f.read()
+
+
 def main_full(names: list[str]):
     import time
     path = os.path.join(HERE, "manifest_full.json")
@@ -133,6 +146,8 @@ def main():
             manifest[name] = dict(flags=flags, reads=rs.n, fastq_md5=md5(fqb),
                                   fasta_md5=md5(fa), info_md5=md5(info), aln_md5=md5(aln),
                                   aln_bytes=len(aln))
+            if name in MAPPING_FIXTURES:
+                manifest[name]["mapping_md5"] = md5(run_reference_mapping(fq, flags, d))
             if name in STORED:
                 for ext, data in ((".fasta.gz", fa), (".info.gz", info)):
                     with gzip.GzipFile(os.path.join(HERE, name + ext), "wb", mtime=0) as g:

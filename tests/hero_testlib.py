@@ -42,7 +42,7 @@ class OracleParams(C.Structure):
     _fields_ = [("k", C.c_int32), ("min_overlap", C.c_int32), ("affine", C.c_int32),
                 ("keep_segments", C.c_int32), ("mis_rate", C.c_double),
                 ("indel_rate", C.c_double), ("consensus_thr", C.c_double),
-                ("aln_mode", C.c_int32), ("merge_pairs", C.c_int32)]
+                ("aln_mode", C.c_int32), ("merge_pairs", C.c_int32), ("mapping", C.c_int32)]
 
 
 class OracleStats(C.Structure):
@@ -82,6 +82,8 @@ class Oracle:
         lib.hero_oracle_aln.argtypes = [vp, vp]
         lib.hero_oracle_merged.argtypes = [vp, vp, vp]
         lib.hero_oracle_overhang.argtypes = [vp, vp]
+        lib.hero_oracle_mapping_histogram.argtypes = [vp, vp, C.c_uint64]
+        lib.hero_oracle_mapping_histogram.restype = C.c_uint64
         lib.hero_oracle_merge_pair.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, vp, vp]
         lib.hero_oracle_merge_pair.restype = C.c_int
         lib.hero_oracle_record_list.argtypes = [C.c_uint32, vp, vp, vp, vp]
@@ -103,13 +105,14 @@ class Oracle:
 
     def correct(self, reads, subjects=None, k=39, min_overlap=40, aligner="global",
                 max_mismatch_rate=1.0, max_indel_rate=1.0, consensus_threshold=0.6,
-                keep_segments=False, threads=8, aln=False, merge=False):
+                keep_segments=False, threads=8, aln=False, merge=False, mapping=False):
         """aln=True: the alignment-output mode (no -c); res["aln"] holds the .aln bytes.
         merge=True: --merge; res["merged_seq"], res["merged_len"], res["overhang"]."""
         subj = subjects if subjects is not None else reads
         p = OracleParams(k, min_overlap, 1 if aligner in ("a", "affine") else 0,
                          1 if keep_segments else 0, max_mismatch_rate, max_indel_rate,
-                         consensus_threshold, 1 if aln else 0, 1 if merge else 0)
+                         consensus_threshold, 1 if aln else 0, 1 if merge else 0,
+                         1 if mapping else 0)
         qs, qo, qu = reads.seq, reads.off.astype(np.uint64), reads.names.astype(np.int64)
         ss, so, su = subj.seq, subj.off.astype(np.uint64), subj.names.astype(np.int64)
         h = self.lib.hero_oracle_correct(C.byref(p), threads, reads.n, _vp(qs), _vp(qo), _vp(qu),
@@ -132,6 +135,11 @@ class Oracle:
                 res["overhang"] = np.zeros(n * 80, np.uint32)
                 self.lib.hero_oracle_merged(h, _vp(res["merged_seq"]), _vp(res["merged_len"]))
                 self.lib.hero_oracle_overhang(h, _vp(res["overhang"]))
+            if mapping:
+                nh = self.lib.hero_oracle_mapping_histogram(h, None, 0)
+                hb = np.zeros(max(1, nh), np.uint8)
+                self.lib.hero_oracle_mapping_histogram(h, _vp(hb), nh)
+                res["histogram"] = hb[:nh].tobytes()
             if aln:
                 buf = np.zeros(max(1, self.lib.hero_oracle_aln_size(h)), np.uint8)
                 self.lib.hero_oracle_aln(h, _vp(buf))

@@ -5,7 +5,7 @@ import json
 import os
 
 import pytest
-from fixtures import FIXTURES, MERGE_FIXTURES, STORED, aln_flags, params, upper
+from fixtures import FIXTURES, MAPPING_FIXTURES, MERGE_FIXTURES, STORED, aln_flags, params, upper
 from hero_testlib import format_outputs
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -60,6 +60,15 @@ def test_oracle_merge_matches_reference(oracle, name):
     assert md5(merged) == m["merged_fasta_md5"]
     assert md5(unmerged) == m["unmerged_fasta_md5"]
     assert md5(info) == m["info_md5"]
+
+
+@pytest.mark.parametrize("name", MAPPING_FIXTURES)
+def test_oracle_mapping_matches_reference(oracle, name):
+    """-c --mapping: the reference's coverage histogram."""
+    gen, flags = FIXTURES[name]
+    kw = params(aln_flags(flags))
+    r = oracle.correct(upper(gen()), mapping=True, **kw)
+    assert md5(r["histogram"]) == MANIFEST[name]["mapping_md5"]
 
 
 def test_quality_filter(oracle):
