@@ -2,45 +2,46 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hero|reference]
 
-Workload (N=1): the affine/indel workload -- a 5 Mbp iid genome with 40 repeat
-copies (1-5 kbp, 0.5 % divergence), 150 bp reads at 50x (1,666,666 reads,
-250 Mbp), substitution rate rising 0.1 %->2 % along each read, 0.05 %/base
-insertions and deletions, seeded synthetic data.  HERO run as `-q X -s X -c
---covinfo --singleReads -a a` (defaults k=39, l=40, m=i=100 %).
+Headline workload (N=1): the plain workload -- a 1 Mbp iid genome, 100 bp
+reads at 30x (300,000 reads, 30 Mbp), strand 50/50, 1 % iid substitutions, no
+indels, seeded synthetic data; HERO run as `-q X -s X -c --covinfo
+--singleReads` (global aligner, defaults k=39, l=40, m=i=100 %).  Both arms
+run exactly this workload: `--impl reference` times the reference itself
+(oracle/_ref/hero_ref, built from the reference sources) on the same FASTQ
+with the same flags on all host cores, so the two lines share one `config`.
 
-A step is one whole correction of that read set: k-mer table build, seeding,
-chaining, banded affine DP, record selection, votes and consensus.
-  value : device-resident reads (uploaded once); CUDA events on the library's
-          stream around each step.
+A step is one whole correction of the read set: k-mer table build, seeding,
+chaining, banded DP, record selection, votes and consensus.
+  value : device-resident reads (uploaded once), the batched form (the round
+          replayed as one CUDA graph); CUDA events on the library's stream
+          around each step, the L2 flushed (a 256 MB write) between steps.
   e2e   : the same through the C ABI with pinned host buffers: every step
-          uploads the reads (H2D) and reads back corrected reads and statistics
-          (D2H).
-Multi-GPU (torchrun): each rank corrects its own copy of the job (independent
-jobs, no data-path collective, weak scaling); value = all ranks' bases / the
-slowest rank's time.  --shard instead splits one job's subject reads over the
-ranks and sums the vote states in one NCCL all-reduce (strong scaling; value =
-the job's bases / the slowest rank's time).
-
---impl reference times the reference itself (oracle/_ref/hero_ref, built
-from the reference sources) on the host cores, on a bounded sample of the same
-workload (same generator, smaller genome, same coverage/read length/errors).
+          uploads the reads (H2D) and reads back corrected reads and
+          statistics (D2H).
+Multi-GPU (torchrun): one job split across the ranks by subject reads (every
+rank aligns its range against the whole table; the vote states are summed in
+one NCCL all-reduce) -- strong scaling, value = the job's bases / the slowest
+rank's device time.  --replicas instead corrects one copy of the job per rank.
 
 The default line also carries:
-  roofline          the DP kernel against the measured int32 add+max peak
+  roofline          the DP kernel against the measured integer peak of the
+                    instruction forms it issues (peaks of each form listed)
   seeding_roofline  probes + hit sort against the measured HBM bandwidth
+  cpu_baseline      the reference on the host cores, one run of the same workload
+  affine_batched    the affine/indel workload (5 Mbp + 40 repeats, 150 bp at
+                    50x, 1.67 M reads, `-a a`) with its own value, e2e,
+                    roofline and plain form; the reference's full-run time on
+                    it is the one recorded by tests/golden/make_golden.py
   served            a stream of independent jobs through a hero_server
-                    (Poisson arrivals at 85 % of its closed-loop capacity):
-                    p50/p99 job latency, aggregate bases/s, served == alone
+                    (Poisson arrivals): p50/p99 job latency, aggregate
+                    bases/s, served == alone
   file_e2e          the drop-in program, FASTQ file to .fasta/.info files
-  alignment_output  the same reads without -c: the whole .aln text in host
-                    memory (aligned bases/s)
-  merge             -c --merge on paired reads of the same size (corrected and
-                    merged bases/s)
-  cpu_baseline      the reference on the host cores (bounded sample)
+  alignment_output  the same reads without -c: the whole .aln text in host memory
+  merge             -c --merge on paired reads (corrected and merged bases/s)
 
-Other workloads (--workload): config1 (plain/global, 300 k x 100 bp),
-config3 (mixed lengths 75-250 bp, 12.3 M reads), config5 (diploid, 20 M
-reads), config4 (the serving stream alone: p50/p99 job latency).
+Other workloads (--workload): config2 (affine/indel alone), config3 (mixed
+lengths 75-250 bp, 12.3 M reads), config5 (diploid, 20 M reads), config4 (the
+serving stream alone: p50/p99 job latency).
 """
 from __future__ import annotations
 
@@ -59,11 +60,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# DRAM traffic (read + write) of the affine DP kernel per band cell, from one ncu
-# capture of a whole launch (profiles/k_dp_wave_affine_100kbp.md: 2.226 GB for
-# 23.19 G cells); the traffic is per segment (codes in, ops and summaries out),
-# so it scales with the cells of a launch
-DP_DRAM_BYTES_PER_CELL = 2.225526e9 / 23_186_600_877
+# DRAM traffic (read + write) of one DP kernel launch per band cell, from one
+# ncu capture of a whole k_dp_wave launch per aligner (dram__bytes_read.sum +
+# dram__bytes_write.sum over that launch's reference cells).  The traffic is per
+# segment (codes in, ops and summaries out), so it scales with the cells of a
+# launch.  None where no capture of the current kernel exists.
+DP_DRAM_BYTES_PER_CELL = {"affine": 2.225526e9 / 23_186_600_877, "global": None}
+
+# the reference's wall time on the whole affine/indel workload (1,666,666 reads,
+# -a a), 8 threads, recorded by tests/golden/make_golden.py --full config2_full
+REF_CONFIG2_FULL_SECONDS_8T = 665.75
+
+L2_FLUSH_BYTES = 256 << 20  # larger than the B200's 126 MB L2
 
 
 def log(*a):
@@ -76,22 +84,27 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="hero", choices=["hero", "reference"])
-    ap.add_argument("--workload", default="config2",
+    ap.add_argument("--workload", default="config1",
                     choices=["config1", "config2", "config3", "config4", "config5"])
     ap.add_argument("--served-jobs", type=int, default=60,
                     help="jobs of the served block added to the default line (0: none)")
     ap.add_argument("--jobs-scale", type=float, default=0.0,
-                    help="genome-size scale of the served jobs (default 0.02, config4 0.05)")
+                    help="genome-size scale of the served jobs (default 1.0: the stream's sizes)")
     ap.add_argument("--genome-bp", type=int, default=0, help="override the genome size")
     ap.add_argument("--cpu-sample-bp", type=int, default=60000,
-                    help="genome size of the bounded sample the CPU reference runs on")
+                    help="genome size of the bounded sample the reference runs on for "
+                         "workloads other than config1 (config1 runs whole)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-affine-block", action="store_true",
+                    help="skip the affine/indel block of the default line")
     ap.add_argument("--no-alignment-output", action="store_true",
                     help="skip the alignment-output (.aln) line")
     ap.add_argument("--no-merge", action="store_true", help="skip the --merge line")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with several ranks: one copy of the job per rank (weak scaling) "
+                         "instead of one job split by subject reads")
     ap.add_argument("--shard", action="store_true",
-                    help="one job split across the ranks by subject reads (strong scaling; "
-                         "votes summed by one NCCL all-reduce) instead of one job per rank")
+                    help="split one job by subject reads even at one rank")
     ap.add_argument("--profile", action="store_true",
                     help="run --warmup then --steps device-resident steps and exit (for ncu)")
     return ap.parse_args()
@@ -195,9 +208,23 @@ def run_reference_once(fq: str, flags: list[str], workdir: str, threads: int) ->
     return time.perf_counter() - t0
 
 
-def cpu_sample(args):
+def workload_config(rs, flags: list[str], desc: str) -> dict:
+    """The `config` object of a line: the same for the GPU arm and the reference
+    arm when both run the same workload."""
+    return {"workload": desc, "reads": rs.n, "bases": rs.total_bases, "flags": " ".join(flags),
+            "l2": "L2 flushed between timed steps (256 MB write); the step's vote state "
+                  f"({20 * rs.total_bases / 1e9:.2f} GB) and table exceed L2"}
+
+
+def reference_workload(args):
+    """What the reference runs: the whole workload for config1 (about ten seconds
+    on the host cores), else a bounded sample of the same generator (smaller
+    genome, same coverage, read lengths and errors)."""
+    if args.workload == "config1":
+        rs, _, flags, desc = make_workload("config1", args.genome_bp)
+        return rs, flags, desc, True
     rs, _, flags, desc = make_workload(args.workload, args.cpu_sample_bp)
-    return rs, flags, desc
+    return rs, flags, desc, False
 
 
 CLI_BIN = os.path.join(ROOT, "hero_b200", "bin", "hero_b200")
@@ -227,15 +254,16 @@ def measure_cpu_baseline(args) -> dict:
     if not os.path.exists(REF_BIN):
         return {"value": None, "unit": "bases/s", "cores": 0, "kind": "reference",
                 "sample": "reference binary not built"}
-    rs, flags, desc = cpu_sample(args)
+    rs, flags, desc, whole = reference_workload(args)
     threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
         fq = os.path.join(d, "in.fq")
         rs.write_fastq(fq)
         wall = run_reference_once(fq, flags, d, threads)
+    what = "the whole workload" if whole else "a bounded sample"
     return {"value": rs.total_bases / wall, "unit": "bases/s", "cores": threads,
             "kind": "reference",
-            "sample": f"{desc}; one whole run, {rs.total_bases} bases, {wall:.2f} s wall "
+            "sample": f"{what}: {desc}; one run, {rs.total_bases} bases, {wall:.2f} s wall "
                       f"(reads parsed from FASTQ, outputs written)"}
 
 
@@ -243,11 +271,11 @@ def bench_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    rs, flags, desc = cpu_sample(args)
-    threads = os.cpu_count() or 1
     if not os.path.exists(REF_BIN):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/hero_ref not built"}))
         return
+    rs, flags, desc, whole = reference_workload(args)
+    threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
         fq = os.path.join(d, "in.fq")
         rs.write_fastq(fq)
@@ -256,19 +284,21 @@ def bench_reference(args):
         walls = [run_reference_once(fq, flags, d, threads) for _ in range(args.steps)]
     total = sum(walls)
     value = rs.total_bases * len(walls) / total
-    sample = (f"{desc}; each step one whole reference run on {threads} host threads "
+    what = "the whole workload" if whole else "a bounded sample of the workload"
+    sample = (f"{what}: {desc}; each step one whole reference run on {threads} host threads "
               f"({rs.total_bases} bases, FASTQ in, .fasta/.info out)")
     line = {
         "impl": "reference", "metric": "corrected bases/s", "value": value, "unit": "bases/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * total / len(walls), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": desc, "reads": rs.n, "bases": rs.total_bases,
-                   "flags": " ".join(flags), "threads": threads},
+        "ms_per_step": 1e3 * total / len(walls), "higher_is_better": True,
+        "scaling": "strong" if args.gpus > 1 else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no public dataset)",
+        "config": workload_config(rs, flags, desc),
         "cpu_baseline": {"value": value, "unit": "bases/s", "cores": threads,
                          "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "bases/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "step_seconds": [round(w, 3) for w in walls],
     }
     print(json.dumps(line), flush=True)
 
@@ -286,14 +316,52 @@ def hbm_peak_gbs() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def int_peak_tops(device: int) -> float | None:
+PEAK_FORMS = {"add_max_c": 0, "viaddmax_s32": 1, "vimax3_s32": 2, "viaddmax_s16x2": 3,
+              "vimax3_s16x2": 4}
+
+
+def int_peaks(device: int) -> dict:
+    """Measured integer peaks (tera-ops/s, every lane's adds and maxes counted) of
+    each instruction form the DP kernels issue (hero_b200/csrc/int_peak.cu)."""
     import ctypes as C
     from hero_b200 import build
     lib = C.CDLL(build.build_peak())
-    lib.hero_int_peak_tops.restype = C.c_double
-    lib.hero_int_peak_tops.argtypes = [C.c_int, C.c_int]
-    v = lib.hero_int_peak_tops(device, 5)
-    return v if v > 0 else None
+    lib.hero_form_peak_tops.restype = C.c_double
+    lib.hero_form_peak_tops.argtypes = [C.c_int, C.c_int, C.c_int]
+    out = {}
+    for name, form in PEAK_FORMS.items():
+        v = lib.hero_form_peak_tops(device, form, 5)
+        out[name] = v if v > 0 else None
+    return out
+
+
+def dp_roofline(cells: int, dp_ms: float, aligner: str, peaks: dict, launches: int,
+                pairs: bool = False) -> dict:
+    """The DP kernel's roofline: cells x ops/cell (survey: 6 global, 10 affine)
+    over its device time, against the largest measured peak of the instruction
+    forms it issues (the 32-bit forms; the packed 16-bit ones when it runs pairs)."""
+    ops_per_cell = 10 if aligner == "affine" else 6
+    achieved = cells * ops_per_cell / (dp_ms / 1e3) / 1e12 if dp_ms > 0 else None
+    forms = (["viaddmax_s16x2", "vimax3_s16x2"] if pairs else
+             ["add_max_c", "viaddmax_s32", "vimax3_s32"])
+    vals = [(peaks.get(f), f) for f in forms if peaks.get(f)]
+    peak, form = max(vals) if vals else (None, None)
+    per_cell = DP_DRAM_BYTES_PER_CELL.get(aligner)
+    traffic = per_cell * cells / launches if (per_cell is not None and launches) else None
+    return {"bound": "alu", "kernel": f"k_dp_wave ({aligner} banded DP + traceback)",
+            "achieved": achieved, "peak": peak, "unit": "Tops/s",
+            "frac": (achieved / peak) if (achieved and peak) else None,
+            "traffic": traffic, "ops_per_cell": ops_per_cell,
+            "peak_source": f"measured in this run: the fastest of the kernel's instruction "
+                           f"forms ({form}); MEASURED_PEAKS.json has no integer peak",
+            "peaks_tops": peaks}
+
+
+def flush_l2(stream, buf):
+    """Writes a buffer larger than L2 on the stream (outside the timed events)."""
+    import torch
+    with torch.cuda.stream(stream):
+        buf.fill_(1)
 
 
 def _job_reads(job):
@@ -398,6 +466,19 @@ def run_served(jobs, reads, dev: int, busy_target: float = 0.85, check: int = 3)
         srv.close()
 
 
+def run_served_block(args, dev: int) -> dict:
+    """The served block of the default line: a stream of independent jobs."""
+    scale = args.jobs_scale or 0.02
+    jobs, reads = served_jobs(args.served_jobs, scale)
+    with ClockSampler(dev) as sclk:
+        served = run_served(jobs, reads, dev)
+    served["clocks"] = sclk.summary()
+    served["workload"] = (f"{args.served_jobs} jobs, Poisson arrivals, genome log-uniform "
+                          f"0.5-20 Mbp x {scale}, L in {{100,150,250}}, coverage U(20,80), "
+                          "affine/indel errors")
+    return served
+
+
 def bench_served(args):
     """The serving workload alone: one JSON line with p50/p99 job latency."""
     import torch
@@ -423,11 +504,118 @@ def bench_served(args):
     print(json.dumps(line), flush=True)
 
 
+def measure_workload(rs, kw, dev: int, steps: int, warmup: int, peaks: dict,
+                     world: int = 1, barrier=None, max_over_ranks=None, clocks: bool = True):
+    """One workload through Hero: the batched form with device-resident reads
+    (value), the same through pinned host buffers (e2e), the plain form, the DP
+    roofline and the seeding roofline."""
+    import torch
+
+    from hero_b200 import Hero
+    n, nb = rs.n, rs.total_bases
+    barrier = barrier or (lambda: None)
+    max_over_ranks = max_over_ranks or (lambda x: x)
+    seq_p = torch.from_numpy(rs.seq).pin_memory()
+    off_p = torch.from_numpy(rs.off.view(np.int64)).pin_memory()
+    uid_p = torch.from_numpy(rs.names.astype(np.int64)).pin_memory()
+    out_seq = torch.empty(nb, dtype=torch.uint8).pin_memory()
+    out_u32 = [torch.empty(n, dtype=torch.int32).pin_memory() for _ in range(3)]
+    out_f64 = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(2)]
+    h2d = nb + 8 * (n + 1) + 8 * n
+    d2h = nb + 3 * 4 * n + 2 * 8 * n
+    stream = torch.cuda.Stream(device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=torch.device("cuda", dev))
+    h = Hero(device=dev, stream=stream.cuda_stream, **kw)
+
+    def e2e_step():
+        # host buffers in, corrected reads and statistics out, every step
+        h.set_queries_ptr(seq_p.data_ptr(), off_p.data_ptr(), uid_p.data_ptr(), n, nb)
+        h.round(graph=True)
+        h.fetch_ptr(out_seq.data_ptr(), out_u32[0].data_ptr(), out_u32[1].data_ptr(),
+                    out_u32[2].data_ptr(), out_f64[0].data_ptr(), out_f64[1].data_ptr())
+
+    def device_step(graph=True):
+        h.round(graph=graph)
+
+    # warm-up: the first round runs eagerly (plain form) and is captured as a
+    # graph; later rounds replay it (the batched form)
+    for _ in range(warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+
+    def timed(fn, k):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        barrier()
+        torch.cuda.synchronize()
+        for a, b in ev:
+            flush_l2(stream, flush)
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3)
+
+    s0 = h.stats()
+    if clocks:
+        with ClockSampler(dev) as clk:
+            t_dev = timed(device_step, steps)
+        clock_summary = clk.summary()
+    else:
+        t_dev = timed(device_step, steps)
+        clock_summary = None
+    s1 = h.stats()
+    t_e2e = timed(e2e_step, steps)
+    p0 = h.stats()
+    plain_steps = max(1, min(steps, 2))
+    t_plain = timed(lambda: device_step(graph=False), plain_steps)
+    p1 = h.stats()
+    h.close()
+
+    launches = s1["kernel_launches"] - s0["kernel_launches"]
+    if launches == 0:  # graph replays launch kernels without host calls: count one plain round
+        launches = (p1["kernel_launches"] - p0["kernel_launches"]) // plain_steps * steps
+    cells = s1["dp_cells"] - s0["dp_cells"]
+    dp_ms = s1["ms_dp_kernel"] - s0["ms_dp_kernel"]
+    per = {k: round((p1[k] - p0[k]) / plain_steps, 3)
+           for k in ("ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_dp_kernel", "ms_record",
+                     "ms_vote", "ms_consensus", "ms_align_wall")}
+    dp_launches = steps * ((n + 131071) // 131072)  # one DP launch per subject batch
+    # seeding against HBM: per probe one 24-byte key+value slot read, per hit the
+    # hit value (8 B) read and the hit tuple (16 B) written, the subject reads at
+    # 2 bits a base (algorithmic bytes of the probe phase)
+    probes = (p1["probes"] - p0["probes"]) / plain_steps
+    hits = (p1["hits"] - p0["hits"]) / plain_steps
+    seed_bytes = 24 * probes + 24 * hits + nb / 4
+    seed_ms = per["ms_seed"]
+    hbm_peak, hbm_src = hbm_peak_gbs()
+    seed_gbs = seed_bytes / (seed_ms / 1e3) / 1e9 if seed_ms > 0 else None
+    return {
+        "value": world * nb * steps / t_dev, "ms_per_step": 1e3 * t_dev / steps,
+        "e2e": {"value": world * nb * steps / t_e2e, "unit": "bases/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": dp_roofline(cells, dp_ms, kw["aligner"], peaks, dp_launches),
+        "seeding_roofline": {"bound": "hbm", "kernels": "k_probe (count, emit) + k_sort_hits",
+                             "achieved": seed_gbs, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": (seed_gbs / hbm_peak) if seed_gbs else None,
+                             "algorithmic_bytes_per_step": seed_bytes, "peak_source": hbm_src},
+        "gcups": cells / (dp_ms / 1e3) / 1e9 if dp_ms > 0 else None,
+        "form": "batched (whole round replayed as one CUDA graph)",
+        "plain_form": {"value": world * nb * plain_steps / t_plain,
+                       "ms_per_step": 1e3 * t_plain / plain_steps, "stage_ms_per_step": per},
+        "clocks": clock_summary, "gpu_launches": launches,
+        "work_per_step": {"dp_cells": cells // steps,
+                          "dp_segments": (s1["dp_segments"] - s0["dp_segments"]) // steps,
+                          "probes": int(probes), "hits": int(hits)},
+    }
+
+
 def bench_hero(args):
     import torch
     import torch.distributed as dist
 
-    from hero_b200 import Hero, build, shard
+    from hero_b200 import build, shard
     if not os.environ.get("HERO_B200_LIB"):
         build.build_library()
 
@@ -447,168 +635,62 @@ def bench_hero(args):
     def max_over_ranks(x: float) -> float:
         return shard.max_over_ranks(x, device="cuda")
 
-    served_in = None
-    if args.served_jobs and world == 1 and not args.profile and args.workload == "config2":
-        served_in = served_jobs(args.served_jobs, args.jobs_scale or 0.02)
     rs, kw, flags, desc = make_workload(args.workload, args.genome_bp)
-    n, nb = rs.n, rs.total_bases
     log(f"[rank {rank}] workload: {desc}")
-
-    # pinned host buffers (the C ABI reads host memory)
-    seq_p = torch.from_numpy(rs.seq).pin_memory()
-    off_p = torch.from_numpy(rs.off.view(np.int64)).pin_memory()
-    uid_p = torch.from_numpy(rs.names.astype(np.int64)).pin_memory()
-    out_seq = torch.empty(nb, dtype=torch.uint8).pin_memory()
-    out_u32 = [torch.empty(n, dtype=torch.int32).pin_memory() for _ in range(3)]
-    out_f64 = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(2)]
-    h2d = nb + 8 * (n + 1) + 8 * n
-    d2h = nb + 3 * 4 * n + 2 * 8 * n
-
-    stream = torch.cuda.Stream(device=dev)
-    h = Hero(device=dev, stream=stream.cuda_stream, **kw)
-
-    def e2e_step():
-        # host buffers in, corrected reads and statistics out, every step
-        h.set_queries_ptr(seq_p.data_ptr(), off_p.data_ptr(), uid_p.data_ptr(), n, nb)
-        h.round(graph=True)
-        h.fetch_ptr(out_seq.data_ptr(), out_u32[0].data_ptr(), out_u32[1].data_ptr(),
-                    out_u32[2].data_ptr(), out_f64[0].data_ptr(), out_f64[1].data_ptr())
-
-    def device_step(graph=True):
-        h.round(graph=graph)
-
     if args.profile:
-        h.set_queries_ptr(seq_p.data_ptr(), off_p.data_ptr(), uid_p.data_ptr(), n, nb)
-        for _ in range(args.warmup + args.steps):
-            device_step(graph=False)
-        torch.cuda.synchronize()
-        log(json.dumps({"rounds": args.warmup + args.steps, "stats": h.stats()}))
-        h.close()
+        from hero_b200 import Hero
+        with Hero(device=dev, **kw) as h:
+            h.set_queries(rs.seq, rs.off, rs.names)
+            for _ in range(args.warmup + args.steps):
+                h.round(graph=False)
+            torch.cuda.synchronize()
+            log(json.dumps({"rounds": args.warmup + args.steps, "stats": h.stats()}))
         return
 
-    # warm-up: the first round runs eagerly (plain form) and is captured as a
-    # graph; later rounds replay it (the batched form)
-    for _ in range(args.warmup):
-        e2e_step()
-    torch.cuda.synchronize()
-
-    def timed(fn, steps):
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(steps)]
-        barrier()
-        torch.cuda.synchronize()
-        for a, b in ev:
-            a.record(stream)
-            fn()
-            b.record(stream)
-        torch.cuda.synchronize()
-        barrier()
-        return max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3)
-
-    # --- value: device-resident reads, batched form ------------------------
-    s0 = h.stats()
-    with ClockSampler(dev) as clk:
-        t_dev = timed(device_step, args.steps)
-    s1 = h.stats()
-    value = world * nb * args.steps / t_dev
-
-    # --- e2e: host buffers through the C ABI ------------------------------
-    t_e2e = timed(e2e_step, args.steps)
-    e2e_value = world * nb * args.steps / t_e2e
-
-    # --- the plain form (one launch per stage, host-sized buffers) ---------
-    p0 = h.stats()
-    plain_steps = max(1, min(args.steps, 2))
-    t_plain = timed(lambda: device_step(graph=False), plain_steps)
-    p1 = h.stats()
-    plain_value = world * nb * plain_steps / t_plain
-
-    launches = s1["kernel_launches"] - s0["kernel_launches"]
-    if launches == 0:  # graph replays launch kernels without host calls: count one plain round
-        launches = (p1["kernel_launches"] - p0["kernel_launches"]) // plain_steps * args.steps
-    cells = s1["dp_cells"] - s0["dp_cells"]
-    dp_ms = s1["ms_dp_kernel"] - s0["ms_dp_kernel"]
-    ops_per_cell = 10 if kw["aligner"] == "affine" else 6
-    achieved = cells * ops_per_cell / (dp_ms / 1e3) / 1e12 if dp_ms > 0 else None
-    peak = int_peak_tops(dev)
-    steps = args.steps
-    per = {k: round((p1[k] - p0[k]) / plain_steps, 3)
-           for k in ("ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_dp_kernel", "ms_record",
-                     "ms_vote", "ms_consensus", "ms_align_wall")}
-    # one DP launch per subject batch of 131072 reads
-    dp_launches = steps * ((n + 131071) // 131072)
-    traffic = (DP_DRAM_BYTES_PER_CELL * cells / dp_launches
-               if DP_DRAM_BYTES_PER_CELL is not None else None)
-    clocks = clk.summary()
-    # seeding against HBM: per probe one 24-byte key+value slot read, per hit the
-    # hit value (8 B) read and the hit tuple (16 B) written, the subject reads at
-    # 2 bits a base (algorithmic bytes of the probe phase)
-    probes = (p1["probes"] - p0["probes"]) / plain_steps
-    hits = (p1["hits"] - p0["hits"]) / plain_steps
-    seed_bytes = 24 * probes + 24 * hits + nb / 4
-    seed_ms = per["ms_seed"]
-    hbm_peak, hbm_src = hbm_peak_gbs()
-    seed_gbs = seed_bytes / (seed_ms / 1e3) / 1e9 if seed_ms > 0 else None
-
-    h.close()
+    peaks = int_peaks(dev)
+    main = measure_workload(rs, kw, dev, args.steps, args.warmup, peaks, world, barrier,
+                            max_over_ranks)
+    solo = rank == 0 and world == 1
+    affine = None
+    if solo and args.workload == "config1" and not args.no_affine_block:
+        rs2, kw2, flags2, desc2 = make_workload("config2")
+        affine = measure_workload(rs2, kw2, dev, args.steps, args.warmup, peaks)
+        affine["config"] = workload_config(rs2, flags2, desc2)
+        affine["reference_full_run"] = {
+            "seconds": REF_CONFIG2_FULL_SECONDS_8T, "threads": 8,
+            "bases_per_s": rs2.total_bases / REF_CONFIG2_FULL_SECONDS_8T,
+            "note": "the reference on this whole workload, timed once on the 8 cores of the "
+                    "build host by tests/golden/make_golden.py (not timed in this run)"}
+        del rs2
     served = None
-    if served_in is not None:
-        with ClockSampler(dev) as sclk:
-            served = run_served(*served_in, dev)
-        served["clocks"] = sclk.summary()
-        served["workload"] = (f"{args.served_jobs} jobs, Poisson arrivals, genome log-uniform "
-                              f"0.5-20 Mbp x {args.jobs_scale or 0.02}, L in {{100,150,250}}, "
-                              "coverage U(20,80), affine/indel errors")
-
-    aln = None
-    if rank == 0 and world == 1 and not args.profile and not args.no_alignment_output:
+    if solo and args.served_jobs:
+        served = run_served_block(args, dev)
+    aln = merge = cpu = file_e2e = None
+    if solo and not args.no_alignment_output:
         aln = measure_alignment_output(rs, kw, dev)
-    merge = None
-    if rank == 0 and world == 1 and not args.profile and not args.no_merge:
+    if solo and not args.no_merge:
         merge = measure_merge(dev)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if solo and not args.no_cpu_baseline:
         cpu = measure_cpu_baseline(args)
-    file_e2e = measure_file_e2e(rs, flags) if rank == 0 and world == 1 and not args.profile else None
+    if solo:
+        file_e2e = measure_file_e2e(rs, flags)
 
     if rank == 0:
         line = {
-            "metric": "corrected bases/s", "value": value, "unit": "bases/s", "n_gpus": world,
-            "steps": steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_dev / steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32",
+            "metric": "corrected bases/s", "value": main["value"], "unit": "bases/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": main["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, no public dataset)",
-            "config": {"workload": desc, "reads": n, "bases": nb, "flags": " ".join(flags),
-                       "parallelism": f"independent jobs x{world}",
-                       "l2": f"inputs larger than L2 ({nb / 1e6:.0f} Mbp reads, "
-                             f"{20 * nb / 1e9:.1f} GB vote matrix)"},
-            "e2e": {"value": e2e_value, "unit": "bases/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "alu", "kernel": "k_dp (banded affine DP + traceback)",
-                         "achieved": achieved, "peak": peak, "unit": "Tops/s",
-                         "frac": (achieved / peak) if (achieved and peak) else None,
-                         "traffic": traffic,
-                         "ops_per_cell": ops_per_cell,
-                         "peak_source": "int add+max microbenchmark in this run "
-                                        "(MEASURED_PEAKS.json has no integer peak)"},
-            "seeding_roofline": {"bound": "hbm", "kernels": "k_probe (count, emit) + k_sort_hits",
-                                 "achieved": seed_gbs, "peak": hbm_peak, "unit": "GB/s",
-                                 "frac": (seed_gbs / hbm_peak) if seed_gbs else None,
-                                 "algorithmic_bytes_per_step": seed_bytes,
-                                 "peak_source": hbm_src},
-            "gcups": cells / (dp_ms / 1e3) / 1e9 if dp_ms > 0 else None,
-            "form": "batched (whole round replayed as one CUDA graph)",
-            "plain_form": {"value": plain_value, "ms_per_step": 1e3 * t_plain / plain_steps,
-                           "stage_ms_per_step": per},
-            "cpu_baseline": cpu,
-            "file_e2e": file_e2e,
-            "clocks": clocks,
-            "gpu_launches": launches,
-            "work_per_step": {"dp_cells": cells // steps,
-                              "dp_segments": (s1["dp_segments"] - s0["dp_segments"]) // steps},
-            "served": served,
-            "alignment_output": aln,
+            "config": workload_config(rs, flags, desc),
+            "parallelism": f"one copy of the job per rank x{world}",
+            "e2e": main["e2e"],
+            "roofline": main["roofline"],
+            "seeding_roofline": main["seeding_roofline"],
+            "gcups": main["gcups"], "form": main["form"], "plain_form": main["plain_form"],
+            "cpu_baseline": cpu, "file_e2e": file_e2e, "clocks": main["clocks"],
+            "gpu_launches": main["gpu_launches"], "work_per_step": main["work_per_step"],
+            "affine_batched": affine, "served": served, "alignment_output": aln,
             "merge": merge,
         }
         print(json.dumps(line), flush=True)
@@ -671,6 +753,7 @@ def bench_sharded(args):
     stream = torch.cuda.Stream(device=dev)
     h = Hero(device=dev, stream=stream.cuda_stream, **kw)
     h.set_queries_ptr(seq_p.data_ptr(), off_p.data_ptr(), uid_p.data_ptr(), n, nb)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=torch.device("cuda", dev))
 
     def device_step():
         h.reset_votes()
@@ -694,6 +777,7 @@ def bench_sharded(args):
             dist.barrier()
         torch.cuda.synchronize()
         for e0, e1 in ev:
+            flush_l2(stream, flush)
             e0.record(stream)
             fn()
             e1.record(stream)
@@ -711,11 +795,11 @@ def bench_sharded(args):
     t_e2e = timed(e2e_step, args.steps)
     cells = s1["dp_cells"] - s0["dp_cells"]
     dp_ms = s1["ms_dp_kernel"] - s0["ms_dp_kernel"]
-    ops_per_cell = 10 if kw["aligner"] == "affine" else 6
-    achieved = cells * ops_per_cell / (dp_ms / 1e3) / 1e12 if dp_ms > 0 else None
-    peak = int_peak_tops(dev)
     launches = s1["kernel_launches"] - s0["kernel_launches"]
     h.close()
+    roof = dp_roofline(cells, dp_ms, kw["aligner"], int_peaks(dev),
+                       args.steps * ((b - a + 131071) // 131072))
+    roof["kernel"] += " (rank 0's DP launches)"
     if rank == 0:
         line = {
             "metric": "corrected bases/s", "value": nb * args.steps / t_dev, "unit": "bases/s",
@@ -723,18 +807,13 @@ def bench_sharded(args):
             "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, no public dataset)",
-            "config": {"workload": desc, "reads": n, "bases": nb, "flags": " ".join(flags),
-                       "parallelism": f"one job, subject reads sharded x{world}, votes summed "
-                                      "by one all-reduce",
-                       "l2": f"inputs larger than L2 ({nb / 1e6:.0f} Mbp reads, "
-                             f"{20 * nb / 1e9:.1f} GB vote state)"},
+            "config": workload_config(rs, flags, desc),
+            "parallelism": f"one job, subject reads sharded x{world}, votes summed by one "
+                           "all-reduce",
             "e2e": {"value": nb * args.steps / t_e2e, "unit": "bases/s",
                     "h2d_bytes_per_step": nb + 8 * (n + 1) + 8 * n,
                     "d2h_bytes_per_step": nb + 3 * 4 * n + 2 * 8 * n},
-            "roofline": {"bound": "alu", "kernel": "k_dp (rank 0's DP launches)",
-                         "achieved": achieved, "peak": peak, "unit": "Tops/s",
-                         "frac": (achieved / peak) if (achieved and peak) else None,
-                         "traffic": None, "ops_per_cell": ops_per_cell},
+            "roofline": roof,
             "cpu_baseline": None,
             "exchange_bytes_per_rank": 20 * nb,
             "clocks": clk.summary(),
@@ -772,11 +851,12 @@ def measure_merge(dev):
 
 def main():
     args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         bench_reference(args)
     elif args.workload == "config4":
         bench_served(args)
-    elif args.shard:
+    elif args.shard or (world > 1 and not args.replicas):
         bench_sharded(args)
     else:
         bench_hero(args)

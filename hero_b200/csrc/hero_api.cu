@@ -871,8 +871,21 @@ extern "C" int hero_round(hero_ctx *c, uint32_t flags) {
     cudaSetDevice(c->dev);
     const bool graph = (flags & HERO_ROUND_GRAPH) != 0;
     if (graph && c->gexec && c->plan_ok && c->plan_fp == c->qfp) {
+        // the device checks of the eager path, read after the replay: buffers are
+        // sized from the plan, so a batch that outgrew it would raise the
+        // lifetime overflow count (the per-batch flag is cleared by every batch)
+        unsigned long long before[C_COUNT], after[C_COUNT];
+        HERO_TRY(c->cuda(cudaMemcpyAsync(before, c->counters.p, sizeof(before), cudaMemcpyDeviceToHost, c->st),
+                         "graph round: counters"));
         HERO_TRY(c->cuda(cudaGraphLaunch(c->gexec, c->st), "graph launch"));
+        HERO_TRY(c->cuda(cudaMemcpyAsync(after, c->counters.p, sizeof(after), cudaMemcpyDeviceToHost, c->st),
+                         "graph round: counters"));
         HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "graph round"));
+        for (int i = 0; i < C_COUNT; i++) c->ctr[i] = after[i];
+        if (after[C_OVERFLOW_ALL] != before[C_OVERFLOW_ALL]) {
+            c->plan_ok = false;  // the next round runs eagerly and re-plans
+            return c->fail(HERO_E_STATE, "graph round: chain buffer overflow (plan outgrown)");
+        }
         std::vector<unsigned long long> t(2 * c->plan.size());
         HERO_TRY(c->cuda(cudaMemcpy(t.data(), c->stamps.p, t.size() * 8, cudaMemcpyDeviceToHost),
                          "graph stamps"));

@@ -76,6 +76,7 @@ enum Counter : int {
     C_ANOMALY,
     C_OVERFLOW,
     C_WIN,          // winners of the current batch (compacted list length)
+    C_OVERFLOW_ALL, // overflows over the context's life (C_OVERFLOW is cleared per batch)
     C_COUNT
 };
 

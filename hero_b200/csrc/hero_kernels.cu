@@ -635,6 +635,7 @@ __global__ void __launch_bounds__(256)
             if (cs + tk > cap_chains || ks + tkeys > cap_keys || ds + tdp > cap_segs) {
                 overflow = 1;
                 atomicAdd(&counters[C_OVERFLOW], 1ull);
+                atomicAdd(&counters[C_OVERFLOW_ALL], 1ull);
             }
             seg_chain_start[seg] = overflow ? 0u : uint32_t(cs);
             seg_chain_count[seg] = overflow ? 0u : tk;

@@ -23,7 +23,8 @@ namespace {
 
 constexpr int kNoallocMaxSide = 128;
 constexpr int kNoallocThreads = 8192;
-constexpr int kNoallocBlock = 128;
+// 32-thread blocks: 256 of them, so every one of a B200's 148 SMs gets work
+constexpr int kNoallocBlock = 32;
 constexpr int kNoallocStrips = (kNoallocMaxSide + kStripW - 1) / kStripW;
 // per thread: traceback codes (u16 per strip row), the boundary column and the
 // base codes of the segment's two sides; all interleaved by thread
@@ -81,9 +82,12 @@ __global__ void __launch_bounds__(kNoallocBlock)
         const int64_t ls_read = si < n_subj ? int64_t(subj_off[si + 1] - subj_off[si]) : -1;
         const int64_t lq_read = qi < n_query ? int64_t(query_off[qi + 1] - query_off[qi]) : -1;
         const int32_t ls = s1 - s0, lq = q1 - q0;
-        const uint64_t cap = ops_off[i + 1] - ops_off[i];
+        // the output slot: ops_off must not decrease (a decreasing pair would
+        // wrap the unsigned capacity and pass the size test below)
+        const uint64_t o0 = ops_off[i], o1 = ops_off[i + 1];
+        const uint64_t cap = o1 >= o0 ? o1 - o0 : 0;
         if (ls_read < 0 || lq_read < 0 || s0 < 0 || ls < 1 || s1 > ls_read || q0 < 0 || lq < 1 ||
-            q1 > lq_read || ls > kNoallocMaxSide || lq > kNoallocMaxSide ||
+            q1 > lq_read || ls > kNoallocMaxSide || lq > kNoallocMaxSide || o1 < o0 ||
             cap < uint64_t(ls + lq)) {
             nops[i] = -1;
             atomicExch(&g_noalloc_status, 1);
@@ -126,9 +130,21 @@ __global__ void __launch_bounds__(kNoallocBlock)
     }
 }
 
+// the array's device address per device, looked up on the first call made on
+// that device; only a successful lookup is kept, so a call that failed (for
+// instance one made while its stream was being captured) is retried by the next
 void *g_scratch_ptr[64];
-std::once_flag g_scratch_once[64];
-cudaError_t g_scratch_err[64];
+std::mutex g_scratch_mu;
+
+void *scratch_address(int dev) {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) == cudaSuccess) g_scratch_ptr[dev] = p;
+        else (void)cudaGetLastError();  // a failed lookup leaves no error behind for the caller
+    }
+    return g_scratch_ptr[dev];
+}
 
 }  // namespace
 }  // namespace hero
@@ -152,18 +168,16 @@ extern "C" int hero_align_segments_noalloc(int affine, const uint8_t *subj, cons
         return HERO_E_INPUT;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HERO_E_CUDA;
-    // once per device, with that device current: the array's device address
-    std::call_once(g_scratch_once[dev], [dev]() {
-        g_scratch_err[dev] = cudaGetSymbolAddress(&g_scratch_ptr[dev], g_noalloc_scratch);
-    });
-    if (g_scratch_err[dev] != cudaSuccess || !g_scratch_ptr[dev]) return HERO_E_CUDA;
+    // the array's device address, with this device current (looked up once)
+    void *scratch = scratch_address(dev);
+    if (!scratch) return HERO_E_CUDA;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const int zero = 0;
     if (cudaMemcpyToSymbolAsync(g_noalloc_status, &zero, sizeof(int), 0, cudaMemcpyHostToDevice,
                                 st) != cudaSuccess)
         return HERO_E_CUDA;
     const unsigned grid = kNoallocThreads / kNoallocBlock;
-    uint8_t *scr = reinterpret_cast<uint8_t *>(g_scratch_ptr[dev]);
+    uint8_t *scr = reinterpret_cast<uint8_t *>(scratch);
     if (affine) {
         k_dp_noalloc<true><<<grid, kNoallocBlock, 0, st>>>(
             scr, subj, subj_off, n_subj, query, query_off, n_query, n_seg, seg_subject, seg_orient,

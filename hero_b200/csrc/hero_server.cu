@@ -124,9 +124,9 @@ void hero_server::run() {
     // jobs still queued at shutdown fail
     for (uint64_t id : queue) {
         Job &j = jobs[id];
-        j.state = HERO_JOB_FAILED;
-        j.status = HERO_E_STATE;
         j.err = "server stopped";
+        j.status = HERO_E_STATE;
+        j.state = HERO_JOB_FAILED;
         failed++;
     }
     queue.clear();
@@ -230,9 +230,9 @@ void hero_server::run_round(std::vector<uint64_t> ids) {
             done++;
             bases_done += jb;
         } else {
-            j->state = HERO_JOB_FAILED;
-            j->status = st;
             j->err = err;
+            j->status = st;
+            j->state = HERO_JOB_FAILED;
             failed++;
         }
         // inputs are no longer needed
@@ -406,7 +406,10 @@ extern "C" const char *hero_job_error(hero_server *s, uint64_t job_id) {
     if (!s) return "";
     std::lock_guard<std::mutex> g(s->mu);
     auto it = s->jobs.find(job_id);
-    return it == s->jobs.end() ? "" : it->second.err.c_str();
+    // the worker writes err before it marks the job failed and never after, so
+    // the string is stable from then until hero_job_release frees the job
+    if (it == s->jobs.end() || it->second.state != HERO_JOB_FAILED) return "";
+    return it->second.err.c_str();
 }
 
 extern "C" int hero_job_release(hero_server *s, uint64_t job_id) {

@@ -246,9 +246,10 @@ int hero_align_segments(hero_ctx *ctx, int affine, const uint8_t *subj, const ui
  * library keeps on every device where it has run, until the process exits.
  * Limits: max_side (the caller's bound on either side of any segment) must be
  * 1..128, else HERO_E_INPUT before any launch; a segment beyond 128 on a side,
- * outside its read or with too little ops room gets nops[i] = -1 and the call
- * returns HERO_E_INPUT.  The first call on a device looks up the working
- * array's address: make it before any stream capture.  Calls share the array,
+ * outside its read, with too little ops room or with ops_off[i+1] < ops_off[i]
+ * gets nops[i] = -1 and the call returns HERO_E_INPUT.  The first call on a
+ * device looks up the working array's address: make it before any stream
+ * capture (a lookup that fails is retried by the next call).  Calls share the array,
  * so calls that overlap on the GPU (other streams, other host threads) race;
  * the call runs on `stream` and returns after it has completed. */
 int hero_align_segments_noalloc(int affine, const uint8_t *subj, const uint64_t *subj_off,
@@ -320,7 +321,8 @@ int hero_job_wait(hero_server *s, uint64_t job_id, int64_t timeout_ms, hero_job_
 int hero_job_result(hero_server *s, uint64_t job_id, uint8_t *seq_out, uint32_t *imin,
                     uint32_t *imed, uint32_t *imax, double *mismatch_rate, double *gc_content,
                     uint8_t *good_out);
-/* Error message of a failed job ("" otherwise); valid until the job is released. */
+/* Error message of a failed job ("" for a job that has not failed).  The
+ * pointer stays valid until hero_job_release of that job; do not use it after. */
 const char *hero_job_error(hero_server *s, uint64_t job_id);
 /* Frees a finished job's results. */
 int hero_job_release(hero_server *s, uint64_t job_id);

@@ -35,6 +35,7 @@ from hero_b200 import synth  # noqa: E402
 FULL = {
     "config1_full": ("synth.config1()", lambda: synth.config1(), []),
     "config2_full": ("synth.config2()", lambda: synth.config2(), ["-a", "a"]),
+    "config3_full": ("synth.config3()", lambda: synth.config3(), ["-a", "a"]),
     "config3_reduced": ("synth.config3(genome_bp=200000)",
                         lambda: synth.config3(genome_bp=200_000), ["-a", "a"]),
     "config5_reduced": ("synth.config5(genome_bp=1000000)",
@@ -106,10 +107,19 @@ def run_reference_mapping(fq: str, flags: list[str], workdir: str) -> bytes:
         return f.read()
 
 
+def _host_ram_gb() -> float:
+    with open("/proc/meminfo") as f:
+        for line in f:
+            if line.startswith("MemTotal:"):
+                return round(int(line.split()[1]) / 2**20, 1)
+    return 0.0
+
+
 def main_full(names: list[str]):
+    import resource
     import time
     path = os.path.join(HERE, "manifest_full.json")
-    manifest = json.load(open(path)) if os.path.exists(path) else {}
+    done = {}
     threads = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
         for name in names:
@@ -119,13 +129,21 @@ def main_full(names: list[str]):
             fq = os.path.join(d, "in.fq")
             with open(fq, "wb") as f:
                 f.write(fqb)
+            nreads, fq_md5 = rs.n, md5(fqb)
+            del rs, fqb
             t0 = time.perf_counter()
             fa, info = run_reference(fq, flags, d)
             secs = time.perf_counter() - t0
-            manifest[name] = {"generator": call, "flags": flags, "reads": rs.n,
-                              "fastq_md5": md5(fqb), "fasta_md5": md5(fa), "info_md5": md5(info),
-                              f"reference_seconds_{threads}_threads": round(secs, 2)}
-            print(name, manifest[name], flush=True)
+            rss = resource.getrusage(resource.RUSAGE_CHILDREN).ru_maxrss / 2**20  # KiB -> GiB
+            done[name] = {"generator": call, "flags": flags, "reads": nreads,
+                          "fastq_md5": fq_md5, "fasta_md5": md5(fa), "info_md5": md5(info),
+                          f"reference_seconds_{threads}_threads": round(secs, 2),
+                          "reference_peak_rss_gb": round(rss, 2),
+                          "host_ram_gb": _host_ram_gb()}
+            print(name, done[name], flush=True)
+    # re-read before writing: other entries may have been regenerated meanwhile
+    manifest = json.load(open(path)) if os.path.exists(path) else {}
+    manifest.update(done)
     with open(path, "w") as f:
         json.dump(manifest, f, indent=1, sort_keys=True)
 

@@ -5,7 +5,8 @@ embedded in a host framework that owns the GPU allocator and hands out device
 buffers.  Here the test plays that caller: it owns every device buffer (made
 with torch), calls the entry point through the C ABI twice in a row, and
 checks each result against the regular hero_align_segments entry point on the
-same segments (exact: the ops of a DP path are integers).
+same segments and directly against the oracle's aligner, segment by segment
+(exact: the ops of a DP path are integers).
 """
 import ctypes as C
 
@@ -105,7 +106,25 @@ def _compare(ops_a, off_a, n_a, ops_b, n_b):
         assert np.array_equal(a, b), i
 
 
-def test_noalloc_matches_regular_entry_point_twice():
+COMP = np.arange(256, dtype=np.uint8)
+COMP[ord("A")], COMP[ord("T")], COMP[ord("C")], COMP[ord("G")] = ord("T"), ord("A"), ord("G"), ord("C")
+
+
+def _oracle_ops(oracle, affine, seq, off, sg, i):
+    """The oracle's aligner on segment i: the subject slice (of the reverse
+    complement for orientation 1) against the query slice."""
+    si, qi = int(sg["subject"][i]), int(sg["query"][i])
+    sread = seq[int(off[si]):int(off[si + 1])]
+    if sg["orient"][i]:
+        sread = COMP[sread[::-1]]
+    s = bytes(sread[int(sg["s0"][i]):int(sg["s1"][i])])
+    q = bytes(seq[int(off[qi]) + int(sg["q0"][i]):int(off[qi]) + int(sg["q1"][i])])
+    f = int(sg["flags"][i])
+    ops, _ = oracle.align(affine, s, q, int(sg["band"][i]), f & 1, (f >> 1) & 1)
+    return ops
+
+
+def test_noalloc_matches_regular_entry_point_twice(oracle):
     lib = _lib()
     # first call: affine aligner; second call, same working array: global aligner
     for call, (seed, affine) in enumerate(((11, 1), (12, 0))):
@@ -114,6 +133,9 @@ def test_noalloc_matches_regular_entry_point_twice():
         rc, got_ops, got_n = _noalloc(lib, affine, seq, off, sg, ops_off)
         assert rc == 0, f"call {call}: rc {rc}"
         _compare(want_ops, ops_off, want_n, got_ops, got_n)
+        for i in range(len(got_n)):
+            got = got_ops[int(ops_off[i]):int(ops_off[i]) + int(got_n[i])]
+            assert np.array_equal(got, _oracle_ops(oracle, affine, seq, off, sg, i)), (call, i)
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit():
@@ -136,3 +158,13 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
     rc, _, n = _noalloc(lib, 1, seq, off, sg, ops_off)
     assert sg["s1"][0] > MAX_SIDE
     assert rc == -1 and n[0] == -1 and (n[1:] > 0).all()
+    # a decreasing ops_off pair: refused for that segment instead of writing
+    # through a wrapped capacity
+    seq, off, sg = _segments(14, n_reads=40, n_seg=50)
+    cap = ((sg["s1"] - sg["s0"]) + (sg["q1"] - sg["q0"])).astype(np.uint64)
+    ops_off = np.zeros(len(cap) + 1, np.uint64)
+    ops_off[1:] = np.cumsum(cap)
+    ops_off[3] = ops_off[1]  # ops_off[3] < ops_off[2]: segment 2 has no valid slot
+    rc, _, n = _noalloc(lib, 1, seq, off, sg, ops_off)
+    assert rc == -1 and n[2] == -1
+    assert (np.delete(n, 2) > 0).all()  # the other segments are still aligned
