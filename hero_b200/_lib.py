@@ -74,14 +74,17 @@ class DpTuning(C.Structure):
                 ("pair_strips", C.c_uint32), ("chunk_strips", C.c_uint32)]
 
 
-def load_tuning(path: str | None = None) -> list[dict]:
-    """Classes recorded by the autotuner (empty when there is no record)."""
+def load_tuning(path: str | None = None, aligner: str = "affine") -> list[dict]:
+    """Classes recorded by the autotuner for an aligner (empty when there is no
+    record): "classes" holds the affine aligner's, "classes_global" the global's."""
     import json
     p = path or os.environ.get("HERO_B200_TUNING") or TUNING_PATH
     if not p or not os.path.exists(p):
         return []
     with open(p) as f:
-        return json.load(f).get("classes", [])
+        rec = json.load(f)
+    key = "classes" if aligner in ("a", "affine") else "classes_global"
+    return rec.get(key, [])
 
 
 class JobInfo(C.Structure):
@@ -218,7 +221,7 @@ class Hero:
         self.nq = 0
         self.nqb = 0
         # DP kernel shapes: the given classes, a record file, or the default record
-        self.set_tuning(load_tuning(tuning) if not isinstance(tuning, list) else tuning)
+        self.set_tuning(load_tuning(tuning, aligner) if not isinstance(tuning, list) else tuning)
 
     def set_tuning(self, classes: list[dict]):
         """DP kernel shapes per class of batch ([] = the library's defaults)."""
@@ -428,7 +431,8 @@ class HeroServer:
             raise HeroError(f"hero_server_create failed: {ERRORS.get(rc, rc)}")
         self.h = h
         self._sizes: dict[int, tuple[int, int]] = {}
-        classes = load_tuning(tuning) if not isinstance(tuning, list) else tuning
+        classes = (load_tuning(tuning, kw.get("aligner", "global")) if not isinstance(tuning, list)
+                   else tuning)
         arr = (DpTuning * max(1, len(classes)))()
         for i, t in enumerate(classes):
             arr[i] = DpTuning(int(t["rows_max"]), int(t["warps_per_block"]),

@@ -12,7 +12,11 @@ at or above it, and the last class covers every longer batch.  Shapes never
 change results: the tests check every candidate against the default on the
 same reads.
 
-    python -m hero_b200.autotune [--out PATH] [--genome-bp N]
+Each aligner has its own classes ("classes" for the affine aligner,
+"classes_global" for the global one): the two recurrences differ in
+instructions and registers, so their fastest shapes may differ.
+
+    python -m hero_b200.autotune [--out PATH] [--genome-bp N] [--aligner affine|global|both]
 """
 from __future__ import annotations
 
@@ -60,10 +64,11 @@ def class_bounds(rows: list[int]) -> list[int]:
     return [(a + b) // 2 for a, b in zip(rows, rows[1:])] + [ROWS_LAST]
 
 
-def tune(genome_bp: int = 60_000, device: int = 0, read_lengths=READ_LENGTHS, log=print) -> dict:
+def tune(genome_bp: int = 60_000, device: int = 0, read_lengths=READ_LENGTHS, log=print,
+         aligner: str = "affine") -> dict:
     from hero_b200 import Hero
     out = {"device": None, "genome_bp": genome_bp, "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
-           "classes": []}
+           "aligner": aligner, "classes": []}
     try:
         import torch
         out["device"] = torch.cuda.get_device_name(device)
@@ -71,7 +76,7 @@ def tune(genome_bp: int = 60_000, device: int = 0, read_lengths=READ_LENGTHS, lo
         pass
     for read_len in sorted(read_lengths):
         reads = sample(read_len, genome_bp)
-        with Hero(aligner="affine", device=device, tuning=[]) as h:
+        with Hero(aligner=aligner, device=device, tuning=[]) as h:
             h.set_queries(reads.seq, reads.off, reads.names)
             timings = []
             for shape in candidates():
@@ -94,8 +99,17 @@ def main():
     ap.add_argument("--out", default=TUNING_PATH)
     ap.add_argument("--genome-bp", type=int, default=60_000)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--aligner", default="both", choices=["affine", "global", "both"])
     args = ap.parse_args()
-    rec = tune(args.genome_bp, args.device)
+    rec = {}
+    if os.path.exists(args.out):
+        with open(args.out) as f:
+            rec = json.load(f)
+    for aligner in (("affine", "global") if args.aligner == "both" else (args.aligner,)):
+        r = tune(args.genome_bp, args.device, aligner=aligner)
+        key = "classes" if aligner == "affine" else "classes_global"
+        rec.update({k: r[k] for k in ("device", "genome_bp", "when")})
+        rec[key] = r["classes"]
     with open(args.out, "w") as f:
         json.dump(rec, f, indent=1)
     print("wrote", os.path.abspath(args.out))

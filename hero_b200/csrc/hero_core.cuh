@@ -1113,19 +1113,37 @@ HERO_HD void dp_whole_left(int32_t wl, bool holds_c, int32_t (&f)[W], int32_t (&
 }
 
 // ---------------------------------------------------------------------------
-// Whole-band rows of two segments at once, as signed 16-bit halves of each
-// 32-bit register (segment A low, B high): one DPX instruction advances a cell
-// of each.  Two segments share a lane when they have the same rows, strips and
+// Whole-band rows of two segments at once, tagged.  Every state is held as
+// 4v + tag in a signed 16-bit half of a 32-bit register (segment A low, B
+// high), so one DPX instruction advances a cell of each segment.  The tag, in
+// the two low bits, names the move a value stands for, in the order that breaks
+// the reference's ties, so the 3-way max of a cell's tagged candidates is at
+// once its value (bits 2..15) and its traceback move (bits 0..1):
+//   affine: IX (up, tag 2) beats FM (diagonal, tag 1) beats IY (left, tag 0)
+//           on equal values -- BM1 is diagonal iff FM > IX && FM >= IY, else
+//           left iff IY > IX, else up (BandAligner.cpp:214-222);
+//   global: diagonal (tag 2) beats left (tag 1) beats up (tag 0) -- diagonal
+//           if >= both, else left if >= up (BandAligner.cpp:99-110).
+// The recurrences keep the tags right by construction: the affine FM carries
+// tag 1 (diagonal input M is stored clean, the score adds 4s + 1), IX tag 2
+// (FM + 4dx + 1 and IX + 4ex), IY tag 0 (FM + 4dy - 1 and IY + 4ex); the
+// global F and the affine M are stored clean (tag masked off) and each
+// candidate adds its tag.  Per cell that leaves one mask for the move, one
+// shift-add into the row's code word and one mask for the clean value.
+// Two segments share a lane when they have the same rows, strips and
 // align-left column (the shape key), so their wavefronts run in lockstep.
-// Every value of a whole-band matrix is a real score, -4(R+C) <= v <= R, and
-// the columns past C start at kNEG16 and lose at most 5 per row, so with
-// R + C <= kPairMaxSide no half ever wraps.
+// Every real value of a whole-band matrix lies in [-4(R+C) - 3, R], so with
+// R + C <= kPairMaxSide no half ever wraps; columns past C start at kPairPad
+// and are never read by a real cell (only cells to their right read them).
 // ---------------------------------------------------------------------------
-constexpr int32_t kNEG16 = -16384;
+constexpr int32_t kPairPad = -8192;
 constexpr int32_t kPairMaxSide = 2000;  // R + C of a segment in a packed pair
-constexpr int kTabWords2 = 40;          // per lane: int16 scores [2][4][8], diag words [2][4]
+constexpr int kTabWords2 = 40;          // per lane: int16 tagged scores [2][4][8], eq words [2][4]
+constexpr uint32_t kTagMask2 = 0x00030003u;
+constexpr uint32_t kLow2 = 0x55555555u;  // the low bit of every 2-bit field
 
 HERO_HD uint32_t pack2(int32_t lo, int32_t hi) { return (uint32_t(lo) & 0xffffu) | (uint32_t(hi) << 16); }
+HERO_HD uint32_t pack2s(int32_t v) { return pack2(v, v); }
 HERO_HD int32_t half_lo(uint32_t v) { return int32_t(int16_t(uint16_t(v & 0xffffu))); }
 HERO_HD int32_t half_hi(uint32_t v) { return int32_t(int16_t(uint16_t(v >> 16))); }
 
@@ -1134,7 +1152,7 @@ HERO_HD uint32_t add_max2(uint32_t a, uint32_t b, uint32_t c) {
 #if defined(__CUDA_ARCH__)
     return __viaddmax_s16x2(a, b, c);
 #else
-    const int32_t l = half_lo(a) + half_lo(b), h = half_hi(a) + half_hi(b);
+    const int32_t l = int16_t(uint16_t(half_lo(a) + half_lo(b))), h = int16_t(uint16_t(half_hi(a) + half_hi(b)));
     return pack2(l > half_lo(c) ? l : half_lo(c), h > half_hi(c) ? h : half_hi(c));
 #endif
 }
@@ -1153,101 +1171,142 @@ HERO_HD uint32_t max3_2(uint32_t a, uint32_t b, uint32_t c) {
 #endif
 }
 
-// per half: a >= b (lo, hi)
-HERO_HD void ge2(uint32_t a, uint32_t b, bool &lo, bool &hi) {
-#if defined(__CUDA_ARCH__)
-    (void)__vibmax_s16x2(a, b, &hi, &lo);
-#else
-    lo = half_lo(a) >= half_lo(b);
-    hi = half_hi(a) >= half_hi(b);
-#endif
-}
+// the tag a candidate of each move adds (see above)
+template <bool AFFINE>
+struct PairTags {
+    static constexpr int32_t diag = AFFINE ? 1 : 2, left = AFFINE ? 0 : 1, up = AFFINE ? 2 : 0;
+};
 
-// Tables of strip j0+1 .. j0+W for segments A and B: int16 scores per base
-// (tab16[seg][base][w]) and the diagonal codes (words 32.. : [seg][base]).
-template <int W>
+// Tables of strip j0+1 .. j0+W for segments A and B: the tagged diagonal
+// increment 4s + tag per base (tab16[seg][base][w]; columns past C never
+// match) and the match bits per base (words 32..: A's in the low 16 bits,
+// B's in the high, bit 2w for column w).
+template <bool AFFINE, int W>
 HERO_HD void dp_pair_table(const SegView &va, const SegView &vb, int32_t j0, uint32_t *tab) {
     uint16_t *sc = reinterpret_cast<uint16_t *>(tab);
     for (int h = 0; h < 2; h++) {
         const SegView &v = h ? vb : va;
-        uint32_t dg[4] = {0, 0, 0, 0};
+        uint32_t eq[4] = {0, 0, 0, 0};
         for (int32_t w = 0; w < W; w++) {
             const int32_t j = j0 + w + 1;
             const uint32_t b = j <= v.C ? v.col(j) : 7u;
             for (uint32_t c = 0; c < 4; c++) {
-                const bool eq = b == c;
-                sc[(h * 4 + c) * W + w] = uint16_t(int16_t(eq ? kHIT : kMISS));
-                dg[c] |= (2u | uint32_t(eq)) << (2 * w);
+                const bool e = b == c;
+                sc[(h * 4 + c) * W + w] = uint16_t(int16_t(4 * (e ? kHIT : kMISS) + PairTags<AFFINE>::diag));
+                eq[c] |= uint32_t(e) << (2 * w);
             }
         }
-        for (int c = 0; c < 4; c++) tab[32 + h * 4 + c] = dg[c];
+        for (int c = 0; c < 4; c++) tab[32 + h * 4 + c] = eq[c] << (16 * h);
     }
 }
 
-// row-0 states of the strip (packed) and M at (0, j0)
-template <int W>
+// row-0 states of the strip (tagged) and the clean M (global: F) at (0, j0)
+template <bool AFFINE, int W>
 HERO_HD void dp_pair_init(const SegView &va, const SegView &vb, int32_t j0, uint32_t (&f)[W],
                           uint32_t (&x)[W], uint32_t (&m)[W], uint32_t &pm) {
+    using T = PairTags<AFFINE>;
 #pragma unroll
     for (int32_t w = 0; w < W; w++) {
         const int32_t j = j0 + w + 1;
-        const Cell3 a = j <= va.C ? dp_row0<true>(va, j) : Cell3{kNEG16, kNEG16, kNEG16};
-        const Cell3 b = j <= vb.C ? dp_row0<true>(vb, j) : Cell3{kNEG16, kNEG16, kNEG16};
-        f[w] = pack2(a.f, b.f);
-        x[w] = pack2(a.x, b.x);
-        m[w] = pack2(max3(a.f, a.x, a.y), max3(b.f, b.x, b.y));
+        int32_t fa = kPairPad, fb = kPairPad, xa = kPairPad, xb = kPairPad, ma = kPairPad, mb = kPairPad;
+        if (j <= va.C) {
+            const Cell3 r = dp_row0<AFFINE>(va, j);
+            fa = AFFINE ? 4 * r.f + T::diag : 4 * r.f;
+            xa = 4 * r.x + T::up;
+            ma = 4 * (AFFINE ? max3(r.f, r.x, r.y) : r.f);
+        }
+        if (j <= vb.C) {
+            const Cell3 r = dp_row0<AFFINE>(vb, j);
+            fb = AFFINE ? 4 * r.f + T::diag : 4 * r.f;
+            xb = 4 * r.x + T::up;
+            mb = 4 * (AFFINE ? max3(r.f, r.x, r.y) : r.f);
+        }
+        f[w] = pack2(fa, fb);
+        x[w] = pack2(xa, xb);
+        m[w] = pack2(ma, mb);
     }
-    const Cell3 a = dp_row0<true>(va, j0), b = dp_row0<true>(vb, j0);
-    pm = pack2(max3(a.f, a.x, a.y), max3(b.f, b.x, b.y));
+    const Cell3 a = dp_row0<AFFINE>(va, j0), b = dp_row0<AFFINE>(vb, j0);
+    pm = AFFINE ? pack2(4 * max3(a.f, a.x, a.y), 4 * max3(b.f, b.x, b.y)) : pack2(4 * a.f, 4 * b.f);
 }
 
-// One affine row of a pair (dp_whole_row on both halves).  Returns the codes
-// of A in the low 16 bits and of B in the high 16 bits.
-template <int W>
-HERO_HD uint32_t dp_pair_row(const uint32_t (&sc)[W], uint32_t diag_a, uint32_t diag_b,
-                             uint32_t (&f)[W], uint32_t (&x)[W], uint32_t (&m)[W], uint32_t &lf,
-                             uint32_t &ly, uint32_t dm) {
-    constexpr uint32_t DY2 = (uint32_t(kDY) & 0xffffu) * 0x10001u;
-    constexpr uint32_t DX2 = (uint32_t(kDX) & 0xffffu) * 0x10001u;
-    constexpr uint32_t EX2 = (uint32_t(kEX) & 0xffffu) * 0x10001u;
-    uint32_t da = 0, db = 0, la = 0, lb = 0;
+// Column-0 states of a pair, row 1, tagged as the recurrences read them: lf
+// (affine FM, tag 1; global F, clean), ly (affine IY, tag 0) and the per-row
+// increment (dp_whole_col0: FM = i * c0[0] + c0[1], IY = i * c0[0] + c0[2]).
+// The clean M (global: F) of column 0 is lf minus its tag: M = FM there.
+template <bool AFFINE>
+HERO_HD void dp_pair_col0(const SegView &va, const SegView &vb, uint32_t &c0f, uint32_t &c0y,
+                          uint32_t &mul) {
+    int32_t ca[3], cb[3];
+    dp_whole_col0<AFFINE>(va, ca);
+    dp_whole_col0<AFFINE>(vb, cb);
+    const int32_t t = PairTags<AFFINE>::diag * int32_t(AFFINE);
+    mul = pack2(4 * ca[0], 4 * cb[0]);
+    c0f = pack2(4 * (ca[0] + ca[1]) + t, 4 * (cb[0] + cb[1]) + t);
+    c0y = pack2(4 * (ca[0] + ca[2]), 4 * (cb[0] + cb[2]));
+}
+
+// One row of a pair (dp_whole_row on both halves, tagged).  Returns the
+// traceback codes (0 up, 1 left, 2 diagonal mismatch, 3 diagonal match) of A
+// in the low 16 bits and of B in the high 16 bits; eq holds the match bits of
+// both rows' bases (dp_pair_table's words).
+template <bool AFFINE, int W>
+HERO_HD uint32_t dp_pair_row(const uint32_t (&sc)[W], uint32_t eq, uint32_t (&f)[W],
+                             uint32_t (&x)[W], uint32_t (&m)[W], uint32_t &lf, uint32_t &ly,
+                             uint32_t dm) {
+    uint32_t acc = 0;
+    if (AFFINE) {
+        constexpr uint32_t DYT = (uint32_t(4 * kDY - 1) & 0xffffu) * 0x10001u;  // FM(tag 1) -> IY (tag 0)
+        constexpr uint32_t DXT = (uint32_t(4 * kDX + 1) & 0xffffu) * 0x10001u;  // FM(tag 1) -> IX (tag 2)
+        constexpr uint32_t EX4 = (uint32_t(4 * kEX) & 0xffffu) * 0x10001u;
+#pragma unroll
+        for (int32_t w = 0; w < W; w++) {
+            const uint32_t yv = add_max2(ly, EX4, add2(lf, DYT));      // BandAligner.cpp:180-188
+            const uint32_t xv = add_max2(f[w], DXT, add2(x[w], EX4));  // BandAligner.cpp:189-201
+            const uint32_t fv = add2(dm, sc[w]);                       // BandAligner.cpp:203-207
+            dm = m[w];
+            const uint32_t mt = max3_2(fv, xv, yv);
+            acc += (mt & kTagMask2) << (2 * w);
+            m[w] = mt & ~kTagMask2;
+            f[w] = fv;
+            x[w] = xv;
+            lf = fv;
+            ly = yv;
+        }
+        // tags (2 up, 1 diagonal, 0 left) to codes: the low tag bit is the
+        // diagonal bit, the match bit joins it there; tag 0 becomes left
+        const uint32_t L = acc & kLow2;
+        const uint32_t lft = ~(acc | (acc >> 1)) & kLow2;
+        return (L << 1) | (L & eq) | lft;
+    }
+    constexpr uint32_t DX4 = (uint32_t(4 * kDX) & 0xffffu) * 0x10001u;      // up: tag 0
+    constexpr uint32_t DYT = (uint32_t(4 * kDY + 1) & 0xffffu) * 0x10001u;  // left: tag 1
 #pragma unroll
     for (int32_t w = 0; w < W; w++) {
-        const uint32_t yv = add_max2(ly, EX2, add2(lf, DY2));      // BandAligner.cpp:180-188
-        const uint32_t xv = add_max2(f[w], DX2, add2(x[w], EX2));  // BandAligner.cpp:189-201
-        const uint32_t fv = add2(dm, sc[w]);                       // BandAligner.cpp:203-207
-        dm = m[w];
-        m[w] = max3_2(fv, xv, yv);
-        // BM1 (BandAligner.cpp:214-222): diagonal iff FM > max(IX, IY - 1); left iff IY > IX
-        bool dlo, dhi, llo, lhi;
-        ge2(add_max2(yv, EX2, xv), fv, dlo, dhi);  // max(IY - 1, IX) >= FM: not diagonal
-        ge2(xv, yv, llo, lhi);                     // IX >= IY: not left
-        if (!dlo) da |= 3u << (2 * w);
-        if (!dhi) db |= 3u << (2 * w);
-        if (!llo) la |= 1u << (2 * w);
-        if (!lhi) lb |= 1u << (2 * w);
-        f[w] = fv;
-        x[w] = xv;
-        lf = fv;
-        ly = yv;
+        const uint32_t vd = add2(dm, sc[w]);  // diagonal, tag 2 (BandAligner.cpp:66-110)
+        dm = f[w];
+        const uint32_t mt = add_max2(lf, DYT, add_max2(f[w], DX4, vd));
+        acc += (mt & kTagMask2) << (2 * w);
+        f[w] = mt & ~kTagMask2;
+        lf = f[w];
     }
-    const uint32_t ca = (da & diag_a) | (~da & la), cb = (db & diag_b) | (~db & lb);
-    return (ca & 0xffffu) | (cb << 16);
+    // tags (2 diagonal, 1 left, 0 up) are the codes; the match bit joins the diagonals
+    return acc | ((acc >> 1) & eq);
 }
 
-// the align-left column of a pair (both segments share it): dp_whole_left on both halves
-template <int W>
+// the align-left column of a pair (both segments share it): dp_whole_left on
+// both halves, scaled by 4 (tags unchanged)
+template <bool AFFINE, int W>
 HERO_HD void dp_pair_left(int32_t wl, bool holds_c, uint32_t (&f)[W], uint32_t (&x)[W]) {
     if (!holds_c) return;
-    constexpr uint32_t SD2 = (uint32_t(kSX - kDX) & 0xffffu) * 0x10001u;
-    constexpr uint32_t SE2 = (uint32_t(kSX - kEX) & 0xffffu) * 0x10001u;
+    constexpr uint32_t SD2 = (uint32_t(4 * (kSX - kDX)) & 0xffffu) * 0x10001u;
+    constexpr uint32_t SE2 = (uint32_t(4 * (kSX - kEX)) & 0xffffu) * 0x10001u;
     switch (wl) {
-#define HERO_PAIR_CASE(w)                                 \
-    case w:                                               \
-        if (w < W) {                                      \
-            f[w < W ? w : 0] = add2(f[w < W ? w : 0], SD2); \
-            x[w < W ? w : 0] = add2(x[w < W ? w : 0], SE2); \
-        }                                                 \
+#define HERO_PAIR_CASE(w)                                               \
+    case w:                                                             \
+        if (w < W) {                                                    \
+            f[w < W ? w : 0] = add2(f[w < W ? w : 0], SD2);             \
+            if (AFFINE) x[w < W ? w : 0] = add2(x[w < W ? w : 0], SE2); \
+        }                                                               \
         break;
         HERO_PAIR_CASE(0)
         HERO_PAIR_CASE(1)

@@ -1143,9 +1143,10 @@ __device__ __forceinline__ void task_single(const DpLaunch a, uint64_t first, ui
                     tabs + size_t(g) * G * TS, uint32_t(G) * TS);
 }
 
-// the wavefront over one warp's pairs of whole-band segments (dp_pair_row):
-// group lanes hold segment A in the low halves and B in the high halves
-template <bool LEFT>
+// the wavefront over one warp's pairs of whole-band segments (dp_pair_row,
+// tagged 16-bit halves): group lanes hold segment A in the low halves and B in
+// the high halves
+template <bool AFFINE, bool LEFT>
 __device__ __noinline__ void wave_pair(const SegView va, const SegView vb, bool active, int32_t R,
                                        int32_t Rw, int G, int s, int lane, int32_t wl,
                                        uint32_t *tb, uint32_t *tab) {
@@ -1155,27 +1156,24 @@ __device__ __noinline__ void wave_pair(const SegView va, const SegView vb, bool 
     const uint8_t *rpa = va.row_base, *rpb = vb.row_base;
     uint32_t cha = 0, chb = 0;
     if (active) {
-        dp_pair_table<kStripW>(va, vb, j0, tab);
-        dp_pair_init<kStripW>(va, vb, j0, f, x, m, pm);
-        int32_t ca[3], cb[3];
-        dp_whole_col0<true>(va, ca);
-        dp_whole_col0<true>(vb, cb);
-        mul = pack2(ca[0], cb[0]);
-        c0f = pack2(ca[0] + ca[1], cb[0] + cb[1]);  // row 1
-        c0y = pack2(ca[0] + ca[2], cb[0] + cb[2]);
+        dp_pair_table<AFFINE, kStripW>(va, vb, j0, tab);
+        dp_pair_init<AFFINE, kStripW>(va, vb, j0, f, x, m, pm);
+        dp_pair_col0<AFFINE>(va, vb, c0f, c0y, mul);
         cha = (rpa[0] ^ va.row_xor) & 3u;
         chb = (rpb[0] ^ vb.row_xor) & 3u;
     }
+    // column 0's clean M is its FM without the FM tag
+    constexpr uint32_t c0tag = AFFINE ? 0x00010001u * uint32_t(PairTags<AFFINE>::diag) : 0u;
     const bool holds_c = LEFT && s == G - 1;
-    const uint32_t neg = pack2(kNEG16, kNEG16);
-    uint32_t pf = neg, py = neg, pmv = neg;  // FM, IY, M published to lane s+1
+    const uint32_t pad = pack2s(kPairPad);
+    uint32_t pf = pad, py = pad, pmv = pad;  // FM (global F), IY, M published to lane s+1
     uint32_t *tp = tb + lane;
     const uint16_t *sc16 = reinterpret_cast<const uint16_t *>(tab);
 #pragma unroll 1
     for (int32_t t = 0; t < Rw + G - 1; t++) {
         const uint32_t inf = __shfl_up_sync(0xffffffffu, pf, 1);
-        const uint32_t iny = __shfl_up_sync(0xffffffffu, py, 1);
-        const uint32_t inm = __shfl_up_sync(0xffffffffu, pmv, 1);
+        const uint32_t iny = AFFINE ? __shfl_up_sync(0xffffffffu, py, 1) : 0u;
+        const uint32_t inm = AFFINE ? __shfl_up_sync(0xffffffffu, pmv, 1) : inf;
         const int32_t i = t - s + 1;
         if (active && uint32_t(i - 1) < uint32_t(R)) {
             const uint32_t ba = cha, bb = chb;
@@ -1193,15 +1191,15 @@ __device__ __noinline__ void wave_pair(const SegView va, const SegView vb, bool 
                                           __byte_perm(A.y, B.y, 0x5410), __byte_perm(A.y, B.y, 0x7632),
                                           __byte_perm(A.z, B.z, 0x5410), __byte_perm(A.z, B.z, 0x7632),
                                           __byte_perm(A.w, B.w, 0x5410), __byte_perm(A.w, B.w, 0x7632)};
-            if (LEFT) dp_pair_left<kStripW>(wl, holds_c, f, x);
-            const uint32_t bits =
-                dp_pair_row<kStripW>(sc, tab[32 + ba], tab[36 + bb], f, x, m, lf, ly, pm);
+            if (LEFT) dp_pair_left<AFFINE, kStripW>(wl, holds_c, f, x);
+            const uint32_t eq = tab[32 + ba] | tab[36 + bb];
+            const uint32_t bits = dp_pair_row<AFFINE, kStripW>(sc, eq, f, x, m, lf, ly, pm);
             *tp = bits;
             tp += 32;
             pf = lf;
             py = ly;
-            pmv = m[kStripW - 1];
-            pm = s == 0 ? c0f : inm;
+            pmv = AFFINE ? m[kStripW - 1] : lf;
+            pm = s == 0 ? c0f - c0tag : inm;
             c0f = add2(c0f, mul);
             c0y = add2(c0y, mul);
         }
@@ -1212,8 +1210,9 @@ __device__ __noinline__ void wave_pair(const SegView va, const SegView vb, bool 
 // halves) and first + 2g + 1 (B, high halves).  Warps whose pairs are not all
 // whole-band (or too long for 16-bit scores) run their A segments, then their
 // B segments, as two tasks of single segments.
+template <bool AFFINE>
 __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint64_t end, int G,
-                                       int lane, uint32_t *tb, uint32_t *tabs) {
+                                          int lane, uint32_t *tb, uint32_t *tabs) {
     const int S = 32 / G, g = lane / G, s = lane % G;
     const uint64_t ia = first + 2u * uint64_t(g), ib = ia + 1u;
     const bool active = g < S && ia < end;
@@ -1237,17 +1236,17 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
     const int32_t wl0 = warp_max(wl);
     if (!(a.whole && __all_sync(0xffffffffu, !active || (ok && wl == wl0)))) {
         uint16_t *tb16 = reinterpret_cast<uint16_t *>(tb);
-        task_single<true>(a, first, 2, end, G, lane, tb16, tabs);
-        task_single<true>(a, first + 1, 2, end, G, lane, tb16, tabs);
+        task_single<AFFINE>(a, first, 2, end, G, lane, tb16, tabs);
+        task_single<AFFINE>(a, first + 1, 2, end, G, lane, tb16, tabs);
         return;
     }
     const int32_t Rw = warp_max(R);
     const uint32_t TS = kTabWords2;
     uint32_t *tab = tabs + size_t(lane) * TS;
     if (wl0 >= 0) {
-        wave_pair<true>(va, vb, active, R, Rw, G, s, lane, wl0, tb, tab);
+        wave_pair<AFFINE, true>(va, vb, active, R, Rw, G, s, lane, wl0, tb, tab);
     } else {
-        wave_pair<false>(va, vb, active, R, Rw, G, s, lane, -1, tb, tab);
+        wave_pair<AFFINE, false>(va, vb, active, R, Rw, G, s, lane, -1, tb, tab);
     }
     __syncwarp();
     uint32_t *stage = tabs + size_t(g) * G * TS;
@@ -1277,12 +1276,12 @@ __global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS))
         const uint64_t task = ntask - 1 - q;
         int G = 1;
         while (G < 32 && tasks[G + 1] <= task) G++;
-        const bool pair = AFFINE && pair_strips(a.pair_mask, G);
+        const bool pair = pair_strips(a.pair_mask, G);
         const uint64_t per = uint64_t(32 / G) * (pair ? 2u : 1u);  // segments per task
         const uint64_t first = tasks[34 + G] + (task - tasks[G]) * per;
         const uint64_t end = tasks[68 + G];
         if (pair) {
-            task_pair(a, first, end, G, lane, reinterpret_cast<uint32_t *>(tbw), tabs);
+            task_pair<AFFINE>(a, first, end, G, lane, reinterpret_cast<uint32_t *>(tbw), tabs);
         } else {
             task_single<AFFINE>(a, first, 1, end, G, lane, reinterpret_cast<uint16_t *>(tbw), tabs);
         }
@@ -2098,8 +2097,8 @@ void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, i
     if (!a_in.nd) return;
     DpLaunch a = a_in;
     if (a.warps != 2) a.warps = 4;
-    // pairs need 32-bit code rows; without the room (or for the global aligner) none run
-    if (!a.affine || wave_smem(a.rmax, 4, a.warps) > 200u * 1024u) a.pair_mask = 0;
+    // pairs need 32-bit code rows; without the room none run
+    if (wave_smem(a.rmax, 4, a.warps) > 200u * 1024u) a.pair_mask = 0;
     a.tb_bytes = a.pair_mask ? 4u : 2u;
     if (!dp_wave_fits(a.rmax)) {  // rows too long for the shared-memory codes
         const unsigned g = unsigned(a.threads / kDpThreads);

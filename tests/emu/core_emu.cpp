@@ -312,10 +312,11 @@ void emu_whole_any(int wl, const SegView &v, int G, std::vector<uint16_t> &tb) {
     }
 }
 
-// two segments of one shape as a 16-bit pair (the kernel's wave_pair), lanes in turn
-template <bool LEFT>
+// two segments of one shape as a tagged 16-bit pair (the kernel's wave_pair), lanes in turn
+template <bool AFFINE, bool LEFT>
 void emu_pair(const SegView &va, const SegView &vb, int G, int32_t wl, std::vector<uint32_t> &tb) {
     constexpr int W = 8;
+    constexpr uint32_t c0tag = AFFINE ? 0x00010001u * uint32_t(PairTags<AFFINE>::diag) : 0u;
     struct Lane {
         uint32_t f[W], x[W], m[W], tab[kTabWords2];
         uint32_t pm, pf, py, pmv, c0f, c0y, mul;
@@ -325,19 +326,14 @@ void emu_pair(const SegView &va, const SegView &vb, int G, int32_t wl, std::vect
     std::vector<Lane> L(G);
     for (int s = 0; s < G; s++) {
         Lane &x = L[s];
-        dp_pair_table<W>(va, vb, s * W, x.tab);
-        dp_pair_init<W>(va, vb, s * W, x.f, x.x, x.m, x.pm);
-        int32_t ca[3], cb[3];
-        dp_whole_col0<true>(va, ca);
-        dp_whole_col0<true>(vb, cb);
-        x.mul = pack2(ca[0], cb[0]);
-        x.c0f = pack2(ca[0] + ca[1], cb[0] + cb[1]);
-        x.c0y = pack2(ca[0] + ca[2], cb[0] + cb[2]);
+        dp_pair_table<AFFINE, W>(va, vb, s * W, x.tab);
+        dp_pair_init<AFFINE, W>(va, vb, s * W, x.f, x.x, x.m, x.pm);
+        dp_pair_col0<AFFINE>(va, vb, x.c0f, x.c0y, x.mul);
         x.rpa = va.row_base;
         x.rpb = vb.row_base;
         x.cha = (x.rpa[0] ^ va.row_xor) & 3u;
         x.chb = (x.rpb[0] ^ vb.row_xor) & 3u;
-        x.pf = x.py = x.pmv = pack2(kNEG16, kNEG16);
+        x.pf = x.py = x.pmv = pack2s(kPairPad);
     }
     std::vector<uint32_t> inf(G), iny(G), inm(G);
     for (int t = 0; t < va.R + G - 1; t++) {
@@ -362,13 +358,14 @@ void emu_pair(const SegView &va, const SegView &vb, int G, int32_t wl, std::vect
             const uint16_t *sc16 = reinterpret_cast<const uint16_t *>(x.tab);
             uint32_t sc[W];
             for (int w = 0; w < W; w++) sc[w] = uint32_t(sc16[ba * W + w]) | (uint32_t(sc16[(4 + bb) * W + w]) << 16);
-            if (LEFT) dp_pair_left<W>(wl, s == G - 1, x.f, x.x);
-            const uint32_t bits = dp_pair_row<W>(sc, x.tab[32 + ba], x.tab[36 + bb], x.f, x.x, x.m, lf, ly, x.pm);
+            if (LEFT) dp_pair_left<AFFINE, W>(wl, s == G - 1, x.f, x.x);
+            const uint32_t eq = x.tab[32 + ba] | x.tab[36 + bb];
+            const uint32_t bits = dp_pair_row<AFFINE, W>(sc, eq, x.f, x.x, x.m, lf, ly, x.pm);
             tb[size_t(i - 1) * 32 + s] = bits;
             x.pf = lf;
             x.py = ly;
-            x.pmv = x.m[W - 1];
-            x.pm = s == 0 ? x.c0f : inm[s];
+            x.pmv = AFFINE ? x.m[W - 1] : lf;
+            x.pm = s == 0 ? x.c0f - c0tag : (AFFINE ? inm[s] : inf[s]);
             x.c0f = add2(x.c0f, x.mul);
             x.c0y = add2(x.c0y, x.mul);
         }
@@ -381,32 +378,34 @@ void emu_pair(const SegView &va, const SegView &vb, int G, int32_t wl, std::vect
 // column) through the 16-bit pair rows; each half's ops are walked and returned
 // (ops_a / ops_b, capacity cap each).  Returns 0, or -1 if the pair does not
 // qualify or a path does not fit.
-int emu_align_pair(const uint8_t *sa, const uint8_t *qa, const uint8_t *sb, const uint8_t *qb,
-                   int32_t ls, int32_t lq, int64_t band_a, int64_t band_b, int flags_a,
-                   int flags_b, uint8_t *ops_a, int32_t *na, uint8_t *ops_b, int32_t *nb,
-                   int32_t cap) {
+int emu_align_pair(int affine, const uint8_t *sa, const uint8_t *qa, const uint8_t *sb,
+                   const uint8_t *qb, int32_t ls, int32_t lq, int32_t lqb, int64_t band_a,
+                   int64_t band_b, int flags_a, int flags_b, uint8_t *ops_a, int32_t *na,
+                   uint8_t *ops_b, int32_t *nb, int32_t cap) {
     constexpr int W = 8;
-    std::vector<uint8_t> sca(ls), qca(lq), scb(ls), qcb(lq);
+    std::vector<uint8_t> sca(ls), qca(lq), scb(ls), qcb(lqb);
     for (int i = 0; i < ls; i++) {
         sca[i] = base_code(sa[i]);
         scb[i] = base_code(sb[i]);
     }
-    for (int i = 0; i < lq; i++) {
-        qca[i] = base_code(qa[i]);
-        qcb[i] = base_code(qb[i]);
-    }
+    for (int i = 0; i < lq; i++) qca[i] = base_code(qa[i]);
+    for (int i = 0; i < lqb; i++) qcb[i] = base_code(qb[i]);
     const SegView va = make_view(sca.data(), ls, 0, qca.data(), 0, ls, 0, lq, uint32_t(flags_a), band_a);
-    const SegView vb = make_view(scb.data(), ls, 0, qcb.data(), 0, ls, 0, lq, uint32_t(flags_b), band_b);
+    const SegView vb = make_view(scb.data(), ls, 0, qcb.data(), 0, ls, 0, lqb, uint32_t(flags_b), band_b);
+    // the kernel's pairing rule: same rows, strips and align-left column
     if (!dp_whole_band(va) || !dp_whole_band(vb) || dp_left_col<W>(va) != dp_left_col<W>(vb) ||
-        va.R + va.C > kPairMaxSide)
+        va.R != vb.R || (va.C + W - 1) / W != (vb.C + W - 1) / W || va.R + va.C > kPairMaxSide ||
+        vb.R + vb.C > kPairMaxSide)
         return -1;
     const int G = (va.C + W - 1) / W;
     std::vector<uint32_t> tb(size_t(va.R) * 32, 0);
     const int32_t wl = dp_left_col<W>(va);
-    if (wl >= 0) {
-        emu_pair<true>(va, vb, G, wl, tb);
+    if (affine) {
+        if (wl >= 0) emu_pair<true, true>(va, vb, G, wl, tb);
+        else emu_pair<true, false>(va, vb, G, -1, tb);
     } else {
-        emu_pair<false>(va, vb, G, -1, tb);
+        if (wl >= 0) emu_pair<false, true>(va, vb, G, wl, tb);
+        else emu_pair<false, false>(va, vb, G, -1, tb);
     }
     for (int h = 0; h < 2; h++) {
         struct Codes {

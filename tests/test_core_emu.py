@@ -123,43 +123,52 @@ def test_rolling_kmers_match_direct(emu):
         assert f(codes.ctypes.data, len(codes), k) == -1, k
 
 
-def test_pair_rows_match_oracle(oracle, emu):
-    """Two segments of one shape in the 16-bit halves of the pair rows: each
-    half's path equals the oracle's affine path (flags may differ in align-right,
-    share align-left)."""
+@pytest.mark.parametrize("affine", [1, 0])
+def test_pair_rows_match_oracle(oracle, emu, affine):
+    """Two segments of one shape in the tagged 16-bit halves of the pair rows:
+    each half's path equals the oracle's path for the aligner (flags may differ
+    in align-right, share align-left)."""
     import ctypes as C
     f = emu.lib.emu_align_pair
     f.restype = C.c_int
-    f.argtypes = [C.c_void_p] * 4 + [C.c_int32, C.c_int32, C.c_int64, C.c_int64, C.c_int, C.c_int,
-                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
-    rng = np.random.default_rng(77)
+    f.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                                                 C.c_int64, C.c_int, C.c_int, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
+    rng = np.random.default_rng(77 + affine)
     done = 0
+
+    def query(rng, s, lq):
+        if rng.random() < 0.7:
+            q = _indels(rng, synth.substitute(rng, np.resize(s, lq).copy(), 0.03), 0.01)
+            return np.resize(q, lq).astype(np.uint8)
+        return ACGT[rng.integers(0, 4, lq)]
+
     for _ in range(400):
         ls = int(rng.integers(1, 200))
-        lq = int(rng.integers(1, 200))
-        seqs = []
-        for _h in range(2):
-            s = ACGT[rng.integers(0, 4, ls)]
-            if rng.random() < 0.7:
-                q = _indels(rng, synth.substitute(rng, np.resize(s, lq).copy(), 0.03), 0.01)
-                q = np.resize(q, lq).astype(np.uint8)
-            else:
-                q = ACGT[rng.integers(0, 4, lq)]
-            seqs.append((bytes(s), bytes(q)))
         left = int(rng.integers(0, 2))
+        if rng.random() < 0.3:  # the query side is the longer one (rows), equal in both
+            lq = lqb = int(rng.integers(ls, 200))
+        else:  # the subject side is the rows; B's columns may differ within the strip count
+            lq = int(rng.integers(1, ls + 1))
+            lo = max(1, 8 * ((lq - 1) // 8) + 1)
+            lqb = lq if left else int(rng.integers(lo, min(ls, lo + 7) + 1))
+        seqs = []
+        for lqh in (lq, lqb):
+            sh = ACGT[rng.integers(0, 4, ls)]
+            seqs.append((bytes(sh), bytes(query(rng, sh, lqh))))
         fa = (int(rng.integers(0, 2)) | (left << 1))
         fb = (int(rng.integers(0, 2)) | (left << 1))
         band_a, band_b = int(rng.choice([400, 1000])), int(rng.choice([400, 1000]))
-        cap = ls + lq + 1
+        cap = ls + max(lq, lqb) + 1
         oa, ob = np.zeros(cap, np.uint8), np.zeros(cap, np.uint8)
         na, nb = C.c_int32(), C.c_int32()
         bufs = [np.frombuffer(x, np.uint8).copy() for x in (seqs[0][0], seqs[0][1], seqs[1][0], seqs[1][1])]
-        rc = f(*[b.ctypes.data for b in bufs], ls, lq, band_a, band_b, fa, fb,
+        rc = f(affine, *[b.ctypes.data for b in bufs], ls, lq, lqb, band_a, band_b, fa, fb,
                oa.ctypes.data, C.byref(na), ob.ctypes.data, C.byref(nb), cap)
-        assert rc == 0
+        assert rc == 0, (ls, lq, lqb, left)
         for (s, q), band, fl, ops, n in ((seqs[0], band_a, fa, oa, na), (seqs[1], band_b, fb, ob, nb)):
-            want, _ = oracle.align(1, s, q, band, bool(fl & 1), bool(fl & 2))
-            assert np.array_equal(want, ops[:n.value]), (ls, lq, band, fl)
+            want, _ = oracle.align(affine, s, q, band, bool(fl & 1), bool(fl & 2))
+            assert np.array_equal(want, ops[:n.value]), (ls, len(q), band, fl)
         done += 1
     assert done == 400
 

@@ -27,7 +27,7 @@ def _run(rs, kw, classes):
     return r
 
 
-@pytest.mark.parametrize("name", ["c2_30k", "mix_affine"])
+@pytest.mark.parametrize("name", ["c2_30k", "mix_affine", "c1_20k", "mix"])
 def test_every_candidate_shape_gives_the_same_result(name):
     gen, flags = FIXTURES[name]
     rs = upper(gen())
