@@ -153,6 +153,20 @@ HERO_HD uint64_t seed_hit(bool aln, int o, uint32_t q, uint32_t posQ, int32_t f,
     if (aln) return hit_pack(q, uint32_t(Lq - (int32_t(posQ) + k)), uint32_t(f));
     return hit_pack(q, posQ, uint32_t(Ls - k - f));
 }
+// A k-mer table value: (query << 32) | (uid_tag << 16) | position.  Read
+// positions are below 2^15, so the low word has room for a 16-bit fold of the
+// query's uniqueId: the self-hit test (SubjectReadAligner.cpp:463-465) loads
+// the query's id only when the folds agree.
+HERO_HD uint32_t uid_tag(int64_t u) {
+    const uint64_t x = uint64_t(u);
+    return uint32_t((x ^ (x >> 16) ^ (x >> 32) ^ (x >> 48)) & 0xffffu);
+}
+HERO_HD uint64_t table_value(uint64_t q, uint32_t tag, int64_t pos) {
+    return (q << 32) | (uint64_t(tag) << 16) | uint64_t(pos);
+}
+HERO_HD uint32_t value_query(uint64_t v) { return uint32_t(v >> 32); }
+HERO_HD uint32_t value_tag(uint64_t v) { return uint32_t(v >> 16) & 0xffffu; }
+HERO_HD uint32_t value_pos(uint64_t v) { return uint32_t(v) & 0xffffu; }
 HERO_HD int32_t hit_posQ(uint64_t h) { return int32_t((h >> 16) & 0xffff); }
 HERO_HD int32_t hit_posS(uint64_t h) { return int32_t(h & 0xffff); }
 

@@ -53,7 +53,7 @@ struct ReadsView {
 
 struct TableView {
     const Slot *slots;
-    const uint64_t *vals;  // (query << 32) | position
+    const uint64_t *vals;  // table_value: (query << 32) | (uid_tag << 16) | position
     uint64_t mask;
 };
 

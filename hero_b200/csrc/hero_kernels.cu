@@ -215,6 +215,7 @@ __global__ void k_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint
         const int32_t nk = query_key_count(L, k);
         const uint8_t *c = q.code + q.off[r];
         uint64_t e = key_off[r];
+        const uint32_t tag = uid_tag(q.uid[r]);
         for (int32_t i = 0; i < nk; i++, e++) {
             const int64_t pos = query_key_pos(L, k, i);
             Kmer m{0, 0};
@@ -222,7 +223,7 @@ __global__ void k_key_emit(ReadsView q, int32_t k, const uint64_t *key_off, uint
             if (q.job) kmer_tag(m, q.job[r], k);
             klo[e] = m.lo;
             khi[e] = m.hi;
-            kval[e] = (uint64_t(r) << 32) | uint64_t(pos);
+            kval[e] = table_value(r, tag, pos);
         }
     }
 }
@@ -318,6 +319,7 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
     for (uint64_t s = uint64_t(blockIdx.x) * kProbeWarps + wib; s < nsub; s += warps) {
         const int32_t L = int32_t(subj.len[s]);
         const int64_t su = subj.uid[s];
+        const uint32_t stag = uid_tag(su);
         const uint8_t *c = subj.code + subj.off[s];
         uint32_t c0 = 0, c1 = 0;
         uint64_t o0 = 0, o1 = 0;
@@ -362,13 +364,15 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
                     if (!table_find(t, o ? rm : fm, st, cnt)) continue;
                     for (uint32_t e = 0; e < cnt; e++) {
                         const uint64_t v = __ldg(&t.vals[st + e]);
-                        const uint32_t qq = uint32_t(v >> 32);
-                        if (__ldg(&q.uid[qq]) == su) continue;  // self hit (SubjectReadAligner.cpp:463-465)
+                        const uint32_t qq = value_query(v);
+                        // self hit (SubjectReadAligner.cpp:463-465): ids compared
+                        // only where their folds agree
+                        if (value_tag(v) == stag && __ldg(&q.uid[qq]) == su) continue;
                         if (EMIT) {
                             const uint32_t slot = atomicAdd(&fill[wib][o], 1u);
                             const int32_t lq = (aln && o) ? int32_t(__ldg(&q.len[qq])) : 0;
                             hits[(o ? o1 : o0) + slot] =
-                                seed_hit(aln, o, qq, uint32_t(v & 0xffffffffu), f, L, lq, k);
+                                seed_hit(aln, o, qq, value_pos(v), f, L, lq, k);
                         } else {
                             if (o) {
                                 c1++;

@@ -13,6 +13,14 @@ histogram of -c --mapping.  Usage:  python tests/golden/make_golden.py
 
 regenerates the named entries of manifest_full.json (whole-size workloads and
 reduced-genome instances of the larger ones; minutes each) and keeps the rest.
+
+    python tests/golden/make_golden.py --config4-sample
+
+runs the reference on the sampled jobs of the serving stream (synth.config4_jobs():
+every job of at most 2 Mbp plus 5 larger ones drawn with a fixed seed; affine,
+-c --covinfo --singleReads -a a) and records each job's .fasta/.info md5 in
+manifest_config4.json, saving after every job (hours in all; a rerun skips the
+jobs already recorded).
 """
 from __future__ import annotations
 
@@ -148,9 +156,56 @@ def main_full(names: list[str]):
         json.dump(manifest, f, indent=1, sort_keys=True)
 
 
+def config4_sample(jobs) -> list:
+    """The serving stream's jobs the reference is run on: every job of at most
+    2 Mbp and 5 of the larger ones (fixed seed)."""
+    import numpy as np
+    small = [j for j in jobs if j.genome_bp <= 2_000_000]
+    large = [j for j in jobs if j.genome_bp > 2_000_000]
+    pick = np.random.default_rng(44).choice(len(large), size=min(5, len(large)), replace=False)
+    return sorted(small + [large[int(i)] for i in pick], key=lambda j: j.job_id)
+
+
+def main_config4():
+    import resource
+    import time
+    path = os.path.join(HERE, "manifest_config4.json")
+    manifest = json.load(open(path)) if os.path.exists(path) else {}
+    threads = os.cpu_count() or 1
+    flags = ["-a", "a"]
+    with tempfile.TemporaryDirectory() as d:
+        for job in config4_sample(synth.config4_jobs()):
+            key = str(job.job_id)
+            if key in manifest:
+                continue
+            rs = job.reads()
+            fqb = rs.to_fastq()
+            fq = os.path.join(d, "in.fq")
+            with open(fq, "wb") as f:
+                f.write(fqb)
+            nreads, fq_md5 = rs.n, md5(fqb)
+            del rs, fqb
+            t0 = time.perf_counter()
+            fa, info = run_reference(fq, flags, d)
+            secs = time.perf_counter() - t0
+            manifest[key] = {"genome_bp": job.genome_bp, "read_len": job.read_len,
+                             "coverage": job.coverage, "seed": job.seed, "reads": nreads,
+                             "flags": flags, "fastq_md5": fq_md5, "fasta_md5": md5(fa),
+                             "info_md5": md5(info),
+                             f"reference_seconds_{threads}_threads": round(secs, 2),
+                             "reference_peak_rss_gb": round(resource.getrusage(
+                                 resource.RUSAGE_CHILDREN).ru_maxrss / 2**20, 2)}
+            print(key, manifest[key], flush=True)
+            with open(path + ".tmp", "w") as f:
+                json.dump(manifest, f, indent=1, sort_keys=True)
+            os.replace(path + ".tmp", path)
+
+
 def main():
     if len(sys.argv) > 1 and sys.argv[1] == "--full":
         return main_full(sys.argv[2:] or list(FULL))
+    if len(sys.argv) > 1 and sys.argv[1] == "--config4-sample":
+        return main_config4()
     manifest = {}
     with tempfile.TemporaryDirectory() as d:
         for name, (gen, flags) in FIXTURES.items():
