@@ -86,7 +86,7 @@ def parse():
     ap.add_argument("--impl", default="hero", choices=["hero", "reference"])
     ap.add_argument("--workload", default="config1",
                     choices=["config1", "config2", "config3", "config4", "config5"])
-    ap.add_argument("--served-jobs", type=int, default=60,
+    ap.add_argument("--served-jobs", type=int, default=24,
                     help="jobs of the served block added to the default line (0: none)")
     ap.add_argument("--jobs-scale", type=float, default=0.0,
                     help="genome-size scale of the served jobs (default 1.0: the stream's sizes)")
@@ -369,129 +369,167 @@ def _job_reads(job):
     return job.job_id, rs.seq, rs.off, rs.names
 
 
-def served_jobs(n_jobs: int, scale: float):
-    """The serving stream (Poisson arrivals, genome log-uniform 0.5-20 Mbp times
-    `scale`, L in {100,150,250}, coverage U(20,80), affine errors), generated in a
-    spawn pool so no process is forked after CUDA starts."""
+def job_stream(jobs, procs: int = 0):
+    """The jobs' reads in job order, each generated from its seed in a spawn
+    pool ahead of its use (no process is forked after CUDA starts)."""
     import multiprocessing as mp
-
-    from hero_b200 import synth
-    jobs = synth.config4_jobs(n_jobs=n_jobs, scale=scale)
-    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
-        out = pool.map(_job_reads, jobs, chunksize=1)
-    reads = {j: (seq, off, names) for j, seq, off, names in out}
-    return jobs, [reads[j.job_id] for j in jobs]
+    procs = procs or min(16, os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        for jid, seq, off, names in pool.imap(_job_reads, jobs, chunksize=1):
+            yield jid, (seq, off, names)
 
 
-def run_served(jobs, reads, dev: int, busy_target: float = 0.85, check: int = 3) -> dict:
-    """Submits the jobs at their (rescaled) Poisson arrival times to one server and
-    reports job latency (submit -> results ready) and aggregate throughput."""
+def _digest(res: dict) -> str:
+    """md5 of a job's corrected reads, statistics and the doubles' bits."""
+    import hashlib
+    h = hashlib.md5()
+    for f in ("seq", "imin", "imed", "imax", "good", "mismatch_rate", "gc"):
+        h.update(np.ascontiguousarray(res[f]).tobytes())
+    return h.hexdigest()
+
+
+def run_alone(stream, dev: int) -> tuple[dict, dict, float, int]:
+    """Every job corrected on its own, one after another, through one context
+    (host reads in, results in host memory out): wall time and digest per job."""
+    from hero_b200 import Hero
+    times, digests, bases = {}, {}, 0
+    with Hero(aligner="affine", device=dev) as h:
+        for jid, (seq, off, names) in stream:
+            t0 = time.perf_counter()
+            h.set_queries(seq, off, names)
+            h.build_index()
+            h.align_self()
+            res = h.consensus()
+            times[jid] = time.perf_counter() - t0
+            digests[jid] = _digest(res)
+            bases += int(off[-1])
+    return times, digests, sum(times.values()), bases
+
+
+def run_server(jobs, stream, dev: int, arrivals=None) -> dict:
+    """Submits the jobs to one server -- all at once (arrivals None) or at the
+    given arrival times (s) -- and reports per-job latency (submit -> results
+    ready), aggregate throughput, the server's busy fraction and the digests."""
     import threading
 
-    from hero_b200 import Hero, HeroServer
+    from hero_b200 import HeroServer
     srv = HeroServer(aligner="affine", device=dev)
     try:
-        # warm-up (the server's context sizes its device buffers), then capacity:
-        # every job of the stream submitted at once, back to back (closed loop)
-        for i in range(min(2, len(jobs))):
-            j = srv.submit(*reads[i])
-            srv.wait(j)
-            srv.release(j)
-        cal = list(range(len(jobs)))  # the whole stream, so the load below is a true fraction
-        t0 = time.perf_counter()
-        ids = [srv.submit(*reads[i]) for i in cal]
-        for j in ids:
-            srv.wait(j)
-            srv.release(j)
-        cal_s = time.perf_counter() - t0
-        cal_bases = sum(int(reads[i][1][-1]) for i in cal)
-        thr = cal_bases / cal_s
-        mean_bases = float(np.mean([int(r[1][-1]) for r in reads]))
-        lam = busy_target * thr / mean_bases  # jobs/s that keep the GPU ~busy_target busy
-        base_rate = 1.0  # config4_jobs draws arrivals at 1 job/s
-        arrivals = [j.arrival_s * base_rate / lam for j in jobs]
-        s0 = srv.stats()
-        ids = [None] * len(jobs)
+        ids = {}
+        late = []
 
         def submitter():
             start = time.perf_counter()
-            for k in range(len(jobs)):
-                dt = arrivals[k] - (time.perf_counter() - start)
-                if dt > 0:
-                    time.sleep(dt)
-                ids[k] = srv.submit(*reads[k])
+            for jid, (seq, off, names) in stream:
+                if arrivals is not None:
+                    dt = arrivals[jid] - (time.perf_counter() - start)
+                    if dt > 0:
+                        time.sleep(dt)
+                    else:
+                        late.append(-dt)
+                ids[jid] = srv.submit(seq, off, names)
 
+        s0 = srv.stats()
         th = threading.Thread(target=submitter)
         th.start()
         th.join()
-        infos = [srv.wait(j) for j in ids]
+        infos = {jid: srv.wait(i) for jid, i in ids.items()}
         s1 = srv.stats()
-        lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos])
-        first = min(i["submit_ms"] for i in infos)
-        last = max(i["done_ms"] for i in infos)
-        bases = sum(i["bases"] for i in infos)
-        # served == alone on `check` jobs (all when check >= jobs): byte-identical
-        # corrected reads and statistics, the doubles bit for bit
-        rng = np.random.default_rng(7)
-        picks = rng.choice(len(jobs), size=min(check, len(jobs)), replace=False)
-        ok = 0
-        with Hero(aligner="affine", device=dev) as alone:
-            for k in picks:
-                got = srv.result(ids[k])
-                seq, off, names = reads[k]
-                alone.set_queries(seq, off, names)
-                alone.build_index()
-                alone.align_self()
-                want = alone.consensus()
-                same = all(np.array_equal(want[f], got[f])
-                           for f in ("seq", "imin", "imed", "imax", "good"))
-                same = same and all(np.array_equal(np.asarray(want[f]).view(np.uint64),
-                                                   np.asarray(got[f]).view(np.uint64))
-                                    for f in ("mismatch_rate", "gc"))
-                ok += int(same)
-        for j in ids:
-            srv.release(j)
-        rounds = s1["rounds"] - s0["rounds"]
-        return {
-            "jobs": len(jobs), "bases": bases,
+        digests = {jid: _digest(srv.result(i)) for jid, i in ids.items()}
+        for i in ids.values():
+            srv.release(i)
+    finally:
+        srv.close()
+    lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos.values()])
+    first = min(i["submit_ms"] for i in infos.values())
+    last = max(i["done_ms"] for i in infos.values())
+    bases = sum(i["bases"] for i in infos.values())
+    rounds = s1["rounds"] - s0["rounds"]
+    return {"jobs": len(infos), "bases": bases,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
             "bases_per_s": bases / ((last - first) / 1e3),
-            "arrival_rate_per_s": lam, "capacity_bases_per_s": thr,
             "busy_frac": (s1["busy_ms"] - s0["busy_ms"]) / (last - first),
-            "rounds": rounds, "mean_jobs_per_round": len(jobs) / max(rounds, 1),
-            "served_equals_alone": f"{ok}/{len(picks)}",
-        }
-    finally:
-        srv.close()
+            "rounds": rounds, "mean_jobs_per_round": len(infos) / max(rounds, 1),
+            "overlapped_rounds": s1["overlapped_rounds"] - s0["overlapped_rounds"],
+            "arrivals_late_s": float(max(late)) if late else 0.0, "_digests": digests}
+
+
+def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.9) -> dict:
+    """The serving stream: each job alone (one at a time), the server with every
+    job submitted at once (its capacity), then the server under Poisson arrivals
+    at `load` of that capacity.  served == alone compares every job's digest."""
+    if in_memory:
+        data = dict(job_stream(jobs))
+
+        def stream():
+            return iter([(j.job_id, data[j.job_id]) for j in jobs])
+    else:
+        def stream():
+            return job_stream(jobs)
+    # warm-up: one small job through a context and a server (device set-up, buffers)
+    small = min(jobs, key=lambda j: j.genome_bp * j.coverage)
+    warm = list(job_stream([small], procs=1))
+    run_alone(iter(warm), dev)
+    run_server([small], iter(warm), dev)
+    times, alone_dig, alone_s, bases = run_alone(stream(), dev)
+    closed = run_server(jobs, stream(), dev)
+    mean_bases = bases / len(jobs)
+    lam = load * closed["bases_per_s"] / mean_bases  # jobs/s
+    # the stream's Poisson arrival times (config4_jobs draws them at 1 job/s), rescaled
+    arrivals = {j.job_id: j.arrival_s / lam for j in jobs}
+    poisson = run_server(jobs, stream(), dev, arrivals)
+    same = sum(int(poisson["_digests"][j] == alone_dig[j] and closed["_digests"][j] == alone_dig[j])
+               for j in alone_dig)
+    for r in (closed, poisson):
+        del r["_digests"]
+    return {
+        "jobs": len(jobs), "bases": bases,
+        "p50_ms": poisson["p50_ms"], "p99_ms": poisson["p99_ms"], "mean_ms": poisson["mean_ms"],
+        "max_ms": poisson["max_ms"], "bases_per_s": poisson["bases_per_s"],
+        "arrival_rate_per_s": lam, "load_of_capacity": load,
+        "busy_frac": poisson["busy_frac"], "rounds": poisson["rounds"],
+        "mean_jobs_per_round": poisson["mean_jobs_per_round"],
+        "overlapped_rounds": poisson["overlapped_rounds"],
+        "arrivals_late_s": poisson["arrivals_late_s"],
+        "capacity_bases_per_s": closed["bases_per_s"],
+        "capacity_mean_jobs_per_round": closed["mean_jobs_per_round"],
+        "one_at_a_time_bases_per_s": bases / alone_s,
+        "capacity_vs_one_at_a_time": closed["bases_per_s"] / (bases / alone_s),
+        "alone_p50_ms": float(np.percentile([1e3 * t for t in times.values()], 50)),
+        "served_equals_alone": f"{same}/{len(alone_dig)}",
+    }
 
 
 def run_served_block(args, dev: int) -> dict:
-    """The served block of the default line: a stream of independent jobs."""
-    scale = args.jobs_scale or 0.02
-    jobs, reads = served_jobs(args.served_jobs, scale)
+    """The served block of the default line: the first jobs of the serving
+    stream at their real sizes (genome log-uniform 0.5-20 Mbp, L in
+    {100,150,250}, coverage U(20,80), affine errors), held in host memory."""
+    from hero_b200 import synth
+    jobs = synth.config4_jobs(n_jobs=args.served_jobs, scale=args.jobs_scale or 1.0)
     with ClockSampler(dev) as sclk:
-        served = run_served(jobs, reads, dev)
+        served = serve_workload(jobs, dev, in_memory=True)
     served["clocks"] = sclk.summary()
-    served["workload"] = (f"{args.served_jobs} jobs, Poisson arrivals, genome log-uniform "
-                          f"0.5-20 Mbp x {scale}, L in {{100,150,250}}, coverage U(20,80), "
-                          "affine/indel errors")
+    served["workload"] = (f"the first {args.served_jobs} jobs of the serving stream: Poisson "
+                          f"arrivals, genome log-uniform 0.5-20 Mbp x {args.jobs_scale or 1.0}, "
+                          "L in {100,150,250}, coverage U(20,80), affine/indel errors")
     return served
 
 
 def bench_served(args):
-    """The serving workload alone: one JSON line with p50/p99 job latency."""
+    """The serving workload alone: 200 jobs generated lazily from their seeds;
+    one JSON line with p50/p99 job latency."""
     import torch
 
-    from hero_b200 import build
+    from hero_b200 import build, synth
     if not os.environ.get("HERO_B200_LIB"):
         build.build_library()
-    scale = args.jobs_scale or 0.05
-    jobs, reads = served_jobs(200, scale)
+    scale = args.jobs_scale or 1.0
+    jobs = synth.config4_jobs(200, scale=scale)
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     with ClockSampler(dev) as clk:
-        r = run_served(jobs, reads, dev, check=len(jobs))  # every job: served == alone
+        r = serve_workload(jobs, dev, in_memory=False)
     line = {"metric": "p50/p99 job latency", "value": r["p50_ms"], "unit": "ms",
             "higher_is_better": False, "n_gpus": 1, "p99_ms": r["p99_ms"],
             "served_bases_per_s": r["bases_per_s"], "dtype": "int32",

@@ -30,12 +30,13 @@ EXPORTS = [
     "hero_server_get_stats", "hero_job_bytes", "hero_round_admit", "hero_set_dp_tuning",
     "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
     "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
-    "hero_merge_pairs", "hero_get_overhang",
+    "hero_merge_pairs", "hero_get_overhang", "hero_mapping_histogram",
 ]
 
 # hero_params.flags: the alignment-output mode (HERO without -c); --merge
 FLAG_ALIGNMENT_OUTPUT = 1
 FLAG_MERGE_PAIRS = 2
+FLAG_MAPPING = 4
 
 # the autotuner's record (hero_b200.autotune); loaded by every Hero unless told otherwise
 TUNING_PATH = os.path.join(HERE, "tuning.json")
@@ -97,7 +98,8 @@ class JobInfo(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in ("jobs_submitted", "jobs_done", "jobs_failed", "rounds",
                                             "bases_done", "round_bytes_budget")] +
-                [("busy_ms", C.c_double), ("uptime_ms", C.c_double)])
+                [("busy_ms", C.c_double), ("uptime_ms", C.c_double),
+                 ("overlapped_rounds", C.c_uint64)])
 
 
 _lib = None
@@ -135,6 +137,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_align_self_range.argtypes = [vp, C.c_uint64, C.c_uint64]
     lib.hero_merge_pairs.argtypes = [vp, vp, vp]
     lib.hero_get_overhang.argtypes = [vp, vp]
+    lib.hero_mapping_histogram.argtypes = [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.hero_votes_words.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_votes_save.argtypes = [vp, vp]
     lib.hero_votes_load.argtypes = [vp, vp]
@@ -192,7 +195,7 @@ class Hero:
                  consensus_threshold: float = 0.6, device: int = 0, subject_batch: int = 0,
                  device_memory_budget: int = 0, stream: int | None = None,
                  tuning: list[dict] | str | None = None, alignment_output: bool = False,
-                 merge_pairs: bool = False):
+                 merge_pairs: bool = False, mapping: bool = False):
         """alignment_output=True: HERO without -c -- the .aln records of every
         subject (alignments()) instead of votes and a consensus.
         merge_pairs=True: --merge -- overhang votes, then merge_pairs() after
@@ -211,7 +214,8 @@ class Hero:
         p.device_memory_budget = device_memory_budget
         p.stream = stream
         p.flags = ((FLAG_ALIGNMENT_OUTPUT if alignment_output else 0) |
-                   (FLAG_MERGE_PAIRS if merge_pairs else 0))
+                   (FLAG_MERGE_PAIRS if merge_pairs else 0) |
+                   (FLAG_MAPPING if mapping else 0))
         self.params = p
         h = C.c_void_p()
         rc = self.lib.hero_create(C.byref(p), C.byref(h))
@@ -358,6 +362,23 @@ class Hero:
         res["merged_seq"] = res["merged_seq"][:self.nqb]
         res["merged_len"] = res["merged_len"][:self.nq // 2]
         return res
+
+    def mapping_histogram(self) -> np.ndarray:
+        """--mapping: bases per vote-count sum (hero_mapping_histogram)."""
+        n = C.c_uint64()
+        self._check(self.lib.hero_mapping_histogram(self.h, None, 0, C.byref(n)), "mapping_histogram")
+        out = np.zeros(n.value, np.uint64)
+        if n.value:
+            self._check(self.lib.hero_mapping_histogram(self.h, _ptr(out), n.value, C.byref(n)),
+                        "mapping_histogram")
+        return out
+
+    @staticmethod
+    def mapping_text(hist: np.ndarray) -> bytes:
+        """The histogram file QueryDataset::getCoverageAndWriteResults writes
+        (QueryDataset.cpp:589-596)."""
+        lines = [b"COV\tFRE\n"] + [b"%d\t%d\n" % (i, int(v)) for i, v in enumerate(hist) if v]
+        return b"".join(lines)
 
     def overhang(self):
         """--merge: the overhang votes, uint32 [reads * 20 * 4]."""

@@ -67,6 +67,8 @@ struct hero_ctx {
     // --merge: overhang votes per query read, merged pairs
     DBuf q_ext, m_seq, m_len;
     bool merge = false;
+    bool mapping = false;  // --mapping: chosen records vote; coverage histogram
+    DBuf map_hist, map_max;
     bool consensus_done = false;  // out_seq holds the consensus of the current votes
     std::vector<uint8_t> aln_host;  // .aln text of every subject aligned since the last take
     // index build temporaries (kept between builds)
@@ -104,7 +106,7 @@ struct hero_ctx {
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
                         &x_fill, &x_tmp, &q_job, &win_sorted, &win_bins, &a_list, &a_n,
                         &a_roff, &a_unit, &a_len, &a_pre, &a_cig, &a_uoff, &a_text, &q_ext,
-                        &m_seq, &m_len};
+                        &m_seq, &m_len, &map_hist, &map_max};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -217,9 +219,12 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
     if (!p || !out) return HERO_E_INPUT;
     *out = nullptr;
     if (p->k < 1 || p->k > 63) return HERO_E_INPUT;
-    if (p->flags & ~(HERO_FLAG_ALIGNMENT_OUTPUT | HERO_FLAG_MERGE_PAIRS)) return HERO_E_INPUT;
-    if ((p->flags & HERO_FLAG_ALIGNMENT_OUTPUT) && (p->flags & HERO_FLAG_MERGE_PAIRS))
-        return HERO_E_INPUT;  // --merge is part of the consensus mode
+    if (p->flags & ~(HERO_FLAG_ALIGNMENT_OUTPUT | HERO_FLAG_MERGE_PAIRS | HERO_FLAG_MAPPING))
+        return HERO_E_INPUT;
+    if ((p->flags & HERO_FLAG_ALIGNMENT_OUTPUT) && (p->flags & (HERO_FLAG_MERGE_PAIRS | HERO_FLAG_MAPPING)))
+        return HERO_E_INPUT;  // --merge and --mapping are parts of the consensus mode
+    if ((p->flags & HERO_FLAG_MERGE_PAIRS) && (p->flags & HERO_FLAG_MAPPING))
+        return HERO_E_INPUT;  // the reference writes the mapping histogram instead
     hero_ctx *c = new hero_ctx();
     c->P = *p;
     c->p.k = p->k;
@@ -230,6 +235,7 @@ extern "C" int hero_create(const hero_params *p, hero_ctx **out) {
     c->p.thr = p->consensus_threshold;
     c->p.aln = (p->flags & HERO_FLAG_ALIGNMENT_OUTPUT) ? 1 : 0;
     c->merge = (p->flags & HERO_FLAG_MERGE_PAIRS) != 0;
+    c->mapping = (p->flags & HERO_FLAG_MAPPING) != 0;
     c->dev = p->device;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -641,8 +647,15 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
             if ((r = c->ensure(c->winners, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
             if ((r = c->ensure(c->win_sorted, std::max<uint64_t>(NC, 1) * 4, "winners"))) break;
             if ((r = c->ensure(c->win_bins, kWinScratch * 4, "winners"))) break;
-            launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
-                          P_<uint32_t>(c->winners), ctr, c->st);
+            if (c->mapping) {
+                if ((r = c->ensure(c->a_list, std::max<uint64_t>(NC, 1) * 4, "mapping lists"))) break;
+                launch_map_choose(c->p, nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount),
+                                  ch, P_<uint32_t>(c->keys), subj, q, P_<DpSum>(c->sums),
+                                  P_<uint32_t>(c->a_list), P_<uint32_t>(c->winners), ctr, c->st);
+            } else {
+                launch_dedupe(nsub, P_<uint32_t>(c->seg_cstart), P_<uint32_t>(c->seg_ccount), ch,
+                              P_<uint32_t>(c->winners), ctr, c->st);
+            }
             rec(5);
             launch_vote(c->p, NC, ch, P_<uint32_t>(c->winners), P_<uint32_t>(c->win_sorted),
                         P_<uint32_t>(c->win_bins), P_<uint32_t>(c->keys), subj, q,
@@ -960,6 +973,36 @@ extern "C" int hero_merge_pairs(hero_ctx *c, uint8_t *seq_out, uint32_t *merged_
     HERO_TRY(c->cuda(cudaMemcpyAsync(seq_out, c->m_seq.p, c->nqb, cudaMemcpyDeviceToHost, c->st), "merge"));
     HERO_TRY(c->cuda(cudaMemcpyAsync(merged_len, c->m_len.p, np * 4, cudaMemcpyDeviceToHost, c->st), "merge"));
     return c->cuda(cudaStreamSynchronize(c->st), "merge");
+}
+
+extern "C" int hero_mapping_histogram(hero_ctx *c, uint64_t *hist, uint64_t cap, uint64_t *n_bins) {
+    if (!c || !n_bins || (cap && !hist)) return HERO_E_INPUT;
+    if (!c->mapping) return c->fail(HERO_E_STATE, "the context was not created with HERO_FLAG_MAPPING");
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    cudaSetDevice(c->dev);
+    const ReadsView q = query_view(c);
+    uint64_t bins = 1u << 16;
+    unsigned long long maxc = 0;
+    for (int pass = 0; pass < 2; pass++) {  // a second pass only when a sum exceeds the bins
+        HERO_TRY(c->ensure(c->map_hist, bins * 8, "mapping histogram"));
+        HERO_TRY(c->ensure(c->map_max, 8, "mapping histogram"));
+        HERO_TRY(c->cuda(cudaMemsetAsync(c->map_hist.p, 0, bins * 8, c->st), "mapping histogram"));
+        HERO_TRY(c->cuda(cudaMemsetAsync(c->map_max.p, 0, 8, c->st), "mapping histogram"));
+        launch_map_hist(q, P_<uint32_t>(c->cov), P_<int32_t>(c->mdiff), bins,
+                        P_<unsigned long long>(c->map_hist), P_<unsigned long long>(c->map_max), c->st);
+        HERO_TRY(c->check_launch("mapping histogram"));
+        HERO_TRY(c->cuda(cudaMemcpyAsync(&maxc, c->map_max.p, 8, cudaMemcpyDeviceToHost, c->st), "mapping histogram"));
+        HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "mapping histogram"));
+        if (maxc < bins) break;
+        bins = maxc + 1;
+    }
+    *n_bins = c->nqb ? uint64_t(maxc) + 1 : 0;
+    const uint64_t m = std::min<uint64_t>(cap, *n_bins);
+    if (m) {
+        HERO_TRY(c->cuda(cudaMemcpyAsync(hist, c->map_hist.p, m * 8, cudaMemcpyDeviceToHost, c->st), "mapping histogram"));
+        HERO_TRY(c->cuda(cudaStreamSynchronize(c->st), "mapping histogram"));
+    }
+    return HERO_OK;
 }
 
 extern "C" int hero_get_overhang(hero_ctx *c, uint32_t *out) {

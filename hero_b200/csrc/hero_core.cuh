@@ -652,6 +652,80 @@ struct OverhangWalk {
     HERO_HD void finish() {}
 };
 
+// --mapping: what SubjectRead::chooseQueryWithBestAlignment (SubjectRead.cpp:
+// 463-500) reads of a record.  AlignmentRecord::isSubjectCoveredByQuery
+// (AlignmentRecord.cpp:343-370) needs the record's position on the subject,
+// the kinds of its first and last CIGAR entries and the bases of every entry
+// that is not an insertion; getAccuracy (AlignmentRecord.cpp:372-381) the
+// mismatch bases.  Entry boundaries do not change either sum, so a walk over
+// the record's runs and DP pieces gives them.
+template <class Sums>
+struct CoverWalk {
+    Sums sums;
+    uint32_t piece = 0;
+    int64_t pos = 0, non_ins = 0, subs = 0;
+    int32_t first = -1, last = -1;
+    HERO_HD void begin(int64_t, int64_t, int64_t) {}
+    HERO_HD void position(int64_t p) { pos = p; }
+    HERO_HD void run(uint8_t t, int64_t c) {
+        if (c <= 0) return;
+        if (first < 0) first = t;
+        last = t;
+        if (t != OP_I) non_ins += c;
+        if (t == OP_X) subs += c;
+    }
+    HERO_HD void dp(int64_t, int64_t, int64_t, int64_t, uint32_t, int64_t) {
+        const DpSum s = sums(piece++);
+        const uint32_t P = uint32_t(s.tot[0]) + s.tot[1] + s.tot[2] + s.tot[3];
+        if (P == 0) return;
+        if (first < 0) first = s.ft;
+        last = s.nruns >= 2 ? s.lt : s.ft;
+        non_ins += int64_t(s.tot[OP_M]) + s.tot[OP_X] + s.tot[OP_D];
+        subs += s.tot[OP_X];
+    }
+    HERO_HD bool check(int64_t, int64_t) { return true; }
+    HERO_HD void finish() {}
+    // isSubjectCoveredByQuery(Ls)
+    HERO_HD bool covers(int64_t Ls) const {
+        return first >= 0 && pos == 0 && first != OP_D && last != OP_D && non_ins >= Ls;
+    }
+};
+
+// chooseQueryWithBestAlignment over a subject's record list (n records in list
+// order; covers(i), subs(i) of each): how many of the list's records vote and
+// which.  No covering record: none (-1 returned, *n_keep = 0).  Exactly one:
+// the whole list keeps voting (the reference returns without touching the
+// list; returns -1, *n_keep = n).  Two or more: the first covering record with
+// the fewest substitutions, below the subject's length (returns its index,
+// *n_keep = 1; none below the length: -1, *n_keep = 0, where the reference
+// reports an error).
+template <class Covers, class Subs>
+HERO_HD int32_t map_choose(uint32_t n, int64_t Ls, const Covers &covers, const Subs &subs,
+                           uint32_t *n_keep) {
+    uint32_t qualified = 0;
+    int32_t best = -1;
+    double least = double(Ls);
+    for (uint32_t i = 0; i < n; i++) {
+        if (!covers(i)) continue;
+        qualified++;
+        const double d = double(subs(i));
+        if (d < least) {
+            least = d;
+            best = int32_t(i);
+        }
+    }
+    if (qualified == 0) {
+        *n_keep = 0;
+        return -1;
+    }
+    if (qualified == 1) {
+        *n_keep = n;
+        return -1;
+    }
+    *n_keep = best >= 0 ? 1u : 0u;
+    return best;
+}
+
 // QueryRead::getComplementBase (QueryRead.cpp:375-382), on the ASCII letter:
 // bit 2 set (C, G) flips C<->G, else A<->T by xor 0x15
 HERO_HD char complement_char(char c) { return (c & 0x02) ? char(c ^ 0x04) : char(c ^ 0x15); }

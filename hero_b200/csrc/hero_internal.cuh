@@ -129,6 +129,12 @@ void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint3
 void launch_probe(bool emit, bool aln, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
                   uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
                   unsigned long long *counters, cudaStream_t st);
+void launch_map_choose(const Params &p, uint64_t nsub, const uint32_t *cstart,
+                       const uint32_t *ccount, ChainArrays ch, const uint32_t *keys,
+                       ReadsView subj, ReadsView q, const DpSum *sums, uint32_t *alist,
+                       uint32_t *winners, unsigned long long *counters, cudaStream_t st);
+void launch_map_hist(ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint64_t bins,
+                     unsigned long long *hist, unsigned long long *maxc, cudaStream_t st);
 void launch_sort_hits(uint64_t nseg, const uint64_t *hit_off, uint64_t *hits, cudaStream_t st);
 void launch_chain(const Params &p, uint64_t nseg, ReadsView subj, ReadsView q,
                   const uint64_t *hit_off, const uint64_t *hits, ChainScratch sc,

@@ -1464,6 +1464,99 @@ __global__ void k_aln_list(uint64_t nsub, const uint32_t *cstart, const uint32_t
     if (lane_id() == 0) atomicAdd(&counters[C_KEPT], kept);
 }
 
+// --mapping, one thread per subject (SubjectReadAligner.cpp:556-561): its
+// accepted records in arrival order kept as SubjectRead::addAlignment keeps
+// them in consensus mode (keyed by the query's inner id, list_add), then
+// chooseQueryWithBestAlignment (SubjectRead.cpp:463-500, map_choose) picks the
+// records that vote; they become the batch's winners for k_vote.
+__global__ void k_map_choose(Params p, uint64_t nsub, const uint32_t *cstart,
+                             const uint32_t *ccount, ChainArrays ch, const uint32_t *keys,
+                             ReadsView subj, ReadsView q, const DpSum *sums, uint32_t *alist,
+                             uint32_t *winners, unsigned long long *counters) {
+    unsigned long long kept = 0;
+    for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < nsub;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        ChainSlots L{alist, cstart[2 * s], ccount[2 * s], cstart[2 * s + 1]};
+        auto key = [&](uint32_t c) { return uint64_t(ch.query[c]); };
+        auto better = [&](uint32_t a, uint32_t b) {
+            return record_better(ch.rate[a], ch.len[a], ch.rate[b], ch.len[b]);
+        };
+        uint32_t n = 0;
+        uint64_t largest = 0;
+        for (int o = 0; o < 2; o++) {
+            const uint32_t b = cstart[2 * s + o], e = b + ccount[2 * s + o];
+            for (uint32_t c = b; c < e; c++)
+                if (ch.status[c] == CH_ACCEPTED) n = list_add(L, n, largest, c, key, better);
+        }
+        const int64_t Ls = subj.len[s];
+        // one walk per listed record: map_choose asks covers(i), then subs(i)
+        int64_t walked = -1;
+        bool cov = false;
+        int64_t sub = 0;
+        auto walk = [&](uint32_t i) {
+            if (int64_t(i) == walked) return;
+            const uint32_t c = L.get(i);
+            const DpSum *sm = sums + ch.seg_off[c];
+            auto piece = [sm](uint32_t k) { return sm[k]; };
+            CoverWalk<decltype(piece)> w{piece};
+            walk_chain(p, int64_t(q.len[ch.query[c]]), Ls, KeyAt{keys + ch.key_off[c]},
+                       int32_t(ch.nkeys[c]), w);
+            cov = w.covers(Ls);
+            sub = w.subs;
+            walked = int64_t(i);
+        };
+        auto covers = [&](uint32_t i) {
+            walk(i);
+            return cov;
+        };
+        auto subs = [&](uint32_t i) {
+            walk(i);
+            return sub;
+        };
+        uint32_t n_keep = 0;
+        const int32_t best = map_choose(n, Ls, covers, subs, &n_keep);
+        for (uint32_t i = 0; i < n_keep; i++) {
+            const uint32_t c = L.get(n_keep == 1 && best >= 0 ? uint32_t(best) : i);
+            ch.win[c] = 1;
+            winners[atomicAdd(&counters[C_WIN], 1ull)] = c;
+        }
+        kept += n_keep;
+    }
+    kept = warp_sum(kept);
+    if (lane_id() == 0) atomicAdd(&counters[C_KEPT], kept);
+}
+
+// --mapping: QueryDataset::getCoverageAndWriteResults (QueryDataset.cpp:560-599)
+// -- per query base the sum of its four vote counts (no self vote), counted
+// into hist[min(sum, bins - 1)]; the largest sum goes to *maxc.  One warp per read.
+__global__ void k_map_hist(ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint64_t bins,
+                           unsigned long long *hist, unsigned long long *maxc) {
+    const uint32_t lane = lane_id();
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    unsigned long long mx = 0;
+    for (uint64_t r = uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < q.n;
+         r += warps) {
+        const uint64_t b = q.off[r];
+        const uint32_t Lr = q.len[r];
+        int32_t carry = 0;  // match-run votes entering the current chunk
+        for (uint32_t c0 = 0; c0 < Lr; c0 += 32) {
+            const uint32_t i = c0 + lane;
+            const int32_t d = i < Lr ? mdiff[b + i] : 0;
+            int32_t tot;
+            const int32_t run = carry + warp_exclusive<int32_t>(d, &tot) + d;
+            carry += tot;
+            if (i < Lr) {
+                const uint64_t sum = uint64_t(cov[(b + i) * 4]) + cov[(b + i) * 4 + 1] +
+                                     cov[(b + i) * 4 + 2] + cov[(b + i) * 4 + 3] + uint64_t(run);
+                atomicAdd(&hist[sum < bins ? sum : bins - 1], 1ull);
+                mx = sum > mx ? sum : mx;
+            }
+        }
+    }
+    mx = warp_max(mx);
+    if (lane == 0) atomicMax(maxc, mx);
+}
+
 // one thread per subject: its units (rec_off = exclusive scan of alist_n)
 __global__ void k_aln_units(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,
                             const uint32_t *alist, const uint32_t *alist_n,
@@ -2181,6 +2274,23 @@ void launch_dedupe(uint64_t nsub, const uint32_t *seg_chain_start,
         k_dedupe<<<grid_1d(nsub, 128), 128, 0, st>>>(nsub, seg_chain_start, seg_chain_count, ch,
                                                      winners, counters);
     }
+}
+
+void launch_map_choose(const Params &p, uint64_t nsub, const uint32_t *cstart,
+                       const uint32_t *ccount, ChainArrays ch, const uint32_t *keys,
+                       ReadsView subj, ReadsView q, const DpSum *sums, uint32_t *alist,
+                       uint32_t *winners, unsigned long long *counters, cudaStream_t st) {
+    if (!nsub) return;
+    counted();
+    k_map_choose<<<grid_1d(nsub, 128), 128, 0, st>>>(p, nsub, cstart, ccount, ch, keys, subj, q,
+                                                     sums, alist, winners, counters);
+}
+
+void launch_map_hist(ReadsView q, const uint32_t *cov, const int32_t *mdiff, uint64_t bins,
+                     unsigned long long *hist, unsigned long long *maxc, cudaStream_t st) {
+    if (!q.n) return;
+    counted();
+    k_map_hist<<<grid_1d(q.n * 32, 256), 256, 0, st>>>(q, cov, mdiff, bins, hist, maxc);
 }
 
 void launch_aln_list(uint64_t nsub, const uint32_t *cstart, const uint32_t *ccount,

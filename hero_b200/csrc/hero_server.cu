@@ -1,14 +1,20 @@
 // hero_server.cu -- serving form: many independent correction jobs on one GPU.
 //
 // The reference corrects one read set per process (main.cpp:36-104).  A server
-// runs a stream of such jobs with continuous batching: a worker thread runs
-// correction rounds back to back, and each round admits the oldest queued jobs
-// that fit in a device-memory budget.  The admitted jobs' reads are
-// concatenated into one query set whose reads carry their job
-// (hero_set_query_jobs), so one set of launches -- index build, seeding,
-// chaining, DP, votes, consensus -- serves every job of the round, and a job's
-// k-mers only ever meet its own reads: each job's output is the output it gets
-// alone.  Results are split back per job and kept until released.
+// runs a stream of such jobs with continuous batching.  Two worker threads,
+// each owning a context with its own stream, run correction rounds; a worker
+// that is free admits the oldest queued jobs that fit in the device-memory
+// budget left by the rounds already in flight.  So while one round's kernels
+// run, the other worker concatenates and uploads the next round's reads and
+// starts it: rounds overlap on the device (their launches share the SMs), host
+// preparation overlaps device work, and a job that arrives while a long round
+// runs is admitted as soon as a worker and memory are free instead of waiting
+// for that round.  Inside a round the admitted jobs' reads are concatenated
+// into one query set whose reads carry their job (hero_set_query_jobs), so one
+// set of launches -- index build, seeding, chaining, DP, votes, consensus --
+// serves every job of the round, and a job's k-mers only ever meet its own
+// reads: each job's output is the output it gets alone.  Results are split
+// back per job and kept until released.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -48,30 +54,52 @@ struct Job {
 
 }  // namespace
 
+// rounds that may be in flight at once (one context and worker thread each)
+constexpr int kServeWorkers = 2;
+
 struct hero_server {
     hero_params p{};
-    hero_ctx *ctx = nullptr;
+    hero_ctx *ctx[kServeWorkers] = {};
     uint64_t round_bytes = 0;
     Clock::time_point t0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<uint64_t> queue;
     std::unordered_map<uint64_t, Job> jobs;
-    std::thread worker;
+    std::thread worker[kServeWorkers];
     bool stop = false;
     uint64_t next_id = 1, rounds = 0, submitted = 0, done = 0, failed = 0, bases_done = 0;
     uint64_t max_jobs = 0;   // jobs a key can tell apart (k-mer bits leave room for the job)
     uint64_t cap_jobs = 0;   // jobs per round after a round ran out of memory (0: no cap)
     std::vector<hero_dp_tuning> tuning;  // DP kernel shapes to apply before the next round
-    bool tuning_new = false;
-    double busy_ms = 0;
+    uint64_t tuning_gen = 0;             // bumped by every hero_server_set_dp_tuning
+    uint64_t in_flight_bytes = 0;        // admission estimates of the rounds running
+    int in_flight = 0;                   // rounds running
+    bool exclusive = false;              // the queue head needs the device to itself
+    double busy_ms = 0, busy_since = 0;  // time with at least one round in flight
+    uint64_t overlapped_rounds = 0;      // rounds that started while another ran
 
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
     }
-    void run();
-    void run_round(std::vector<uint64_t> ids);
+    void run(int w);
+    void run_round(int w, std::vector<uint64_t> ids, uint64_t bytes);
+    void round_begin(uint64_t bytes);  // with mu held
+    void round_end(uint64_t bytes);    // with mu held
 };
+
+void hero_server::round_begin(uint64_t bytes) {
+    if (in_flight == 0) busy_since = now_ms();
+    else overlapped_rounds++;
+    in_flight++;
+    in_flight_bytes += bytes;
+}
+
+void hero_server::round_end(uint64_t bytes) {
+    in_flight--;
+    in_flight_bytes -= bytes;
+    if (in_flight == 0) busy_ms += now_ms() - busy_since;
+}
 
 extern "C" uint64_t hero_job_bytes(uint64_t bases, uint64_t reads, int32_t k) {
     // per base: read copies and codes (2), vote matrix (16 + 4), corrected bases (1);
@@ -92,36 +120,52 @@ extern "C" uint64_t hero_round_admit(const uint64_t *bytes, uint64_t n_queued, u
     return n;
 }
 
-void hero_server::run() {
+void hero_server::run(int w) {
+    uint64_t my_tuning_gen = 0;
     std::unique_lock<std::mutex> lk(mu);
     while (true) {
-        cv_work.wait(lk, [&] { return stop || !queue.empty(); });
+        // admissible: the queue head fits the budget the running rounds leave
+        // (a head that needs the device to itself waits for every round to end)
+        auto admissible = [&] {
+            if (queue.empty()) return false;
+            if (in_flight == 0) return true;
+            if (exclusive) return false;
+            return in_flight_bytes + jobs[queue.front()].bytes <= round_bytes;
+        };
+        cv_work.wait(lk, [&] { return stop || admissible(); });
         if (stop) break;
+        const uint64_t room = in_flight == 0 ? round_bytes : round_bytes - in_flight_bytes;
         std::vector<uint64_t> sizes;
         for (uint64_t id : queue) sizes.push_back(jobs[id].bytes);
-        uint64_t take = hero_round_admit(sizes.data(), sizes.size(), round_bytes);
+        uint64_t take = hero_round_admit(sizes.data(), sizes.size(), room);
         take = std::min(take, max_jobs);
         if (cap_jobs) take = std::min(take, cap_jobs);
         std::vector<uint64_t> ids(queue.begin(), queue.begin() + long(take));
         queue.erase(queue.begin(), queue.begin() + long(take));
+        exclusive = false;
+        uint64_t bytes = 0;
         const double t = now_ms();
         for (uint64_t id : ids) {
             jobs[id].state = HERO_JOB_RUNNING;
             jobs[id].start_ms = t;
+            bytes += jobs[id].bytes;
         }
+        round_begin(bytes);
         std::vector<hero_dp_tuning> tun;
-        const bool retune = tuning_new;
+        const bool retune = tuning_gen != my_tuning_gen;
         if (retune) {
             tun = tuning;
-            tuning_new = false;
+            my_tuning_gen = tuning_gen;
         }
         lk.unlock();
-        if (retune) hero_set_dp_tuning(ctx, tun.data(), uint32_t(tun.size()));
-        run_round(ids);
+        cv_work.notify_all();  // the other worker may admit what is left
+        if (retune) hero_set_dp_tuning(ctx[w], tun.data(), uint32_t(tun.size()));
+        run_round(w, ids, bytes);
         lk.lock();
         cv_done.notify_all();
+        cv_work.notify_all();
     }
-    // jobs still queued at shutdown fail
+    // jobs still queued at shutdown fail (the first worker to get here fails them)
     for (uint64_t id : queue) {
         Job &j = jobs[id];
         j.err = "server stopped";
@@ -133,10 +177,10 @@ void hero_server::run() {
     cv_done.notify_all();
 }
 
-// One round over the given jobs (the worker owns the context; job inputs are
-// not touched by other threads while the job is running).
-void hero_server::run_round(std::vector<uint64_t> ids) {
-    const double t_begin = now_ms();
+// One round over the given jobs on worker w's context (the worker owns it; job
+// inputs are not touched by other threads while the job is running).
+void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est) {
+    hero_ctx *ctx = this->ctx[w];
     std::vector<Job *> js;
     {
         std::lock_guard<std::mutex> g(mu);
@@ -195,22 +239,23 @@ void hero_server::run_round(std::vector<uint64_t> ids) {
         st = hero_consensus(ctx, out_seq.data(), imin.data(), imed.data(), imax.data(), mis.data(),
                             gc.data(), good.data());
     const std::string err = st == HERO_OK ? std::string() : std::string(hero_last_error(ctx));
-    if (st == HERO_E_OOM && js.size() > 1) {
-        // the estimate was short: requeue the jobs in order and admit half as many
-        std::lock_guard<std::mutex> g(mu);
+    std::lock_guard<std::mutex> g(mu);
+    if (st == HERO_E_OOM && (js.size() > 1 || in_flight > 1)) {
+        // the estimate was short, or another round held the memory: requeue the
+        // jobs in order, then admit half as many (one job: with the device to itself)
         for (size_t t = js.size(); t-- > 0;) {
             js[t]->state = HERO_JOB_QUEUED;
             queue.push_front(ids[t]);
         }
-        cap_jobs = js.size() / 2;
-        busy_ms += now_ms() - t_begin;
+        if (js.size() > 1) cap_jobs = js.size() / 2;
+        else exclusive = true;
+        round_end(round_est);
         return;
     }
-    std::lock_guard<std::mutex> g(mu);
     if (st == HERO_OK && cap_jobs) cap_jobs *= 2;
     rounds++;
     const double t_end = now_ms();
-    busy_ms += t_end - t_begin;
+    round_end(round_est);
     r = 0;
     b = 0;
     for (Job *j : js) {
@@ -247,33 +292,39 @@ extern "C" int hero_server_create(const hero_params *p, uint64_t round_bytes, he
     *out = nullptr;
     hero_server *s = new hero_server();
     s->p = *p;
+    s->p.stream = nullptr;  // every worker context creates its own stream
     s->t0 = Clock::now();
-    int st = hero_create(p, &s->ctx);
-    if (st != HERO_OK) {
-        delete s;
-        return st;
+    for (int w = 0; w < kServeWorkers; w++) {
+        const int st = hero_create(&s->p, &s->ctx[w]);
+        if (st != HERO_OK) {
+            for (int v = 0; v < w; v++) hero_destroy(s->ctx[v]);
+            delete s;
+            return st;
+        }
     }
     if (round_bytes == 0) {
-        // per-batch working set (hits, chains, DP segments of one subject batch)
+        // per-batch working set of each worker (hits, chains, DP segments of one
+        // subject batch)
         const uint64_t reserve = 12ull << 30;
         uint64_t budget = p->device_memory_budget;
         if (!budget) {
             size_t fr = 0, tot = 0;
             cudaSetDevice(p->device);
             if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-                hero_destroy(s->ctx);
+                for (int w = 0; w < kServeWorkers; w++) hero_destroy(s->ctx[w]);
                 delete s;
                 return HERO_E_CUDA;
             }
             budget = uint64_t(double(fr) * 0.8);
         }
-        round_bytes = budget > 2 * reserve ? budget - reserve : budget / 2;
+        const uint64_t res = kServeWorkers * reserve;
+        round_bytes = budget > 2 * res ? budget - res : budget / 2;
     }
     s->round_bytes = round_bytes;
     // job tags share a 128-bit key with the 2k k-mer bits (hero_set_query_jobs)
     const int free_bits = 2 * p->k <= 64 ? 32 : std::min(32, 128 - 2 * p->k);
     s->max_jobs = free_bits >= 32 ? 0xffffffffull : (1ull << free_bits);
-    s->worker = std::thread([s] { s->run(); });
+    for (int w = 0; w < kServeWorkers; w++) s->worker[w] = std::thread([s, w] { s->run(w); });
     *out = s;
     return HERO_OK;
 }
@@ -285,8 +336,9 @@ extern "C" void hero_server_destroy(hero_server *s) {
         s->stop = true;
     }
     s->cv_work.notify_all();
-    if (s->worker.joinable()) s->worker.join();
-    hero_destroy(s->ctx);
+    for (int w = 0; w < kServeWorkers; w++)
+        if (s->worker[w].joinable()) s->worker[w].join();
+    for (int w = 0; w < kServeWorkers; w++) hero_destroy(s->ctx[w]);
     delete s;
 }
 
@@ -296,7 +348,7 @@ extern "C" int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t
         if (t[i].warps_per_block != 2 && t[i].warps_per_block != 4) return HERO_E_INPUT;
     std::lock_guard<std::mutex> g(s->mu);
     s->tuning.assign(t, t + n);
-    s->tuning_new = true;
+    s->tuning_gen++;
     return HERO_OK;
 }
 
@@ -432,7 +484,8 @@ extern "C" int hero_server_get_stats(hero_server *s, hero_server_stats *out) {
     out->rounds = s->rounds;
     out->bases_done = s->bases_done;
     out->round_bytes_budget = s->round_bytes;
-    out->busy_ms = s->busy_ms;
+    out->busy_ms = s->busy_ms + (s->in_flight ? s->now_ms() - s->busy_since : 0.0);
     out->uptime_ms = s->now_ms();
+    out->overlapped_rounds = s->overlapped_rounds;
     return HERO_OK;
 }

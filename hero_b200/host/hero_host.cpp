@@ -121,7 +121,9 @@ bool Config::parse(int argc, char **argv) {
             subject_batch = uint32_t(std::strtoul(v.c_str(), nullptr, 10));
         } else if (a == "--merge") {
             merge = true;
-        } else if (a == "-v" || a == "--mapping" || a == "--covfilter" ||
+        } else if (a == "--mapping") {
+            mapping = true;
+        } else if (a == "-v" || a == "--covfilter" ||
                    a == "--suffix" || a == "--size" || a == "--notification") {
             std::cerr << a << ": not part of the path this build replaces\n";
             return false;
@@ -497,7 +499,10 @@ bool HashTableGpu::createHashTables(const Config &c, QueryDataset *q, std::strin
     p.consensus_threshold = c.consensus_thr;
     p.device = c.device;
     p.subject_batch = c.subject_batch;
-    p.flags = c.consensus ? (c.merge ? HERO_FLAG_MERGE_PAIRS : 0u) : HERO_FLAG_ALIGNMENT_OUTPUT;
+    p.flags = !c.consensus ? HERO_FLAG_ALIGNMENT_OUTPUT
+              : c.mapping  ? HERO_FLAG_MAPPING
+              : c.merge    ? HERO_FLAG_MERGE_PAIRS
+                           : 0u;
     if (!ok(nullptr, hero_create(&p, &ctx), "hero_create", err)) return false;
     const ReadSet &r = q->reads;
     return ok(ctx, hero_set_queries(ctx, reinterpret_cast<const uint8_t *>(r.seq.data()),
@@ -577,6 +582,35 @@ bool merge_pairs(HashTableGpu &t, QueryDataset &q, std::string *err) {
     return ok(t.ctx, hero_merge_pairs(t.ctx, reinterpret_cast<uint8_t *>(&q.merged[0]),
                                       q.merged_len.data()),
               "hero_merge_pairs", err);
+}
+
+}  // namespace herohost
+
+namespace herohost {
+
+bool write_mapping(HashTableGpu &t, const Config &c, std::string *err) {
+    uint64_t n = 0;
+    if (hero_mapping_histogram(t.ctx, nullptr, 0, &n) != HERO_OK) {
+        *err = hero_last_error(t.ctx);
+        return false;
+    }
+    std::vector<uint64_t> hist(n);
+    if (n && hero_mapping_histogram(t.ctx, hist.data(), n, &n) != HERO_OK) {
+        *err = hero_last_error(t.ctx);
+        return false;
+    }
+    // QueryDataset.cpp:589-596: the output name as given, opened for appending
+    std::FILE *f = std::fopen(c.out.c_str(), "ab");
+    if (!f) {
+        *err = "cannot open " + c.out;
+        return false;
+    }
+    std::fputs("COV\tFRE\n", f);
+    for (uint64_t i = 0; i < n; i++)
+        if (hist[i]) std::fprintf(f, "%llu\t%llu\n", (unsigned long long)i, (unsigned long long)hist[i]);
+    const bool ok = std::fclose(f) == 0;
+    if (!ok) *err = "cannot write " + c.out;
+    return ok;
 }
 
 }  // namespace herohost

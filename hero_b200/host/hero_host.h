@@ -22,6 +22,7 @@ struct Config {
     double mis_rate = 1.0, indel_rate = 1.0, consensus_thr = 0.6;
     bool affine = false, consensus = false, covinfo = false, single_reads = false;
     bool merge = false;  // --merge: paired reads (2i, 2i+1) merged after the consensus
+    bool mapping = false;  // --mapping: chosen records vote; the coverage histogram is written
     uint64_t stream_chunk = 400, query_chunk = 800;
     int device = 0;
     uint32_t subject_batch = 0;
@@ -96,5 +97,9 @@ bool call_consensus(HashTableGpu &t, QueryDataset &q, std::string *err);
 
 // QueryDataset::mergePairedReads (QueryDataset.cpp:539-558) on the device (--merge)
 bool merge_pairs(HashTableGpu &t, QueryDataset &q, std::string *err);
+
+// QueryDataset::getCoverageAndWriteResults (QueryDataset.cpp:560-599): the
+// coverage histogram of the votes, appended to the output name (--mapping)
+bool write_mapping(HashTableGpu &t, const Config &c, std::string *err);
 
 }  // namespace herohost

@@ -11,6 +11,9 @@ using namespace herohost;
 int main(int argc, char **argv) {
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
+    auto sec_since = [](clk::time_point a) {
+        return std::chrono::duration<double>(clk::now() - a).count();
+    };
     Config cfg;
     if (!cfg.parse(argc, argv)) {
         std::cout << "Please follow the above help information." << std::endl;
@@ -40,6 +43,14 @@ int main(int argc, char **argv) {
         return 1;
     }
     const auto t3 = clk::now();
+    if (cfg.consensus && cfg.mapping) {  // main.cpp:83-87: the histogram instead of reads
+        if (!write_mapping(table, cfg, &err)) {
+            std::cerr << "Error: " << err << std::endl;
+            return 1;
+        }
+        std::cout << sec_since(t0) << " seconds (Total time used)" << std::endl;
+        return 0;
+    }
     if (cfg.consensus && !call_consensus(table, query, &err)) {
         std::cerr << "Error: " << err << std::endl;
         return 1;

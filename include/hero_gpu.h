@@ -78,6 +78,16 @@ typedef struct hero_ctx hero_ctx;
  * QueryDataset::mergePairedReads does (QueryDataset.cpp:539-558). */
 #define HERO_FLAG_MERGE_PAIRS 2u
 
+/* --mapping (with -c): per subject, of the records SubjectRead::addAlignment
+ * keeps, only those SubjectRead::chooseQueryWithBestAlignment keeps vote
+ * (SubjectRead.cpp:463-500; SubjectReadAligner.cpp:556-561): no record that
+ * covers the whole subject -- none; exactly one -- all of the subject's
+ * records; two or more -- the covering one with the fewest substitutions.
+ * hero_mapping_histogram then gives QueryDataset::getCoverageAndWriteResults'
+ * histogram (QueryDataset.cpp:560-599).  Reads keep HERO's own limit of this
+ * path, shorter than 32768 bases. */
+#define HERO_FLAG_MAPPING 4u
+
 typedef struct {
     int32_t k;              /* k-mer length, 1..63 (Config::iKmer, -k; default 39) */
     int32_t min_overlap;    /* Config::minimumOverlapLength, -l (default 40) */
@@ -261,6 +271,15 @@ int hero_align_segments_noalloc(int affine, const uint8_t *subj, const uint64_t 
                                 int32_t max_side, const uint64_t *ops_off, uint8_t *ops,
                                 int32_t *nops, void *stream);
 
+/* --mapping: coverage histogram of the current votes (QueryDataset::
+ * getCoverageAndWriteResults, QueryDataset.cpp:560-599).  hist[c] = the number
+ * of query bases whose four vote counts sum to c (no self vote), for
+ * c = 0 .. *n_bins - 1, where *n_bins is the largest sum + 1.  Copies
+ * min(cap, *n_bins) entries (hist may be NULL with cap 0 to learn *n_bins).
+ * The writer prints "COV\tFRE" and "c\thist[c]" for every c with hist[c] > 0.
+ * Needs a context created with HERO_FLAG_MAPPING (else HERO_E_STATE). */
+int hero_mapping_histogram(hero_ctx *ctx, uint64_t *hist, uint64_t cap, uint64_t *n_bins);
+
 /* ------------------------------------------------------------------------
  * Serving: many independent correction jobs (each its own -q X -s X run)
  * corrected together.  No reference counterpart: HERO runs one job per
@@ -295,18 +314,21 @@ typedef struct {
 typedef struct {
     uint64_t jobs_submitted, jobs_done, jobs_failed, rounds, bases_done;
     uint64_t round_bytes_budget; /* admission limit of one round (estimated device bytes) */
-    double busy_ms;              /* wall time spent inside rounds */
+    double busy_ms;              /* wall time with at least one round in flight */
     double uptime_ms;
+    uint64_t overlapped_rounds;  /* rounds started while another round ran */
 } hero_server_stats;
 
-/* A server owns one context on p->device and a worker thread that runs
- * correction rounds back to back (continuous batching).  Each round admits the
- * oldest queued jobs whose estimated device memory (hero_job_bytes) fits in
- * round_bytes (0 = p->device_memory_budget, or 80 % of the device's free memory
- * at creation, minus the per-batch working set); a job larger than that runs
- * in a round of its own.  All jobs of a server share p's parameters. */
+/* A server owns two contexts on p->device, each with its own stream and worker
+ * thread (continuous batching with overlapping rounds).  A free worker admits
+ * the oldest queued jobs whose estimated device memory (hero_job_bytes) fits in
+ * what the rounds in flight leave of round_bytes (0 = p->device_memory_budget,
+ * or 80 % of the device's free memory at creation, minus each worker's
+ * per-batch working set); a job larger than round_bytes runs in a round of its
+ * own once no other round is in flight.  p->stream is ignored.  All jobs of a
+ * server share p's parameters. */
 int hero_server_create(const hero_params *p, uint64_t round_bytes, hero_server **out);
-/* Stops the worker after the round in flight; jobs still queued fail. */
+/* Stops the workers after the rounds in flight; jobs still queued fail. */
 void hero_server_destroy(hero_server *s);
 
 /* Copies a job's reads (layout of hero_set_queries) into the server and queues
