@@ -35,7 +35,7 @@ def test_alignment_output_mode_without_c(cli, tmp_path):
     assert r.returncode == 1 and "Unable to open file" in r.stderr
 
 
-@pytest.mark.parametrize("flag", ["-v", "--mapping", "--covfilter"])
+@pytest.mark.parametrize("flag", ["-v", "--covfilter", "--suffix"])
 def test_refuses_modes_outside_the_path(cli, flag):
     r = run(cli, "-q", "a.fq", "-s", "a.fq", "-c", flag)
     assert r.returncode == 1 and "not part of the path" in r.stderr
