@@ -86,7 +86,7 @@ def parse():
     ap.add_argument("--impl", default="hero", choices=["hero", "reference"])
     ap.add_argument("--workload", default="config1",
                     choices=["config1", "config2", "config3", "config4", "config5"])
-    ap.add_argument("--served-jobs", type=int, default=24,
+    ap.add_argument("--served-jobs", type=int, default=40,
                     help="jobs of the served block added to the default line (0: none)")
     ap.add_argument("--jobs-scale", type=float, default=0.0,
                     help="genome-size scale of the served jobs (default 1.0: the stream's sizes)")
@@ -336,12 +336,14 @@ def int_peaks(device: int) -> dict:
 
 
 def dp_roofline(cells: int, dp_ms: float, aligner: str, peaks: dict, launches: int,
-                pairs: bool = False) -> dict:
+                pair_share: float = 0.0) -> dict:
     """The DP kernel's roofline: cells x ops/cell (survey: 6 global, 10 affine)
     over its device time, against the largest measured peak of the instruction
-    forms it issues (the 32-bit forms; the packed 16-bit ones when it runs pairs)."""
+    forms it issues: the packed 16-bit DPX forms (2 lanes each) when most of its
+    cells ran as 16-bit pairs (pair_share > 0.5), else the 32-bit forms."""
     ops_per_cell = 10 if aligner == "affine" else 6
     achieved = cells * ops_per_cell / (dp_ms / 1e3) / 1e12 if dp_ms > 0 else None
+    pairs = pair_share > 0.5
     forms = (["viaddmax_s16x2", "vimax3_s16x2"] if pairs else
              ["add_max_c", "viaddmax_s32", "vimax3_s32"])
     vals = [(peaks.get(f), f) for f in forms if peaks.get(f)]
@@ -354,6 +356,7 @@ def dp_roofline(cells: int, dp_ms: float, aligner: str, peaks: dict, launches: i
             "traffic": traffic, "ops_per_cell": ops_per_cell,
             "peak_source": f"measured in this run: the fastest of the kernel's instruction "
                            f"forms ({form}); MEASURED_PEAKS.json has no integer peak",
+            "cells_as_16bit_pairs": round(pair_share, 4),
             "peaks_tops": peaks}
 
 
@@ -458,7 +461,8 @@ def run_server(jobs, stream, dev: int, arrivals=None) -> dict:
 def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.9) -> dict:
     """The serving stream: each job alone (one at a time), the server with every
     job submitted at once (its capacity), then the server under Poisson arrivals
-    at `load` of that capacity.  served == alone compares every job's digest."""
+    at `load` of the better of the two rates (so the load is a true fraction of
+    what the device sustains).  served == alone compares every job's digest."""
     if in_memory:
         data = dict(job_stream(jobs))
 
@@ -475,7 +479,7 @@ def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.9) -> dict:
     times, alone_dig, alone_s, bases = run_alone(stream(), dev)
     closed = run_server(jobs, stream(), dev)
     mean_bases = bases / len(jobs)
-    lam = load * closed["bases_per_s"] / mean_bases  # jobs/s
+    lam = load * max(closed["bases_per_s"], bases / alone_s) / mean_bases  # jobs/s
     # the stream's Poisson arrival times (config4_jobs draws them at 1 job/s), rescaled
     arrivals = {j.job_id: j.arrival_s / lam for j in jobs}
     poisson = run_server(jobs, stream(), dev, arrivals)
@@ -616,6 +620,8 @@ def measure_workload(rs, kw, dev: int, steps: int, warmup: int, peaks: dict,
         launches = (p1["kernel_launches"] - p0["kernel_launches"]) // plain_steps * steps
     cells = s1["dp_cells"] - s0["dp_cells"]
     dp_ms = s1["ms_dp_kernel"] - s0["ms_dp_kernel"]
+    computed = s1["dp_cells_computed"] - s0["dp_cells_computed"]
+    pair_share = (s1["dp_cells_pairs"] - s0["dp_cells_pairs"]) / computed if computed else 0.0
     per = {k: round((p1[k] - p0[k]) / plain_steps, 3)
            for k in ("ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_dp_kernel", "ms_record",
                      "ms_vote", "ms_consensus", "ms_align_wall")}
@@ -633,7 +639,7 @@ def measure_workload(rs, kw, dev: int, steps: int, warmup: int, peaks: dict,
         "value": world * nb * steps / t_dev, "ms_per_step": 1e3 * t_dev / steps,
         "e2e": {"value": world * nb * steps / t_e2e, "unit": "bases/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": dp_roofline(cells, dp_ms, kw["aligner"], peaks, dp_launches),
+        "roofline": dp_roofline(cells, dp_ms, kw["aligner"], peaks, dp_launches, pair_share),
         "seeding_roofline": {"bound": "hbm", "kernels": "k_probe (count, emit) + k_sort_hits",
                              "achieved": seed_gbs, "peak": hbm_peak, "unit": "GB/s",
                              "frac": (seed_gbs / hbm_peak) if seed_gbs else None,
@@ -835,8 +841,10 @@ def bench_sharded(args):
     dp_ms = s1["ms_dp_kernel"] - s0["ms_dp_kernel"]
     launches = s1["kernel_launches"] - s0["kernel_launches"]
     h.close()
+    computed = s1["dp_cells_computed"] - s0["dp_cells_computed"]
     roof = dp_roofline(cells, dp_ms, kw["aligner"], int_peaks(dev),
-                       args.steps * ((b - a + 131071) // 131072))
+                       args.steps * ((b - a + 131071) // 131072),
+                       (s1["dp_cells_pairs"] - s0["dp_cells_pairs"]) / computed if computed else 0.0)
     roof["kernel"] += " (rank 0's DP launches)"
     if rank == 0:
         line = {

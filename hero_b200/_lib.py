@@ -67,12 +67,13 @@ _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record"
 class HeroStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
                 [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64),
-                 ("dp_rows_max", C.c_uint64)])
+                 ("dp_rows_max", C.c_uint64), ("dp_cells_pairs", C.c_uint64)])
 
 
 class DpTuning(C.Structure):
     _fields_ = [("rows_max", C.c_int32), ("warps_per_block", C.c_int32),
-                ("pair_strips", C.c_uint32), ("chunk_strips", C.c_uint32)]
+                ("pair_strips", C.c_uint32), ("chunk_strips", C.c_uint32),
+                ("regs_per_thread", C.c_int32)]
 
 
 def load_tuning(path: str | None = None, aligner: str = "affine") -> list[dict]:
@@ -232,7 +233,8 @@ class Hero:
         arr = (DpTuning * max(1, len(classes)))()
         for i, t in enumerate(classes):
             arr[i] = DpTuning(int(t["rows_max"]), int(t["warps_per_block"]),
-                              int(t["pair_strips"]), int(t["chunk_strips"]))
+                              int(t["pair_strips"]), int(t["chunk_strips"]),
+                              int(t.get("regs_per_thread", 0)))
         self._check(self.lib.hero_set_dp_tuning(self.h, arr, len(classes)), "set_tuning")
 
     def _check(self, rc: int, what: str):
@@ -457,7 +459,8 @@ class HeroServer:
         arr = (DpTuning * max(1, len(classes)))()
         for i, t in enumerate(classes):
             arr[i] = DpTuning(int(t["rows_max"]), int(t["warps_per_block"]),
-                              int(t["pair_strips"]), int(t["chunk_strips"]))
+                              int(t["pair_strips"]), int(t["chunk_strips"]),
+                              int(t.get("regs_per_thread", 0)))
         self.lib.hero_server_set_dp_tuning(self.h, arr, len(classes))
 
     def close(self):

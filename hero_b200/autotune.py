@@ -2,7 +2,7 @@
 
 For each sample read length it builds a correction job with reads of that
 length, runs the DP kernel under every candidate shape -- warps per block,
-16-bit pairs of segments, row-chunk or one-lane tracebacks -- and records the
+16-bit pairs of segments, row-chunk tracebacks, registers a thread -- and records the
 fastest, with every candidate's time, in a JSON file (hero_b200/tuning.json by
 default), which hero_b200.Hero loads.  A class is keyed on the longest DP side
 the sample's batches showed (read length - k for reads that share a k-mer
@@ -36,8 +36,10 @@ ROWS_LAST = 1023
 
 
 def candidates():
-    for warps, pair, chunk in itertools.product((4, 2), (0, ALL), (ALL, 0, FROM3)):
-        yield {"warps_per_block": warps, "pair_strips": pair, "chunk_strips": chunk}
+    # row-chunk walks for all strip counts or from three on (one-lane walks never won)
+    for warps, pair, chunk, regs in itertools.product((4, 2, 1), (0, ALL), (ALL, FROM3), (128, 168)):
+        yield {"warps_per_block": warps, "pair_strips": pair, "chunk_strips": chunk,
+               "regs_per_thread": regs}
 
 
 def sample(read_len: int, genome_bp: int, seed: int = 91):

@@ -68,6 +68,8 @@ struct hero_ctx {
     DBuf q_ext, m_seq, m_len;
     bool merge = false;
     bool mapping = false;  // --mapping: chosen records vote; coverage histogram
+    std::vector<uint64_t> q_off_h;  // host copy of the query offsets (sizes of subject batches)
+    DBuf wcache;                    // per batch: the table slot each probe window found
     DBuf map_hist, map_max;
     bool consensus_done = false;  // out_seq holds the consensus of the current votes
     std::vector<uint8_t> aln_host;  // .aln text of every subject aligned since the last take
@@ -106,7 +108,7 @@ struct hero_ctx {
                         &x_klo, &x_khi, &x_kval, &x_owner, &x_count, &x_slot_of, &x_start,
                         &x_fill, &x_tmp, &q_job, &win_sorted, &win_bins, &a_list, &a_n,
                         &a_roff, &a_unit, &a_len, &a_pre, &a_cig, &a_uoff, &a_text, &q_ext,
-                        &m_seq, &m_len, &map_hist, &map_max};
+                        &m_seq, &m_len, &map_hist, &map_max, &wcache};
         for (DBuf *b : list) all.push_back(b);
     }
 
@@ -191,7 +193,8 @@ static ReadsView query_view(hero_ctx *c) {
 static void apply_tuning(const hero_ctx *c, DpLaunch &a) {
     for (const hero_dp_tuning &t : c->tuning)
         if (a.rmax <= t.rows_max) {
-            a.warps = t.warps_per_block == 2 ? 2 : 4;
+            a.warps = (t.warps_per_block == 1 || t.warps_per_block == 2) ? t.warps_per_block : 4;
+            a.regs = t.regs_per_thread == 168 ? 168 : 128;
             a.pair_mask = t.pair_strips;
             a.chunk_mask = t.chunk_strips;
             return;
@@ -332,6 +335,7 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     cudaEventRecord(e0, c->st);
     c->nq = n;
     c->nqb = n ? off[n] : 0;
+    c->q_off_h.assign(off, off + (n ? n + 1 : 0));
     c->have_index = false;
     c->consensus_done = false;
     c->tagged = false;
@@ -371,8 +375,10 @@ extern "C" int hero_set_dp_tuning(hero_ctx *c, const hero_dp_tuning *t, uint32_t
     if (!c) return HERO_E_INPUT;
     if (n && !t) return c->fail(HERO_E_INPUT, "null tuning table");
     for (uint32_t i = 0; i < n; i++)
-        if (t[i].warps_per_block != 2 && t[i].warps_per_block != 4)
-            return c->fail(HERO_E_INPUT, "warps_per_block must be 2 or 4");
+        if (t[i].warps_per_block != 1 && t[i].warps_per_block != 2 && t[i].warps_per_block != 4)
+            return c->fail(HERO_E_INPUT, "warps_per_block must be 1, 2 or 4");
+        else if (t[i].regs_per_thread != 0 && t[i].regs_per_thread != 128 && t[i].regs_per_thread != 168)
+            return c->fail(HERO_E_INPUT, "regs_per_thread must be 0, 128 or 168");
     c->tuning.assign(t, t + n);
     c->plan_ok = false;  // a captured round keeps the shapes it was captured with
     return HERO_OK;
@@ -526,7 +532,7 @@ static int aln_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, ReadsView q,
 }
 
 // runs every stage for subjects [0, nsub) of the given reads
-static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6]) {
+static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, uint64_t nbases, double ms[6]) {
     const uint64_t nseg = 2 * nsub;
     ReadsView q = query_view(c);
     TableView t{P_<Slot>(c->t_slots), P_<uint64_t>(c->t_vals), c->t_mask};
@@ -550,7 +556,10 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         if ((r = c->cuda(cudaMemsetAsync(ctr + C_NC, 0, sizeof(unsigned long long) * (C_MAXC - C_NC + 1), c->st), "batch: counters"))) break;
         static_assert(C_WIN == C_OVERFLOW + 1, "overflow flag and winner count are cleared together");
         if ((r = c->cuda(cudaMemsetAsync(ctr + C_OVERFLOW, 0, 2 * sizeof(unsigned long long), c->st), "batch: counters"))) break;
-        launch_probe(false, c->p.aln != 0, subj, nsub, q, t, c->p.k, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
+        // the count pass leaves the slot of every window (2 x 8 bytes a subject base) for the emit pass
+        if ((r = c->ensure(c->wcache, std::max<uint64_t>(nbases, 1) * 16, "probe windows"))) break;
+        uint2 *wc = P_<uint2>(c->wcache);
+        launch_probe(false, c->p.aln != 0, subj, nsub, q, t, c->p.k, wc, P_<uint32_t>(c->seg_hits), nullptr, nullptr, ctr, c->st);
         launch_scan_u32(P_<uint32_t>(c->seg_hits), P_<uint64_t>(c->hit_off), nseg, c->scan_tmp.p, c->st);
         uint64_t H = 0;
         if (cap) {
@@ -562,7 +571,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
         }
         const uint64_t Hc = std::max<uint64_t>(H, 1);
         if ((r = c->ensure(c->hits, Hc * 8, "hits"))) break;
-        launch_probe(true, c->p.aln != 0, subj, nsub, q, t, c->p.k, nullptr, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), ctr, c->st);
+        launch_probe(true, c->p.aln != 0, subj, nsub, q, t, c->p.k, wc, nullptr, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), ctr, c->st);
         launch_sort_hits(nseg, P_<uint64_t>(c->hit_off), P_<uint64_t>(c->hits), c->st);
         if ((r = c->check_launch("seed"))) break;
         rec(1);
@@ -632,7 +641,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
                    q.code, q.off, P_<uint32_t>(c->ops), stride, P_<DpSum>(c->sums),
                    P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
                    c->p.affine, 1,  // reads with a non-ACGT base never reach the DP
-                   0u, 0u, kStripsAll, 4};
+                   0u, 0u, kStripsAll, 4, ctr + C_CELLS_PAIR};
         apply_tuning(c, a);
         launch_dp(a, P_<uint64_t>(c->bin_off), P_<uint64_t>(c->dp_tasks), cmax, c->st);
         if ((r = c->check_launch("dp"))) break;
@@ -682,7 +691,8 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, double ms[6])
     return r;
 }
 
-static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
+// off_h: host offsets of the n reads (n + 1 entries), for the batch sizes
+static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n, const uint64_t *off_h) {
     c->consensus_done = false;
     const auto wall0 = std::chrono::steady_clock::now();
     uint64_t B = c->P.subject_batch ? c->P.subject_batch : 131072;
@@ -696,7 +706,7 @@ static int align_reads(hero_ctx *c, const ReadsView &all, uint64_t n) {
         // a batch is a window of the read arrays: shift the per-read pointers
         ReadsView v{all.code, all.off + b,  all.len + b, all.uid + b, all.good + b,
                     nb,       all.job ? all.job + b : nullptr};
-        HERO_TRY(align_batch(c, v, nb, ms));
+        HERO_TRY(align_batch(c, v, nb, off_h[b + nb] - off_h[b], ms));
     }
     if (c->capturing) return HERO_OK;
     c->stats.subjects += n;
@@ -720,7 +730,7 @@ extern "C" int hero_align_self(hero_ctx *c) {
     cudaSetDevice(c->dev);
     ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
                 P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq, job_tags(c)};
-    return align_reads(c, v, c->nq);
+    return align_reads(c, v, c->nq, c->q_off_h.data());
 }
 
 extern "C" int hero_align_self_range(hero_ctx *c, uint64_t first, uint64_t count) {
@@ -733,7 +743,7 @@ extern "C" int hero_align_self_range(hero_ctx *c, uint64_t first, uint64_t count
     ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off) + first, P_<uint32_t>(c->q_len) + first,
                 P_<int64_t>(c->q_uid) + first, P_<uint8_t>(c->q_sgood) + first, count,
                 job ? job + first : nullptr};
-    return align_reads(c, v, count);
+    return align_reads(c, v, count, c->q_off_h.data() + first);
 }
 
 extern "C" int hero_votes_words(hero_ctx *c, uint64_t *words) {
@@ -790,7 +800,7 @@ extern "C" int hero_align_subjects(hero_ctx *c, const uint8_t *seq, const uint64
     cudaEventDestroy(e1);
     ReadsView v{P_<uint8_t>(c->s_code), P_<uint64_t>(c->s_off), P_<uint32_t>(c->s_len),
                 P_<int64_t>(c->s_uid), P_<uint8_t>(c->s_good), n};
-    return align_reads(c, v, n);
+    return align_reads(c, v, n, off);
 }
 
 extern "C" int hero_consensus(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uint32_t *imed,
@@ -873,7 +883,7 @@ static int round_body(hero_ctx *c) {
     HERO_TRY(hero_build_index(c));
     ReadsView v{P_<uint8_t>(c->q_code), P_<uint64_t>(c->q_off), P_<uint32_t>(c->q_len),
                 P_<int64_t>(c->q_uid), P_<uint8_t>(c->q_sgood), c->nq, job_tags(c)};
-    HERO_TRY(align_reads(c, v, c->nq));
+    HERO_TRY(align_reads(c, v, c->nq, c->q_off_h.data()));
     return consensus_device(c);
 }
 
@@ -1068,6 +1078,7 @@ extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
     s.dp_segments_ref = c->ctr[C_DP_REF];
     s.dp_cells = c->ctr[C_CELLS];
     s.dp_cells_computed = c->ctr[C_CELLS_ALL];
+    s.dp_cells_pairs = c->ctr[C_CELLS_PAIR];
     s.dp_rows_max = c->ctr[C_MAXR];
     s.vote_anomalies = c->ctr[C_ANOMALY];
     s.device_bytes_peak = c->bytes_peak;

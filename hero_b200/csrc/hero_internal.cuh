@@ -77,6 +77,7 @@ enum Counter : int {
     C_OVERFLOW,
     C_WIN,          // winners of the current batch (compacted list length)
     C_OVERFLOW_ALL, // overflows over the context's life (C_OVERFLOW is cleared per batch)
+    C_CELLS_PAIR,   // band cells computed in 16-bit pairs (of C_CELLS_ALL's)
     C_COUNT
 };
 
@@ -127,7 +128,7 @@ void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint3
 
 // aln: the alignment output's positions (seed_hit)
 void launch_probe(bool emit, bool aln, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
-                  uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
+                  uint2 *wcache, uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
                   unsigned long long *counters, cudaStream_t st);
 void launch_map_choose(const Params &p, uint64_t nsub, const uint32_t *cstart,
                        const uint32_t *ccount, ChainArrays ch, const uint32_t *keys,
@@ -169,7 +170,9 @@ struct DpLaunch {
     uint32_t pair_mask;     // bit n: segments of n strips run as 16-bit pairs (affine)
     uint32_t tb_bytes;      // bytes of traceback codes per lane and row (set by launch_dp)
     uint32_t chunk_mask;    // bit n: tracebacks of n-strip segments walk in row chunks
-    int32_t warps;          // warps per block of the wavefront kernel (2 or 4)
+    int32_t warps;          // warps per block of the wavefront kernel (1, 2 or 4)
+    unsigned long long *pair_cells;  // += band cells of the segments run as 16-bit pairs (may be NULL)
+    int32_t regs;           // registers a thread of the wavefront kernel: 128 (0 too) or 168
 };
 constexpr int kStripW = 8;
 constexpr uint32_t kStripsAll = 0xfffffffeu;  // every strip count 1..31 (bit n: n strips)

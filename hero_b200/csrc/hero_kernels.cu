@@ -302,41 +302,35 @@ __device__ __forceinline__ bool table_find(const TableView &t, const Kmer &m, ui
 
 // ---------------------------------------------------------------------------
 // seeding: SubjectReadAligner::searchHashTable2 (SubjectReadAligner.cpp:444-491)
-// One warp per subject read; lane f takes windows f, f+32, ...  The forward
-// window at f and the reverse-complement window at L-k-f are the same bases.
+// Count pass: one warp per subject read; lane f takes the contiguous windows
+// [fa, fb), so both k-mers roll one base per window (the forward window at f
+// and the reverse-complement window at L-k-f are the same bases).  It probes
+// the table for each window and orientation, counts the hits of each
+// (subject, orientation) and leaves the slot it found (start, count) in the
+// window cache, indexed by the window's base in the batch: 2 entries a base.
+// Emit pass: the same warps read the cache (lanes interleaved, so the reads
+// are coalesced) and write the hits without probing the table again.
 // ---------------------------------------------------------------------------
 constexpr int kProbeWarps = 8;
 
-template <bool EMIT>
 __global__ void __launch_bounds__(kProbeWarps * 32)
-    k_probe(ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k, bool aln,
-            uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
-            unsigned long long *counters) {
-    __shared__ uint32_t fill[kProbeWarps][2];
+    k_probe_count(ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k, uint2 *wcache,
+                  uint32_t *seg_hits, unsigned long long *counters) {
     const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
     const uint64_t warps = uint64_t(gridDim.x) * kProbeWarps;
+    const uint64_t base0 = subj.off[0];
     unsigned long long probes = 0, nhits = 0;
     for (uint64_t s = uint64_t(blockIdx.x) * kProbeWarps + wib; s < nsub; s += warps) {
         const int32_t L = int32_t(subj.len[s]);
         const int64_t su = subj.uid[s];
         const uint32_t stag = uid_tag(su);
         const uint8_t *c = subj.code + subj.off[s];
+        uint2 *wc = wcache + 2 * (subj.off[s] - base0);
         uint32_t c0 = 0, c1 = 0;
-        uint64_t o0 = 0, o1 = 0;
-        if (EMIT) {
-            if (lane == 0) {
-                fill[wib][0] = 0;
-                fill[wib][1] = 0;
-            }
-            o0 = hit_off[2 * s];
-            o1 = hit_off[2 * s + 1];
-            __syncwarp();
-        }
         if (subj.good[s] && L >= k) {
             const int32_t P = L - k + 1;
             if (lane == 0) probes += 2ull * uint64_t(P);
-            // lane takes the windows [fa, fb): contiguous, so both k-mers roll one
-            // base per window; nbad counts the non-ACGT bases in the window
+            // nbad counts the non-ACGT bases in the window
             const int32_t fa = int32_t(int64_t(P) * lane / 32), fb = int32_t(int64_t(P) * (lane + 1) / 32);
             Kmer fr{0, 0}, rr{0, 0};
             int32_t nbad = 0;
@@ -353,27 +347,22 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
                 if (f > fa) nbad -= c[f - 1] >= 4;
                 kmer_push(fr, x & 3u, k);
                 kmer_push_front(rr, (x & 3u) ^ 2u, k);
-                if (nbad) continue;
-                Kmer fm = fr, rm = rr;
-                if (subj.job) {
-                    kmer_tag(fm, subj.job[s], k);
-                    kmer_tag(rm, subj.job[s], k);
-                }
-                for (int o = 0; o < 2; o++) {
-                    uint32_t st = 0, cnt = 0;
-                    if (!table_find(t, o ? rm : fm, st, cnt)) continue;
-                    for (uint32_t e = 0; e < cnt; e++) {
-                        const uint64_t v = __ldg(&t.vals[st + e]);
-                        const uint32_t qq = value_query(v);
-                        // self hit (SubjectReadAligner.cpp:463-465): ids compared
-                        // only where their folds agree
-                        if (value_tag(v) == stag && __ldg(&q.uid[qq]) == su) continue;
-                        if (EMIT) {
-                            const uint32_t slot = atomicAdd(&fill[wib][o], 1u);
-                            const int32_t lq = (aln && o) ? int32_t(__ldg(&q.len[qq])) : 0;
-                            hits[(o ? o1 : o0) + slot] =
-                                seed_hit(aln, o, qq, value_pos(v), f, L, lq, k);
-                        } else {
+                uint2 found[2] = {make_uint2(0, 0), make_uint2(0, 0)};
+                if (!nbad) {
+                    Kmer fm = fr, rm = rr;
+                    if (subj.job) {
+                        kmer_tag(fm, subj.job[s], k);
+                        kmer_tag(rm, subj.job[s], k);
+                    }
+                    for (int o = 0; o < 2; o++) {
+                        uint32_t st = 0, cnt = 0;
+                        if (!table_find(t, o ? rm : fm, st, cnt)) continue;
+                        found[o] = make_uint2(st, cnt);
+                        for (uint32_t e = 0; e < cnt; e++) {
+                            const uint64_t v = __ldg(&t.vals[st + e]);
+                            // self hit (SubjectReadAligner.cpp:463-465): ids compared
+                            // only where their folds agree
+                            if (value_tag(v) == stag && __ldg(&q.uid[value_query(v)]) == su) continue;
                             if (o) {
                                 c1++;
                             } else {
@@ -382,23 +371,59 @@ __global__ void __launch_bounds__(kProbeWarps * 32)
                         }
                     }
                 }
+                reinterpret_cast<uint4 *>(wc)[f] = make_uint4(found[0].x, found[0].y, found[1].x, found[1].y);
             }
         }
-        if (!EMIT) {
-            c0 = warp_sum(c0);
-            c1 = warp_sum(c1);
-            if (lane == 0) {
-                seg_hits[2 * s] = c0;
-                seg_hits[2 * s + 1] = c1;
-                nhits += c0 + c1;
-            }
-        } else {
-            __syncwarp();
+        c0 = warp_sum(c0);
+        c1 = warp_sum(c1);
+        if (lane == 0) {
+            seg_hits[2 * s] = c0;
+            seg_hits[2 * s + 1] = c1;
+            nhits += c0 + c1;
         }
     }
-    if (!EMIT && lane == 0) {
+    if (lane == 0) {
         atomicAdd(&counters[C_PROBES], probes);
         atomicAdd(&counters[C_HITS], nhits);
+    }
+}
+
+__global__ void __launch_bounds__(kProbeWarps * 32)
+    k_probe_emit(ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k, bool aln,
+                 const uint2 *wcache, const uint64_t *hit_off, uint64_t *hits) {
+    __shared__ uint32_t fill[kProbeWarps][2];
+    const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+    const uint64_t warps = uint64_t(gridDim.x) * kProbeWarps;
+    const uint64_t base0 = subj.off[0];
+    for (uint64_t s = uint64_t(blockIdx.x) * kProbeWarps + wib; s < nsub; s += warps) {
+        const int32_t L = int32_t(subj.len[s]);
+        if (lane == 0) {
+            fill[wib][0] = 0;
+            fill[wib][1] = 0;
+        }
+        __syncwarp();
+        if (subj.good[s] && L >= k) {
+            const int64_t su = subj.uid[s];
+            const uint32_t stag = uid_tag(su);
+            const uint64_t o0 = hit_off[2 * s], o1 = hit_off[2 * s + 1];
+            const uint4 *wc = reinterpret_cast<const uint4 *>(wcache + 2 * (subj.off[s] - base0));
+            const int32_t P = L - k + 1;
+            for (int32_t f = int32_t(lane); f < P; f += 32) {
+                const uint4 w = wc[f];
+                for (int o = 0; o < 2; o++) {
+                    const uint32_t st = o ? w.z : w.x, cnt = o ? w.w : w.y;
+                    for (uint32_t e = 0; e < cnt; e++) {
+                        const uint64_t v = __ldg(&t.vals[st + e]);
+                        const uint32_t qq = value_query(v);
+                        if (value_tag(v) == stag && __ldg(&q.uid[qq]) == su) continue;
+                        const uint32_t slot = atomicAdd(&fill[wib][o], 1u);
+                        const int32_t lq = (aln && o) ? int32_t(__ldg(&q.len[qq])) : 0;
+                        hits[(o ? o1 : o0) + slot] = seed_hit(aln, o, qq, value_pos(v), f, L, lq, k);
+                    }
+                }
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -840,7 +865,10 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
 // warps per block of k_dp_wave: 4 (default) or 2; blocks per SM are set so that
 // every thread keeps 128 registers
 constexpr int kWaveWarps = 4;
-constexpr int kWaveRegBlocks(int warps) { return 16 / warps; }
+// warps per SM the register budget is set for: 16 (128 registers a thread) or,
+// for the wide shapes, 12 (168 registers: the affine pair rows spill less)
+constexpr int kWaveSmWarps(bool wide) { return wide ? 12 : 16; }
+constexpr int kWaveRegBlocks(int warps, bool wide) { return kWaveSmWarps(wide) / warps; }
 
 constexpr int kTaskQueue = 127;  // tasks[127]: next task to hand out
 
@@ -1253,6 +1281,13 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
         wave_pair<AFFINE, false>(va, vb, active, R, Rw, G, s, lane, -1, tb, tab);
     }
     __syncwarp();
+    if (a.pair_cells) {  // the cells this warp computed as pairs
+        unsigned long long pc = 0;
+        if (active && s == 0)
+            pc = band_cells(va.R, va.C, va.band) + (has_b ? band_cells(vb.R, vb.C, vb.band) : 0ull);
+        pc = warp_sum(pc);
+        if (lane == 0 && pc) atomicAdd(a.pair_cells, pc);
+    }
     uint32_t *stage = tabs + size_t(g) * G * TS;
     group_traceback(a, SmemCodesPair{tb, g * G, 0}, va, active, sa, G, g, s, stage,
                     uint32_t(G) * TS);
@@ -1260,8 +1295,8 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
                     uint32_t(G) * TS);
 }
 
-template <bool AFFINE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS))
+template <bool AFFINE, int WARPS, bool WIDE>
+__global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS, WIDE))
     k_dp_wave(DpLaunch a, uint64_t *tasks) {
     extern __shared__ int4 wave_smem[];
     const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
@@ -2127,16 +2162,15 @@ void launch_table_finalize(const uint64_t *klo, const uint64_t *khi, const uint3
 }
 
 void launch_probe(bool emit, bool aln, ReadsView subj, uint64_t nsub, ReadsView q, TableView t, int32_t k,
-                  uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
+                  uint2 *wcache, uint32_t *seg_hits, const uint64_t *hit_off, uint64_t *hits,
                   unsigned long long *counters, cudaStream_t st) {
     if (!nsub) return;
     const unsigned g = grid_1d(nsub, kProbeWarps, 148u * 16u);
+    counted();
     if (emit) {
-        counted();
-        k_probe<true><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, aln, seg_hits, hit_off, hits, counters);
+        k_probe_emit<<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, aln, wcache, hit_off, hits);
     } else {
-        counted();
-        k_probe<false><<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, aln, seg_hits, hit_off, hits, counters);
+        k_probe_count<<<g, kProbeWarps * 32, 0, st>>>(subj, nsub, q, t, k, wcache, seg_hits, counters);
     }
 }
 
@@ -2193,7 +2227,7 @@ void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, i
                cudaStream_t st) {
     if (!a_in.nd) return;
     DpLaunch a = a_in;
-    if (a.warps != 2) a.warps = 4;
+    if (a.warps != 1 && a.warps != 2) a.warps = 4;
     // pairs need 32-bit code rows; without the room none run
     if (wave_smem(a.rmax, 4, a.warps) > 200u * 1024u) a.pair_mask = 0;
     a.tb_bytes = a.pair_mask ? 4u : 2u;
@@ -2215,37 +2249,34 @@ void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, i
     const size_t smem = wave_smem(a.rmax, a.tb_bytes, a.warps);
     // a persistent grid: twice the blocks that fit for registers (the work queue
     // stops the extra ones at once)
-    const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps));
+    const bool wide = a.regs > 128;
+    const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps, wide));
     // the opt-in is set once per size increase (never while a graph is being captured
     // for a size not seen before: the eager round that precedes a capture sets it)
     // (per device, and shared by the host threads of every context in the process)
     constexpr int kOptDevices = 64;
     static std::mutex opt_mu;
-    static size_t opted[kOptDevices][2][2] = {};
-    const int ai = a.affine ? 1 : 0, wi = a.warps == 2 ? 0 : 1;
+    static size_t opted[kOptDevices][2][3][2] = {};
+    const int ai = a.affine ? 1 : 0, wi = a.warps == 1 ? 0 : (a.warps == 2 ? 1 : 2), ri = wide ? 1 : 0;
+    using WaveFn = void (*)(DpLaunch, uint64_t *);
+    const WaveFn fns[2][3][2] = {
+        {{k_dp_wave<false, 1, false>, k_dp_wave<false, 1, true>},
+         {k_dp_wave<false, 2, false>, k_dp_wave<false, 2, true>},
+         {k_dp_wave<false, 4, false>, k_dp_wave<false, 4, true>}},
+        {{k_dp_wave<true, 1, false>, k_dp_wave<true, 1, true>},
+         {k_dp_wave<true, 2, false>, k_dp_wave<true, 2, true>},
+         {k_dp_wave<true, 4, false>, k_dp_wave<true, 4, true>}}};
+    const WaveFn fn = fns[ai][wi][ri];
     if (smem > 48u * 1024u) {
         std::lock_guard<std::mutex> lock(opt_mu);
-        if (dev >= kOptDevices || smem > opted[dev][ai][wi]) {
-            const void *fn = a.affine ? (a.warps == 2 ? (const void *)k_dp_wave<true, 2> : (const void *)k_dp_wave<true, 4>)
-                                      : (a.warps == 2 ? (const void *)k_dp_wave<false, 2> : (const void *)k_dp_wave<false, 4>);
-            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-            if (dev < kOptDevices) opted[dev][ai][wi] = smem;
+        if (dev >= kOptDevices || smem > opted[dev][ai][wi][ri]) {
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(fn),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            if (dev < kOptDevices) opted[dev][ai][wi][ri] = smem;
         }
     }
     counted();
-    if (a.affine) {
-        if (a.warps == 2) {
-            k_dp_wave<true, 2><<<g, 64, smem, st>>>(a, tasks);
-        } else {
-            k_dp_wave<true, 4><<<g, 128, smem, st>>>(a, tasks);
-        }
-    } else {
-        if (a.warps == 2) {
-            k_dp_wave<false, 2><<<g, 64, smem, st>>>(a, tasks);
-        } else {
-            k_dp_wave<false, 4><<<g, 128, smem, st>>>(a, tasks);
-        }
-    }
+    fn<<<g, unsigned(32 * a.warps), smem, st>>>(a, tasks);
     if (cmax > 32 * kStripW) {
         const unsigned gw = unsigned(a.threads / kDpThreads);
         counted();

@@ -212,32 +212,62 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
         n += j->n();
         nb += j->seq.size();
     }
-    std::vector<uint8_t> seq(nb);
-    std::vector<uint64_t> off(n + 1, 0);
-    std::vector<int64_t> uid(n);
-    std::vector<uint32_t> tag(n);
-    uint64_t r = 0, b = 0;
-    for (size_t t = 0; t < js.size(); t++) {
-        const Job &j = *js[t];
-        if (!j.seq.empty()) std::memcpy(seq.data() + b, j.seq.data(), j.seq.size());
-        for (uint64_t i = 0; i < j.n(); i++) {
-            off[r + i + 1] = b + j.off[i + 1];
-            uid[r + i] = j.uid[i];
-            tag[r + i] = uint32_t(t);
+    const bool single = js.size() == 1;
+    std::vector<uint8_t> seq, out_seq, good;
+    std::vector<uint64_t> off;
+    std::vector<int64_t> uid;
+    std::vector<uint32_t> tag, imin, imed, imax;
+    std::vector<double> mis, gc;
+    int st = HERO_OK;
+    if (single) {
+        // one job: its own buffers in and its result buffers out (no concatenation
+        // and no split; nobody reads a running job's results)
+        Job &j = *js[0];
+        j.out_seq.resize(nb);
+        j.good.resize(n);
+        j.imin.resize(n);
+        j.imed.resize(n);
+        j.imax.resize(n);
+        j.mis.resize(n);
+        j.gc.resize(n);
+        st = hero_set_queries(ctx, j.seq.data(), j.off.data(), j.uid.data(), n);
+        if (st == HERO_OK) st = hero_build_index(ctx);
+        if (st == HERO_OK) st = hero_align_self(ctx);
+        if (st == HERO_OK)
+            st = hero_consensus(ctx, j.out_seq.data(), j.imin.data(), j.imed.data(), j.imax.data(),
+                                j.mis.data(), j.gc.data(), j.good.data());
+    } else {
+        seq.resize(nb);
+        off.assign(n + 1, 0);
+        uid.resize(n);
+        tag.resize(n);
+        uint64_t r = 0, b = 0;
+        for (size_t t = 0; t < js.size(); t++) {
+            const Job &j = *js[t];
+            if (!j.seq.empty()) std::memcpy(seq.data() + b, j.seq.data(), j.seq.size());
+            for (uint64_t i = 0; i < j.n(); i++) {
+                off[r + i + 1] = b + j.off[i + 1];
+                uid[r + i] = j.uid[i];
+                tag[r + i] = uint32_t(t);
+            }
+            r += j.n();
+            b += j.seq.size();
         }
-        r += j.n();
-        b += j.seq.size();
+        out_seq.resize(nb);
+        good.resize(n);
+        imin.resize(n);
+        imed.resize(n);
+        imax.resize(n);
+        mis.resize(n);
+        gc.resize(n);
+        st = hero_set_queries(ctx, seq.data(), off.data(), uid.data(), n);
+        if (st == HERO_OK) st = hero_set_query_jobs(ctx, tag.data(), n);
+        if (st == HERO_OK) st = hero_build_index(ctx);
+        if (st == HERO_OK) st = hero_align_self(ctx);
+        if (st == HERO_OK)
+            st = hero_consensus(ctx, out_seq.data(), imin.data(), imed.data(), imax.data(),
+                                mis.data(), gc.data(), good.data());
     }
-    std::vector<uint8_t> out_seq(seq), good(n);  // reads that are not good stay as read
-    std::vector<uint32_t> imin(n), imed(n), imax(n);
-    std::vector<double> mis(n), gc(n);
-    int st = hero_set_queries(ctx, seq.data(), off.data(), uid.data(), n);
-    if (st == HERO_OK && js.size() > 1) st = hero_set_query_jobs(ctx, tag.data(), n);
-    if (st == HERO_OK) st = hero_build_index(ctx);
-    if (st == HERO_OK) st = hero_align_self(ctx);
-    if (st == HERO_OK)
-        st = hero_consensus(ctx, out_seq.data(), imin.data(), imed.data(), imax.data(), mis.data(),
-                            gc.data(), good.data());
     const std::string err = st == HERO_OK ? std::string() : std::string(hero_last_error(ctx));
     std::lock_guard<std::mutex> g(mu);
     if (st == HERO_E_OOM && (js.size() > 1 || in_flight > 1)) {
@@ -256,14 +286,17 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
     rounds++;
     const double t_end = now_ms();
     round_end(round_est);
-    r = 0;
-    b = 0;
+    uint64_t r = 0, b = 0;
     for (Job *j : js) {
         const uint64_t jn = j->n(), jb = j->seq.size();
         j->round = rounds;
         j->round_jobs = uint32_t(js.size());
         j->done_ms = t_end;
-        if (st == HERO_OK) {
+        if (st == HERO_OK && single) {
+            j->state = HERO_JOB_DONE;
+            done++;
+            bases_done += jb;
+        } else if (st == HERO_OK) {
             j->out_seq.assign(out_seq.begin() + long(b), out_seq.begin() + long(b + jb));
             j->good.assign(good.begin() + long(r), good.begin() + long(r + jn));
             j->imin.assign(imin.begin() + long(r), imin.begin() + long(r + jn));
@@ -345,7 +378,9 @@ extern "C" void hero_server_destroy(hero_server *s) {
 extern "C" int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t, uint32_t n) {
     if (!s || (n && !t)) return HERO_E_INPUT;
     for (uint32_t i = 0; i < n; i++)
-        if (t[i].warps_per_block != 2 && t[i].warps_per_block != 4) return HERO_E_INPUT;
+        if ((t[i].warps_per_block != 1 && t[i].warps_per_block != 2 && t[i].warps_per_block != 4) ||
+            (t[i].regs_per_thread != 0 && t[i].regs_per_thread != 128 && t[i].regs_per_thread != 168))
+            return HERO_E_INPUT;
     std::lock_guard<std::mutex> g(s->mu);
     s->tuning.assign(t, t + n);
     s->tuning_gen++;

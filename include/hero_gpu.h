@@ -119,6 +119,7 @@ typedef struct {
     uint64_t dp_cells_computed; /* band cells of every DP segment computed on the device */
     uint64_t dp_rows_max;      /* longest DP side (the row count of a segment) seen so far;
                                   the key of hero_dp_tuning classes */
+    uint64_t dp_cells_pairs;   /* of dp_cells_computed, the cells computed as 16-bit pairs */
 } hero_stats;
 
 /* Returns the default parameters of the reference's Config. */
@@ -221,9 +222,10 @@ int hero_get_stats(hero_ctx *ctx, hero_stats *out);
  * strip count.  No reference counterpart (the reference has one CPU aligner). */
 typedef struct {
     int32_t rows_max;          /* class bound on the longest DP side of a batch */
-    int32_t warps_per_block;   /* 2 or 4 */
-    uint32_t pair_strips;      /* bit n: n-strip segments run as 16-bit pairs (affine) */
+    int32_t warps_per_block;   /* 1, 2 or 4 */
+    uint32_t pair_strips;      /* bit n: n-strip segments run as 16-bit pairs */
     uint32_t chunk_strips;     /* bit n: n-strip tracebacks walk in row chunks */
+    int32_t regs_per_thread;   /* 0 or 128 (16 warps an SM), or 168 (12 warps, fewer spills) */
 } hero_dp_tuning;
 
 /* Replaces the context's tuning table (n = 0 clears it). */

@@ -44,7 +44,7 @@ def test_tuning_record_parses(tmp_path):
 
     from hero_b200 import autotune
     from hero_b200._lib import load_tuning
-    assert len(list(autotune.candidates())) == 12
+    assert len(list(autotune.candidates())) == 24
     p = tmp_path / "t.json"
     p.write_text(json.dumps({"classes": [{"rows_max": 168, "warps_per_block": 2, "pair_strips": 0,
                                           "chunk_strips": autotune.ALL}]}))

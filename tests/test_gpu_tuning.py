@@ -56,4 +56,4 @@ def test_tuner_records_the_fastest_candidate(tmp_path):
     p = tmp_path / "tuning.json"
     p.write_text(json.dumps(rec))
     from hero_b200._lib import load_tuning
-    assert load_tuning(str(p))[0]["warps_per_block"] in (2, 4)
+    assert load_tuning(str(p))[0]["warps_per_block"] in (1, 2, 4)
