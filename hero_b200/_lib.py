@@ -30,7 +30,8 @@ EXPORTS = [
     "hero_server_get_stats", "hero_job_bytes", "hero_round_admit", "hero_set_dp_tuning",
     "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
     "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
-    "hero_merge_pairs", "hero_get_overhang", "hero_mapping_histogram",
+    "hero_merge_pairs", "hero_get_overhang", "hero_mapping_histogram", "hero_set_vote_buffer",
+    "hero_consensus_range",
 ]
 
 # hero_params.flags: the alignment-output mode (HERO without -c); --merge
@@ -139,6 +140,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_merge_pairs.argtypes = [vp, vp, vp]
     lib.hero_get_overhang.argtypes = [vp, vp]
     lib.hero_mapping_histogram.argtypes = [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
+    lib.hero_set_vote_buffer.argtypes = [vp, vp, C.c_uint64]
+    lib.hero_consensus_range.argtypes = [vp, C.c_uint64, C.c_uint64] + [vp] * 7
     lib.hero_votes_words.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_votes_save.argtypes = [vp, vp]
     lib.hero_votes_load.argtypes = [vp, vp]
@@ -345,6 +348,34 @@ class Hero:
         n = C.c_uint64()
         self._check(self.lib.hero_votes_words(self.h, C.byref(n)), "votes_words")
         return n.value
+
+    def set_vote_buffer(self, dev_ptr: int, nbytes: int):
+        """Votes into caller-owned device memory from the next set_queries on
+        (hero_set_vote_buffer); 0 returns to the context's own buffers."""
+        self._check(self.lib.hero_set_vote_buffer(self.h, C.c_void_p(dev_ptr) if dev_ptr else None,
+                                                  int(nbytes)), "set_vote_buffer")
+
+    def consensus_range(self, first: int, count: int, nbases: int | None = None,
+                        fetch: bool = True) -> dict | None:
+        """The consensus of the query reads [first, first + count) (hero_consensus_range);
+        nbases, the range's bases, is needed when the reads were set by pointer.
+        fetch=False leaves the results on the device."""
+        if not fetch:
+            self._check(self.lib.hero_consensus_range(self.h, int(first), int(count), *([None] * 7)),
+                        "consensus_range")
+            return None
+        if nbases is None:
+            off = self._qkeep[1]
+            nbases = int(off[first + count] - off[first])
+        nb = int(nbases)
+        res = dict(seq=np.empty(nb, np.uint8), imin=np.empty(count, np.uint32),
+                   imed=np.empty(count, np.uint32), imax=np.empty(count, np.uint32),
+                   mismatch_rate=np.empty(count, np.float64), gc=np.empty(count, np.float64),
+                   good=np.empty(count, np.uint8))
+        self._check(self.lib.hero_consensus_range(
+            self.h, int(first), int(count), *[_ptr(res[k]) for k in (
+                "seq", "imin", "imed", "imax", "mismatch_rate", "gc", "good")]), "consensus_range")
+        return res
 
     def votes_save(self, dev_ptr: int):
         """Copies the vote state into a device buffer (e.g. a CUDA tensor's data_ptr())."""

@@ -22,6 +22,7 @@ namespace {
 struct DBuf {
     void *p = nullptr;
     size_t cap = 0;
+    bool external = false;  // caller-owned memory: never freed or grown here
 };
 
 struct Timer {
@@ -69,6 +70,8 @@ struct hero_ctx {
     bool merge = false;
     bool mapping = false;  // --mapping: chosen records vote; coverage histogram
     std::vector<uint64_t> q_off_h;  // host copy of the query offsets (sizes of subject batches)
+    void *vote_ext = nullptr;       // caller-owned vote state (hero_set_vote_buffer), or NULL
+    uint64_t vote_ext_bytes = 0;
     DBuf wcache;                    // per batch: the table slot each probe window found
     DBuf map_hist, map_max;
     bool consensus_done = false;  // out_seq holds the consensus of the current votes
@@ -126,17 +129,19 @@ struct hero_ctx {
         return cuda(e, what);
     }
     void release(DBuf &b) {
-        if (b.p) {
+        if (b.p && !b.external) {
             cudaFree(b.p);
             bytes -= b.cap;
         }
         b.p = nullptr;
         b.cap = 0;
+        b.external = false;
     }
     // grows a device buffer to at least `need` bytes (contents are not kept)
     int ensure(DBuf &b, size_t need, const char *what) {
         if (need == 0) need = 16;
         if (b.cap >= need) return HERO_OK;
+        if (b.external) return fail(HERO_E_INPUT, std::string("caller's buffer too small for ") + what);
         release(b);
         size_t want = need + need / 4 + 256;
         if (P.device_memory_budget && bytes + want > P.device_memory_budget) {
@@ -344,6 +349,13 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     HERO_TRY(c->ensure(c->fp, 8, "fingerprint"));
     launch_fingerprint(P_<uint8_t>(c->q_raw), c->nqb, P_<uint64_t>(c->q_off), P_<int64_t>(c->q_uid), n,
                        P_<unsigned long long>(c->fp), c->st);
+    if (c->vote_ext) {  // the caller's buffer: mismatch votes, then match-run differences
+        if (c->vote_ext_bytes < c->nqb * 20) return c->fail(HERO_E_INPUT, "vote buffer smaller than 20 bytes a query base");
+        c->release(c->cov);
+        c->release(c->mdiff);
+        c->cov = DBuf{c->vote_ext, size_t(c->nqb * 16), true};
+        c->mdiff = DBuf{static_cast<uint8_t *>(c->vote_ext) + c->nqb * 16, size_t(c->nqb * 4), true};
+    }
     HERO_TRY(c->ensure(c->cov, c->nqb * 16, "vote matrix"));
     HERO_TRY(c->ensure(c->mdiff, c->nqb * 4, "vote matrix"));
     HERO_TRY(c->cuda(cudaMemsetAsync(c->cov.p, 0, c->nqb * 16, c->st), "memset"));
@@ -778,6 +790,67 @@ extern "C" int hero_votes_load(hero_ctx *c, const void *src) {
     HERO_TRY(c->cuda(cudaMemcpyAsync(c->cov.p, s, c->nqb * 16, cudaMemcpyDeviceToDevice, c->st), "votes load"));
     HERO_TRY(c->cuda(cudaMemcpyAsync(c->mdiff.p, s + c->nqb * 16, c->nqb * 4, cudaMemcpyDeviceToDevice, c->st), "votes load"));
     return c->cuda(cudaStreamSynchronize(c->st), "votes load");
+}
+
+extern "C" int hero_set_vote_buffer(hero_ctx *c, void *dev_ptr, uint64_t bytes) {
+    if (!c) return HERO_E_INPUT;
+    if (c->merge) return c->fail(HERO_E_STATE, "the overhang votes of --merge are not part of the exchanged state");
+    if (dev_ptr && (reinterpret_cast<uintptr_t>(dev_ptr) & 255u))
+        return c->fail(HERO_E_INPUT, "vote buffer not 256-byte aligned");
+    c->vote_ext = dev_ptr;
+    c->vote_ext_bytes = dev_ptr ? bytes : 0;
+    if (!dev_ptr) {  // back to the context's own buffers at the next hero_set_queries
+        if (c->cov.external) c->release(c->cov);
+        if (c->mdiff.external) c->release(c->mdiff);
+        c->have_queries = false;
+        c->have_index = false;
+    }
+    return HERO_OK;
+}
+
+extern "C" int hero_consensus_range(hero_ctx *c, uint64_t first, uint64_t count, uint8_t *seq_out,
+                                    uint32_t *imin, uint32_t *imed, uint32_t *imax,
+                                    double *mismatch_rate, double *gc_content, uint8_t *good_out) {
+    if (!c) return HERO_E_INPUT;
+    if (!c->have_queries) return c->fail(HERO_E_STATE, "no query set");
+    if (c->p.aln) return c->fail(HERO_E_STATE, "an alignment-output context has no consensus");
+    if (first > c->nq || count > c->nq - first) return c->fail(HERO_E_INPUT, "range outside the query set");
+    if (count == 0) return HERO_OK;
+    cudaSetDevice(c->dev);
+    const uint64_t n = c->nq, nb = c->nqb;
+    HERO_TRY(c->ensure(c->out_seq, nb, "consensus"));
+    HERO_TRY(c->ensure(c->colsum, nb * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imin, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imed, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_imax, n * 4, "consensus"));
+    HERO_TRY(c->ensure(c->o_mis, n * 8, "consensus"));
+    const uint64_t b0 = c->q_off_h[first], b1 = c->q_off_h[first + count];
+    uint8_t *os = P_<uint8_t>(c->out_seq);
+    if (b1 > b0)
+        HERO_TRY(c->cuda(cudaMemcpyAsync(os + b0, P_<uint8_t>(c->q_raw) + b0, b1 - b0, cudaMemcpyDeviceToDevice, c->st), "consensus"));
+    // the reads of the range: per-read arrays shifted, bases and votes absolute
+    ReadsView v = query_view(c);
+    v.off += first;
+    v.len += first;
+    v.uid += first;
+    v.good += first;
+    v.n = count;
+    v.job = nullptr;
+    launch_consensus(c->p, v, P_<uint32_t>(c->cov), P_<int32_t>(c->mdiff), os, P_<uint32_t>(c->colsum),
+                     P_<uint32_t>(c->o_imin) + first, P_<uint32_t>(c->o_imed) + first,
+                     P_<uint32_t>(c->o_imax) + first, P_<double>(c->o_mis) + first, c->st);
+    HERO_TRY(c->check_launch("consensus"));
+    auto d2h = [&](void *dst, const void *src, size_t bytes) {
+        return dst && bytes ? c->cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st), "consensus") : HERO_OK;
+    };
+    HERO_TRY(d2h(seq_out, os + b0, b1 - b0));
+    HERO_TRY(d2h(imin, P_<uint32_t>(c->o_imin) + first, count * 4));
+    HERO_TRY(d2h(imed, P_<uint32_t>(c->o_imed) + first, count * 4));
+    HERO_TRY(d2h(imax, P_<uint32_t>(c->o_imax) + first, count * 4));
+    HERO_TRY(d2h(mismatch_rate, P_<double>(c->o_mis) + first, count * 8));
+    HERO_TRY(d2h(gc_content, P_<double>(c->q_gc) + first, count * 8));
+    HERO_TRY(d2h(good_out, P_<uint8_t>(c->q_good) + first, count));
+    return c->cuda(cudaStreamSynchronize(c->st), "consensus");
 }
 
 extern "C" int hero_align_subjects(hero_ctx *c, const uint8_t *seq, const uint64_t *off,

@@ -165,6 +165,24 @@ int hero_votes_words(hero_ctx *ctx, uint64_t *words);
 int hero_votes_save(hero_ctx *ctx, void *dev_dst);
 int hero_votes_load(hero_ctx *ctx, const void *dev_src);
 
+/* Keeps the vote state in caller-owned memory of this context's device, laid
+ * out as hero_votes_words describes (bytes >= 20 per query base, 256-byte
+ * aligned): from the next hero_set_queries on, the context votes there instead
+ * of into its own buffers, so shards can add their states in place (one NCCL
+ * reduce of each owner's slice to its owner, no copies).  The buffer must
+ * outlive its use; NULL returns to the context's own buffers (the query set
+ * must then be set again).  HERO_FLAG_MERGE_PAIRS contexts refuse it.  No
+ * reference counterpart (HERO runs on one host). */
+int hero_set_vote_buffer(hero_ctx *ctx, void *dev_ptr, uint64_t bytes);
+
+/* QueryDataset::callConsensus (QueryDataset.cpp:393-412) for the query reads
+ * [first, first + count) only, once their votes are complete (a shard that
+ * owns those reads): outputs as hero_consensus's, holding just those reads
+ * (seq_out from the range's first base). */
+int hero_consensus_range(hero_ctx *ctx, uint64_t first, uint64_t count, uint8_t *seq_out,
+                         uint32_t *imin, uint32_t *imed, uint32_t *imax, double *mismatch_rate,
+                         double *gc_content, uint8_t *good_out);
+
 /* Clears the vote matrix for a new correction of the same query set, as
  * QueryRead::initilizeCoverageMatrix zeroes it at load (QueryRead.cpp:100-115). */
 int hero_reset_votes(hero_ctx *ctx);

@@ -48,6 +48,21 @@ def main():
             t = torch.from_numpy(v.view(np.int32).copy())
             shard.allreduce_votes(t)
             np.save(os.path.join(out, f"votes{rank}.npy"), t.numpy().view(np.uint32))
+        elif case == "owners":
+            # the shards' oracle vote matrices ([bases][4] words) reduced to the
+            # owners of query-read ranges: each owner's slice is the whole run's
+            from fixtures import FIXTURES, params, upper
+            from hero_testlib import Oracle
+            gen, flags = FIXTURES["mix_affine"]
+            rs = upper(gen())
+            a, b = shard.shard_range(rs.n, rank, world)
+            v = Oracle().correct(rs, subjects=Slice(rs, a, b), threads=2, **params(flags))["votes"]
+            t = torch.from_numpy(v.view(np.int32).copy())
+            owners = shard.owner_slices(rs.off, world, words_per_base=4, tail_words=0)
+            shard.reduce_votes_to_owners(t, owners)
+            lo, hi = owners[rank][3][0]
+            np.save(os.path.join(out, f"own{rank}.npy"), t[lo:hi].numpy().view(np.uint32))
+            res["slice"] = [lo, hi]
         elif case == "lost_rank":
             if rank == 1:
                 os._exit(0)  # leaves between steps, before the exchange

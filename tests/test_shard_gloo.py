@@ -73,6 +73,29 @@ def test_vote_exchange_gives_the_whole_runs_votes(tmp_path, oracle):
         assert np.array_equal(got, want)
 
 
+def test_reduce_to_owners_gives_each_owner_the_whole_runs_votes(tmp_path, oracle):
+    from fixtures import FIXTURES, params, upper
+    procs, outs, res = _run("owners", tmp_path)
+    assert all(p.returncode == 0 for p in procs), outs
+    gen, flags = FIXTURES["mix_affine"]
+    want = oracle.correct(upper(gen()), **params(flags))["votes"]
+    slices = [res[r]["slice"] for r in range(2)]
+    assert slices[0][0] == 0 and slices[0][1] == slices[1][0] and slices[1][1] == len(want)
+    for r in range(2):
+        lo, hi = slices[r]
+        assert np.array_equal(np.load(tmp_path / f"own{r}.npy"), want[lo:hi])
+
+
+def test_owner_slices_cover_the_state():
+    from hero_b200.shard import owner_slices
+    off = np.array([0, 10, 25, 25, 40, 100], np.uint64)
+    for world in (1, 2, 3):
+        o = owner_slices(off, world)
+        assert sum(c for _, c, _, _ in o) == 5 and sum(nb for _, _, nb, _ in o) == 100
+        assert o[0][3][0][0] == 0 and o[-1][3][0][1] == 400
+        assert o[0][3][1][0] == 400 and o[-1][3][1][1] == 500
+
+
 def test_a_rank_that_leaves_ends_the_exchange_with_an_error(tmp_path):
     procs, outs, res = _run("lost_rank", tmp_path, timeout=120)
     assert procs[1].returncode == 0
