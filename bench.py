@@ -458,7 +458,7 @@ def run_server(jobs, stream, dev: int, arrivals=None) -> dict:
             "arrivals_late_s": float(max(late)) if late else 0.0, "_digests": digests}
 
 
-def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.9) -> dict:
+def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.95) -> dict:
     """The serving stream: each job alone (one at a time), the server with every
     job submitted at once (its capacity), then the server under Poisson arrivals
     at `load` of the better of the two rates (so the load is a true fraction of
@@ -505,18 +505,20 @@ def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.9) -> dict:
     }
 
 
-def run_served_block(args, dev: int) -> dict:
-    """The served block of the default line: the first jobs of the serving
-    stream at their real sizes (genome log-uniform 0.5-20 Mbp, L in
-    {100,150,250}, coverage U(20,80), affine errors), held in host memory."""
+def run_served_block(args, dev: int, n_jobs: int = 0, scale: float = 0.0) -> dict:
+    """A served block of the default line: the first jobs of the serving stream
+    (genome log-uniform 0.5-20 Mbp times `scale`, L in {100,150,250}, coverage
+    U(20,80), affine errors), held in host memory."""
     from hero_b200 import synth
-    jobs = synth.config4_jobs(n_jobs=args.served_jobs, scale=args.jobs_scale or 1.0)
+    n_jobs = n_jobs or args.served_jobs
+    scale = scale or args.jobs_scale or 1.0
+    jobs = synth.config4_jobs(n_jobs=n_jobs, scale=scale)
     with ClockSampler(dev) as sclk:
         served = serve_workload(jobs, dev, in_memory=True)
     served["clocks"] = sclk.summary()
-    served["workload"] = (f"the first {args.served_jobs} jobs of the serving stream: Poisson "
-                          f"arrivals, genome log-uniform 0.5-20 Mbp x {args.jobs_scale or 1.0}, "
-                          "L in {100,150,250}, coverage U(20,80), affine/indel errors")
+    served["workload"] = (f"the first {n_jobs} jobs of the serving stream: Poisson arrivals, "
+                          f"genome log-uniform 0.5-20 Mbp x {scale}, L in {{100,150,250}}, "
+                          "coverage U(20,80), affine/indel errors")
     return served
 
 
@@ -706,9 +708,12 @@ def bench_hero(args):
             "note": "the reference on this whole workload, timed once on the 8 cores of the "
                     "build host by tests/golden/make_golden.py (not timed in this run)"}
         del rs2
-    served = None
+    served = served_small = None
     if solo and args.served_jobs:
         served = run_served_block(args, dev)
+        # small jobs (genome sizes x 0.02): where sharing rounds pays, since a
+        # round's fixed cost outweighs a small job's alignment work
+        served_small = run_served_block(args, dev, n_jobs=100, scale=0.02)
     aln = merge = cpu = file_e2e = None
     if solo and not args.no_alignment_output:
         aln = measure_alignment_output(rs, kw, dev)
@@ -734,7 +739,8 @@ def bench_hero(args):
             "gcups": main["gcups"], "form": main["form"], "plain_form": main["plain_form"],
             "cpu_baseline": cpu, "file_e2e": file_e2e, "clocks": main["clocks"],
             "gpu_launches": main["gpu_launches"], "work_per_step": main["work_per_step"],
-            "affine_batched": affine, "served": served, "alignment_output": aln,
+            "affine_batched": affine, "served": served, "served_small_jobs": served_small,
+            "alignment_output": aln,
             "merge": merge,
         }
         print(json.dumps(line), flush=True)
