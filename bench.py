@@ -708,16 +708,37 @@ def bench_hero(args):
             "note": "the reference on this whole workload, timed once on the 8 cores of the "
                     "build host by tests/golden/make_golden.py (not timed in this run)"}
         del rs2
+    served_form = None
+    if solo and args.workload in ("config3", "config5"):
+        # the same job through a hero_server (host reads in, results in host
+        # memory out), against the plain and batched forms of the main line
+        from hero_b200 import HeroServer
+        with HeroServer(aligner=kw["aligner"], device=dev) as srv:
+            walls = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                jid = srv.submit(rs.seq, rs.off, rs.names)
+                srv.wait(jid)
+                srv.result(jid)
+                walls.append(time.perf_counter() - t0)
+                srv.release(jid)
+        sv = rs.total_bases / walls[-1]
+        served_form = {"value": sv, "unit": "bases/s", "seconds": walls[-1],
+                       "batched_vs_plain": main["value"] / main["plain_form"]["value"],
+                       "served_vs_plain": sv / main["plain_form"]["value"],
+                       "note": "one job submitted to a hero_server, submit to results in host "
+                               "memory (second of two runs)"}
     served = served_small = None
-    if solo and args.served_jobs:
+    if solo and args.served_jobs and args.workload == "config1":
         served = run_served_block(args, dev)
         # small jobs (genome sizes x 0.02): where sharing rounds pays, since a
         # round's fixed cost outweighs a small job's alignment work
         served_small = run_served_block(args, dev, n_jobs=100, scale=0.02)
     aln = merge = cpu = file_e2e = None
-    if solo and not args.no_alignment_output:
+    small = args.workload in ("config1", "config2")  # the .aln text of a large job is tens of GB
+    if solo and not args.no_alignment_output and small:
         aln = measure_alignment_output(rs, kw, dev)
-    if solo and not args.no_merge:
+    if solo and not args.no_merge and small:
         merge = measure_merge(dev)
     if solo and not args.no_cpu_baseline:
         cpu = measure_cpu_baseline(args)
@@ -739,7 +760,8 @@ def bench_hero(args):
             "gcups": main["gcups"], "form": main["form"], "plain_form": main["plain_form"],
             "cpu_baseline": cpu, "file_e2e": file_e2e, "clocks": main["clocks"],
             "gpu_launches": main["gpu_launches"], "work_per_step": main["work_per_step"],
-            "affine_batched": affine, "served": served, "served_small_jobs": served_small,
+            "affine_batched": affine, "served_form": served_form, "served": served,
+            "served_small_jobs": served_small,
             "alignment_output": aln,
             "merge": merge,
         }
