@@ -1997,30 +1997,29 @@ __global__ void __launch_bounds__(kConsWarps * 32)
         mn = warp_min(mn);
         mx = warp_max(mx);
         __syncwarp();
-        // median of the column sums by rank counting (QueryRead.cpp:204-211)
+        // median of the column sums (QueryRead.cpp:204-211: the sorted sums'
+        // middle one, or the mean of the middle two): the p-th smallest value by
+        // a binary search over [mn, mx] -- the smallest v with more than p sums
+        // at or below it, each count one pass over the sums and a warp sum
         const uint32_t p_hi = L / 2, p_lo = (L % 2 == 0) ? L / 2 - 1 : (L - 1) / 2;
-        uint32_t v_hi = 0, v_lo = 0;
-        bool f_hi = false, f_lo = false;
-        for (uint32_t i = lane; i < L; i += 32) {
-            const uint32_t x = cs[i];
-            uint32_t lt = 0, le = 0;
-            for (uint32_t j = 0; j < L; j++) {
-                const uint32_t y = cs[j];
-                lt += y < x;
-                le += y <= x;
+        auto count_le = [&](uint32_t v) {
+            uint32_t c = 0;
+            for (uint32_t i = lane; i < L; i += 32) c += cs[i] <= v;
+            return warp_sum(c);
+        };
+        auto select = [&](uint32_t p, uint32_t lo, uint32_t hi) {
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (count_le(mid) > p) {
+                    hi = mid;
+                } else {
+                    lo = mid + 1;
+                }
             }
-            if (lt <= p_hi && p_hi < le) {
-                v_hi = x;
-                f_hi = true;
-            }
-            if (lt <= p_lo && p_lo < le) {
-                v_lo = x;
-                f_lo = true;
-            }
-        }
-        const uint32_t m_hi = __ballot_sync(0xffffffffu, f_hi), m_lo = __ballot_sync(0xffffffffu, f_lo);
-        v_hi = __shfl_sync(0xffffffffu, v_hi, __ffs(m_hi) - 1);
-        v_lo = __shfl_sync(0xffffffffu, v_lo, __ffs(m_lo) - 1);
+            return lo;
+        };
+        const uint32_t v_lo = select(p_lo, mn, mx);
+        const uint32_t v_hi = (p_hi == p_lo || count_le(v_lo) > p_hi) ? v_lo : select(p_hi, v_lo, mx);
         if (lane == 0) {
             imin[r] = mn;
             imax[r] = mx;

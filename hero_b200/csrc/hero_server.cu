@@ -52,6 +52,48 @@ struct Job {
     uint64_t n() const { return uid.size(); }
 };
 
+// Host memory a worker stages a round in: page-locked, so the uploads and
+// downloads run at the link's speed, and reused from round to round (grown,
+// never shrunk).
+struct Staging {
+    uint8_t *p = nullptr;
+    size_t cap = 0;
+    bool ensure(size_t need) {
+        if (need <= cap) return true;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        const size_t want = need + need / 4 + 4096;
+        if (cudaHostAlloc(reinterpret_cast<void **>(&p), want, cudaHostAllocDefault) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return false;
+        }
+        cap = want;
+        return true;
+    }
+    ~Staging() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// memcpy spread over a few threads (a round's reads and results are up to GBs)
+void copy_parallel(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kChunk = size_t(16) << 20;
+    const size_t nt = std::min<size_t>(8, (bytes + kChunk - 1) / kChunk);
+    if (nt <= 1) {
+        if (bytes) std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (bytes + nt - 1) / nt;
+    for (size_t t = 0; t < nt; t++) {
+        const size_t a = t * per, b = std::min(bytes, a + per);
+        if (a < b)
+            th.emplace_back([=] { std::memcpy(static_cast<uint8_t *>(dst) + a, static_cast<const uint8_t *>(src) + a, b - a); });
+    }
+    for (auto &x : th) x.join();
+}
+
 }  // namespace
 
 // rounds that may be in flight at once (one context and worker thread each)
@@ -60,6 +102,7 @@ constexpr int kServeWorkers = 2;
 struct hero_server {
     hero_params p{};
     hero_ctx *ctx[kServeWorkers] = {};
+    Staging stage[kServeWorkers];  // each worker's round inputs and outputs
     uint64_t round_bytes = 0;
     Clock::time_point t0;
     std::mutex mu;
@@ -212,39 +255,34 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
         n += j->n();
         nb += j->seq.size();
     }
-    const bool single = js.size() == 1;
-    std::vector<uint8_t> seq, out_seq, good;
-    std::vector<uint64_t> off;
-    std::vector<int64_t> uid;
-    std::vector<uint32_t> tag, imin, imed, imax;
-    std::vector<double> mis, gc;
-    int st = HERO_OK;
-    if (single) {
-        // one job: its own buffers in and its result buffers out (no concatenation
-        // and no split; nobody reads a running job's results)
-        Job &j = *js[0];
-        j.out_seq.resize(nb);
-        j.good.resize(n);
-        j.imin.resize(n);
-        j.imed.resize(n);
-        j.imax.resize(n);
-        j.mis.resize(n);
-        j.gc.resize(n);
-        st = hero_set_queries(ctx, j.seq.data(), j.off.data(), j.uid.data(), n);
-        if (st == HERO_OK) st = hero_build_index(ctx);
-        if (st == HERO_OK) st = hero_align_self(ctx);
-        if (st == HERO_OK)
-            st = hero_consensus(ctx, j.out_seq.data(), j.imin.data(), j.imed.data(), j.imax.data(),
-                                j.mis.data(), j.gc.data(), j.good.data());
-    } else {
-        seq.resize(nb);
-        off.assign(n + 1, 0);
-        uid.resize(n);
-        tag.resize(n);
+    // the round's reads and results staged in the worker's page-locked
+    // buffer: reads | offsets | ids | job tags, then corrected bases | good |
+    // imin | imed | imax | mismatch rate | GC
+    Staging &sg = stage[w];
+    const size_t off_at = (nb + 7) & ~size_t(7);
+    const size_t in_bytes = off_at + 8 * (n + 1) + 8 * n + 4 * n;
+    const size_t out_at = (in_bytes + 255) & ~size_t(255);
+    const size_t out_bytes = nb + n + 12 * n + 16 * n + 64;
+    int st = sg.ensure(out_at + out_bytes) ? HERO_OK : HERO_E_OOM;
+    uint8_t *seq = sg.p;
+    uint64_t *off = reinterpret_cast<uint64_t *>(sg.p + off_at);
+    int64_t *uid = reinterpret_cast<int64_t *>(off + n + 1);
+    uint32_t *tag = reinterpret_cast<uint32_t *>(uid + n);
+    uint8_t *o_seq = sg.p + out_at;
+    uint8_t *o_good = o_seq + nb;
+    // 8-byte alignment for the doubles: after the bytes, round up
+    uint8_t *o_u32 = o_good + n;
+    while (reinterpret_cast<uintptr_t>(o_u32) & 7u) o_u32++;
+    uint32_t *o_imin = reinterpret_cast<uint32_t *>(o_u32), *o_imed = o_imin + n, *o_imax = o_imed + n;
+    uint8_t *o_d = reinterpret_cast<uint8_t *>(o_imax + n);
+    while (reinterpret_cast<uintptr_t>(o_d) & 7u) o_d++;
+    double *o_mis = reinterpret_cast<double *>(o_d), *o_gc = o_mis + n;
+    if (st == HERO_OK) {
         uint64_t r = 0, b = 0;
+        off[0] = 0;
         for (size_t t = 0; t < js.size(); t++) {
             const Job &j = *js[t];
-            if (!j.seq.empty()) std::memcpy(seq.data() + b, j.seq.data(), j.seq.size());
+            copy_parallel(seq + b, j.seq.data(), j.seq.size());
             for (uint64_t i = 0; i < j.n(); i++) {
                 off[r + i + 1] = b + j.off[i + 1];
                 uid[r + i] = j.uid[i];
@@ -253,22 +291,31 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
             r += j.n();
             b += j.seq.size();
         }
-        out_seq.resize(nb);
-        good.resize(n);
-        imin.resize(n);
-        imed.resize(n);
-        imax.resize(n);
-        mis.resize(n);
-        gc.resize(n);
-        st = hero_set_queries(ctx, seq.data(), off.data(), uid.data(), n);
-        if (st == HERO_OK) st = hero_set_query_jobs(ctx, tag.data(), n);
+        st = hero_set_queries(ctx, seq, off, uid, n);
+        if (st == HERO_OK && js.size() > 1) st = hero_set_query_jobs(ctx, tag, n);
         if (st == HERO_OK) st = hero_build_index(ctx);
         if (st == HERO_OK) st = hero_align_self(ctx);
-        if (st == HERO_OK)
-            st = hero_consensus(ctx, out_seq.data(), imin.data(), imed.data(), imax.data(),
-                                mis.data(), gc.data(), good.data());
+        if (st == HERO_OK) st = hero_consensus(ctx, o_seq, o_imin, o_imed, o_imax, o_mis, o_gc, o_good);
     }
-    const std::string err = st == HERO_OK ? std::string() : std::string(hero_last_error(ctx));
+    const std::string err = st == HERO_OK ? std::string()
+                            : (sg.p ? std::string(hero_last_error(ctx))
+                                    : std::string("page-locked staging memory not available"));
+    if (st == HERO_OK) {  // results into the jobs, before the lock (nobody reads a running job)
+        uint64_t r = 0, b = 0;
+        for (Job *j : js) {
+            const uint64_t jn = j->n(), jb = j->seq.size();
+            j->out_seq.resize(jb);
+            copy_parallel(j->out_seq.data(), o_seq + b, jb);
+            j->good.assign(o_good + r, o_good + r + jn);
+            j->imin.assign(o_imin + r, o_imin + r + jn);
+            j->imed.assign(o_imed + r, o_imed + r + jn);
+            j->imax.assign(o_imax + r, o_imax + r + jn);
+            j->mis.assign(o_mis + r, o_mis + r + jn);
+            j->gc.assign(o_gc + r, o_gc + r + jn);
+            r += jn;
+            b += jb;
+        }
+    }
     std::lock_guard<std::mutex> g(mu);
     if (st == HERO_E_OOM && (js.size() > 1 || in_flight > 1)) {
         // the estimate was short, or another round held the memory: requeue the
@@ -286,24 +333,12 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
     rounds++;
     const double t_end = now_ms();
     round_end(round_est);
-    uint64_t r = 0, b = 0;
     for (Job *j : js) {
-        const uint64_t jn = j->n(), jb = j->seq.size();
+        const uint64_t jb = j->seq.size();
         j->round = rounds;
         j->round_jobs = uint32_t(js.size());
         j->done_ms = t_end;
-        if (st == HERO_OK && single) {
-            j->state = HERO_JOB_DONE;
-            done++;
-            bases_done += jb;
-        } else if (st == HERO_OK) {
-            j->out_seq.assign(out_seq.begin() + long(b), out_seq.begin() + long(b + jb));
-            j->good.assign(good.begin() + long(r), good.begin() + long(r + jn));
-            j->imin.assign(imin.begin() + long(r), imin.begin() + long(r + jn));
-            j->imed.assign(imed.begin() + long(r), imed.begin() + long(r + jn));
-            j->imax.assign(imax.begin() + long(r), imax.begin() + long(r + jn));
-            j->mis.assign(mis.begin() + long(r), mis.begin() + long(r + jn));
-            j->gc.assign(gc.begin() + long(r), gc.begin() + long(r + jn));
+        if (st == HERO_OK) {
             j->state = HERO_JOB_DONE;
             done++;
             bases_done += jb;
@@ -315,8 +350,6 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
         }
         // inputs are no longer needed
         std::vector<uint8_t>().swap(j->seq);
-        r += jn;
-        b += jb;
     }
 }
 
