@@ -409,7 +409,7 @@ def run_alone(stream, dev: int) -> tuple[dict, dict, float, int]:
     return times, digests, sum(times.values()), bases
 
 
-def run_server(jobs, stream, dev: int, arrivals=None) -> dict:
+def run_server(jobs, stream, dev: int, arrivals=None, policy=None) -> dict:
     """Submits the jobs to one server -- all at once (arrivals None) or at the
     given arrival times (s) -- and reports per-job latency (submit -> results
     ready), aggregate throughput, the server's busy fraction and the digests."""
@@ -417,6 +417,8 @@ def run_server(jobs, stream, dev: int, arrivals=None) -> dict:
 
     from hero_b200 import HeroServer
     srv = HeroServer(aligner="affine", device=dev)
+    if policy is not None:
+        srv.set_round_policy(*policy)
     try:
         ids = {}
         late = []
@@ -455,6 +457,9 @@ def run_server(jobs, stream, dev: int, arrivals=None) -> dict:
             "busy_frac": (s1["busy_ms"] - s0["busy_ms"]) / (last - first),
             "rounds": rounds, "mean_jobs_per_round": len(infos) / max(rounds, 1),
             "overlapped_rounds": s1["overlapped_rounds"] - s0["overlapped_rounds"],
+            "worker_ms": {k: round(s1[k] - s0[k], 1) for k in
+                          ("ms_stage_in", "ms_round_calls", "ms_stage_out", "ms_alloc")},
+            "buffer_allocs": s1["buffer_allocs"] - s0["buffer_allocs"],
             "arrivals_late_s": float(max(late)) if late else 0.0, "_digests": digests}
 
 

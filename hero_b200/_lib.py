@@ -31,7 +31,7 @@ EXPORTS = [
     "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
     "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
     "hero_merge_pairs", "hero_get_overhang", "hero_mapping_histogram", "hero_set_vote_buffer",
-    "hero_consensus_range",
+    "hero_consensus_range", "hero_server_set_round_policy",
 ]
 
 # hero_params.flags: the alignment-output mode (HERO without -c); --merge
@@ -68,7 +68,8 @@ _STAT_MS = ["ms_upload", "ms_index", "ms_seed", "ms_chain", "ms_dp", "ms_record"
 class HeroStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
                 [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64),
-                 ("dp_rows_max", C.c_uint64), ("dp_cells_pairs", C.c_uint64)])
+                 ("dp_rows_max", C.c_uint64), ("dp_cells_pairs", C.c_uint64),
+                 ("buffer_allocs", C.c_uint64), ("ms_alloc", C.c_double)])
 
 
 class DpTuning(C.Structure):
@@ -101,7 +102,9 @@ class ServerStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in ("jobs_submitted", "jobs_done", "jobs_failed", "rounds",
                                             "bases_done", "round_bytes_budget")] +
                 [("busy_ms", C.c_double), ("uptime_ms", C.c_double),
-                 ("overlapped_rounds", C.c_uint64)])
+                 ("overlapped_rounds", C.c_uint64), ("ms_stage_in", C.c_double),
+                 ("ms_round_calls", C.c_double), ("ms_stage_out", C.c_double),
+                 ("buffer_allocs", C.c_uint64), ("ms_alloc", C.c_double)])
 
 
 _lib = None
@@ -141,6 +144,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_get_overhang.argtypes = [vp, vp]
     lib.hero_mapping_histogram.argtypes = [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.hero_set_vote_buffer.argtypes = [vp, vp, C.c_uint64]
+    lib.hero_server_set_round_policy.argtypes = [vp, C.c_uint64, C.c_uint64]
     lib.hero_consensus_range.argtypes = [vp, C.c_uint64, C.c_uint64] + [vp] * 7
     lib.hero_votes_words.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_votes_save.argtypes = [vp, vp]
@@ -493,6 +497,18 @@ class HeroServer:
                               int(t["pair_strips"]), int(t["chunk_strips"]),
                               int(t.get("regs_per_thread", 0)))
         self.lib.hero_server_set_dp_tuning(self.h, arr, len(classes))
+
+    ROUND_BASES_DEFAULT = 8_000_000
+    OVERLAP_BASES_DEFAULT = 64_000_000
+
+    def set_round_policy(self, round_bases_max: int = ROUND_BASES_DEFAULT,
+                         overlap_bases_max: int = OVERLAP_BASES_DEFAULT):
+        """Round policy (hero_server_set_round_policy): bases a round admits
+        beyond its first job, and the size under which a round may run beside
+        another (0: no limit for either)."""
+        rc = self.lib.hero_server_set_round_policy(self.h, int(round_bases_max), int(overlap_bases_max))
+        if rc != HERO_OK:
+            raise HeroError(f"hero_server_set_round_policy: {ERRORS.get(rc, rc)}")
 
     def close(self):
         if getattr(self, "h", None):

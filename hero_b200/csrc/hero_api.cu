@@ -23,6 +23,7 @@ struct DBuf {
     void *p = nullptr;
     size_t cap = 0;
     bool external = false;  // caller-owned memory: never freed or grown here
+    bool pooled = false;    // allocated stream-ordered (freed the same way)
 };
 
 struct Timer {
@@ -128,20 +129,30 @@ struct hero_ctx {
         cudaError_t e = cudaGetLastError();
         return cuda(e, what);
     }
+    // Buffers are allocated and freed stream-ordered on the context's stream
+    // (the device's default memory pool, which returns freed memory to the
+    // device at the stream's next synchronisation): growing one waits for no
+    // other stream, so contexts that run side by side -- the serving workers --
+    // do not stall each other's launches the way cudaFree's device-wide
+    // synchronisation does.  Inside a stream capture (no growth is expected
+    // there: sizes come from the eager round's plan) the plain calls are used.
     void release(DBuf &b) {
         if (b.p && !b.external) {
-            cudaFree(b.p);
+            if (b.pooled) cudaFreeAsync(b.p, st);
+            else cudaFree(b.p);
             bytes -= b.cap;
         }
         b.p = nullptr;
         b.cap = 0;
         b.external = false;
+        b.pooled = false;
     }
     // grows a device buffer to at least `need` bytes (contents are not kept)
     int ensure(DBuf &b, size_t need, const char *what) {
         if (need == 0) need = 16;
         if (b.cap >= need) return HERO_OK;
         if (b.external) return fail(HERO_E_INPUT, std::string("caller's buffer too small for ") + what);
+        const auto t0 = std::chrono::steady_clock::now();
         release(b);
         size_t want = need + need / 4 + 256;
         if (P.device_memory_budget && bytes + want > P.device_memory_budget) {
@@ -149,16 +160,27 @@ struct hero_ctx {
             if (bytes + want > P.device_memory_budget)
                 return fail(HERO_E_OOM, std::string("device memory budget exceeded at ") + what);
         }
-        cudaError_t e = cudaMalloc(&b.p, want);
+        const bool pooled = !capturing && st;
+        cudaError_t e = pooled ? cudaMallocAsync(&b.p, want, st) : cudaMalloc(&b.p, want);
+        if (e != cudaSuccess && pooled) {
+            // memory freed on other streams may still wait in the pool: settle
+            // this stream and try once more
+            cudaGetLastError();
+            cudaStreamSynchronize(st);
+            e = cudaMallocAsync(&b.p, want, st);
+        }
         if (e != cudaSuccess) {
             cudaGetLastError();
             b.p = nullptr;
-            return fail(HERO_E_OOM, std::string("cudaMalloc failed for ") + what + ": " +
+            return fail(HERO_E_OOM, std::string("device allocation failed for ") + what + ": " +
                                         cudaGetErrorString(e));
         }
         b.cap = want;
+        b.pooled = pooled;
         bytes += want;
         bytes_peak = std::max(bytes_peak, bytes);
+        stats.buffer_allocs++;
+        stats.ms_alloc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         return HERO_OK;
     }
     void drop_graph() {

@@ -13,14 +13,17 @@
 // into one query set whose reads carry their job (hero_set_query_jobs), so one
 // set of launches -- index build, seeding, chaining, DP, votes, consensus --
 // serves every job of the round, and a job's k-mers only ever meet its own
-// reads: each job's output is the output it gets alone.  Results are split
-// back per job and kept until released.
+// reads: each job's output is the output it gets alone.  A round's results
+// stay in one host block that its jobs share, each job reading its own slice,
+// until every job of the round is released.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -34,6 +37,28 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Host array left uninitialised (results are written over it by the device
+// copy; zero-filling GBs first would cost as much as the copy).
+template <class T>
+struct HostArray {
+    std::unique_ptr<T[]> p;
+    size_t n = 0;
+    bool alloc(size_t k) {
+        p.reset(k ? new (std::nothrow) T[k] : nullptr);
+        n = p ? k : 0;
+        return p || !k;
+    }
+    T *data() const { return p.get(); }
+};
+
+// One round's results, shared by its jobs: each job reads its own slice, so a
+// round's output is never split or copied before a caller fetches it.
+struct RoundOut {
+    HostArray<uint8_t> seq, good;
+    HostArray<uint32_t> imin, imed, imax;
+    HostArray<double> mis, gc;
+};
+
 struct Job {
     uint64_t id = 0;
     int32_t state = HERO_JOB_QUEUED, status = HERO_OK;
@@ -42,38 +67,13 @@ struct Job {
     std::vector<uint64_t> off;
     std::vector<int64_t> uid;
     uint64_t bytes = 0;  // admission estimate
-    // results
-    std::vector<uint8_t> out_seq, good;
-    std::vector<uint32_t> imin, imed, imax;
-    std::vector<double> mis, gc;
+    // results: a slice of the round's output (reads [out_read, +n), bases [out_base, +bases))
+    std::shared_ptr<const RoundOut> out;
+    uint64_t out_read = 0, out_base = 0;
     uint64_t round = 0;
     uint32_t round_jobs = 0;
     double submit_ms = 0, start_ms = 0, done_ms = 0;
     uint64_t n() const { return uid.size(); }
-};
-
-// Host memory a worker stages a round in: page-locked, so the uploads and
-// downloads run at the link's speed, and reused from round to round (grown,
-// never shrunk).
-struct Staging {
-    uint8_t *p = nullptr;
-    size_t cap = 0;
-    bool ensure(size_t need) {
-        if (need <= cap) return true;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-        const size_t want = need + need / 4 + 4096;
-        if (cudaHostAlloc(reinterpret_cast<void **>(&p), want, cudaHostAllocDefault) != cudaSuccess) {
-            (void)cudaGetLastError();
-            return false;
-        }
-        cap = want;
-        return true;
-    }
-    ~Staging() {
-        if (p) cudaFreeHost(p);
-    }
 };
 
 // memcpy spread over a few threads (a round's reads and results are up to GBs)
@@ -96,13 +96,23 @@ void copy_parallel(void *dst, const void *src, size_t bytes) {
 
 }  // namespace
 
+// Round policy defaults, measured on the serving stream (jobs of 0.2-30 Mbp and
+// of 10 Mbp-1.6 Gbp): rounds of up to ~8 Mbp beyond their first job, and no
+// two rounds above 64 Mbp side by side (two large rounds only share the SMs
+// and the L2 and lose ~8 % against running one after the other; a small round
+// beside a large one fills its host-side gaps).
+constexpr uint64_t kRoundBasesDefault = 8000000;
+constexpr uint64_t kOverlapBasesDefault = 64000000;
+
 // rounds that may be in flight at once (one context and worker thread each)
-constexpr int kServeWorkers = 2;
+#ifndef HERO_SERVE_WORKERS
+#define HERO_SERVE_WORKERS 2
+#endif
+constexpr int kServeWorkers = HERO_SERVE_WORKERS;
 
 struct hero_server {
     hero_params p{};
     hero_ctx *ctx[kServeWorkers] = {};
-    Staging stage[kServeWorkers];  // each worker's round inputs and outputs
     uint64_t round_bytes = 0;
     Clock::time_point t0;
     std::mutex mu;
@@ -121,7 +131,19 @@ struct hero_server {
     bool exclusive = false;              // the queue head needs the device to itself
     double busy_ms = 0, busy_since = 0;  // time with at least one round in flight
     uint64_t overlapped_rounds = 0;      // rounds that started while another ran
+    // round policy (hero_server_set_round_policy)
+    uint64_t round_bases_max = kRoundBasesDefault;      // bases a round admits beyond its first job
+    uint64_t overlap_bases_max = kOverlapBasesDefault;  // a round starts beside another only if one is this small
+    uint64_t running_bases[kServeWorkers] = {};         // bases of each worker's round in flight
+    double ms_stage_in = 0, ms_round_calls = 0, ms_stage_out = 0;  // worker wall time, all rounds
+    uint64_t allocs[kServeWorkers] = {};  // buffer growth of each worker's context
+    double ms_alloc[kServeWorkers] = {};
 
+    bool large_running() const {  // a round above the overlap limit is in flight
+        for (int v = 0; v < kServeWorkers; v++)
+            if (running_bases[v] > overlap_bases_max) return true;
+        return false;
+    }
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
     }
@@ -173,7 +195,9 @@ void hero_server::run(int w) {
             if (queue.empty()) return false;
             if (in_flight == 0) return true;
             if (exclusive) return false;
-            return in_flight_bytes + jobs[queue.front()].bytes <= round_bytes;
+            const Job &head = jobs[queue.front()];
+            if (in_flight_bytes + head.bytes > round_bytes) return false;
+            return !overlap_bases_max || head.seq.size() <= overlap_bases_max || !large_running();
         };
         cv_work.wait(lk, [&] { return stop || admissible(); });
         if (stop) break;
@@ -183,17 +207,34 @@ void hero_server::run(int w) {
         uint64_t take = hero_round_admit(sizes.data(), sizes.size(), room);
         take = std::min(take, max_jobs);
         if (cap_jobs) take = std::min(take, cap_jobs);
+        // bases beyond the first job: the round limit, and beside a large
+        // round the overlap limit (the round must stay small)
+        uint64_t cap_bases = round_bases_max ? round_bases_max : ~0ull;
+        if (in_flight && overlap_bases_max && large_running()) cap_bases = std::min(cap_bases, overlap_bases_max);
+        {
+            uint64_t nb = 0, t = 0;
+            for (uint64_t id : queue) {
+                if (t >= take) break;
+                const uint64_t jb = jobs[id].seq.size();
+                if (t > 0 && nb + jb > cap_bases) break;
+                nb += jb;
+                t++;
+            }
+            take = t;
+        }
         std::vector<uint64_t> ids(queue.begin(), queue.begin() + long(take));
         queue.erase(queue.begin(), queue.begin() + long(take));
         exclusive = false;
-        uint64_t bytes = 0;
+        uint64_t bytes = 0, bases = 0;
         const double t = now_ms();
         for (uint64_t id : ids) {
             jobs[id].state = HERO_JOB_RUNNING;
             jobs[id].start_ms = t;
             bytes += jobs[id].bytes;
+            bases += jobs[id].seq.size();
         }
         round_begin(bytes);
+        running_bases[w] = bases;
         std::vector<hero_dp_tuning> tun;
         const bool retune = tuning_gen != my_tuning_gen;
         if (retune) {
@@ -205,6 +246,7 @@ void hero_server::run(int w) {
         if (retune) hero_set_dp_tuning(ctx[w], tun.data(), uint32_t(tun.size()));
         run_round(w, ids, bytes);
         lk.lock();
+        running_bases[w] = 0;
         cv_done.notify_all();
         cv_work.notify_all();
     }
@@ -255,68 +297,74 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
         n += j->n();
         nb += j->seq.size();
     }
-    // the round's reads and results staged in the worker's page-locked
-    // buffer: reads | offsets | ids | job tags, then corrected bases | good |
-    // imin | imed | imax | mismatch rate | GC
-    Staging &sg = stage[w];
-    const size_t off_at = (nb + 7) & ~size_t(7);
-    const size_t in_bytes = off_at + 8 * (n + 1) + 8 * n + 4 * n;
-    const size_t out_at = (in_bytes + 255) & ~size_t(255);
-    const size_t out_bytes = nb + n + 12 * n + 16 * n + 64;
-    int st = sg.ensure(out_at + out_bytes) ? HERO_OK : HERO_E_OOM;
-    uint8_t *seq = sg.p;
-    uint64_t *off = reinterpret_cast<uint64_t *>(sg.p + off_at);
-    int64_t *uid = reinterpret_cast<int64_t *>(off + n + 1);
-    uint32_t *tag = reinterpret_cast<uint32_t *>(uid + n);
-    uint8_t *o_seq = sg.p + out_at;
-    uint8_t *o_good = o_seq + nb;
-    // 8-byte alignment for the doubles: after the bytes, round up
-    uint8_t *o_u32 = o_good + n;
-    while (reinterpret_cast<uintptr_t>(o_u32) & 7u) o_u32++;
-    uint32_t *o_imin = reinterpret_cast<uint32_t *>(o_u32), *o_imed = o_imin + n, *o_imax = o_imed + n;
-    uint8_t *o_d = reinterpret_cast<uint8_t *>(o_imax + n);
-    while (reinterpret_cast<uintptr_t>(o_d) & 7u) o_d++;
-    double *o_mis = reinterpret_cast<double *>(o_d), *o_gc = o_mis + n;
-    if (st == HERO_OK) {
+    // one job: its own buffers go up as they are; several: concatenated
+    // (reads | offsets | ids | job tags), each read carrying its job
+    HostArray<uint8_t> cat_seq;
+    HostArray<uint64_t> cat_off;
+    HostArray<int64_t> cat_uid;
+    HostArray<uint32_t> cat_tag;
+    const uint8_t *seq = js[0]->seq.data();
+    const uint64_t *off = js[0]->off.data();
+    const int64_t *uid = js[0]->uid.data();
+    const double t_in = now_ms();
+    bool host_ok = true;
+    if (js.size() > 1) {
+        host_ok = cat_seq.alloc(nb) && cat_off.alloc(n + 1) && cat_uid.alloc(n) && cat_tag.alloc(n);
+    }
+    if (js.size() > 1 && host_ok) {
         uint64_t r = 0, b = 0;
-        off[0] = 0;
+        cat_off.p[0] = 0;
         for (size_t t = 0; t < js.size(); t++) {
             const Job &j = *js[t];
-            copy_parallel(seq + b, j.seq.data(), j.seq.size());
+            copy_parallel(cat_seq.data() + b, j.seq.data(), j.seq.size());
             for (uint64_t i = 0; i < j.n(); i++) {
-                off[r + i + 1] = b + j.off[i + 1];
-                uid[r + i] = j.uid[i];
-                tag[r + i] = uint32_t(t);
+                cat_off.p[r + i + 1] = b + j.off[i + 1];
+                cat_uid.p[r + i] = j.uid[i];
+                cat_tag.p[r + i] = uint32_t(t);
             }
             r += j.n();
             b += j.seq.size();
         }
-        st = hero_set_queries(ctx, seq, off, uid, n);
-        if (st == HERO_OK && js.size() > 1) st = hero_set_query_jobs(ctx, tag, n);
-        if (st == HERO_OK) st = hero_build_index(ctx);
-        if (st == HERO_OK) st = hero_align_self(ctx);
-        if (st == HERO_OK) st = hero_consensus(ctx, o_seq, o_imin, o_imed, o_imax, o_mis, o_gc, o_good);
+        seq = cat_seq.data();
+        off = cat_off.data();
+        uid = cat_uid.data();
     }
+    auto out = std::make_shared<RoundOut>();
+    host_ok = host_ok && out->seq.alloc(nb) && out->good.alloc(n) && out->imin.alloc(n) &&
+              out->imed.alloc(n) && out->imax.alloc(n) && out->mis.alloc(n) && out->gc.alloc(n);
+    const double t_calls = now_ms();
+    int st = host_ok ? hero_set_queries(ctx, seq, off, uid, n) : HERO_E_OOM;
+    if (st == HERO_OK && js.size() > 1) st = hero_set_query_jobs(ctx, cat_tag.data(), n);
+    if (st == HERO_OK) st = hero_build_index(ctx);
+    if (st == HERO_OK) st = hero_align_self(ctx);
+    if (st == HERO_OK)
+        st = hero_consensus(ctx, out->seq.data(), out->imin.data(), out->imed.data(),
+                            out->imax.data(), out->mis.data(), out->gc.data(), out->good.data());
+    const double t_out = now_ms();
     const std::string err = st == HERO_OK ? std::string()
-                            : (sg.p ? std::string(hero_last_error(ctx))
-                                    : std::string("page-locked staging memory not available"));
-    if (st == HERO_OK) {  // results into the jobs, before the lock (nobody reads a running job)
+                            : host_ok ? std::string(hero_last_error(ctx))
+                                      : std::string("host memory for the round's reads or results not available");
+    if (st == HERO_OK) {  // each job's slice of the round's output (nobody reads a running job)
         uint64_t r = 0, b = 0;
         for (Job *j : js) {
-            const uint64_t jn = j->n(), jb = j->seq.size();
-            j->out_seq.resize(jb);
-            copy_parallel(j->out_seq.data(), o_seq + b, jb);
-            j->good.assign(o_good + r, o_good + r + jn);
-            j->imin.assign(o_imin + r, o_imin + r + jn);
-            j->imed.assign(o_imed + r, o_imed + r + jn);
-            j->imax.assign(o_imax + r, o_imax + r + jn);
-            j->mis.assign(o_mis + r, o_mis + r + jn);
-            j->gc.assign(o_gc + r, o_gc + r + jn);
-            r += jn;
-            b += jb;
+            j->out = out;
+            j->out_read = r;
+            j->out_base = b;
+            r += j->n();
+            b += j->seq.size();
         }
     }
+    hero_stats cs{};
+    const bool have_cs = hero_get_stats(ctx, &cs) == HERO_OK;
+    const double t_done = now_ms();
     std::lock_guard<std::mutex> g(mu);
+    if (have_cs) {
+        allocs[w] = cs.buffer_allocs;
+        ms_alloc[w] = cs.ms_alloc;
+    }
+    ms_stage_in += t_calls - t_in;
+    ms_round_calls += t_out - t_calls;
+    ms_stage_out += t_done - t_out;
     if (st == HERO_E_OOM && (js.size() > 1 || in_flight > 1)) {
         // the estimate was short, or another round held the memory: requeue the
         // jobs in order, then admit half as many (one job: with the device to itself)
@@ -406,6 +454,18 @@ extern "C" void hero_server_destroy(hero_server *s) {
         if (s->worker[w].joinable()) s->worker[w].join();
     for (int w = 0; w < kServeWorkers; w++) hero_destroy(s->ctx[w]);
     delete s;
+}
+
+extern "C" int hero_server_set_round_policy(hero_server *s, uint64_t round_bases_max,
+                                            uint64_t overlap_bases_max) {
+    if (!s) return HERO_E_INPUT;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->round_bases_max = round_bases_max;
+        s->overlap_bases_max = overlap_bases_max;
+    }
+    s->cv_work.notify_all();
+    return HERO_OK;
 }
 
 extern "C" int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t, uint32_t n) {
@@ -503,22 +563,33 @@ extern "C" int hero_job_result(hero_server *s, uint64_t job_id, uint8_t *seq_out
                                uint32_t *imed, uint32_t *imax, double *mismatch_rate,
                                double *gc_content, uint8_t *good_out) {
     if (!s) return HERO_E_INPUT;
-    std::lock_guard<std::mutex> g(s->mu);
-    auto it = s->jobs.find(job_id);
-    if (it == s->jobs.end()) return HERO_E_INPUT;
-    const Job &j = it->second;
-    if (j.state == HERO_JOB_FAILED) return j.status;
-    if (j.state != HERO_JOB_DONE) return HERO_E_STATE;
-    auto put = [](auto *dst, const auto &v) {
-        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    std::shared_ptr<const RoundOut> out;
+    uint64_t r = 0, b = 0, n = 0, nb = 0;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        auto it = s->jobs.find(job_id);
+        if (it == s->jobs.end()) return HERO_E_INPUT;
+        const Job &j = it->second;
+        if (j.state == HERO_JOB_FAILED) return j.status;
+        if (j.state != HERO_JOB_DONE) return HERO_E_STATE;
+        out = j.out;
+        r = j.out_read;
+        b = j.out_base;
+        n = j.n();
+        nb = j.off.empty() ? 0 : j.off.back();
+    }
+    if (!out || n == 0) return HERO_OK;  // a job without reads has no output
+    // the copy runs outside the lock (the shared slice outlives a concurrent release)
+    auto put = [](auto *dst, const auto &a, uint64_t at, uint64_t k) {
+        if (dst && k) std::memcpy(dst, a.data() + at, k * sizeof(a.data()[0]));
     };
-    put(seq_out, j.out_seq);
-    put(imin, j.imin);
-    put(imed, j.imed);
-    put(imax, j.imax);
-    put(mismatch_rate, j.mis);
-    put(gc_content, j.gc);
-    put(good_out, j.good);
+    put(seq_out, out->seq, b, nb);
+    put(imin, out->imin, r, n);
+    put(imed, out->imed, r, n);
+    put(imax, out->imax, r, n);
+    put(mismatch_rate, out->mis, r, n);
+    put(gc_content, out->gc, r, n);
+    put(good_out, out->good, r, n);
     return HERO_OK;
 }
 
@@ -555,5 +626,14 @@ extern "C" int hero_server_get_stats(hero_server *s, hero_server_stats *out) {
     out->busy_ms = s->busy_ms + (s->in_flight ? s->now_ms() - s->busy_since : 0.0);
     out->uptime_ms = s->now_ms();
     out->overlapped_rounds = s->overlapped_rounds;
+    out->ms_stage_in = s->ms_stage_in;
+    out->ms_round_calls = s->ms_round_calls;
+    out->ms_stage_out = s->ms_stage_out;
+    out->buffer_allocs = 0;
+    out->ms_alloc = 0;
+    for (int w = 0; w < kServeWorkers; w++) {
+        out->buffer_allocs += s->allocs[w];
+        out->ms_alloc += s->ms_alloc[w];
+    }
     return HERO_OK;
 }

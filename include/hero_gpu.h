@@ -120,6 +120,8 @@ typedef struct {
     uint64_t dp_rows_max;      /* longest DP side (the row count of a segment) seen so far;
                                   the key of hero_dp_tuning classes */
     uint64_t dp_cells_pairs;   /* of dp_cells_computed, the cells computed as 16-bit pairs */
+    uint64_t buffer_allocs;    /* device buffers grown (allocated stream-ordered) */
+    double ms_alloc;           /* host time spent growing device buffers */
 } hero_stats;
 
 /* Returns the default parameters of the reference's Config. */
@@ -337,6 +339,12 @@ typedef struct {
     double busy_ms;              /* wall time with at least one round in flight */
     double uptime_ms;
     uint64_t overlapped_rounds;  /* rounds started while another round ran */
+    /* worker wall time summed over rounds: staging the round's reads (host
+       copies), the round's library calls (upload, index, alignment, consensus
+       and the download of results), and splitting results back to the jobs */
+    double ms_stage_in, ms_round_calls, ms_stage_out;
+    uint64_t buffer_allocs;      /* device buffers the workers' contexts have grown */
+    double ms_alloc;             /* host time the workers spent growing them */
 } hero_server_stats;
 
 /* A server owns two contexts on p->device, each with its own stream and worker
@@ -370,6 +378,18 @@ const char *hero_job_error(hero_server *s, uint64_t job_id);
 int hero_job_release(hero_server *s, uint64_t job_id);
 int hero_server_get_stats(hero_server *s, hero_server_stats *out);
 
+/* Round policy.  round_bases_max: the most bases a round admits beyond its
+ * first job (0: as many as fit the memory budget).  overlap_bases_max: a round
+ * starts while another runs only if one of the two has at most this many
+ * bases, and a round admitted beside a larger one stays within it (0: rounds
+ * always overlap).  A round's device work is the same whether its jobs run
+ * together or apart; what serving gains is the host side of one round (upload,
+ * download, buffer growth) hidden behind the device work of the other, while
+ * two large rounds side by side only share the SMs and the L2.  Defaults:
+ * 8,000,000 and 64,000,000, measured best on streams of small (0.2-30 Mbp)
+ * and large (10 Mbp-1.6 Gbp) jobs. */
+int hero_server_set_round_policy(hero_server *s, uint64_t round_bases_max,
+                                 uint64_t overlap_bases_max);
 /* DP kernel shapes (hero_set_dp_tuning) for the rounds the server runs next. */
 int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t, uint32_t n);
 

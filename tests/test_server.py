@@ -90,6 +90,52 @@ def test_rounds_tagged_by_hand_match_rounds_alone():
     assert np.array_equal(res["imed"][n0:], alone[1]["imed"])
 
 
+def _same(a, b, k):
+    for f in ("seq", "imin", "imed", "imax", "good"):
+        assert np.array_equal(a[f], b[f]), (k, f)
+    for f in ("mismatch_rate", "gc"):
+        assert np.array_equal(a[f].view(np.uint64), b[f].view(np.uint64)), (k, f)
+
+
+@pytest.mark.gpu
+def test_a_shared_round_outlives_the_release_of_its_other_jobs():
+    """A round's results are one block its jobs share: releasing some jobs of
+    the round leaves the others' slices intact."""
+    from hero_b200 import HeroServer, correct
+    jobs = _jobs()
+    alone = [correct(rs, aligner="affine") for rs in jobs]
+    with HeroServer(aligner="affine") as srv:
+        srv.set_round_policy(0, 0)
+        ids = [srv.submit(rs.seq, rs.off, rs.names) for rs in jobs]
+        infos = [srv.wait(j, 120_000) for j in ids]
+        assert max(i["round_jobs"] for i in infos) > 1
+        for j in ids[::2]:
+            srv.release(j)
+        for k in range(1, len(jobs), 2):
+            _same(alone[k], srv.result(ids[k]), k)
+
+
+@pytest.mark.gpu
+def test_round_policy_one_job_a_round_and_no_overlap():
+    """round_bases_max=1 admits no job beside a round's first; overlap_bases_max=1
+    starts no round while another (of more than one base) runs."""
+    from hero_b200 import HeroServer, correct
+    jobs = _jobs()
+    alone = [correct(rs, aligner="affine") for rs in jobs]
+    with HeroServer(aligner="affine") as srv:
+        srv.set_round_policy(1, 1)
+        s0 = srv.stats()
+        ids = [srv.submit(rs.seq, rs.off, rs.names) for rs in jobs]
+        infos = [srv.wait(j, 120_000) for j in ids]
+        got = [srv.result(j) for j in ids]
+        s1 = srv.stats()
+    assert all(i["round_jobs"] == 1 for i in infos)
+    assert s1["rounds"] - s0["rounds"] == len(jobs)
+    assert s1["overlapped_rounds"] == s0["overlapped_rounds"]
+    for k, (a, b) in enumerate(zip(alone, got)):
+        _same(a, b, k)
+
+
 @pytest.mark.gpu
 def test_wait_with_a_limit_times_out_and_later_completes():
     from hero_b200 import HeroError, HeroServer
