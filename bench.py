@@ -64,8 +64,12 @@ sys.path.insert(0, ROOT)
 # ncu capture of a whole k_dp_wave launch per aligner (dram__bytes_read.sum +
 # dram__bytes_write.sum over that launch's reference cells).  The traffic is per
 # segment (codes in, ops and summaries out), so it scales with the cells of a
-# launch.  None where no capture of the current kernel exists.
-DP_DRAM_BYTES_PER_CELL = {"affine": 2.225526e9 / 23_186_600_877, "global": None}
+# launch.  Captures of the tuned shapes (1-warp blocks, tagged 16-bit pairs):
+# global, 100 bp reads at 30x on a 200 kbp genome: 180.80 MB + 89.73 MB over
+# 1,766,508,768 cells; affine, 150 bp reads at 50x on a 100 kbp genome:
+# 1.4559 GB + 0.7077 GB over 23,186,600,877 cells.
+DP_DRAM_BYTES_PER_CELL = {"affine": (1.455896e9 + 0.707741e9) / 23_186_600_877,
+                          "global": (180.799744e6 + 89.734656e6) / 1_766_508_768}
 
 # the reference's wall time on the whole affine/indel workload (1,666,666 reads,
 # -a a), 8 threads, recorded by tests/golden/make_golden.py --full config2_full
@@ -391,60 +395,60 @@ def _digest(res: dict) -> str:
     return h.hexdigest()
 
 
-def run_alone(stream, dev: int) -> tuple[dict, dict, float, int]:
+def run_alone(stream, h) -> tuple[dict, dict, float, int]:
     """Every job corrected on its own, one after another, through one context
     (host reads in, results in host memory out): wall time and digest per job."""
-    from hero_b200 import Hero
     times, digests, bases = {}, {}, 0
-    with Hero(aligner="affine", device=dev) as h:
-        for jid, (seq, off, names) in stream:
-            t0 = time.perf_counter()
-            h.set_queries(seq, off, names)
-            h.build_index()
-            h.align_self()
-            res = h.consensus()
-            times[jid] = time.perf_counter() - t0
-            digests[jid] = _digest(res)
-            bases += int(off[-1])
+    for jid, (seq, off, names) in stream:
+        t0 = time.perf_counter()
+        h.set_queries(seq, off, names)
+        h.build_index()
+        h.align_self()
+        res = h.consensus()
+        times[jid] = time.perf_counter() - t0
+        digests[jid] = _digest(res)
+        bases += int(off[-1])
     return times, digests, sum(times.values()), bases
 
 
-def run_server(jobs, stream, dev: int, arrivals=None, policy=None) -> dict:
-    """Submits the jobs to one server -- all at once (arrivals None) or at the
+def warm_server(srv, item):
+    """Both workers' contexts sized for the given job (one copy each, submitted
+    together), as a server that has run for a while is."""
+    _, (seq, off, names) = item
+    ids = [srv.submit(seq, off, names) for _ in range(2)]
+    for i in ids:
+        srv.wait(i)
+        srv.release(i)
+
+
+def run_server(srv, stream, arrivals=None) -> dict:
+    """Submits the jobs to a server -- all at once (arrivals None) or at the
     given arrival times (s) -- and reports per-job latency (submit -> results
     ready), aggregate throughput, the server's busy fraction and the digests."""
     import threading
+    ids = {}
+    late = []
 
-    from hero_b200 import HeroServer
-    srv = HeroServer(aligner="affine", device=dev)
-    if policy is not None:
-        srv.set_round_policy(*policy)
-    try:
-        ids = {}
-        late = []
+    def submitter():
+        start = time.perf_counter()
+        for jid, (seq, off, names) in stream:
+            if arrivals is not None:
+                dt = arrivals[jid] - (time.perf_counter() - start)
+                if dt > 0:
+                    time.sleep(dt)
+                else:
+                    late.append(-dt)
+            ids[jid] = srv.submit(seq, off, names)
 
-        def submitter():
-            start = time.perf_counter()
-            for jid, (seq, off, names) in stream:
-                if arrivals is not None:
-                    dt = arrivals[jid] - (time.perf_counter() - start)
-                    if dt > 0:
-                        time.sleep(dt)
-                    else:
-                        late.append(-dt)
-                ids[jid] = srv.submit(seq, off, names)
-
-        s0 = srv.stats()
-        th = threading.Thread(target=submitter)
-        th.start()
-        th.join()
-        infos = {jid: srv.wait(i) for jid, i in ids.items()}
-        s1 = srv.stats()
-        digests = {jid: _digest(srv.result(i)) for jid, i in ids.items()}
-        for i in ids.values():
-            srv.release(i)
-    finally:
-        srv.close()
+    s0 = srv.stats()
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    infos = {jid: srv.wait(i) for jid, i in ids.items()}
+    s1 = srv.stats()
+    digests = {jid: _digest(srv.result(i)) for jid, i in ids.items()}
+    for i in ids.values():
+        srv.release(i)
     lat = np.array([i["done_ms"] - i["submit_ms"] for i in infos.values()])
     first = min(i["submit_ms"] for i in infos.values())
     last = max(i["done_ms"] for i in infos.values())
@@ -457,6 +461,7 @@ def run_server(jobs, stream, dev: int, arrivals=None, policy=None) -> dict:
             "busy_frac": (s1["busy_ms"] - s0["busy_ms"]) / (last - first),
             "rounds": rounds, "mean_jobs_per_round": len(infos) / max(rounds, 1),
             "overlapped_rounds": s1["overlapped_rounds"] - s0["overlapped_rounds"],
+            "overlapped_device_phases": s1["overlapped_compute"] - s0["overlapped_compute"],
             "worker_ms": {k: round(s1[k] - s0[k], 1) for k in
                           ("ms_stage_in", "ms_round_calls", "ms_stage_out", "ms_alloc")},
             "buffer_allocs": s1["buffer_allocs"] - s0["buffer_allocs"],
@@ -464,10 +469,15 @@ def run_server(jobs, stream, dev: int, arrivals=None, policy=None) -> dict:
 
 
 def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.95) -> dict:
-    """The serving stream: each job alone (one at a time), the server with every
-    job submitted at once (its capacity), then the server under Poisson arrivals
-    at `load` of the better of the two rates (so the load is a true fraction of
-    what the device sustains).  served == alone compares every job's digest."""
+    """The serving stream: each job alone (one at a time, one context), the
+    server with every job submitted at once (its capacity), then the same
+    server under Poisson arrivals at `load` of the better of the two rates (so
+    the load is a true fraction of what the device sustains).  Both arms are
+    warm: the context and both server workers first run the stream's largest
+    job, so device buffers are sized as in a long-running service (buffer
+    growth is a one-time cost either arm would pay).  served == alone compares
+    every job's digest."""
+    from hero_b200 import Hero, HeroServer
     if in_memory:
         data = dict(job_stream(jobs))
 
@@ -476,18 +486,19 @@ def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.95) -> dict:
     else:
         def stream():
             return job_stream(jobs)
-    # warm-up: one small job through a context and a server (device set-up, buffers)
-    small = min(jobs, key=lambda j: j.genome_bp * j.coverage)
-    warm = list(job_stream([small], procs=1))
-    run_alone(iter(warm), dev)
-    run_server([small], iter(warm), dev)
-    times, alone_dig, alone_s, bases = run_alone(stream(), dev)
-    closed = run_server(jobs, stream(), dev)
-    mean_bases = bases / len(jobs)
-    lam = load * max(closed["bases_per_s"], bases / alone_s) / mean_bases  # jobs/s
-    # the stream's Poisson arrival times (config4_jobs draws them at 1 job/s), rescaled
-    arrivals = {j.job_id: j.arrival_s / lam for j in jobs}
-    poisson = run_server(jobs, stream(), dev, arrivals)
+    big = max(jobs, key=lambda j: j.genome_bp * j.coverage)
+    warm = (list(job_stream([big], procs=1)) if not in_memory else [(big.job_id, data[big.job_id])])
+    with Hero(aligner="affine", device=dev) as h:
+        run_alone(iter(warm), h)
+        times, alone_dig, alone_s, bases = run_alone(stream(), h)
+    with HeroServer(aligner="affine", device=dev) as srv:
+        warm_server(srv, warm[0])
+        closed = run_server(srv, stream())
+        mean_bases = bases / len(jobs)
+        lam = load * max(closed["bases_per_s"], bases / alone_s) / mean_bases  # jobs/s
+        # the stream's Poisson arrival times (config4_jobs draws them at 1 job/s), rescaled
+        arrivals = {j.job_id: j.arrival_s / lam for j in jobs}
+        poisson = run_server(srv, stream(), arrivals)
     same = sum(int(poisson["_digests"][j] == alone_dig[j] and closed["_digests"][j] == alone_dig[j])
                for j in alone_dig)
     for r in (closed, poisson):
@@ -500,13 +511,16 @@ def serve_workload(jobs, dev: int, in_memory: bool, load: float = 0.95) -> dict:
         "busy_frac": poisson["busy_frac"], "rounds": poisson["rounds"],
         "mean_jobs_per_round": poisson["mean_jobs_per_round"],
         "overlapped_rounds": poisson["overlapped_rounds"],
+        "overlapped_device_phases": poisson["overlapped_device_phases"],
         "arrivals_late_s": poisson["arrivals_late_s"],
         "capacity_bases_per_s": closed["bases_per_s"],
         "capacity_mean_jobs_per_round": closed["mean_jobs_per_round"],
+        "capacity_worker_ms": closed["worker_ms"],
         "one_at_a_time_bases_per_s": bases / alone_s,
         "capacity_vs_one_at_a_time": closed["bases_per_s"] / (bases / alone_s),
         "alone_p50_ms": float(np.percentile([1e3 * t for t in times.values()], 50)),
         "served_equals_alone": f"{same}/{len(alone_dig)}",
+        "warm": "context and both workers first ran the stream's largest job",
     }
 
 

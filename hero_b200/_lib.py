@@ -31,7 +31,8 @@ EXPORTS = [
     "hero_server_set_dp_tuning", "hero_alignments_size", "hero_alignments_take",
     "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
     "hero_merge_pairs", "hero_get_overhang", "hero_mapping_histogram", "hero_set_vote_buffer",
-    "hero_consensus_range", "hero_server_set_round_policy",
+    "hero_consensus_range", "hero_server_set_round_policy", "hero_server_worker_stats",
+    "hero_server_workers", "hero_dp_tuning_check",
 ]
 
 # hero_params.flags: the alignment-output mode (HERO without -c); --merge
@@ -104,7 +105,8 @@ class ServerStats(C.Structure):
                 [("busy_ms", C.c_double), ("uptime_ms", C.c_double),
                  ("overlapped_rounds", C.c_uint64), ("ms_stage_in", C.c_double),
                  ("ms_round_calls", C.c_double), ("ms_stage_out", C.c_double),
-                 ("buffer_allocs", C.c_uint64), ("ms_alloc", C.c_double)])
+                 ("buffer_allocs", C.c_uint64), ("ms_alloc", C.c_double),
+                 ("overlapped_compute", C.c_uint64)])
 
 
 _lib = None
@@ -145,6 +147,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.hero_mapping_histogram.argtypes = [vp, vp, C.c_uint64, C.POINTER(C.c_uint64)]
     lib.hero_set_vote_buffer.argtypes = [vp, vp, C.c_uint64]
     lib.hero_server_set_round_policy.argtypes = [vp, C.c_uint64, C.c_uint64]
+    lib.hero_server_worker_stats.argtypes = [vp, C.c_int32, C.POINTER(HeroStats)]
+    lib.hero_server_workers.restype = C.c_int32
     lib.hero_consensus_range.argtypes = [vp, C.c_uint64, C.c_uint64] + [vp] * 7
     lib.hero_votes_words.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.hero_votes_save.argtypes = [vp, vp]
@@ -496,7 +500,10 @@ class HeroServer:
             arr[i] = DpTuning(int(t["rows_max"]), int(t["warps_per_block"]),
                               int(t["pair_strips"]), int(t["chunk_strips"]),
                               int(t.get("regs_per_thread", 0)))
-        self.lib.hero_server_set_dp_tuning(self.h, arr, len(classes))
+        rc = self.lib.hero_server_set_dp_tuning(self.h, arr, len(classes))
+        if rc != HERO_OK:
+            self.close()
+            raise HeroError(f"hero_server_set_dp_tuning: {ERRORS.get(rc, rc)} (a class the library refuses)")
 
     ROUND_BASES_DEFAULT = 8_000_000
     OVERLAP_BASES_DEFAULT = 64_000_000
@@ -570,6 +577,15 @@ class HeroServer:
         s = ServerStats()
         self.lib.hero_server_get_stats(self.h, C.byref(s))
         return {f: getattr(s, f) for f, _ in s._fields_}
+
+    def worker_stats(self) -> list[dict]:
+        """Each worker context's statistics as of its last round."""
+        out = []
+        for w in range(self.lib.hero_server_workers()):
+            s = HeroStats()
+            self.lib.hero_server_worker_stats(self.h, w, C.byref(s))
+            out.append({f: getattr(s, f) for f, _ in s._fields_})
+        return out
 
 
 def correct(reads, **kw):

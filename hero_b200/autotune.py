@@ -37,7 +37,10 @@ ROWS_LAST = 1023
 
 def candidates():
     # row-chunk walks for all strip counts or from three on (one-lane walks never won)
-    for warps, pair, chunk, regs in itertools.product((4, 2, 1), (0, ALL), (ALL, FROM3), (128, 168)):
+    # 255 registers (8 warps a SM) only with 1-warp blocks
+    for warps, pair, chunk, regs in itertools.product((4, 2, 1), (0, ALL), (ALL, FROM3), (128, 168, 255)):
+        if regs == 255 and warps != 1:
+            continue
         yield {"warps_per_block": warps, "pair_strips": pair, "chunk_strips": chunk,
                "regs_per_thread": regs}
 

@@ -221,7 +221,7 @@ static void apply_tuning(const hero_ctx *c, DpLaunch &a) {
     for (const hero_dp_tuning &t : c->tuning)
         if (a.rmax <= t.rows_max) {
             a.warps = (t.warps_per_block == 1 || t.warps_per_block == 2) ? t.warps_per_block : 4;
-            a.regs = t.regs_per_thread == 168 ? 168 : 128;
+            a.regs = (t.regs_per_thread == 168 || t.regs_per_thread == 255) ? t.regs_per_thread : 128;
             a.pair_mask = t.pair_strips;
             a.chunk_mask = t.chunk_strips;
             return;
@@ -405,14 +405,25 @@ extern "C" int hero_set_queries(hero_ctx *c, const uint8_t *seq, const uint64_t 
     return HERO_OK;
 }
 
-extern "C" int hero_set_dp_tuning(hero_ctx *c, const hero_dp_tuning *t, uint32_t n) {
-    if (!c) return HERO_E_INPUT;
-    if (n && !t) return c->fail(HERO_E_INPUT, "null tuning table");
+// the first fault of a tuning table, or nullptr
+static const char *dp_tuning_fault(const hero_dp_tuning *t, uint32_t n) {
+    if (n && !t) return "null tuning table";
     for (uint32_t i = 0; i < n; i++)
         if (t[i].warps_per_block != 1 && t[i].warps_per_block != 2 && t[i].warps_per_block != 4)
-            return c->fail(HERO_E_INPUT, "warps_per_block must be 1, 2 or 4");
-        else if (t[i].regs_per_thread != 0 && t[i].regs_per_thread != 128 && t[i].regs_per_thread != 168)
-            return c->fail(HERO_E_INPUT, "regs_per_thread must be 0, 128 or 168");
+            return "warps_per_block must be 1, 2 or 4";
+        else if (t[i].regs_per_thread != 0 && t[i].regs_per_thread != 128 && t[i].regs_per_thread != 168 &&
+                 !(t[i].regs_per_thread == 255 && t[i].warps_per_block == 1))
+            return "regs_per_thread must be 0, 128 or 168 (or 255 with 1-warp blocks)";
+    return nullptr;
+}
+
+extern "C" int hero_dp_tuning_check(const hero_dp_tuning *t, uint32_t n) {
+    return dp_tuning_fault(t, n) ? HERO_E_INPUT : HERO_OK;
+}
+
+extern "C" int hero_set_dp_tuning(hero_ctx *c, const hero_dp_tuning *t, uint32_t n) {
+    if (!c) return HERO_E_INPUT;
+    if (const char *f = dp_tuning_fault(t, n)) return c->fail(HERO_E_INPUT, f);
     c->tuning.assign(t, t + n);
     c->plan_ok = false;  // a captured round keeps the shapes it was captured with
     return HERO_OK;
@@ -1046,7 +1057,7 @@ extern "C" int hero_fetch(hero_ctx *c, uint8_t *seq_out, uint32_t *imin, uint32_
                           uint32_t *imax, double *mismatch_rate, double *gc_content,
                           uint8_t *good_out) {
     if (!c) return HERO_E_INPUT;
-    if (!c->plan_ok) return c->fail(HERO_E_STATE, "no round to fetch");
+    if (!c->consensus_done) return c->fail(HERO_E_STATE, "no consensus to fetch");
     cudaSetDevice(c->dev);
     const uint64_t n = c->nq, nb = c->nqb;
     if (seq_out && nb) cudaMemcpyAsync(seq_out, c->out_seq.p, nb, cudaMemcpyDeviceToHost, c->st);

@@ -865,10 +865,16 @@ __global__ void __launch_bounds__(kDpThreads) k_dp(DpLaunch a) {
 // warps per block of k_dp_wave: 4 (default) or 2; blocks per SM are set so that
 // every thread keeps 128 registers
 constexpr int kWaveWarps = 4;
-// warps per SM the register budget is set for: 16 (128 registers a thread) or,
-// for the wide shapes, 12 (168 registers: the affine pair rows spill less)
-constexpr int kWaveSmWarps(bool wide) { return wide ? 12 : 16; }
-constexpr int kWaveRegBlocks(int warps, bool wide) { return kWaveSmWarps(wide) / warps; }
+// warps per SM the register budget is set for, by register tier: 16 (128
+// registers a thread), 12 (168: the affine pair rows spill less) or 8 (up to
+// 255: no spills, at two warps a scheduler).  A scheduler's 16K registers are
+// shared by its warps, so 9-11 warps a SM allow no more than 12 do.
+constexpr int kWaveSmWarps(int tier) { return tier == 2 ? 8 : (tier == 1 ? 12 : 16); }
+constexpr int kWaveRegBlocks(int warps, int tier) {
+    return kWaveSmWarps(tier) / warps > 0 ? kWaveSmWarps(tier) / warps : 1;
+}
+// register tier of a regs_per_thread value (0 = the default 128)
+inline int wave_reg_tier(int32_t regs) { return regs > 168 ? 2 : (regs > 128 ? 1 : 0); }
 
 constexpr int kTaskQueue = 127;  // tasks[127]: next task to hand out
 
@@ -1295,8 +1301,8 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
                     uint32_t(G) * TS);
 }
 
-template <bool AFFINE, int WARPS, bool WIDE>
-__global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS, WIDE))
+template <bool AFFINE, int WARPS, int TIER>
+__global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS, TIER))
     k_dp_wave(DpLaunch a, uint64_t *tasks) {
     extern __shared__ int4 wave_smem[];
     const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
@@ -2248,23 +2254,25 @@ void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, i
     const size_t smem = wave_smem(a.rmax, a.tb_bytes, a.warps);
     // a persistent grid: twice the blocks that fit for registers (the work queue
     // stops the extra ones at once)
-    const bool wide = a.regs > 128;
-    const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps, wide));
+    const int tier = (a.warps == 1 || wave_reg_tier(a.regs) < 2) ? wave_reg_tier(a.regs) : 1;
+    const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps, tier));
     // the opt-in is set once per size increase (never while a graph is being captured
     // for a size not seen before: the eager round that precedes a capture sets it)
     // (per device, and shared by the host threads of every context in the process)
     constexpr int kOptDevices = 64;
     static std::mutex opt_mu;
-    static size_t opted[kOptDevices][2][3][2] = {};
-    const int ai = a.affine ? 1 : 0, wi = a.warps == 1 ? 0 : (a.warps == 2 ? 1 : 2), ri = wide ? 1 : 0;
+    static size_t opted[kOptDevices][2][3][3] = {};
+    const int ai = a.affine ? 1 : 0, wi = a.warps == 1 ? 0 : (a.warps == 2 ? 1 : 2), ri = tier;
     using WaveFn = void (*)(DpLaunch, uint64_t *);
-    const WaveFn fns[2][3][2] = {
-        {{k_dp_wave<false, 1, false>, k_dp_wave<false, 1, true>},
-         {k_dp_wave<false, 2, false>, k_dp_wave<false, 2, true>},
-         {k_dp_wave<false, 4, false>, k_dp_wave<false, 4, true>}},
-        {{k_dp_wave<true, 1, false>, k_dp_wave<true, 1, true>},
-         {k_dp_wave<true, 2, false>, k_dp_wave<true, 2, true>},
-         {k_dp_wave<true, 4, false>, k_dp_wave<true, 4, true>}}};
+    // the 255-register tier is built for 1-warp blocks only (the tuning
+    // table refuses it with larger blocks); their slots take tier 1
+    const WaveFn fns[2][3][3] = {
+        {{k_dp_wave<false, 1, 0>, k_dp_wave<false, 1, 1>, k_dp_wave<false, 1, 2>},
+         {k_dp_wave<false, 2, 0>, k_dp_wave<false, 2, 1>, k_dp_wave<false, 2, 1>},
+         {k_dp_wave<false, 4, 0>, k_dp_wave<false, 4, 1>, k_dp_wave<false, 4, 1>}},
+        {{k_dp_wave<true, 1, 0>, k_dp_wave<true, 1, 1>, k_dp_wave<true, 1, 2>},
+         {k_dp_wave<true, 2, 0>, k_dp_wave<true, 2, 1>, k_dp_wave<true, 2, 1>},
+         {k_dp_wave<true, 4, 0>, k_dp_wave<true, 4, 1>, k_dp_wave<true, 4, 1>}}};
     const WaveFn fn = fns[ai][wi][ri];
     if (smem > 48u * 1024u) {
         std::lock_guard<std::mutex> lock(opt_mu);

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -29,6 +30,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <sys/mman.h>
+
 #include <cuda_runtime.h>
 
 #include "../../include/hero_gpu.h"
@@ -38,17 +41,59 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 // Host array left uninitialised (results are written over it by the device
-// copy; zero-filling GBs first would cost as much as the copy).
+// copy; zero-filling GBs first would cost as much as the copy).  Arrays of 2 MB
+// and more sit on 2 MB-aligned memory advised for huge pages: the first touch
+// of a GB-sized array -- the driver's copy of a round's results, a job's reads
+// copied in at submission -- then takes 512x fewer page faults.
 template <class T>
 struct HostArray {
-    std::unique_ptr<T[]> p;
+    static constexpr size_t kHuge = size_t(2) << 20;
+    T *p = nullptr;
     size_t n = 0;
-    bool alloc(size_t k) {
-        p.reset(k ? new (std::nothrow) T[k] : nullptr);
-        n = p ? k : 0;
-        return p || !k;
+    HostArray() = default;
+    HostArray(const HostArray &) = delete;
+    HostArray &operator=(const HostArray &) = delete;
+    HostArray(HostArray &&o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
     }
-    T *data() const { return p.get(); }
+    HostArray &operator=(HostArray &&o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    ~HostArray() { release(); }
+    void release() {
+        std::free(p);
+        p = nullptr;
+        n = 0;
+    }
+    bool alloc(size_t k) {
+        release();
+        if (!k) return true;
+        const size_t b = k * sizeof(T);
+        void *q = nullptr;
+        if (b >= kHuge) {
+            const size_t rb = (b + kHuge - 1) & ~(kHuge - 1);
+            if (posix_memalign(&q, kHuge, rb) != 0) return false;
+            madvise(q, rb, MADV_HUGEPAGE);  // advice only: without it the array still works
+        } else if (!(q = std::malloc(b))) {
+            return false;
+        }
+        p = static_cast<T *>(q);
+        n = k;
+        return true;
+    }
+    size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+    T *data() const { return p; }
+    T &operator[](size_t i) const { return p[i]; }
+    T back() const { return p[n - 1]; }
 };
 
 // One round's results, shared by its jobs: each job reads its own slice, so a
@@ -63,9 +108,10 @@ struct Job {
     uint64_t id = 0;
     int32_t state = HERO_JOB_QUEUED, status = HERO_OK;
     std::string err;
-    std::vector<uint8_t> seq;
-    std::vector<uint64_t> off;
-    std::vector<int64_t> uid;
+    HostArray<uint8_t> seq;   // freed when the job's round ends
+    HostArray<uint64_t> off;
+    HostArray<int64_t> uid;
+    uint64_t bases = 0;
     uint64_t bytes = 0;  // admission estimate
     // results: a slice of the round's output (reads [out_read, +n), bases [out_base, +bases))
     std::shared_ptr<const RoundOut> out;
@@ -135,10 +181,26 @@ struct hero_server {
     uint64_t round_bases_max = kRoundBasesDefault;      // bases a round admits beyond its first job
     uint64_t overlap_bases_max = kOverlapBasesDefault;  // a round starts beside another only if one is this small
     uint64_t running_bases[kServeWorkers] = {};         // bases of each worker's round in flight
+    uint64_t computing[kServeWorkers] = {};             // bases of each worker's round in its device phase
+    uint64_t overlapped_compute = 0;                    // device phases started beside another
+    std::condition_variable cv_gate;
     double ms_stage_in = 0, ms_round_calls = 0, ms_stage_out = 0;  // worker wall time, all rounds
-    uint64_t allocs[kServeWorkers] = {};  // buffer growth of each worker's context
-    double ms_alloc[kServeWorkers] = {};
+    hero_stats ctx_stats[kServeWorkers] = {};  // each worker context's statistics after its last round
 
+    // The device phase of a round (index, seeding, alignment, votes, consensus)
+    // may start beside another only if one of the two rounds is within the
+    // overlap limit and the other above it: two small rounds or two large ones
+    // run their device phases one after the other (side by side they only share
+    // the SMs and the L2, and lose against running in turn), while a small round
+    // beside a large one is not held up for the whole large round.  Uploads and
+    // downloads are outside the gate: they overlap the other round's device phase.
+    bool may_compute(int w, uint64_t bases) const {
+        for (int v = 0; v < kServeWorkers; v++) {
+            if (v == w || !computing[v] || !overlap_bases_max) continue;
+            if ((bases <= overlap_bases_max) == (computing[v] <= overlap_bases_max)) return false;
+        }
+        return true;
+    }
     bool large_running() const {  // a round above the overlap limit is in flight
         for (int v = 0; v < kServeWorkers; v++)
             if (running_bases[v] > overlap_bases_max) return true;
@@ -197,7 +259,7 @@ void hero_server::run(int w) {
             if (exclusive) return false;
             const Job &head = jobs[queue.front()];
             if (in_flight_bytes + head.bytes > round_bytes) return false;
-            return !overlap_bases_max || head.seq.size() <= overlap_bases_max || !large_running();
+            return true;
         };
         cv_work.wait(lk, [&] { return stop || admissible(); });
         if (stop) break;
@@ -215,7 +277,7 @@ void hero_server::run(int w) {
             uint64_t nb = 0, t = 0;
             for (uint64_t id : queue) {
                 if (t >= take) break;
-                const uint64_t jb = jobs[id].seq.size();
+                const uint64_t jb = jobs[id].bases;
                 if (t > 0 && nb + jb > cap_bases) break;
                 nb += jb;
                 t++;
@@ -231,7 +293,7 @@ void hero_server::run(int w) {
             jobs[id].state = HERO_JOB_RUNNING;
             jobs[id].start_ms = t;
             bytes += jobs[id].bytes;
-            bases += jobs[id].seq.size();
+            bases += jobs[id].bases;
         }
         round_begin(bytes);
         running_bases[w] = bases;
@@ -295,7 +357,7 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
     uint64_t n = 0, nb = 0;
     for (Job *j : js) {
         n += j->n();
-        nb += j->seq.size();
+        nb += j->bases;
     }
     // one job: its own buffers go up as they are; several: concatenated
     // (reads | offsets | ids | job tags), each read carrying its job
@@ -316,14 +378,14 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
         cat_off.p[0] = 0;
         for (size_t t = 0; t < js.size(); t++) {
             const Job &j = *js[t];
-            copy_parallel(cat_seq.data() + b, j.seq.data(), j.seq.size());
+            copy_parallel(cat_seq.data() + b, j.seq.data(), j.bases);
             for (uint64_t i = 0; i < j.n(); i++) {
                 cat_off.p[r + i + 1] = b + j.off[i + 1];
                 cat_uid.p[r + i] = j.uid[i];
                 cat_tag.p[r + i] = uint32_t(t);
             }
             r += j.n();
-            b += j.seq.size();
+            b += j.bases;
         }
         seq = cat_seq.data();
         off = cat_off.data();
@@ -335,11 +397,30 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
     const double t_calls = now_ms();
     int st = host_ok ? hero_set_queries(ctx, seq, off, uid, n) : HERO_E_OOM;
     if (st == HERO_OK && js.size() > 1) st = hero_set_query_jobs(ctx, cat_tag.data(), n);
-    if (st == HERO_OK) st = hero_build_index(ctx);
-    if (st == HERO_OK) st = hero_align_self(ctx);
+    if (st == HERO_OK) {
+        {  // the device phase, through the gate
+            std::unique_lock<std::mutex> lk(mu);
+            cv_gate.wait(lk, [&] { return may_compute(w, nb); });
+            for (int v = 0; v < kServeWorkers; v++)
+                if (v != w && computing[v]) {
+                    overlapped_compute++;
+                    break;
+                }
+            computing[w] = nb;
+        }
+        st = hero_build_index(ctx);
+        if (st == HERO_OK) st = hero_align_self(ctx);
+        // results stay on the device until the fetch below, outside the gate
+        if (st == HERO_OK) st = hero_consensus(ctx, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        {
+            std::lock_guard<std::mutex> g(mu);
+            computing[w] = 0;
+        }
+        cv_gate.notify_all();
+    }
     if (st == HERO_OK)
-        st = hero_consensus(ctx, out->seq.data(), out->imin.data(), out->imed.data(),
-                            out->imax.data(), out->mis.data(), out->gc.data(), out->good.data());
+        st = hero_fetch(ctx, out->seq.data(), out->imin.data(), out->imed.data(), out->imax.data(),
+                        out->mis.data(), out->gc.data(), out->good.data());
     const double t_out = now_ms();
     const std::string err = st == HERO_OK ? std::string()
                             : host_ok ? std::string(hero_last_error(ctx))
@@ -351,17 +432,14 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
             j->out_read = r;
             j->out_base = b;
             r += j->n();
-            b += j->seq.size();
+            b += j->bases;
         }
     }
     hero_stats cs{};
     const bool have_cs = hero_get_stats(ctx, &cs) == HERO_OK;
     const double t_done = now_ms();
     std::lock_guard<std::mutex> g(mu);
-    if (have_cs) {
-        allocs[w] = cs.buffer_allocs;
-        ms_alloc[w] = cs.ms_alloc;
-    }
+    if (have_cs) ctx_stats[w] = cs;
     ms_stage_in += t_calls - t_in;
     ms_round_calls += t_out - t_calls;
     ms_stage_out += t_done - t_out;
@@ -382,7 +460,7 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
     const double t_end = now_ms();
     round_end(round_est);
     for (Job *j : js) {
-        const uint64_t jb = j->seq.size();
+        const uint64_t jb = j->bases;
         j->round = rounds;
         j->round_jobs = uint32_t(js.size());
         j->done_ms = t_end;
@@ -396,8 +474,8 @@ void hero_server::run_round(int w, std::vector<uint64_t> ids, uint64_t round_est
             j->state = HERO_JOB_FAILED;
             failed++;
         }
-        // inputs are no longer needed
-        std::vector<uint8_t>().swap(j->seq);
+        // the reads are no longer needed (offsets and ids stay for the job's info)
+        j->seq.release();
     }
 }
 
@@ -469,11 +547,7 @@ extern "C" int hero_server_set_round_policy(hero_server *s, uint64_t round_bases
 }
 
 extern "C" int hero_server_set_dp_tuning(hero_server *s, const hero_dp_tuning *t, uint32_t n) {
-    if (!s || (n && !t)) return HERO_E_INPUT;
-    for (uint32_t i = 0; i < n; i++)
-        if ((t[i].warps_per_block != 1 && t[i].warps_per_block != 2 && t[i].warps_per_block != 4) ||
-            (t[i].regs_per_thread != 0 && t[i].regs_per_thread != 128 && t[i].regs_per_thread != 168))
-            return HERO_E_INPUT;
+    if (!s || hero_dp_tuning_check(t, n) != HERO_OK) return HERO_E_INPUT;
     std::lock_guard<std::mutex> g(s->mu);
     s->tuning.assign(t, t + n);
     s->tuning_gen++;
@@ -488,10 +562,15 @@ extern "C" int hero_job_submit(hero_server *s, const uint8_t *seq, const uint64_
         if (off[i + 1] < off[i] || off[i + 1] - off[i] > 32767) return HERO_E_INPUT;
     Job j;
     const uint64_t nb = n ? off[n] : 0;
-    j.seq.assign(seq, seq + nb);
-    j.off.assign(off, off + n + 1);
-    if (!n) j.off.assign(1, 0);
-    j.uid.assign(uid, uid + n);
+    if (!j.seq.alloc(nb) || !j.off.alloc(n + 1) || !j.uid.alloc(n)) return HERO_E_OOM;
+    copy_parallel(j.seq.data(), seq, nb);
+    if (n) {
+        copy_parallel(j.off.data(), off, (n + 1) * sizeof(uint64_t));
+        copy_parallel(j.uid.data(), uid, n * sizeof(int64_t));
+    } else {
+        j.off[0] = 0;
+    }
+    j.bases = nb;
     j.bytes = hero_job_bytes(nb, n, s->p.k);
     std::lock_guard<std::mutex> g(s->mu);
     if (s->stop) return HERO_E_STATE;
@@ -626,14 +705,25 @@ extern "C" int hero_server_get_stats(hero_server *s, hero_server_stats *out) {
     out->busy_ms = s->busy_ms + (s->in_flight ? s->now_ms() - s->busy_since : 0.0);
     out->uptime_ms = s->now_ms();
     out->overlapped_rounds = s->overlapped_rounds;
+    out->overlapped_compute = s->overlapped_compute;
     out->ms_stage_in = s->ms_stage_in;
     out->ms_round_calls = s->ms_round_calls;
     out->ms_stage_out = s->ms_stage_out;
     out->buffer_allocs = 0;
     out->ms_alloc = 0;
     for (int w = 0; w < kServeWorkers; w++) {
-        out->buffer_allocs += s->allocs[w];
-        out->ms_alloc += s->ms_alloc[w];
+        out->buffer_allocs += s->ctx_stats[w].buffer_allocs;
+        out->ms_alloc += s->ctx_stats[w].ms_alloc;
     }
     return HERO_OK;
 }
+
+extern "C" int hero_server_worker_stats(hero_server *s, int32_t worker, hero_stats *out) {
+    if (!s || !out || worker < 0) return HERO_E_INPUT;
+    if (worker >= kServeWorkers) return HERO_E_INPUT;
+    std::lock_guard<std::mutex> g(s->mu);
+    *out = s->ctx_stats[worker];
+    return HERO_OK;
+}
+
+extern "C" int32_t hero_server_workers(void) { return kServeWorkers; }

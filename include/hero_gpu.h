@@ -207,7 +207,8 @@ int hero_consensus(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *im
 #define HERO_ROUND_GRAPH 1u
 int hero_round(hero_ctx *ctx, uint32_t flags);
 
-/* Results of the last round (same outputs as hero_consensus). */
+/* Results of the last round, or of the last hero_consensus (whose NULL outputs
+ * stay on the device until fetched here); same outputs as hero_consensus. */
 int hero_fetch(hero_ctx *ctx, uint8_t *seq_out, uint32_t *imin, uint32_t *imed, uint32_t *imax,
                double *mismatch_rate, double *gc_content, uint8_t *good_out);
 
@@ -245,11 +246,15 @@ typedef struct {
     int32_t warps_per_block;   /* 1, 2 or 4 */
     uint32_t pair_strips;      /* bit n: n-strip segments run as 16-bit pairs */
     uint32_t chunk_strips;     /* bit n: n-strip tracebacks walk in row chunks */
-    int32_t regs_per_thread;   /* 0 or 128 (16 warps an SM), or 168 (12 warps, fewer spills) */
+    int32_t regs_per_thread;   /* 0 or 128 (16 warps an SM), 168 (12 warps, fewer spills),
+                                  or 255 with 1-warp blocks (8 warps, no spills) */
 } hero_dp_tuning;
 
 /* Replaces the context's tuning table (n = 0 clears it). */
 int hero_set_dp_tuning(hero_ctx *ctx, const hero_dp_tuning *t, uint32_t n);
+/* Checks a tuning table the way hero_set_dp_tuning and
+ * hero_server_set_dp_tuning do (HERO_OK or HERO_E_INPUT), without a context. */
+int hero_dp_tuning_check(const hero_dp_tuning *t, uint32_t n);
 
 /* Aligns an explicit list of DP segments on the device (test and tooling entry
  * point).  subj/query: concatenated reads (same layout as above); per segment
@@ -345,10 +350,12 @@ typedef struct {
     double ms_stage_in, ms_round_calls, ms_stage_out;
     uint64_t buffer_allocs;      /* device buffers the workers' contexts have grown */
     double ms_alloc;             /* host time the workers spent growing them */
+    uint64_t overlapped_compute; /* rounds whose device phase started beside another's */
 } hero_server_stats;
 
 /* A server owns two contexts on p->device, each with its own stream and worker
- * thread (continuous batching with overlapping rounds).  A free worker admits
+ * thread (continuous batching with overlapping rounds: one round's upload and
+ * download run while the other round is on the device).  A free worker admits
  * the oldest queued jobs whose estimated device memory (hero_job_bytes) fits in
  * what the rounds in flight leave of round_bytes (0 = p->device_memory_budget,
  * or 80 % of the device's free memory at creation, minus each worker's
@@ -377,17 +384,21 @@ const char *hero_job_error(hero_server *s, uint64_t job_id);
 /* Frees a finished job's results. */
 int hero_job_release(hero_server *s, uint64_t job_id);
 int hero_server_get_stats(hero_server *s, hero_server_stats *out);
+/* Statistics of one worker's context (0 <= worker < hero_server_workers()),
+ * as of the end of its last round: where the workers' time went, per stage. */
+int hero_server_worker_stats(hero_server *s, int32_t worker, hero_stats *out);
+int32_t hero_server_workers(void);
 
 /* Round policy.  round_bases_max: the most bases a round admits beyond its
- * first job (0: as many as fit the memory budget).  overlap_bases_max: a round
- * starts while another runs only if one of the two has at most this many
- * bases, and a round admitted beside a larger one stays within it (0: rounds
- * always overlap).  A round's device work is the same whether its jobs run
- * together or apart; what serving gains is the host side of one round (upload,
- * download, buffer growth) hidden behind the device work of the other, while
- * two large rounds side by side only share the SMs and the L2.  Defaults:
- * 8,000,000 and 64,000,000, measured best on streams of small (0.2-30 Mbp)
- * and large (10 Mbp-1.6 Gbp) jobs. */
+ * first job (0: as many as fit the memory budget).  overlap_bases_max: the
+ * device phase of a round (index to consensus) starts beside another round's
+ * only if one of the two has at most this many bases and the other more, and a
+ * round admitted beside a larger one stays within it; two small rounds, or two
+ * large ones, take the device in turn (0: device phases always overlap; 1: they
+ * never do).  Uploads and downloads are not held: they overlap the other
+ * round's device phase.  A round's device work is the same whether its jobs
+ * run together or apart; side by side, two rounds only share the SMs and the
+ * L2.  Defaults: 8,000,000 and 64,000,000. */
 int hero_server_set_round_policy(hero_server *s, uint64_t round_bases_max,
                                  uint64_t overlap_bases_max);
 /* DP kernel shapes (hero_set_dp_tuning) for the rounds the server runs next. */

@@ -118,7 +118,7 @@ def test_a_shared_round_outlives_the_release_of_its_other_jobs():
 @pytest.mark.gpu
 def test_round_policy_one_job_a_round_and_no_overlap():
     """round_bases_max=1 admits no job beside a round's first; overlap_bases_max=1
-    starts no round while another (of more than one base) runs."""
+    starts no round's device phase while another's (of more than one base) runs."""
     from hero_b200 import HeroServer, correct
     jobs = _jobs()
     alone = [correct(rs, aligner="affine") for rs in jobs]
@@ -131,7 +131,7 @@ def test_round_policy_one_job_a_round_and_no_overlap():
         s1 = srv.stats()
     assert all(i["round_jobs"] == 1 for i in infos)
     assert s1["rounds"] - s0["rounds"] == len(jobs)
-    assert s1["overlapped_rounds"] == s0["overlapped_rounds"]
+    assert s1["overlapped_compute"] == s0["overlapped_compute"]
     for k, (a, b) in enumerate(zip(alone, got)):
         _same(a, b, k)
 
