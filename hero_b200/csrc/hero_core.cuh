@@ -1562,54 +1562,82 @@ HERO_HD int32_t popc32(uint32_t x) {
 #endif
 }
 
-HERO_HD void ops_summary(const uint32_t *w, uint32_t first, uint32_t P, DpSum &sum) {
+// index of the lowest / highest set bit of x != 0
+HERO_HD int32_t low_bit(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return __ffs(int(x)) - 1;
+#else
+    return __builtin_ctz(x);
+#endif
+}
+HERO_HD int32_t high_bit(uint32_t x) {
+#if defined(__CUDA_ARCH__)
+    return 31 - __clz(int(x));
+#else
+    return 31 - __builtin_clz(x);
+#endif
+}
+
+// What the words k0 + s, k0 + s + G, ... of an op range [first, first + P)
+// contribute to its DpSum: op counts of kinds 1..3, the first field that
+// differs from the range's first op (fpos, ~0u: none) and one past the last
+// field that differs from its last op (lpos, 0: none).  Parts of disjoint word
+// sets merge (ops_part_merge), so G lanes can each take every G-th word.
+struct OpsPart {
+    int32_t c1, c2, c3;
+    uint32_t fpos, lpos;
+};
+
+HERO_HD OpsPart ops_part(const uint32_t *w, uint32_t first, uint32_t P, uint32_t s, uint32_t G) {
+    OpsPart r{0, 0, 0, ~0u, 0u};
+    if (P == 0) return r;
     const uint32_t end = first + P, k0 = first >> 4, k1 = (end - 1) >> 4;
-    int32_t c1 = 0, c2 = 0, c3 = 0;
-    for (uint32_t k = k0; k <= k1; k++) {
+    const uint32_t f = ops_field(w, first) * 0x55555555u, l = ops_field(w, end - 1) * 0x55555555u;
+    for (uint32_t k = k0 + s; k <= k1; k += G) {
         const uint32_t m = ops_mask(k == k0 ? (first & 15) : 0, k == k1 ? ((end - 1) & 15) : 15);
         const uint32_t x = w[k], xl = x & 0x55555555u, xh = (x >> 1) & 0x55555555u;
-        c1 += popc32(xl & ~xh & m);
-        c2 += popc32(xh & ~xl & m);
-        c3 += popc32(xl & xh & m);
+        r.c1 += popc32(xl & ~xh & m);
+        r.c2 += popc32(xh & ~xl & m);
+        r.c3 += popc32(xl & xh & m);
+        const uint32_t yf = x ^ f, zf = (yf | (yf >> 1)) & m;
+        if (zf && r.fpos == ~0u) r.fpos = (k << 4) + uint32_t(low_bit(zf) >> 1);  // words rise: the first is the least
+        const uint32_t yl = x ^ l, zl = (yl | (yl >> 1)) & m;
+        if (zl) r.lpos = (k << 4) + uint32_t(high_bit(zl) >> 1) + 1u;  // the last is the greatest
     }
-    sum.tot[0] = uint16_t(int32_t(P) - c1 - c2 - c3);
-    sum.tot[1] = uint16_t(c1);
-    sum.tot[2] = uint16_t(c2);
-    sum.tot[3] = uint16_t(c3);
-    // first run: fields equal to the first op, from `first` on
-    const uint32_t f = ops_field(w, first);
-    uint32_t fc = P;
-    for (uint32_t k = k0; k <= k1; k++) {
-        const uint32_t m = ops_mask(k == k0 ? (first & 15) : 0, k == k1 ? ((end - 1) & 15) : 15);
-        const uint32_t y = w[k] ^ (f * 0x55555555u);
-        const uint32_t z = (y | (y >> 1)) & m;
-        if (z) {
-            int32_t bit = 0;
-            while (!((z >> bit) & 1u)) bit++;
-            fc = (k << 4) + uint32_t(bit >> 1) - first;
-            break;
-        }
-    }
-    // last run: fields equal to the last op, backwards from end - 1
-    const uint32_t l = ops_field(w, end - 1);
-    uint32_t lc = P;
-    for (uint32_t k = k1 + 1; k-- > k0;) {
-        const uint32_t m = ops_mask(k == k0 ? (first & 15) : 0, k == k1 ? ((end - 1) & 15) : 15);
-        const uint32_t y = w[k] ^ (l * 0x55555555u);
-        const uint32_t z = (y | (y >> 1)) & m;
-        if (z) {
-            int32_t bit = 31;
-            while (!((z >> bit) & 1u)) bit--;
-            lc = end - 1 - ((k << 4) + uint32_t(bit >> 1));
-            break;
-        }
-    }
-    sum.ft = uint8_t(f);
+    return r;
+}
+
+HERO_HD OpsPart ops_part_merge(OpsPart a, const OpsPart &b) {
+    a.c1 += b.c1;
+    a.c2 += b.c2;
+    a.c3 += b.c3;
+    a.fpos = b.fpos < a.fpos ? b.fpos : a.fpos;
+    a.lpos = b.lpos > a.lpos ? b.lpos : a.lpos;
+    return a;
+}
+
+// the DpSum of the range from the merged part of all its words
+HERO_HD void ops_part_sum(const OpsPart &p, const uint32_t *w, uint32_t first, uint32_t P,
+                          DpSum &sum) {
+    const uint32_t end = first + P;
+    sum.tot[0] = uint16_t(int32_t(P) - p.c1 - p.c2 - p.c3);
+    sum.tot[1] = uint16_t(p.c1);
+    sum.tot[2] = uint16_t(p.c2);
+    sum.tot[3] = uint16_t(p.c3);
+    // first run: fields equal to the first op, from `first` on; last run:
+    // fields equal to the last op, backwards from end - 1
+    const uint32_t fc = p.fpos == ~0u ? P : p.fpos - first;
+    const uint32_t lc = p.lpos == 0u ? P : end - p.lpos;
+    sum.ft = uint8_t(P ? ops_field(w, first) : 0u);
     sum.fc = uint16_t(fc);
-    sum.lt = uint8_t(l);
+    sum.lt = uint8_t(P ? ops_field(w, end - 1) : 0u);
     sum.lc = uint16_t(lc);
     sum.nruns = fc == P ? 1 : 2;
     sum.pad = 0;
+}
+
+HERO_HD void ops_summary(const uint32_t *w, uint32_t first, uint32_t P, DpSum &sum) {
+    ops_part_sum(ops_part(w, first, P, 0, 1), w, first, P, sum);
 }
 
 // walk + per-op run tracking, for callers that emit ops one by one

@@ -950,6 +950,40 @@ int emu_merge_pair(const uint8_t *left, int32_t lenL, const uint8_t *right, int3
                           reinterpret_cast<char *>(out)));
 }
 
+// ops_summary of the packed op range [first, first + P) of w against the
+// fields read one by one (-1 when they differ), then against the parts of G
+// lanes (each taking every G-th word) merged as the kernel's shuffle tree
+// merges them, for G = 1..32 (the first G that differs, 0 when none does)
+int32_t emu_ops_summary_groups(const uint32_t *w, uint32_t first, uint32_t P) {
+    DpSum ref;
+    ops_summary(w, first, P, ref);
+    {
+        auto field = [&](uint32_t p) { return (w[p >> 4] >> (2 * (p & 15))) & 3u; };
+        uint32_t tot[4] = {0, 0, 0, 0};
+        for (uint32_t q = first; q < first + P; q++) tot[field(q)]++;
+        const uint32_t ft = field(first), lt = field(first + P - 1);
+        uint32_t fc = 0, lc = 0;
+        while (fc < P && field(first + fc) == ft) fc++;
+        while (lc < P && field(first + P - 1 - lc) == lt) lc++;
+        for (int k = 0; k < 4; k++)
+            if (ref.tot[k] != tot[k]) return -1;
+        if (ref.ft != ft || ref.fc != fc || ref.lt != lt || ref.lc != lc || ref.nruns != (fc == P ? 1 : 2))
+            return -1;
+    }
+    for (uint32_t G = 1; G <= 32; G++) {
+        std::vector<OpsPart> part(G);
+        for (uint32_t s = 0; s < G; s++) part[s] = ops_part(w, first, P, s, G);
+        for (uint32_t d = 1; d < G; d <<= 1) {
+            const std::vector<OpsPart> old = part;  // a shuffle reads every lane's value before the step
+            for (uint32_t s = 0; s + d < G; s++) part[s] = ops_part_merge(old[s], old[s + d]);
+        }
+        DpSum got;
+        ops_part_sum(part[0], w, first, P, got);
+        if (std::memcmp(&got, &ref, sizeof(DpSum)) != 0) return int32_t(G);
+    }
+    return 0;
+}
+
 // RecState over the same events: runs through add, the steps of each DP piece
 // packed as the kernel packs ops (2 bits each, at the end of the words) and
 // summarised by ops_summary for add_piece

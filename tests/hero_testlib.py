@@ -209,6 +209,8 @@ class Emu:
         lib.emu_record_text.restype = C.c_int32
         lib.emu_key_positions.argtypes = [C.c_int64, C.c_int64, vp]
         lib.emu_key_positions.restype = C.c_int32
+        lib.emu_ops_summary_groups.argtypes = [vp, C.c_uint32, C.c_uint32]
+        lib.emu_ops_summary_groups.restype = C.c_int32
         self.lib = lib
 
     def merge(self, reads, k=39, min_overlap=40, aligner="global", max_mismatch_rate=1.0,

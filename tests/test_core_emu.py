@@ -213,3 +213,30 @@ def test_emulated_merge_matches_reference(oracle, emu, name):
     merged, unmerged = format_merged(rs.names, got["merged_seq"], rs.off, got["merged_len"])
     assert hashlib.md5(merged).hexdigest() == m["merged_fasta_md5"]
     assert hashlib.md5(unmerged).hexdigest() == m["unmerged_fasta_md5"]
+
+
+def test_ops_summary_by_lane_groups(emu):
+    """The DP summary of a packed op range: against the fields read one by one,
+    and as the parts of G lanes (every G-th word each) merged by the kernel's
+    shuffle tree, for every G from 1 to 32."""
+    import numpy as np
+    rng = np.random.default_rng(17)
+    for trial in range(400):
+        words = int(rng.integers(1, 40))
+        kind = trial % 4
+        if kind == 0:    # uniform random ops
+            w = rng.integers(0, 2**32, size=words, dtype=np.uint64).astype(np.uint32)
+        else:            # long runs of one op, a few others
+            ops = np.full(words * 16, int(rng.integers(0, 4)), np.uint32)
+            for _ in range(int(rng.integers(0, 4))):
+                a = int(rng.integers(0, words * 16))
+                ops[a:a + int(rng.integers(1, 20))] = int(rng.integers(0, 4))
+            w = np.zeros(words, np.uint32)
+            for p in range(words * 16):
+                w[p >> 4] |= np.uint32(ops[p] << (2 * (p & 15)))
+        total = words * 16
+        P = int(rng.integers(1, total + 1))
+        first = int(rng.integers(0, total - P + 1)) if trial % 3 else total - P  # kernel: ranges end at the last word
+        w = np.ascontiguousarray(w)
+        r = emu.lib.emu_ops_summary_groups(w.ctypes.data, first, P)
+        assert r == 0, (trial, words, first, P, r)
