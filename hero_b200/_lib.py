@@ -70,7 +70,8 @@ class HeroStats(C.Structure):
     _fields_ = ([(f, C.c_uint64) for f in _STAT_FIELDS] + [(f, C.c_double) for f in _STAT_MS] +
                 [("graph_rounds", C.c_uint64), ("dp_cells_computed", C.c_uint64),
                  ("dp_rows_max", C.c_uint64), ("dp_cells_pairs", C.c_uint64),
-                 ("buffer_allocs", C.c_uint64), ("ms_alloc", C.c_double)])
+                 ("buffer_allocs", C.c_uint64), ("ms_alloc", C.c_double),
+                 ("dp_tasks_staged", C.c_uint64), ("dp_stage_timeouts", C.c_uint64)])
 
 
 class DpTuning(C.Structure):

@@ -318,7 +318,9 @@ static int upload_reads(hero_ctx *c, const uint8_t *seq, const uint64_t *off, co
                         DBuf *gq, DBuf *gs, DBuf *gc) {
     const uint64_t nb = n ? off[n] : 0;
     HERO_TRY(c->ensure(raw, nb, "reads"));
-    HERO_TRY(c->ensure(code, nb, "codes"));
+    // 16 bytes past the last base: the DP's bulk copies of a segment's rows
+    // round their end up to 16 bytes
+    HERO_TRY(c->ensure(code, nb + 16, "codes"));
     HERO_TRY(c->ensure(doff, (n + 1) * 8, "offsets"));
     HERO_TRY(c->ensure(len, n * 4, "lengths"));
     HERO_TRY(c->ensure(duid, n * 8, "ids"));
@@ -687,6 +689,7 @@ static int align_batch(hero_ctx *c, ReadsView subj, uint64_t nsub, uint64_t nbas
                    P_<uint32_t>(c->cells), P_<uint16_t>(c->tb), P_<int32_t>(c->bnd), c->dp_T, rmax,
                    c->p.affine, 1,  // reads with a non-ACGT base never reach the DP
                    0u, 0u, kStripsAll, 4, ctr + C_CELLS_PAIR};
+        a.staged = ctr + C_STAGED;
         apply_tuning(c, a);
         launch_dp(a, P_<uint64_t>(c->bin_off), P_<uint64_t>(c->dp_tasks), cmax, c->st);
         if ((r = c->check_launch("dp"))) break;
@@ -1185,6 +1188,8 @@ extern "C" int hero_get_stats(hero_ctx *c, hero_stats *out) {
     s.dp_cells = c->ctr[C_CELLS];
     s.dp_cells_computed = c->ctr[C_CELLS_ALL];
     s.dp_cells_pairs = c->ctr[C_CELLS_PAIR];
+    s.dp_tasks_staged = c->ctr[C_STAGED];
+    s.dp_stage_timeouts = c->ctr[C_STAGE_FAIL];
     s.dp_rows_max = c->ctr[C_MAXR];
     s.vote_anomalies = c->ctr[C_ANOMALY];
     s.device_bytes_peak = c->bytes_peak;

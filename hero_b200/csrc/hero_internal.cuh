@@ -78,6 +78,8 @@ enum Counter : int {
     C_WIN,          // winners of the current batch (compacted list length)
     C_OVERFLOW_ALL, // overflows over the context's life (C_OVERFLOW is cleared per batch)
     C_CELLS_PAIR,   // band cells computed in 16-bit pairs (of C_CELLS_ALL's)
+    C_STAGED,       // wavefront tasks whose row bases were staged by the bulk copy engine
+    C_STAGE_FAIL,   // staging waits that ran out (the rows were read from global memory)
     C_COUNT
 };
 
@@ -173,6 +175,7 @@ struct DpLaunch {
     int32_t warps;          // warps per block of the wavefront kernel (1, 2 or 4)
     unsigned long long *pair_cells;  // += band cells of the segments run as 16-bit pairs (may be NULL)
     int32_t regs;           // registers a thread of the wavefront kernel: 128 (0 too) or 168
+    unsigned long long *staged = nullptr;  // counters: C_STAGED, then C_STAGE_FAIL (may be NULL)
 };
 constexpr int kStripW = 8;
 constexpr uint32_t kStripsAll = 0xfffffffeu;  // every strip count 1..31 (bit n: n strips)

@@ -1181,6 +1181,129 @@ __device__ __forceinline__ void task_single(const DpLaunch a, uint64_t first, ui
                     tabs + size_t(g) * G * TS, uint32_t(G) * TS);
 }
 
+// ---------------------------------------------------------------------------
+// Row bases staged by the bulk copy engine.  Before a pair task's fill, each
+// group's leader lane copies the bases of its two segments' rows (contiguous
+// bytes of one read each, forward or reversed) from global memory into shared
+// memory with one cp.async.bulk each; the copies complete on the warp's
+// mbarrier, whose phase the whole warp waits for.  The staging space is the
+// rows of the warp's traceback-code area that the task leaves unused (rows
+// Rw .. rmax - 1), so it costs no shared memory; a task without room, or a
+// wait that runs out (bounded: it sets a counter and the rows are read from
+// global memory as without staging), keeps the global row pointers.  Copies
+// start on 16-byte boundaries and move whole 16-byte units: a span is widened
+// to them (the code buffers hold 16 bytes past their last base).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes) {
+    uint64_t state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                 : "=l"(state)
+                 : "r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    (void)state;
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// global -> shared, `bytes` (a multiple of 16) from a 16-byte aligned source
+// to a 16-byte aligned destination, completing on `bar`
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+constexpr uint32_t kStageSpins = 1u << 22;  // try_wait rounds before a staging wait gives up
+
+// the 16-byte units covering rows 1..R of a segment: first unit's address, bytes
+__device__ __forceinline__ void row_span(const SegView &v, uintptr_t &lo, uint32_t &bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(v.row_base);
+    const uintptr_t b = a + uintptr_t(intptr_t(v.row_dir) * intptr_t(v.R - 1));
+    const uintptr_t first = a < b ? a : b, last = a < b ? b : a;
+    lo = first & ~uintptr_t(15);
+    bytes = uint32_t(((last + 1 - lo) + 15) & ~uintptr_t(15));
+}
+
+struct StageState {
+    uint64_t *bar;     // the warp's mbarrier
+    uint32_t phase;    // parity of the barrier's next phase
+    bool on;           // off after a wait ran out (its copy may still land)
+    uint32_t staged;   // tasks staged by this warp
+};
+
+// Points va / vb (the fill's copies) at staged rows when the warp's copies fit
+// in `room` bytes at `space`; every lane of the warp calls it.
+__device__ __forceinline__ void stage_rows(const DpLaunch &a, SegView &va, SegView &vb, bool active,
+                                           bool has_b, int G, int g, int s, int lane,
+                                           uint8_t *space, uint32_t room, StageState &st) {
+    if (!st.on) return;
+    const bool lead = active && s == 0;
+    uintptr_t loa = 0, lob = 0;
+    uint32_t na = 0, nb = 0;
+    if (lead && va.R > 0) {
+        row_span(va, loa, na);
+        if (has_b) row_span(vb, lob, nb);
+    }
+    // exclusive scan of the leaders' bytes: each group's place in the space
+    const uint32_t need = na + nb;
+    uint32_t incl = need;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0u || total > room) return;  // warp-uniform
+    const uint32_t off = incl - need;
+    if (lane == 0) mbar_expect(st.bar, total);
+    __syncwarp();
+    // the space was last read by this warp's generic loads; order those
+    // before the copy engine's writes
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (lead) {
+        bulk_g2s(space + off, reinterpret_cast<const void *>(loa), na, st.bar);
+        if (nb) bulk_g2s(space + off + na, reinterpret_cast<const void *>(lob), nb, st.bar);
+    }
+    bool done = false;
+    for (uint32_t k = 0; k < kStageSpins && !done; k++) done = mbar_try_wait(st.bar, st.phase);
+    done = __all_sync(0xffffffffu, done);
+    if (!done) {  // keep the global rows; this warp stages no more
+        st.on = false;
+        if (lane == 0 && a.staged) atomicAdd(a.staged + 1, 1ull);
+        return;
+    }
+    st.phase ^= 1u;
+    st.staged++;
+    // the group's rows in shared memory, at the same offsets from their units
+    const int lead_lane = (g * G) & 31;
+    const uint32_t goff = __shfl_sync(0xffffffffu, off, lead_lane);
+    const uint32_t gna = __shfl_sync(0xffffffffu, na, lead_lane);
+    const unsigned long long gloa = __shfl_sync(0xffffffffu, (unsigned long long)loa, lead_lane);
+    const unsigned long long glob = __shfl_sync(0xffffffffu, (unsigned long long)lob, lead_lane);
+    if (active && va.R > 0) {
+        const uint8_t *ra = space + goff + (reinterpret_cast<uintptr_t>(va.row_base) - uintptr_t(gloa));
+        const uint8_t *rb = has_b ? space + goff + gna + (reinterpret_cast<uintptr_t>(vb.row_base) - uintptr_t(glob))
+                                  : ra;
+        va.row_base = ra;
+        vb.row_base = rb;
+    }
+}
+
 // the wavefront over one warp's pairs of whole-band segments (dp_pair_row,
 // tagged 16-bit halves): group lanes hold segment A in the low halves and B in
 // the high halves
@@ -1250,7 +1373,7 @@ __device__ __noinline__ void wave_pair(const SegView va, const SegView vb, bool 
 // B segments, as two tasks of single segments.
 template <bool AFFINE>
 __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint64_t end, int G,
-                                          int lane, uint32_t *tb, uint32_t *tabs) {
+                                          int lane, uint32_t *tb, uint32_t *tabs, StageState &stg) {
     const int S = 32 / G, g = lane / G, s = lane % G;
     const uint64_t ia = first + 2u * uint64_t(g), ib = ia + 1u;
     const bool active = g < S && ia < end;
@@ -1281,10 +1404,18 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
     const int32_t Rw = warp_max(R);
     const uint32_t TS = kTabWords2;
     uint32_t *tab = tabs + size_t(lane) * TS;
+    // the fill reads its row bases through copies of the views, staged in the
+    // code rows this task leaves free when they fit
+    SegView fa = va, fb = vb;
+    {
+        uint8_t *space = reinterpret_cast<uint8_t *>(tb + size_t(Rw) * 32u);
+        const uint32_t room = a.rmax > Rw ? uint32_t(a.rmax - Rw) * 32u * 4u : 0u;
+        stage_rows(a, fa, fb, active, has_b, G, g, s, lane, space, room, stg);
+    }
     if (wl0 >= 0) {
-        wave_pair<AFFINE, true>(va, vb, active, R, Rw, G, s, lane, wl0, tb, tab);
+        wave_pair<AFFINE, true>(fa, fb, active, R, Rw, G, s, lane, wl0, tb, tab);
     } else {
-        wave_pair<AFFINE, false>(va, vb, active, R, Rw, G, s, lane, -1, tb, tab);
+        wave_pair<AFFINE, false>(fa, fb, active, R, Rw, G, s, lane, -1, tb, tab);
     }
     __syncwarp();
     if (a.pair_cells) {  // the cells this warp computed as pairs
@@ -1310,6 +1441,14 @@ __global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS, TIER))
     uint32_t *tabs = reinterpret_cast<uint32_t *>(wave_smem) + size_t(wib) * 32u * TS;
     uint8_t *tbw = reinterpret_cast<uint8_t *>(wave_smem) + size_t(WARPS) * 32u * TS * 4u +
                    size_t(wib) * size_t(a.rmax) * 32u * a.tb_bytes;
+    // the warps' mbarriers for staged rows: 16 bytes each, after every code area
+    uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(wave_smem) +
+                                                 size_t(WARPS) * 32u * TS * 4u +
+                                                 size_t(WARPS) * size_t(a.rmax) * 32u * a.tb_bytes) +
+                    2u * size_t(wib);
+    StageState stg{bar, 0u, a.tb_bytes == 4u, 0u};  // pairs only (4-byte code rows)
+    if (stg.on && lane == 0) mbar_init(bar);
+    __syncwarp();
     // a persistent grid fed by a work queue: each warp takes the next task, the
     // largest shapes first (tasks are sorted by strips, then rows)
     const uint64_t ntask = tasks[33];
@@ -1326,10 +1465,17 @@ __global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS, TIER))
         const uint64_t first = tasks[34 + G] + (task - tasks[G]) * per;
         const uint64_t end = tasks[68 + G];
         if (pair) {
-            task_pair<AFFINE>(a, first, end, G, lane, reinterpret_cast<uint32_t *>(tbw), tabs);
+            task_pair<AFFINE>(a, first, end, G, lane, reinterpret_cast<uint32_t *>(tbw), tabs, stg);
         } else {
             task_single<AFFINE>(a, first, 1, end, G, lane, reinterpret_cast<uint16_t *>(tbw), tabs);
         }
+    }
+    if (a.tb_bytes == 4u) {
+        if (!stg.on) {  // a copy whose wait ran out: give it its time before the block ends
+            bool done = false;
+            for (uint32_t k = 0; k < kStageSpins && !done; k++) done = mbar_try_wait(bar, stg.phase);
+        }
+        if (lane == 0 && a.staged && stg.staged) atomicAdd(a.staged, (unsigned long long)stg.staged);
     }
 }
 
@@ -2223,7 +2369,8 @@ uint64_t dp_threads(int device) {
 // shared memory of a wavefront block: per warp, the lanes' strip tables and
 // rmax rows of 2-bit codes (32 lanes x 16 bits, or x 32 bits for pairs)
 static size_t wave_smem(int32_t rmax, uint32_t tb_bytes, int warps) {
-    return size_t(warps) * (32u * tab_stride(tb_bytes) * 4u + size_t(rmax) * 32u * tb_bytes);
+    // + a 16-byte mbarrier slot per warp (staged row bases)
+    return size_t(warps) * (32u * tab_stride(tb_bytes) * 4u + size_t(rmax) * 32u * tb_bytes + 16u);
 }
 
 bool dp_wave_fits(int32_t rmax) { return wave_smem(rmax, 2, kWaveWarps) <= 200u * 1024u; }

@@ -122,6 +122,10 @@ typedef struct {
     uint64_t dp_cells_pairs;   /* of dp_cells_computed, the cells computed as 16-bit pairs */
     uint64_t buffer_allocs;    /* device buffers grown (allocated stream-ordered) */
     double ms_alloc;           /* host time spent growing device buffers */
+    uint64_t dp_tasks_staged;  /* DP wavefront tasks whose row bases the bulk copy engine
+                                  staged in shared memory */
+    uint64_t dp_stage_timeouts; /* staging waits that ran out (those rows were read from
+                                   global memory instead; results are unaffected) */
 } hero_stats;
 
 /* Returns the default parameters of the reference's Config. */

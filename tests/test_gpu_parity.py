@@ -56,6 +56,22 @@ def test_gpu_matches_reference(gpu_lib, oracle, name):
     assert st["dp_segments_ref"] == ost["dp_segments"]
     assert st["dp_cells"] == ost["dp_cells"]
     assert st["vote_anomalies"] == 0
+    assert st["dp_stage_timeouts"] == 0
+
+
+def test_pair_rows_staged_by_bulk_copies(gpu_lib, oracle):
+    """The pair wavefront stages its row bases in shared memory with the bulk
+    copy engine (cp.async.bulk on an mbarrier): on a workload of 16-bit pairs
+    most tasks are staged, no wait runs out, and the output is the oracle's."""
+    gen, flags = FIXTURES["c2_30k"]
+    rs = upper(gen())
+    kw = params(flags)
+    got = run_gpu(rs, **kw)
+    st = got["stats"]
+    assert st["dp_cells_pairs"] > 0
+    assert st["dp_tasks_staged"] > 0
+    assert st["dp_stage_timeouts"] == 0
+    assert_same_consensus(oracle.correct(rs, **kw), got, "c2_30k staged")
 
 
 @pytest.mark.parametrize("batch", [1, 7, 1000])
