@@ -176,6 +176,7 @@ struct DpLaunch {
     unsigned long long *pair_cells;  // += band cells of the segments run as 16-bit pairs (may be NULL)
     int32_t regs;           // registers a thread of the wavefront kernel: 128 (0 too) or 168
     unsigned long long *staged = nullptr;  // counters: C_STAGED, then C_STAGE_FAIL (may be NULL)
+    uint32_t stage_extra = 0;  // bytes a warp's code area has past its rmax rows (set by launch_dp)
 };
 constexpr int kStripW = 8;
 constexpr uint32_t kStripsAll = 0xfffffffeu;  // every strip count 1..31 (bit n: n strips)

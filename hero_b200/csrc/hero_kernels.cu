@@ -1409,7 +1409,7 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
     SegView fa = va, fb = vb;
     {
         uint8_t *space = reinterpret_cast<uint8_t *>(tb + size_t(Rw) * 32u);
-        const uint32_t room = a.rmax > Rw ? uint32_t(a.rmax - Rw) * 32u * 4u : 0u;
+        const uint32_t room = uint32_t(a.rmax - Rw) * 32u * 4u + a.stage_extra;
         stage_rows(a, fa, fb, active, has_b, G, g, s, lane, space, room, stg);
     }
     if (wl0 >= 0) {
@@ -1439,12 +1439,14 @@ __global__ void __launch_bounds__(WARPS * 32, kWaveRegBlocks(WARPS, TIER))
     const int lane = int(threadIdx.x & 31u), wib = int(threadIdx.x >> 5);
     const uint32_t TS = tab_stride(a.tb_bytes);
     uint32_t *tabs = reinterpret_cast<uint32_t *>(wave_smem) + size_t(wib) * 32u * TS;
+    // a warp's code area: rmax rows, then stage_extra bytes of staging space
+    const size_t code_area = size_t(a.rmax) * 32u * a.tb_bytes + a.stage_extra;
     uint8_t *tbw = reinterpret_cast<uint8_t *>(wave_smem) + size_t(WARPS) * 32u * TS * 4u +
-                   size_t(wib) * size_t(a.rmax) * 32u * a.tb_bytes;
+                   size_t(wib) * code_area;
     // the warps' mbarriers for staged rows: 16 bytes each, after every code area
     uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(wave_smem) +
                                                  size_t(WARPS) * 32u * TS * 4u +
-                                                 size_t(WARPS) * size_t(a.rmax) * 32u * a.tb_bytes) +
+                                                 size_t(WARPS) * code_area) +
                     2u * size_t(wib);
     StageState stg{bar, 0u, a.tb_bytes == 4u, 0u};  // pairs only (4-byte code rows)
     if (stg.on && lane == 0) mbar_init(bar);
@@ -2368,9 +2370,29 @@ uint64_t dp_threads(int device) {
 
 // shared memory of a wavefront block: per warp, the lanes' strip tables and
 // rmax rows of 2-bit codes (32 lanes x 16 bits, or x 32 bits for pairs)
-static size_t wave_smem(int32_t rmax, uint32_t tb_bytes, int warps) {
-    // + a 16-byte mbarrier slot per warp (staged row bases)
-    return size_t(warps) * (32u * tab_stride(tb_bytes) * 4u + size_t(rmax) * 32u * tb_bytes + 16u);
+static size_t wave_smem(int32_t rmax, uint32_t tb_bytes, int warps, uint32_t stage_extra = 0) {
+    // + the staging space and a 16-byte mbarrier slot per warp (staged row bases)
+    return size_t(warps) *
+           (32u * tab_stride(tb_bytes) * 4u + size_t(rmax) * 32u * tb_bytes + stage_extra + 16u);
+}
+
+// Staging space a warp can have past its code rows without costing a block an
+// SM: the shared memory the register budget's block count leaves unused (a
+// multiple of 16 bytes, at most 16 KB; 0 when shared memory already limits).
+static uint32_t wave_stage_extra(int dev, int32_t rmax, uint32_t tb_bytes, int warps, int tier) {
+    if (tb_bytes != 4u) return 0u;  // only the pair tasks stage
+    int smem_sm = 0, reserved = 0;
+    if (cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0u;
+    }
+    const size_t blocks = size_t(kWaveRegBlocks(warps, tier));
+    const size_t per_block = size_t(smem_sm) / blocks;
+    const size_t base = wave_smem(rmax, tb_bytes, warps) + size_t(reserved);
+    if (per_block <= base) return 0u;
+    const size_t extra = ((per_block - base) / size_t(warps)) & ~size_t(15);
+    return uint32_t(extra < 16384u ? extra : 16384u);
 }
 
 bool dp_wave_fits(int32_t rmax) { return wave_smem(rmax, 2, kWaveWarps) <= 200u * 1024u; }
@@ -2398,10 +2420,11 @@ void launch_dp(const DpLaunch &a_in, const uint64_t *bin_off, uint64_t *tasks, i
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = wave_smem(a.rmax, a.tb_bytes, a.warps);
     // a persistent grid: twice the blocks that fit for registers (the work queue
     // stops the extra ones at once)
     const int tier = (a.warps == 1 || wave_reg_tier(a.regs) < 2) ? wave_reg_tier(a.regs) : 1;
+    a.stage_extra = wave_stage_extra(dev, a.rmax, a.tb_bytes, a.warps, tier);
+    const size_t smem = wave_smem(a.rmax, a.tb_bytes, a.warps, a.stage_extra);
     const unsigned g = unsigned(sms) * unsigned(2 * kWaveRegBlocks(a.warps, tier));
     // the opt-in is set once per size increase (never while a graph is being captured
     // for a size not seen before: the eager round that precedes a capture sets it)
