@@ -32,7 +32,7 @@ EXPORTS = [
     "hero_align_self_range", "hero_votes_words", "hero_votes_save", "hero_votes_load",
     "hero_merge_pairs", "hero_get_overhang", "hero_mapping_histogram", "hero_set_vote_buffer",
     "hero_consensus_range", "hero_server_set_round_policy", "hero_server_worker_stats",
-    "hero_server_workers", "hero_dp_tuning_check",
+    "hero_server_workers", "hero_dp_tuning_check", "hero_device_init",
 ]
 
 # hero_params.flags: the alignment-output mode (HERO without -c); --merge

@@ -234,6 +234,14 @@ static double elapsed(cudaEvent_t a, cudaEvent_t b) {
     return double(ms);
 }
 
+extern "C" int hero_device_init(int32_t device) {
+    if (cudaSetDevice(device) != cudaSuccess || cudaFree(nullptr) != cudaSuccess) {
+        cudaGetLastError();
+        return HERO_E_CUDA;
+    }
+    return HERO_OK;
+}
+
 extern "C" void hero_default_params(hero_params *p) {
     std::memset(p, 0, sizeof(*p));
     p->k = 39;

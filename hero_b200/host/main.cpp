@@ -3,6 +3,7 @@
 // the same .aln output without it.
 #include <chrono>
 #include <iostream>
+#include <thread>
 
 #include "hero_host.h"
 
@@ -19,6 +20,13 @@ int main(int argc, char **argv) {
         std::cout << "Please follow the above help information." << std::endl;
         return 1;
     }
+    // the device's CUDA context is created while the queries are parsed
+    struct Joined {
+        std::thread t;
+        ~Joined() {
+            if (t.joinable()) t.join();
+        }
+    } device_init{std::thread([&cfg] { hero_device_init(cfg.device); })};
     std::string err;
     QueryDataset query;
     if (!query.build(cfg, &err)) {
@@ -30,6 +38,7 @@ int main(int argc, char **argv) {
                   << "Further processing is aborted. " << std::endl;
         return 1;
     }
+    device_init.t.join();
     const auto t1 = clk::now();
     HashTableGpu table;
     if (!table.createHashTables(cfg, &query, &err) || !table.insertQueryDataset(&err)) {

@@ -130,6 +130,11 @@ typedef struct {
 
 /* Returns the default parameters of the reference's Config. */
 void hero_default_params(hero_params *p);
+/* Creates the CUDA context of a device ahead of the first context (the first
+ * CUDA call of a process pays it, often a second or more): a caller may run it
+ * on a thread of its own while it parses its input.  HERO_OK, or HERO_E_CUDA
+ * when the device cannot be opened.  Thread-safe; later calls return at once. */
+int hero_device_init(int32_t device);
 
 int hero_create(const hero_params *p, hero_ctx **out);
 void hero_destroy(hero_ctx *ctx);
