@@ -341,7 +341,7 @@ def int_peaks(device: int) -> dict:
 
 def dp_roofline(cells: int, dp_ms: float, aligner: str, peaks: dict, launches: int,
                 pair_share: float = 0.0) -> dict:
-    """The DP kernel's roofline: cells x ops/cell (survey: 6 global, 10 affine)
+    """The DP kernel's roofline: cells x ops a cell (6 global, 10 affine)
     over its device time, against the largest measured peak of the instruction
     forms it issues: the packed 16-bit DPX forms (2 lanes each) when most of its
     cells ran as 16-bit pairs (pair_share > 0.5), else the 32-bit forms."""
