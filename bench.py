@@ -65,10 +65,11 @@ sys.path.insert(0, ROOT)
 # dram__bytes_write.sum over that launch's reference cells).  The traffic is per
 # segment (codes in, ops and summaries out), so it scales with the cells of a
 # launch.  Captures of the tuned shapes (1-warp blocks, tagged 16-bit pairs):
-# global, 100 bp reads at 30x on a 200 kbp genome: 180.80 MB + 89.73 MB over
-# 1,766,508,768 cells; affine, 150 bp reads at 50x on a 100 kbp genome:
-# 1.4559 GB + 0.7077 GB over 23,186,600,877 cells.
-DP_DRAM_BYTES_PER_CELL = {"affine": (1.455896e9 + 0.707741e9) / 23_186_600_877,
+# affine, 150 bp reads at 50x on a 100 kbp genome, rows staged by bulk copies:
+# 1.4643 GB + 0.7123 GB over 23,186,600,877 cells; global, 100 bp reads at 30x
+# on a 200 kbp genome, before row staging: 180.80 MB + 89.73 MB over
+# 1,766,508,768 cells.
+DP_DRAM_BYTES_PER_CELL = {"affine": (1.464261e9 + 0.712347e9) / 23_186_600_877,
                           "global": (180.799744e6 + 89.734656e6) / 1_766_508_768}
 
 # the reference's wall time on the whole affine/indel workload (1,666,666 reads,
