@@ -816,9 +816,10 @@ def measure_alignment_output(rs, kw, dev):
 def bench_sharded(args):
     """One correction split across the ranks by subject reads (hero_b200.shard):
     every rank holds the whole query set and table, aligns its range of subject
-    reads, the vote states are summed by one all-reduce (NCCL over NVLink), and
-    every rank calls the consensus.  Strong scaling: value = the job's bases
-    over the slowest rank's device time of a step."""
+    reads into a vote buffer of its own, each owner's slice of the votes is
+    reduced to it in place (one NCCL reduce a slice, over NVLink), and every
+    rank calls the consensus of the query reads it owns.  Strong scaling: value
+    = the job's bases over the slowest rank's device time of a step."""
     import torch
     import torch.distributed as dist
 
@@ -914,8 +915,8 @@ def bench_sharded(args):
             "scaling": "strong", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, no public dataset)",
             "config": workload_config(rs, flags, desc),
-            "parallelism": f"one job, subject reads sharded x{world}, votes summed by one "
-                           "all-reduce",
+            "parallelism": f"one job, subject reads sharded x{world}, each owner's slice of "
+                           "the votes reduced to it",
             "e2e": {"value": nb * args.steps / t_e2e, "unit": "bases/s",
                     "h2d_bytes_per_step": nb + 8 * (n + 1) + 8 * n,
                     "d2h_bytes_per_step": own_bases + 3 * 4 * count + 2 * 8 * count + count},
