@@ -1409,7 +1409,7 @@ __device__ __forceinline__ void task_pair(const DpLaunch a, uint64_t first, uint
     SegView fa = va, fb = vb;
     {
         uint8_t *space = reinterpret_cast<uint8_t *>(tb + size_t(Rw) * 32u);
-        const uint32_t room = uint32_t(a.rmax - Rw) * 32u * 4u + a.stage_extra;
+        const uint32_t room = (a.rmax > Rw ? uint32_t(a.rmax - Rw) * 32u * 4u : 0u) + a.stage_extra;
         stage_rows(a, fa, fb, active, has_b, G, g, s, lane, space, room, stg);
     }
     if (wl0 >= 0) {
