@@ -5,11 +5,12 @@
 // each owning a context with its own stream, run correction rounds; a worker
 // that is free admits the oldest queued jobs that fit in the device-memory
 // budget left by the rounds already in flight.  So while one round's kernels
-// run, the other worker concatenates and uploads the next round's reads and
-// starts it: rounds overlap on the device (their launches share the SMs), host
-// preparation overlaps device work, and a job that arrives while a long round
-// runs is admitted as soon as a worker and memory are free instead of waiting
-// for that round.  Inside a round the admitted jobs' reads are concatenated
+// run, the other worker gathers and uploads the next round's reads, and it
+// downloads its results while the next round runs: host work and copies
+// overlap device work.  The device phases themselves pass a gate (may_compute):
+// a small round may run beside a large one, so a job arriving during a long
+// round is not held up for all of it, while two small or two large rounds take
+// the device in turn.  Inside a round the admitted jobs' reads are concatenated
 // into one query set whose reads carry their job (hero_set_query_jobs), so one
 // set of launches -- index build, seeding, chaining, DP, votes, consensus --
 // serves every job of the round, and a job's k-mers only ever meet its own
@@ -143,10 +144,10 @@ void copy_parallel(void *dst, const void *src, size_t bytes) {
 }  // namespace
 
 // Round policy defaults, measured on the serving stream (jobs of 0.2-30 Mbp and
-// of 10 Mbp-1.6 Gbp): rounds of up to ~8 Mbp beyond their first job, and no
-// two rounds above 64 Mbp side by side (two large rounds only share the SMs
-// and the L2 and lose ~8 % against running one after the other; a small round
-// beside a large one fills its host-side gaps).
+// of 10 Mbp-1.6 Gbp): rounds of up to ~8 Mbp beyond their first job, and 64 Mbp
+// as the line between small and large rounds for the device-phase gate (two
+// device phases side by side lost 3-18 % against taking turns; a small round
+// still runs beside a large one, so it is not held up for all of it).
 constexpr uint64_t kRoundBasesDefault = 8000000;
 constexpr uint64_t kOverlapBasesDefault = 64000000;
 
@@ -179,7 +180,7 @@ struct hero_server {
     uint64_t overlapped_rounds = 0;      // rounds that started while another ran
     // round policy (hero_server_set_round_policy)
     uint64_t round_bases_max = kRoundBasesDefault;      // bases a round admits beyond its first job
-    uint64_t overlap_bases_max = kOverlapBasesDefault;  // a round starts beside another only if one is this small
+    uint64_t overlap_bases_max = kOverlapBasesDefault;  // small / large line of the device-phase gate
     uint64_t running_bases[kServeWorkers] = {};         // bases of each worker's round in flight
     uint64_t computing[kServeWorkers] = {};             // bases of each worker's round in its device phase
     uint64_t overlapped_compute = 0;                    // device phases started beside another
