@@ -30,9 +30,18 @@
  *                         (SubjectReadAligner.cpp:854-906; HERO_FLAG_ALIGNMENT_OUTPUT)
  *   hero_merge_pairs      QueryDataset::mergePairedReads of --merge
  *                         (QueryDataset.cpp:539-558; HERO_FLAG_MERGE_PAIRS)
- *   hero_align_self_range, hero_votes_save / _load
+ *   hero_align_self_range, hero_set_vote_buffer, hero_consensus_range
  *                         one correction split across devices by subject reads
- *                         (SubjectReadAligner::start's chunks on several GPUs)
+ *                         (SubjectReadAligner::start's chunks on several GPUs),
+ *                         each owner's slice of the votes reduced to it
+ *                         (hero_votes_save / _load: the whole state instead)
+ *   hero_mapping_histogram
+ *                         the coverage histogram of -c --mapping
+ *                         (QueryDataset::getCoverageAndWriteResults,
+ *                         QueryDataset.cpp:560-600; HERO_FLAG_MAPPING)
+ *   hero_server_*, hero_job_*
+ *                         serving: independent correction jobs (one main.cpp
+ *                         run each) with continuous batching on one device
  *
  * Conventions: plain pointers and sizes only; host buffers belong to the
  * caller and are only read during the call.  Every call returns 0 or a
